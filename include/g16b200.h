@@ -1,0 +1,224 @@
+/*
+ * g16b200: B200-native Groth16 / BN254 proving hot path behind a C ABI.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and
+ * returns a status code (G16_OK = 0).  The text of the last error on the
+ * calling thread is available from g16_last_error().  No entry point panics,
+ * aborts or throws across the boundary.
+ *
+ * Byte layouts (identical to the reference's crates/gpu-layout packing,
+ * crates/gpu-layout/src/lib.rs:30-200, 351):
+ *   Fr / Fq element   32 bytes, 4 x u64 (= 8 x u32) little-endian limbs,
+ *                     Montgomery form with R = 2^256 -- the in-memory bits of
+ *                     arkworks' Fp, i.e. a Rust &[Fr] can be passed as is;
+ *   scalar, standard  32 bytes little-endian integer in [0, r);
+ *   G1 affine         64 bytes: x, y (Montgomery Fq);
+ *   G2 affine         128 bytes: x.c0, x.c1, y.c0, y.c1;
+ *   point at infinity all-zero bytes.
+ * Host buffers are owned by the caller and only read (or written, for
+ * outputs) during the call.  Handles are owned by the library and released
+ * by their *_free function.
+ */
+#ifndef G16B200_H
+#define G16B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes, mirroring ProveError (crates/groth16/src/lib.rs:81-154) and
+ * ZkeyError (crates/formats/src/lib.rs). */
+enum {
+    G16_OK = 0,
+    G16_ERR_WITNESS_LENGTH = 1,   /* ProveError::WitnessLength */
+    G16_ERR_CONSTANT_WIRE = 2,    /* ProveError::ConstantWire: w[0] != 1 */
+    G16_ERR_BACKEND = 3,          /* ProveError::Backend: malformed key or shape */
+    G16_ERR_DEVICE = 4,           /* ProveError::Device: a CUDA call failed */
+    G16_ERR_DEVICE_MEMORY = 5,    /* ProveError::DeviceMemory: refused before allocating */
+    G16_ERR_SELF_VERIFY = 6,      /* ProveError::SelfVerify (reserved) */
+    G16_ERR_TIMEOUT = 7,          /* a bounded device wait gave up */
+    G16_ERR_INVALID_ARGUMENT = 8, /* null pointer, bad size, bad enum */
+    G16_ERR_FORMAT = 9            /* ZkeyError: malformed .zkey / .wtns bytes */
+};
+
+/* Scalar encodings accepted by the MSM entry points. */
+enum { G16_SCALARS_STANDARD = 0, G16_SCALARS_MONTGOMERY = 1 };
+
+/* NTT modes (crates/ntt/src/lib.rs:415-584). */
+enum {
+    G16_NTT_FORWARD = 0,         /* CpuNtt::ntt(.., Forward): natural in/out */
+    G16_NTT_INVERSE = 1,         /* CpuNtt::ntt(.., Inverse): includes 1/n */
+    G16_NTT_INTT_COSET_NTT = 2,  /* CpuNtt::intt_coset_ntt with the proving coset shift */
+    G16_NTT_COSET_FORWARD = 3,   /* distribute_powers(shift) then forward */
+    G16_NTT_COSET_INVERSE = 4    /* inverse then distribute_powers(1/shift) */
+};
+
+typedef struct g16_backend g16_backend;   /* CudaBackend (crates/cuda/src/backend.rs:94-232) */
+typedef struct g16_circuit g16_circuit;   /* CudaCircuit: PreparedCircuit (crates/groth16/src/lib.rs:371-455) */
+typedef struct g16_hpoly g16_hpoly;       /* HPoly::Device (crates/groth16/src/lib.rs:207-308) */
+typedef struct g16_zkey g16_zkey;         /* ProvingKey (crates/formats/src/lib.rs:35-65) */
+
+/* StageTimings (crates/groth16/src/lib.rs:322-338), microseconds, accumulated. */
+typedef struct {
+    uint64_t gather_us, ntt_us, pointwise_us, msm_us, assemble_us, verify_us;
+} g16_stage_timings;
+
+/* Proof (crates/groth16/src/lib.rs:187-192), affine packed. */
+typedef struct {
+    uint8_t a[64];
+    uint8_t b[128];
+    uint8_t c[64];
+} g16_proof;
+
+/* MsmOutputs (crates/groth16/src/lib.rs:311-318), affine packed. */
+typedef struct {
+    uint8_t a_g1[64];
+    uint8_t b_g2[128];
+    uint8_t b_g1[64];
+    uint8_t l_g1[64];
+    uint8_t h_g1[64];
+} g16_msm_outputs;
+
+/* A parsed proving key, field by field (ProvingKey, crates/formats/src/lib.rs:35-65,
+ * section 4 in CSR form with interned values as in Coefficients, :140-223). */
+typedef struct {
+    uint32_t n_vars, n_public, domain_size;
+    const uint8_t *alpha_g1, *beta_g1, *beta_g2, *gamma_g2, *delta_g1, *delta_g2;
+    const uint8_t *ic;            /* (n_public + 1) G1 */
+    const uint32_t *row_ptr[2];   /* [A, B], domain_size + 1 each */
+    const uint32_t *signal[2];    /* nnz[m] each, < n_vars */
+    const uint32_t *value_id[2];  /* nnz[m] each, < n_values */
+    uint32_t nnz[2];
+    const uint8_t *values;        /* n_values Fr, Montgomery */
+    uint32_t n_values;
+    const uint8_t *a_query;       /* n_vars G1 (section 5) */
+    const uint8_t *b_g1_query;    /* n_vars G1 (section 6) */
+    const uint8_t *b_g2_query;    /* n_vars G2 (section 7) */
+    const uint8_t *l_query;       /* n_vars - n_public - 1 G1 (section 8) */
+    const uint8_t *h_query;       /* domain_size G1 (section 9) */
+} g16_zkey_view;
+
+/* ---------------- errors ---------------- */
+/* Copies the calling thread's last error text into buf (NUL-terminated);
+ * returns its full length. */
+size_t g16_last_error(char *buf, size_t len);
+
+/* ---------------- backend (CudaBackend::new, backend.rs:137-190) ---------------- */
+/* Opens CUDA device `ordinal`.  vram_limit caps this backend's device
+ * allocations in bytes (0 = the device's free memory).  Fails with
+ * G16_ERR_DEVICE when no CUDA device is present: there is no CPU fallback. */
+int g16_backend_open(int ordinal, uint64_t vram_limit, g16_backend **out);
+void g16_backend_free(g16_backend *b);
+const char *g16_backend_name(const g16_backend *b);   /* "cuda-b200" */
+uint64_t g16_backend_vram_used(const g16_backend *b);
+
+/* ---------------- .zkey / .wtns (crates/formats) ---------------- */
+/* ProvingKey::load (formats/src/lib.rs:430-505).  check_points != 0 also runs
+ * the on-curve check of every query point (load vs load_unchecked). */
+int g16_zkey_parse(const uint8_t *bytes, size_t len, int check_points, g16_zkey **out);
+int g16_zkey_view_get(const g16_zkey *k, g16_zkey_view *out);
+void g16_zkey_free(g16_zkey *k);
+/* Witness::load (formats/src/wtns.rs:17-40): values out in Montgomery form.
+ * Pass out = NULL to learn the count. */
+int g16_wtns_parse(const uint8_t *bytes, size_t len, uint8_t *out_mont, size_t cap, size_t *n_out);
+/* .wtns writer (plain little-endian values), for tooling. out = NULL sizes. */
+int g16_wtns_write(const uint8_t *w_mont, size_t n, uint8_t *out, size_t cap, size_t *len_out);
+
+/* ---------------- circuits (Backend::prepare, backend.rs:325-457) ---------------- */
+int g16_prepare(g16_backend *b, const g16_zkey_view *key, g16_circuit **out);
+void g16_circuit_free(g16_circuit *c);
+uint32_t g16_circuit_n_vars(const g16_circuit *c);
+uint32_t g16_circuit_n_public(const g16_circuit *c);
+uint32_t g16_circuit_domain_size(const g16_circuit *c);
+uint64_t g16_circuit_device_bytes(const g16_circuit *c);
+
+/* PreparedCircuit::compute_h (stages 0-4; lib.rs:397-400, cuda stages.rs:929).
+ * witness: n Fr in Montgomery form (a &[Fr]). */
+int g16_compute_h(g16_circuit *c, const uint8_t *witness_mont, size_t n, g16_hpoly **out);
+/* PreparedCircuit::h_to_host: n = domain_size Fr, Montgomery. */
+int g16_h_to_host(const g16_hpoly *h, uint8_t *out_mont, size_t cap);
+void g16_hpoly_free(g16_hpoly *h);
+/* PreparedCircuit::msms (stages 5-9; lib.rs:401-412). */
+int g16_msms(g16_circuit *c, const uint8_t *witness_mont, size_t n, const g16_hpoly *h, g16_msm_outputs *out);
+/* PreparedCircuit::h_and_msms (stages 0-9; lib.rs:420-423). */
+int g16_h_and_msms(g16_circuit *c, const uint8_t *witness_mont, size_t n, g16_msm_outputs *out);
+/* prove_with_blinders (crates/groth16/src/prove.rs:175-184): stages 0-11 with
+ * the caller's r and s (Montgomery Fr). */
+int g16_prove_with_blinders(g16_circuit *c, const uint8_t *witness_mont, size_t n, const uint8_t *r_mont,
+                            const uint8_t *s_mont, g16_proof *out);
+/* The same with the witness already resident in device memory (a device
+ * pointer to n Montgomery Fr); no host-to-device copy. */
+int g16_prove_with_blinders_device(g16_circuit *c, const void *d_witness_mont, size_t n, const uint8_t *r_mont,
+                                   const uint8_t *s_mont, g16_proof *out);
+int g16_stage_timings_get(const g16_circuit *c, g16_stage_timings *out);
+
+/* ---------------- batched and served proving ---------------- */
+/* Proves count independent jobs (circuits may repeat or differ) in one
+ * submission; outputs are bit-identical to count single calls.
+ * witnesses[i] has lens[i] Montgomery Fr; r, s: count x 32 bytes. */
+int g16_prove_batch(g16_backend *b, size_t count, g16_circuit *const *circuits, const uint8_t *const *witnesses,
+                    const size_t *lens, const uint8_t *r_mont, const uint8_t *s_mont, g16_proof *out);
+
+/* ---------------- primitives (MsmBackend, crates/msm/src/lib.rs:52-82) ---------------- */
+/* sum_i scalars[i] * bases[i]; host buffers; result affine packed. */
+int g16_msm_g1(g16_backend *b, const uint8_t *bases, const uint8_t *scalars, size_t n, int scalars_form,
+               uint8_t *out64);
+int g16_msm_g2(g16_backend *b, const uint8_t *bases, const uint8_t *scalars, size_t n, int scalars_form,
+               uint8_t *out128);
+/* Device-resident inputs (device pointers), for callers that keep bases in HBM. */
+int g16_msm_g1_device(g16_backend *b, const void *d_bases, const void *d_scalars, size_t n, int scalars_form,
+                      uint8_t *out64);
+int g16_msm_g2_device(g16_backend *b, const void *d_bases, const void *d_scalars, size_t n, int scalars_form,
+                      uint8_t *out128);
+
+/* ---------------- NTT (CpuNtt API, crates/ntt/src/lib.rs:415-584) ---------------- */
+/* In place on 2^log_n Montgomery Fr in host memory.  shift_mont is the coset
+ * shift for the COSET modes (NULL = the proving coset shift omega_2n). */
+int g16_ntt(g16_backend *b, int mode, uint32_t log_n, uint8_t *data_mont, const uint8_t *shift_mont);
+/* The same on a device pointer. */
+int g16_ntt_device(g16_backend *b, int mode, uint32_t log_n, void *d_data_mont, const uint8_t *shift_mont);
+
+/* ---------------- kernel timing (CUDA events on the launching stream) ---------------- */
+void g16_kernel_timing_enable(int on);
+void g16_kernel_timing_reset(void);
+/* Writes "name ms launches\n" lines; returns the full length. */
+size_t g16_kernel_timing_report(char *buf, size_t len);
+
+/* ---------------- device memory helpers (for callers without a CUDA runtime) ---------------- */
+int g16_device_alloc(g16_backend *b, size_t bytes, void **d_out);
+int g16_device_free(g16_backend *b, void *d);
+int g16_device_upload(g16_backend *b, void *d_dst, const void *src, size_t bytes);
+int g16_device_sync(g16_backend *b);
+
+/* ---------------- synthetic circuits, witnesses and keys ---------------- */
+/* A seeded R1CS: wire 0 = 1, n_inputs input wires (the first n_public of them
+ * public), one new wire per constraint w_k = (A.w)(B.w) with 2-3 terms per A
+ * and B row on earlier wires.  Witness values about 60% {0,1}, 20% below
+ * 2^32, 20% uniform.  The key is written as a snarkjs .zkey from seeded
+ * toxic waste (tau, alpha, beta, delta; gamma = 1): the key a one-
+ * contribution snarkjs/snarkrs ceremony + setup + zkey contribute yields. */
+typedef struct g16_synth g16_synth;
+int g16_synth_new(uint64_t seed, uint32_t n_constraints, uint32_t n_inputs, uint32_t n_public, g16_synth **out);
+void g16_synth_free(g16_synth *s);
+uint32_t g16_synth_n_vars(const g16_synth *s);
+uint32_t g16_synth_domain_size(const g16_synth *s);
+/* n_vars Montgomery Fr; inputs drawn from witness_seed. */
+int g16_synth_witness(const g16_synth *s, uint64_t witness_seed, uint8_t *out_mont);
+/* .zkey bytes; out = NULL to size. threads = 0 uses all cores. */
+int g16_synth_zkey(const g16_synth *s, uint64_t toxic_seed, int threads, uint8_t *out, size_t cap, size_t *len_out);
+/* circom .r1cs bytes; out = NULL to size. */
+int g16_synth_r1cs(const g16_synth *s, uint8_t *out, size_t cap, size_t *len_out);
+/* n affine points k_i G with k_i uniform in [1, r) (group 1 = G1, 64 B each;
+ * group 2 = G2, 128 B each); threads = 0 uses all cores. */
+int g16_synth_points(int group, uint64_t seed, size_t n, int threads, uint8_t *out);
+/* n standard-form scalars: dist 0 uniform in [0, r); dist 1 = 35% zero,
+ * 35% one, 30% uniform (the "70% in {0,1}" distribution). */
+int g16_synth_scalars(uint64_t seed, size_t n, int dist, uint8_t *out_std);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* G16B200_H */

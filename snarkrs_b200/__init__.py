@@ -1,0 +1,567 @@
+"""snarkrs_b200: B200-native Groth16 / BN254 proving hot path.
+
+A Python mirror of the reference's backend interface for the prove path
+(zemse/snarkrs ``crates/groth16/src/lib.rs:371-455`` Backend /
+PreparedCircuit, ``crates/msm/src/lib.rs:52-82`` MsmBackend,
+``crates/ntt/src/lib.rs:415-584`` the NTT API), bound through ctypes to the
+C ABI in ``include/g16b200.h`` implemented by ``libg16b200.so`` (hand-written
+sm_100a CUDA).  There is no CPU fallback: every compute call runs on the GPU
+or raises.
+
+Byte conventions follow the reference's packed layout: field elements are 32
+little-endian bytes in Montgomery form (the in-memory bits of an arkworks
+``Fr``), MSM scalars may be standard or Montgomery form, G1 points are 64
+bytes, G2 points 128 bytes, the point at infinity is all-zero.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libg16b200.so")
+
+G16_OK = 0
+SCALARS_STANDARD, SCALARS_MONTGOMERY = 0, 1
+NTT_FORWARD, NTT_INVERSE, NTT_INTT_COSET_NTT, NTT_COSET_FORWARD, NTT_COSET_INVERSE = range(5)
+
+R_MOD = 21888242871839275222246405745257275088548364400416034343698204186575808495617
+Q_MOD = 21888242871839275222246405745257275088696311157297823662689037894645226208583
+
+
+# ---- errors: ProveError (crates/groth16/src/lib.rs:81-154) ----
+class ProveError(Exception):
+    code = -1
+
+
+class WitnessLengthError(ProveError):
+    code = 1
+
+
+class ConstantWireError(ProveError):
+    code = 2
+
+
+class BackendError(ProveError):
+    code = 3
+
+
+class DeviceError(ProveError):
+    code = 4
+
+
+class DeviceMemoryError(ProveError):
+    code = 5
+
+
+class SelfVerifyError(ProveError):
+    code = 6
+
+
+class TimeoutError_(ProveError):
+    code = 7
+
+
+class InvalidArgumentError(ProveError):
+    code = 8
+
+
+class FormatError(ProveError):
+    """ZkeyError: malformed .zkey / .wtns bytes."""
+    code = 9
+
+
+_ERRORS = {c.code: c for c in (WitnessLengthError, ConstantWireError, BackendError, DeviceError,
+                                DeviceMemoryError, SelfVerifyError, TimeoutError_, InvalidArgumentError,
+                                FormatError)}
+
+_lib = None
+
+
+def lib():
+    """Load libg16b200.so; raise if it is missing (no fallback exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libg16b200.so is not built; run `python -m snarkrs_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        L.g16_last_error.restype = ctypes.c_size_t
+        L.g16_backend_name.restype = ctypes.c_char_p
+        L.g16_backend_vram_used.restype = ctypes.c_uint64
+        L.g16_backend_free.argtypes = [vp]
+        L.g16_zkey_free.argtypes = [vp]
+        L.g16_circuit_free.argtypes = [vp]
+        L.g16_hpoly_free.argtypes = [vp]
+        L.g16_synth_free.argtypes = [vp]
+        for f in ("g16_circuit_n_vars", "g16_circuit_n_public", "g16_circuit_domain_size",
+                  "g16_synth_n_vars", "g16_synth_domain_size"):
+            getattr(L, f).restype = ctypes.c_uint32
+            getattr(L, f).argtypes = [vp]
+        L.g16_circuit_device_bytes.restype = ctypes.c_uint64
+        L.g16_circuit_device_bytes.argtypes = [vp]
+        L.g16_kernel_timing_report.restype = ctypes.c_size_t
+        _lib = L
+    return _lib
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(2048)
+    lib().g16_last_error(buf, 2048)
+    return buf.value.decode(errors="replace")
+
+
+def check(rc):
+    if rc != G16_OK:
+        raise _ERRORS.get(rc, ProveError)("g16 status %d: %s" % (rc, last_error()))
+
+
+def _buf(data):
+    if isinstance(data, (bytes, bytearray)):
+        return ctypes.c_char_p(bytes(data)) if isinstance(data, bytes) else (ctypes.c_char * len(data)).from_buffer(data)
+    # numpy arrays and other buffer objects
+    mv = memoryview(data).cast("B")
+    return (ctypes.c_char * mv.nbytes).from_buffer(mv) if not mv.readonly else ctypes.c_char_p(mv.tobytes())
+
+
+def _nbytes(data):
+    return memoryview(data).nbytes
+
+
+# ---- StageTimings (crates/groth16/src/lib.rs:322-338) ----
+class StageTimings(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in
+                ("gather_us", "ntt_us", "pointwise_us", "msm_us", "assemble_us", "verify_us")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class _Proof(ctypes.Structure):
+    _fields_ = [("a", ctypes.c_uint8 * 64), ("b", ctypes.c_uint8 * 128), ("c", ctypes.c_uint8 * 64)]
+
+
+class _MsmOutputs(ctypes.Structure):
+    _fields_ = [("a_g1", ctypes.c_uint8 * 64), ("b_g2", ctypes.c_uint8 * 128), ("b_g1", ctypes.c_uint8 * 64),
+                ("l_g1", ctypes.c_uint8 * 64), ("h_g1", ctypes.c_uint8 * 64)]
+
+
+class Proof:
+    """Proof{a: G1Affine, b: G2Affine, c: G1Affine} (crates/groth16/src/lib.rs:187-192), packed bytes."""
+
+    def __init__(self, a, b, c):
+        self.a, self.b, self.c = bytes(a), bytes(b), bytes(c)
+
+    def to_bytes(self):
+        return self.a + self.b + self.c
+
+    def __eq__(self, other):
+        return isinstance(other, Proof) and self.to_bytes() == other.to_bytes()
+
+    def __repr__(self):
+        return "Proof(a=%s.., b=%s.., c=%s..)" % (self.a[:4].hex(), self.b[:4].hex(), self.c[:4].hex())
+
+
+class MsmOutputs:
+    """MsmOutputs (crates/groth16/src/lib.rs:311-318): five affine points, packed."""
+
+    FIELDS = ("a_g1", "b_g2", "b_g1", "l_g1", "h_g1")
+
+    def __init__(self, raw):
+        for f in self.FIELDS:
+            setattr(self, f, bytes(getattr(raw, f)))
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f in self.FIELDS}
+
+
+class _ZkeyView(ctypes.Structure):
+    P = ctypes.POINTER(ctypes.c_uint8)
+    U = ctypes.POINTER(ctypes.c_uint32)
+    _fields_ = [("n_vars", ctypes.c_uint32), ("n_public", ctypes.c_uint32), ("domain_size", ctypes.c_uint32),
+                ("alpha_g1", P), ("beta_g1", P), ("beta_g2", P), ("gamma_g2", P), ("delta_g1", P), ("delta_g2", P),
+                ("ic", P), ("row_ptr", U * 2), ("signal", U * 2), ("value_id", U * 2), ("nnz", ctypes.c_uint32 * 2),
+                ("values", P), ("n_values", ctypes.c_uint32),
+                ("a_query", P), ("b_g1_query", P), ("b_g2_query", P), ("l_query", P), ("h_query", P)]
+
+
+class ProvingKey:
+    """A parsed snarkjs .zkey (ProvingKey, crates/formats/src/lib.rs:35-65)."""
+
+    def __init__(self, handle):
+        self._h = handle
+        self._view = _ZkeyView()
+        check(lib().g16_zkey_view_get(self._h, ctypes.byref(self._view)))
+        self.n_vars = self._view.n_vars
+        self.n_public = self._view.n_public
+        self.domain_size = self._view.domain_size
+
+    @classmethod
+    def from_bytes(cls, data, check_points=True):
+        """ProvingKey::from_bytes / load (check_points) / load_unchecked (not check_points)."""
+        h = ctypes.c_void_p()
+        check(lib().g16_zkey_parse(_buf(data), ctypes.c_size_t(_nbytes(data)), int(bool(check_points)),
+                                   ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def load(cls, path, check_points=True):
+        with open(path, "rb") as f:
+            return cls.from_bytes(f.read(), check_points)
+
+    def _point(self, name, size):
+        return ctypes.string_at(getattr(self._view, name), size)
+
+    @property
+    def alpha_g1(self):
+        return self._point("alpha_g1", 64)
+
+    @property
+    def beta_g2(self):
+        return self._point("beta_g2", 128)
+
+    @property
+    def gamma_g2(self):
+        return self._point("gamma_g2", 128)
+
+    @property
+    def delta_g2(self):
+        return self._point("delta_g2", 128)
+
+    @property
+    def ic(self):
+        raw = ctypes.string_at(self._view.ic, 64 * (self.n_public + 1))
+        return [raw[64 * i:64 * i + 64] for i in range(self.n_public + 1)]
+
+    def close(self):
+        if self._h:
+            lib().g16_zkey_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def load_witness(data):
+    """Witness::load from .wtns bytes -> Montgomery bytes (crates/formats/src/wtns.rs:17-40)."""
+    n = ctypes.c_size_t()
+    check(lib().g16_wtns_parse(_buf(data), ctypes.c_size_t(_nbytes(data)), None, ctypes.c_size_t(0), ctypes.byref(n)))
+    out = ctypes.create_string_buffer(32 * n.value)
+    check(lib().g16_wtns_parse(_buf(data), ctypes.c_size_t(_nbytes(data)), out, n, ctypes.byref(n)))
+    return out.raw
+
+
+def write_witness(w_mont):
+    n = _nbytes(w_mont) // 32
+    ln = ctypes.c_size_t()
+    check(lib().g16_wtns_write(_buf(w_mont), ctypes.c_size_t(n), None, ctypes.c_size_t(0), ctypes.byref(ln)))
+    out = ctypes.create_string_buffer(ln.value)
+    check(lib().g16_wtns_write(_buf(w_mont), ctypes.c_size_t(n), out, ln, ctypes.byref(ln)))
+    return out.raw
+
+
+class HPoly:
+    """HPoly::Device (crates/groth16/src/lib.rs:207-308): H on the device, valid only on its circuit."""
+
+    def __init__(self, handle, circuit):
+        self._h = handle
+        self.circuit = circuit
+        self.len = circuit.domain_size
+
+    def close(self):
+        if self._h:
+            lib().g16_hpoly_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CudaCircuit:
+    """PreparedCircuit on the B200 (crates/groth16/src/lib.rs:371-455; crates/cuda/src/backend.rs CudaCircuit)."""
+
+    def __init__(self, backend, handle, key):
+        self.backend = backend
+        self._h = handle
+        self._key = key
+        self.n_vars = lib().g16_circuit_n_vars(handle)
+        self.n_public = lib().g16_circuit_n_public(handle)
+        self.domain_size = lib().g16_circuit_domain_size(handle)
+
+    def backend_name(self):
+        return "cuda-b200"
+
+    def key(self):
+        return self._key
+
+    def device_bytes(self):
+        return lib().g16_circuit_device_bytes(self._h)
+
+    def compute_h(self, witness_mont):
+        h = ctypes.c_void_p()
+        check(lib().g16_compute_h(self._h, _buf(witness_mont), ctypes.c_size_t(_nbytes(witness_mont) // 32),
+                                  ctypes.byref(h)))
+        return HPoly(h, self)
+
+    def h_to_host(self, hpoly):
+        out = ctypes.create_string_buffer(32 * hpoly.len)
+        check(lib().g16_h_to_host(hpoly._h, out, ctypes.c_size_t(hpoly.len)))
+        return out.raw
+
+    def msms(self, witness_mont, hpoly):
+        o = _MsmOutputs()
+        check(lib().g16_msms(self._h, _buf(witness_mont), ctypes.c_size_t(_nbytes(witness_mont) // 32), hpoly._h,
+                             ctypes.byref(o)))
+        return MsmOutputs(o)
+
+    def h_and_msms(self, witness_mont):
+        o = _MsmOutputs()
+        check(lib().g16_h_and_msms(self._h, _buf(witness_mont), ctypes.c_size_t(_nbytes(witness_mont) // 32),
+                                   ctypes.byref(o)))
+        return MsmOutputs(o)
+
+    def prove_with_blinders(self, witness_mont, r_mont, s_mont):
+        """prove_with_blinders (crates/groth16/src/prove.rs:175-184); r, s: 32-byte Montgomery Fr."""
+        p = _Proof()
+        check(lib().g16_prove_with_blinders(self._h, _buf(witness_mont), ctypes.c_size_t(_nbytes(witness_mont) // 32),
+                                            bytes(r_mont), bytes(s_mont), ctypes.byref(p)))
+        return Proof(p.a, p.b, p.c)
+
+    def prove_with_blinders_device(self, d_witness, n, r_mont, s_mont):
+        p = _Proof()
+        check(lib().g16_prove_with_blinders_device(self._h, ctypes.c_void_p(d_witness), ctypes.c_size_t(n),
+                                                   bytes(r_mont), bytes(s_mont), ctypes.byref(p)))
+        return Proof(p.a, p.b, p.c)
+
+    def stage_timings(self):
+        t = StageTimings()
+        check(lib().g16_stage_timings_get(self._h, ctypes.byref(t)))
+        return t.as_dict()
+
+    def close(self):
+        if self._h:
+            lib().g16_circuit_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CudaBackend:
+    """Backend (crates/groth16/src/lib.rs:371-380) over one B200: name() and prepare()."""
+
+    def __init__(self, ordinal=0, vram_limit=0):
+        h = ctypes.c_void_p()
+        check(lib().g16_backend_open(int(ordinal), ctypes.c_uint64(vram_limit), ctypes.byref(h)))
+        self._h = h
+
+    def name(self):
+        return lib().g16_backend_name(self._h).decode()
+
+    def vram_used(self):
+        return lib().g16_backend_vram_used(self._h)
+
+    def prepare(self, pk):
+        c = ctypes.c_void_p()
+        check(lib().g16_prepare(self._h, ctypes.byref(pk._view), ctypes.byref(c)))
+        return CudaCircuit(self, c, pk)
+
+    def prove_batch(self, jobs):
+        """Prove [(circuit, witness_mont, r_mont, s_mont), ...] in one submission."""
+        n = len(jobs)
+        circ = (ctypes.c_void_p * n)(*[j[0]._h for j in jobs])
+        bufs = [bytes(j[1]) for j in jobs]
+        wits = (ctypes.c_char_p * n)(*bufs)
+        lens = (ctypes.c_size_t * n)(*[len(b) // 32 for b in bufs])
+        r = b"".join(bytes(j[2]) for j in jobs)
+        s = b"".join(bytes(j[3]) for j in jobs)
+        out = (_Proof * n)()
+        check(lib().g16_prove_batch(self._h, ctypes.c_size_t(n), circ, wits, lens, r, s, out))
+        return [Proof(p.a, p.b, p.c) for p in out]
+
+    # device memory helpers
+    def alloc(self, nbytes):
+        d = ctypes.c_void_p()
+        check(lib().g16_device_alloc(self._h, ctypes.c_size_t(nbytes), ctypes.byref(d)))
+        return d.value
+
+    def free(self, d):
+        check(lib().g16_device_free(self._h, ctypes.c_void_p(d)))
+
+    def upload(self, d, data):
+        check(lib().g16_device_upload(self._h, ctypes.c_void_p(d), _buf(data), ctypes.c_size_t(_nbytes(data))))
+
+    def sync(self):
+        check(lib().g16_device_sync(self._h))
+
+    def close(self):
+        if self._h:
+            lib().g16_backend_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CudaMsm:
+    """MsmBackend (crates/msm/src/lib.rs:52-82) on the B200."""
+
+    def __init__(self, backend):
+        self.backend = backend
+
+    def name(self):
+        return "cuda-b200"
+
+    def _run(self, fn, size, bases, scalars, form):
+        n = _nbytes(scalars) // 32
+        if _nbytes(bases) != n * size:
+            raise BackendError("MSM length mismatch: %d bases but %d scalars" % (_nbytes(bases) // size, n))
+        out = ctypes.create_string_buffer(size)
+        check(fn(self.backend._h, _buf(bases), _buf(scalars), ctypes.c_size_t(n), int(form), out))
+        return out.raw
+
+    def msm_g1(self, bases, scalars, form=SCALARS_STANDARD):
+        return self._run(lib().g16_msm_g1, 64, bases, scalars, form)
+
+    def msm_g2(self, bases, scalars, form=SCALARS_STANDARD):
+        return self._run(lib().g16_msm_g2, 128, bases, scalars, form)
+
+    try_msm_g1 = msm_g1
+    try_msm_g2 = msm_g2
+
+    def msm_g1_device(self, d_bases, d_scalars, n, form=SCALARS_STANDARD):
+        out = ctypes.create_string_buffer(64)
+        check(lib().g16_msm_g1_device(self.backend._h, ctypes.c_void_p(d_bases), ctypes.c_void_p(d_scalars),
+                                      ctypes.c_size_t(n), int(form), out))
+        return out.raw
+
+    def msm_g2_device(self, d_bases, d_scalars, n, form=SCALARS_STANDARD):
+        out = ctypes.create_string_buffer(128)
+        check(lib().g16_msm_g2_device(self.backend._h, ctypes.c_void_p(d_bases), ctypes.c_void_p(d_scalars),
+                                      ctypes.c_size_t(n), int(form), out))
+        return out.raw
+
+
+class CudaNtt:
+    """The CpuNtt API (crates/ntt/src/lib.rs:415-584) on the B200; data is Montgomery bytes, in place semantics."""
+
+    def __init__(self, backend):
+        self.backend = backend
+
+    def _run(self, mode, data, shift_mont=None):
+        n = _nbytes(data) // 32
+        log_n = n.bit_length() - 1
+        if n < 2 or (1 << log_n) != n:
+            raise InvalidArgumentError("NTT length %d is not a power of two >= 2" % n)
+        buf = ctypes.create_string_buffer(bytes(data), _nbytes(data))
+        sh = None if shift_mont is None else bytes(shift_mont)
+        check(lib().g16_ntt(self.backend._h, int(mode), ctypes.c_uint32(log_n), buf, sh))
+        return buf.raw
+
+    def ntt(self, data, inverse=False):
+        return self._run(NTT_INVERSE if inverse else NTT_FORWARD, data)
+
+    def intt_coset_ntt(self, data):
+        return self._run(NTT_INTT_COSET_NTT, data)
+
+    def coset_ntt(self, data, shift_mont=None, inverse=False):
+        return self._run(NTT_COSET_INVERSE if inverse else NTT_COSET_FORWARD, data, shift_mont)
+
+    def ntt_device(self, mode, log_n, d_data, shift_mont=None):
+        sh = None if shift_mont is None else bytes(shift_mont)
+        check(lib().g16_ntt_device(self.backend._h, int(mode), ctypes.c_uint32(log_n), ctypes.c_void_p(d_data), sh))
+
+
+class SynthCircuit:
+    """A seeded synthetic R1CS with its witness generator and toxic-waste .zkey writer."""
+
+    def __init__(self, seed, n_constraints, n_inputs=256, n_public=16):
+        h = ctypes.c_void_p()
+        check(lib().g16_synth_new(ctypes.c_uint64(seed), ctypes.c_uint32(n_constraints), ctypes.c_uint32(n_inputs),
+                                  ctypes.c_uint32(n_public), ctypes.byref(h)))
+        self._h = h
+        self.n_public = n_public
+        self.n_vars = lib().g16_synth_n_vars(h)
+        self.domain_size = lib().g16_synth_domain_size(h)
+
+    def witness(self, witness_seed):
+        out = ctypes.create_string_buffer(32 * self.n_vars)
+        check(lib().g16_synth_witness(self._h, ctypes.c_uint64(witness_seed), out))
+        return out.raw
+
+    def zkey(self, toxic_seed, threads=0):
+        n = ctypes.c_size_t()
+        check(lib().g16_synth_zkey(self._h, ctypes.c_uint64(toxic_seed), int(threads), None, ctypes.c_size_t(0),
+                                   ctypes.byref(n)))
+        out = ctypes.create_string_buffer(n.value)
+        check(lib().g16_synth_zkey(self._h, ctypes.c_uint64(toxic_seed), int(threads), out, n, ctypes.byref(n)))
+        return out.raw
+
+    def r1cs(self):
+        n = ctypes.c_size_t()
+        check(lib().g16_synth_r1cs(self._h, None, ctypes.c_size_t(0), ctypes.byref(n)))
+        out = ctypes.create_string_buffer(n.value)
+        check(lib().g16_synth_r1cs(self._h, out, n, ctypes.byref(n)))
+        return out.raw
+
+    def close(self):
+        if self._h:
+            lib().g16_synth_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def synth_points(group, seed, n, threads=0):
+    """n affine points k_i G, k_i uniform (group 1 = G1, 2 = G2), packed bytes."""
+    out = ctypes.create_string_buffer((64 if group == 1 else 128) * n)
+    check(lib().g16_synth_points(int(group), ctypes.c_uint64(seed), ctypes.c_size_t(n), int(threads), out))
+    return out.raw
+
+
+def synth_scalars(seed, n, dist=0):
+    """n standard-form scalars; dist 0 uniform, dist 1 = 70% in {0, 1}."""
+    out = ctypes.create_string_buffer(32 * n)
+    check(lib().g16_synth_scalars(ctypes.c_uint64(seed), ctypes.c_size_t(n), int(dist), out))
+    return out.raw
+
+
+def kernel_timing(enable=True):
+    lib().g16_kernel_timing_enable(int(bool(enable)))
+
+
+def kernel_timing_reset():
+    lib().g16_kernel_timing_reset()
+
+
+def kernel_timing_report():
+    """{kernel class: (total ms, launches)} from CUDA events on the launching stream."""
+    buf = ctypes.create_string_buffer(1 << 16)
+    lib().g16_kernel_timing_report(buf, 1 << 16)
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, ms, cnt = line.split()
+        out[name] = (float(ms), int(cnt))
+    return out
+
+
+def fr_to_mont_bytes(x):
+    return ((int(x) << 256) % R_MOD).to_bytes(32, "little")
+
+
+def fr_from_mont_bytes(b):
+    return int.from_bytes(bytes(b), "little") * pow(1 << 256, -1, R_MOD) % R_MOD

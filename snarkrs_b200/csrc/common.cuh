@@ -1,0 +1,95 @@
+// Shared host-side plumbing: error capture and optional per-kernel event timing.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace g16 {
+
+// thread-local last error text, surfaced through g16_last_error()
+void set_error(const char* fmt, ...);
+
+#define G16_CUDA(call)                                                              \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) {                                                    \
+            ::g16::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call,             \
+                             cudaGetErrorString(e_));                               \
+            return e_;                                                              \
+        }                                                                           \
+    } while (0)
+
+// Kernel-class timing with CUDA events on the launching stream.  Disabled by
+// default; when enabled every tagged launch is bracketed by two events and the
+// elapsed times are folded in at collect() (after the stream has synchronised).
+struct KernelTimer {
+    bool enabled = false;
+    struct Pending {
+        std::string name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+    std::map<std::string, std::pair<double, long>> totals;   // ms, launches
+    std::mutex mu;
+
+    cudaEvent_t take() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(const char* name, cudaStream_t s) {
+        if (!enabled) return;
+        std::lock_guard<std::mutex> g(mu);
+        Pending p;
+        p.name = name;
+        p.a = take();
+        p.b = take();
+        cudaEventRecord(p.a, s);
+        pending.push_back(p);
+    }
+    void end(cudaStream_t s) {
+        if (!enabled) return;
+        std::lock_guard<std::mutex> g(mu);
+        if (!pending.empty()) cudaEventRecord(pending.back().b, s);
+    }
+    void collect() {
+        std::lock_guard<std::mutex> g(mu);
+        for (auto& p : pending) {
+            float ms = 0.f;
+            if (cudaEventSynchronize(p.b) == cudaSuccess && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+                auto& t = totals[p.name];
+                t.first += ms;
+                t.second += 1;
+            }
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    void reset() {
+        collect();
+        std::lock_guard<std::mutex> g(mu);
+        totals.clear();
+    }
+};
+
+KernelTimer& timer();
+
+struct TimedLaunch {
+    cudaStream_t s;
+    TimedLaunch(const char* name, cudaStream_t st) : s(st) { timer().begin(name, st); }
+    ~TimedLaunch() { timer().end(s); }
+};
+
+inline unsigned blocks_for(size_t n, unsigned threads) { return (unsigned)((n + threads - 1) / threads); }
+
+}  // namespace g16

@@ -1,0 +1,300 @@
+// BN254 Fr / Fq / Fq2 arithmetic for sm_100a.
+//
+// Eight 32-bit little-endian limbs, Montgomery form with R = 2^256: the same
+// bits as arkworks' in-memory Fp and snarkrs' PackedFr / PackedFq
+// (crates/gpu-layout/src/lib.rs:30-46, 75-113).  Every value leaving a
+// function is fully reduced into [0, p), so device results compare bit for
+// bit with the CPU prover.
+//
+// The Montgomery product is CIOS (Koc, Acar and Kaliski, "Analyzing and
+// comparing Montgomery multiplication algorithms", 1996) written as PTX
+// multiply-add carry chains: per limb of b, one mad.lo.cc/madc.lo.cc chain
+// and one mad.hi.cc/madc.hi.cc chain for a*b[i], then the same pair for
+// m*p.  Each chain lives in a single asm statement, so no compiler-scheduled
+// instruction can land between a carry producer and its consumer.
+// BN254's moduli are below 2^254, so the running sum stays below 2^287 and
+// fits nine limbs; the carry out of the ninth is provably zero.
+#pragma once
+#include <cstdint>
+
+namespace g16d {
+
+// Limb tables as constexpr functions: every use sits in a fully unrolled loop
+// or an "n" asm operand, so each call folds to an immediate.
+struct FrParams {
+    __host__ __device__ static constexpr uint32_t P(int i) {
+        constexpr uint32_t v[8] = {0xf0000001u, 0x43e1f593u, 0x79b97091u, 0x2833e848u,
+                                   0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u};
+        return v[i];
+    }
+    static constexpr uint32_t N0 = 0xefffffffu;
+    // R mod r, the Montgomery form of one
+    __host__ __device__ static constexpr uint32_t ONE(int i) {
+        constexpr uint32_t v[8] = {0x4ffffffbu, 0xac96341cu, 0x9f60cd29u, 0x36fc7695u,
+                                   0x7879462eu, 0x666ea36fu, 0x9a07df2fu, 0x0e0a77c1u};
+        return v[i];
+    }
+};
+
+struct FqParams {
+    __host__ __device__ static constexpr uint32_t P(int i) {
+        constexpr uint32_t v[8] = {0xd87cfd47u, 0x3c208c16u, 0x6871ca8du, 0x97816a91u,
+                                   0x8181585du, 0xb85045b6u, 0xe131a029u, 0x30644e72u};
+        return v[i];
+    }
+    static constexpr uint32_t N0 = 0xe4866389u;
+    __host__ __device__ static constexpr uint32_t ONE(int i) {
+        constexpr uint32_t v[8] = {0xc58f0d9du, 0xd35d438du, 0xf5c70b3du, 0x0a78eb28u,
+                                   0x7879462cu, 0x666ea36fu, 0x9a07df2fu, 0x0e0a77c1u};
+        return v[i];
+    }
+};
+
+template <class Params>
+struct __align__(16) Fp {
+    uint32_t v[8];
+
+    __device__ __forceinline__ static Fp zero() {
+        Fp r;
+#pragma unroll
+        for (int i = 0; i < 8; i++) r.v[i] = 0;
+        return r;
+    }
+    __device__ __forceinline__ static Fp one() {
+        Fp r;
+#pragma unroll
+        for (int i = 0; i < 8; i++) r.v[i] = Params::ONE(i);
+        return r;
+    }
+    __device__ __forceinline__ bool is_zero() const {
+        uint32_t acc = v[0];
+#pragma unroll
+        for (int i = 1; i < 8; i++) acc |= v[i];
+        return acc == 0;
+    }
+    __device__ __forceinline__ bool eq(const Fp& o) const {
+        uint32_t acc = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) acc |= v[i] ^ o.v[i];
+        return acc == 0;
+    }
+    __device__ __forceinline__ bool is_one() const { return eq(one()); }
+};
+
+// r = a - p if a >= p (a < 2p), in registers
+template <class Params>
+__device__ __forceinline__ void reduce_once(uint32_t* a) {
+    uint32_t d[8], borrow;
+    asm("sub.cc.u32  %0, %9, %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+          "=r"(borrow)
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]),
+          "n"(Params::P(0)), "n"(Params::P(1)), "n"(Params::P(2)), "n"(Params::P(3)), "n"(Params::P(4)),
+          "n"(Params::P(5)), "n"(Params::P(6)), "n"(Params::P(7)));
+    // borrow == 0xffffffff when a < p: keep a
+#pragma unroll
+    for (int i = 0; i < 8; i++) a[i] = borrow ? a[i] : d[i];
+}
+
+template <class Params>
+__device__ __forceinline__ Fp<Params> add(const Fp<Params>& a, const Fp<Params>& b) {
+    Fp<Params> r;
+    asm("add.cc.u32  %0, %8, %16;\n\t"
+        "addc.cc.u32 %1, %9, %17;\n\t"
+        "addc.cc.u32 %2, %10, %18;\n\t"
+        "addc.cc.u32 %3, %11, %19;\n\t"
+        "addc.cc.u32 %4, %12, %20;\n\t"
+        "addc.cc.u32 %5, %13, %21;\n\t"
+        "addc.cc.u32 %6, %14, %22;\n\t"
+        "addc.u32    %7, %15, %23;"
+        : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
+          "=r"(r.v[7])
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
+          "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+    reduce_once<Params>(r.v);
+    return r;
+}
+
+template <class Params>
+__device__ __forceinline__ Fp<Params> sub(const Fp<Params>& a, const Fp<Params>& b) {
+    Fp<Params> r;
+    uint32_t borrow;
+    asm("sub.cc.u32  %0, %9, %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
+          "=r"(r.v[7]), "=r"(borrow)
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
+          "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+    // add p back when the subtraction borrowed (p & mask)
+    uint32_t m = borrow;
+    asm("add.cc.u32  %0, %0, %8;\n\t"
+        "addc.cc.u32 %1, %1, %9;\n\t"
+        "addc.cc.u32 %2, %2, %10;\n\t"
+        "addc.cc.u32 %3, %3, %11;\n\t"
+        "addc.cc.u32 %4, %4, %12;\n\t"
+        "addc.cc.u32 %5, %5, %13;\n\t"
+        "addc.cc.u32 %6, %6, %14;\n\t"
+        "addc.u32    %7, %7, %15;"
+        : "+r"(r.v[0]), "+r"(r.v[1]), "+r"(r.v[2]), "+r"(r.v[3]), "+r"(r.v[4]), "+r"(r.v[5]), "+r"(r.v[6]),
+          "+r"(r.v[7])
+        : "r"(Params::P(0) & m), "r"(Params::P(1) & m), "r"(Params::P(2) & m), "r"(Params::P(3) & m),
+          "r"(Params::P(4) & m), "r"(Params::P(5) & m), "r"(Params::P(6) & m), "r"(Params::P(7) & m));
+    return r;
+}
+
+template <class Params>
+__device__ __forceinline__ Fp<Params> neg(const Fp<Params>& a) {
+    return a.is_zero() ? a : sub(Fp<Params>::zero(), a);
+}
+
+template <class Params>
+__device__ __forceinline__ Fp<Params> dbl(const Fp<Params>& a) {
+    return add(a, a);
+}
+
+// t[0..8] += a[0..7] * b  (lo halves into t0..t7 with carry into t8, then hi halves into t1..t8)
+#define G16_MAD_ROW(T, A, B)                                                                         \
+    asm("mad.lo.cc.u32  %0, %9, %17, %0;\n\t"                                                        \
+        "madc.lo.cc.u32 %1, %10, %17, %1;\n\t"                                                       \
+        "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"                                                       \
+        "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"                                                       \
+        "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"                                                       \
+        "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"                                                       \
+        "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"                                                       \
+        "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"                                                       \
+        "addc.u32       %8, %8, 0;\n\t"                                                              \
+        "mad.hi.cc.u32  %1, %9, %17, %1;\n\t"                                                        \
+        "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"                                                       \
+        "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"                                                       \
+        "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"                                                       \
+        "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"                                                       \
+        "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"                                                       \
+        "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"                                                       \
+        "madc.hi.u32    %8, %16, %17, %8;"                                                           \
+        : "+r"(T[0]), "+r"(T[1]), "+r"(T[2]), "+r"(T[3]), "+r"(T[4]), "+r"(T[5]), "+r"(T[6]),        \
+          "+r"(T[7]), "+r"(T[8])                                                                     \
+        : "r"(A[0]), "r"(A[1]), "r"(A[2]), "r"(A[3]), "r"(A[4]), "r"(A[5]), "r"(A[6]), "r"(A[7]),    \
+          "r"(B))
+
+// t[0..8] += m * P, then shift down one limb
+#define G16_REDUCE_ROW(T, M, PP)                                                                     \
+    asm("mad.lo.cc.u32  %0, %9, %10, %0;\n\t"                                                        \
+        "madc.lo.cc.u32 %1, %9, %11, %1;\n\t"                                                        \
+        "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"                                                        \
+        "madc.lo.cc.u32 %3, %9, %13, %3;\n\t"                                                        \
+        "madc.lo.cc.u32 %4, %9, %14, %4;\n\t"                                                        \
+        "madc.lo.cc.u32 %5, %9, %15, %5;\n\t"                                                        \
+        "madc.lo.cc.u32 %6, %9, %16, %6;\n\t"                                                        \
+        "madc.lo.cc.u32 %7, %9, %17, %7;\n\t"                                                        \
+        "addc.u32       %8, %8, 0;\n\t"                                                              \
+        "mad.hi.cc.u32  %1, %9, %10, %1;\n\t"                                                        \
+        "madc.hi.cc.u32 %2, %9, %11, %2;\n\t"                                                        \
+        "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"                                                        \
+        "madc.hi.cc.u32 %4, %9, %13, %4;\n\t"                                                        \
+        "madc.hi.cc.u32 %5, %9, %14, %5;\n\t"                                                        \
+        "madc.hi.cc.u32 %6, %9, %15, %6;\n\t"                                                        \
+        "madc.hi.cc.u32 %7, %9, %16, %7;\n\t"                                                        \
+        "madc.hi.u32    %8, %9, %17, %8;"                                                            \
+        : "+r"(T[0]), "+r"(T[1]), "+r"(T[2]), "+r"(T[3]), "+r"(T[4]), "+r"(T[5]), "+r"(T[6]),        \
+          "+r"(T[7]), "+r"(T[8])                                                                     \
+        : "r"(M), "n"(PP::P(0)), "n"(PP::P(1)), "n"(PP::P(2)), "n"(PP::P(3)), "n"(PP::P(4)),         \
+          "n"(PP::P(5)), "n"(PP::P(6)), "n"(PP::P(7)))
+
+template <class Params>
+__device__ __forceinline__ Fp<Params> mul(const Fp<Params>& a, const Fp<Params>& b) {
+    uint32_t t[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        G16_MAD_ROW(t, a.v, b.v[i]);
+        uint32_t m = t[0] * Params::N0;
+        G16_REDUCE_ROW(t, m, Params);
+        // t0 is now zero: shift down
+#pragma unroll
+        for (int j = 0; j < 8; j++) t[j] = t[j + 1];
+        t[8] = 0;
+    }
+    reduce_once<Params>(t);
+    Fp<Params> r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = t[i];
+    return r;
+}
+
+template <class Params>
+__device__ __forceinline__ Fp<Params> sqr(const Fp<Params>& a) {
+    return mul(a, a);
+}
+
+// Montgomery -> standard form: a * 1 * R^-1
+template <class Params>
+__device__ __forceinline__ Fp<Params> from_mont(const Fp<Params>& a) {
+    Fp<Params> one_raw = Fp<Params>::zero();
+    one_raw.v[0] = 1;
+    return mul(a, one_raw);
+}
+
+typedef Fp<FrParams> Fr;
+typedef Fp<FqParams> Fq;
+
+// ---- Fq2 = Fq[u]/(u^2 + 1) ----
+struct __align__(16) Fq2 {
+    Fq c0, c1;
+    __device__ __forceinline__ static Fq2 zero() { return {Fq::zero(), Fq::zero()}; }
+    __device__ __forceinline__ static Fq2 one() { return {Fq::one(), Fq::zero()}; }
+    __device__ __forceinline__ bool is_zero() const { return c0.is_zero() && c1.is_zero(); }
+};
+
+__device__ __forceinline__ Fq2 add(const Fq2& a, const Fq2& b) { return {add(a.c0, b.c0), add(a.c1, b.c1)}; }
+__device__ __forceinline__ Fq2 sub(const Fq2& a, const Fq2& b) { return {sub(a.c0, b.c0), sub(a.c1, b.c1)}; }
+__device__ __forceinline__ Fq2 neg(const Fq2& a) { return {neg(a.c0), neg(a.c1)}; }
+__device__ __forceinline__ Fq2 dbl(const Fq2& a) { return {dbl(a.c0), dbl(a.c1)}; }
+// Karatsuba: three Fq products
+__device__ __forceinline__ Fq2 mul(const Fq2& a, const Fq2& b) {
+    Fq t0 = mul(a.c0, b.c0);
+    Fq t1 = mul(a.c1, b.c1);
+    Fq m = mul(add(a.c0, a.c1), add(b.c0, b.c1));
+    return {sub(t0, t1), sub(sub(m, t0), t1)};
+}
+// (a0 + a1 u)^2 = (a0 + a1)(a0 - a1) + 2 a0 a1 u
+__device__ __forceinline__ Fq2 sqr(const Fq2& a) {
+    Fq p = mul(add(a.c0, a.c1), sub(a.c0, a.c1));
+    Fq q = mul(a.c0, a.c1);
+    return {p, dbl(q)};
+}
+
+// ---- 128-bit vector loads / stores of 32-byte elements ----
+template <class T>
+__device__ __forceinline__ T load32(const T* p) {
+    static_assert(sizeof(T) == 32, "32-byte element");
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    uint4 lo = q[0], hi = q[1];
+    T r;
+    r.v[0] = lo.x; r.v[1] = lo.y; r.v[2] = lo.z; r.v[3] = lo.w;
+    r.v[4] = hi.x; r.v[5] = hi.y; r.v[6] = hi.z; r.v[7] = hi.w;
+    return r;
+}
+template <class T>
+__device__ __forceinline__ void store32(T* p, const T& x) {
+    uint4* q = reinterpret_cast<uint4*>(p);
+    q[0] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
+    q[1] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
+}
+
+}  // namespace g16d

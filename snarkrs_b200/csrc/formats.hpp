@@ -1,0 +1,41 @@
+// snarkjs binfile formats (.zkey, .wtns, .r1cs): host-side structures.
+#pragma once
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include "host_bn254.hpp"
+
+#include "g16b200.h"
+
+namespace g16 {
+
+// A parsed proving key (ProvingKey, crates/formats/src/lib.rs:35-65).
+struct ZkeyHost {
+    uint32_t n_vars = 0, n_public = 0, domain_size = 0;
+    std::vector<uint8_t> alpha_g1, beta_g1, beta_g2, gamma_g2, delta_g1, delta_g2, ic;
+    std::vector<uint32_t> row_ptr[2], signal[2], value_id[2];
+    std::vector<uint8_t> values;   // interned Fr, Montgomery, 32 bytes each
+    std::vector<uint8_t> a_query, b_g1_query, b_g2_query, l_query, h_query;
+};
+
+int zkey_parse(const uint8_t* d, size_t len, bool check_points, ZkeyHost& k);
+void zkey_view(const ZkeyHost& k, g16_zkey_view& v);
+int wtns_parse(const uint8_t* d, size_t len, std::vector<uint8_t>& out_mont);
+std::vector<uint8_t> wtns_write(const uint8_t* w_mont, size_t n);
+
+// iden3 binfile writer
+struct BinWriter {
+    std::vector<uint8_t> buf;
+    size_t sec_start = 0;
+    void begin(const char* magic, uint32_t version, uint32_t nsec);
+    void section(uint32_t id);
+    void end_section();
+    void u32(uint32_t x) { bytes(&x, 4); }
+    void u64(uint64_t x) { bytes(&x, 8); }
+    void bytes(const void* p, size_t n) {
+        const uint8_t* b = (const uint8_t*)p;
+        buf.insert(buf.end(), b, b + n);
+    }
+};
+
+}  // namespace g16

@@ -1,0 +1,534 @@
+// Pippenger MSM kernels and engine (see msm.cuh for the pipeline).
+#include "msm.cuh"
+#include "common.cuh"
+#include "curve.cuh"
+#include <algorithm>
+#include <vector>
+
+namespace g16d {
+
+// Bits [off, off + width) of a 256-bit little-endian scalar held in shared
+// memory (8 words, row stride 9 to spread banks); reads past bit 255 are 0.
+__device__ __forceinline__ uint32_t read_bits(const uint32_t* s, int off, int width) {
+    int idx = off >> 5;
+    if (idx >= 8) return 0;
+    int sh = off & 31;
+    uint64_t w = s[idx];
+    if (idx + 1 < 8) w |= (uint64_t)s[idx + 1] << 32;
+    return (uint32_t)(w >> sh) & ((1u << width) - 1u);
+}
+
+// Window w's digit of the carry-free signed recoding, in [-2^(c-1), 2^(c-1)]:
+// the raw window b borrows 2^c when its top bit is set, and the bit just below
+// the window repays the borrow of the window beneath.  255 recoding bits keep
+// the top window's borrow zero for every scalar below 2^254.
+__device__ __forceinline__ int signed_digit(const uint32_t* s, int w, int c) {
+    int off = w * c;
+    int b = (int)read_bits(s, off, c);
+    int d = b - ((b >> (c - 1)) << c);
+    int carry = off ? (int)read_bits(s, off - 1, 1) : 0;
+    return d + carry;
+}
+
+constexpr uint32_t NO_KEY = 0xffffffffu;
+
+__global__ void __launch_bounds__(256) k_digits_count(const uint4* __restrict__ scalars, int mont, uint32_t n, int c,
+                                                      int W, uint32_t B, uint4* __restrict__ scalars_std,
+                                                      uint32_t* __restrict__ counts) {
+    __shared__ uint32_t sh[256 * 9];
+    uint32_t i = blockIdx.x * 256 + threadIdx.x;
+    bool valid = i < n;
+    Fr s = Fr::zero();
+    if (valid) {
+        uint4 a = __ldg(scalars + 2 * (size_t)i), b = __ldg(scalars + 2 * (size_t)i + 1);
+        s.v[0] = a.x; s.v[1] = a.y; s.v[2] = a.z; s.v[3] = a.w;
+        s.v[4] = b.x; s.v[5] = b.y; s.v[6] = b.z; s.v[7] = b.w;
+        if (mont) s = from_mont(s);
+        scalars_std[2 * (size_t)i] = make_uint4(s.v[0], s.v[1], s.v[2], s.v[3]);
+        scalars_std[2 * (size_t)i + 1] = make_uint4(s.v[4], s.v[5], s.v[6], s.v[7]);
+    }
+    uint32_t* row = sh + threadIdx.x * 9;
+#pragma unroll
+    for (int j = 0; j < 8; j++) row[j] = s.v[j];
+    unsigned lane = threadIdx.x & 31;
+    for (int w = 0; w < W; w++) {
+        int d = signed_digit(row, w, c);
+        uint32_t key = (valid && d != 0) ? (uint32_t)w * B + (uint32_t)(d < 0 ? -d : d) - 1u : NO_KEY;
+        unsigned mask = __match_any_sync(0xffffffffu, key);
+        if (key != NO_KEY && lane == (unsigned)(__ffs(mask) - 1)) atomicAdd(&counts[key], (uint32_t)__popc(mask));
+    }
+}
+
+__global__ void __launch_bounds__(256) k_scatter(const uint4* __restrict__ scalars_std, uint32_t n, int c, int W,
+                                                 uint32_t B, uint32_t* __restrict__ cursor,
+                                                 uint32_t* __restrict__ entries) {
+    __shared__ uint32_t sh[256 * 9];
+    uint32_t i = blockIdx.x * 256 + threadIdx.x;
+    bool valid = i < n;
+    uint32_t* row = sh + threadIdx.x * 9;
+    if (valid) {
+        uint4 a = scalars_std[2 * (size_t)i], b = scalars_std[2 * (size_t)i + 1];
+        row[0] = a.x; row[1] = a.y; row[2] = a.z; row[3] = a.w;
+        row[4] = b.x; row[5] = b.y; row[6] = b.z; row[7] = b.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; j++) row[j] = 0;
+    }
+    unsigned lane = threadIdx.x & 31;
+    unsigned lt = (1u << lane) - 1u;
+    for (int w = 0; w < W; w++) {
+        int d = signed_digit(row, w, c);
+        uint32_t key = (valid && d != 0) ? (uint32_t)w * B + (uint32_t)(d < 0 ? -d : d) - 1u : NO_KEY;
+        unsigned mask = __match_any_sync(0xffffffffu, key);
+        int leader = __ffs(mask) - 1;
+        uint32_t base = 0;
+        if (key != NO_KEY && (int)lane == leader) base = atomicAdd(&cursor[key], (uint32_t)__popc(mask));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (key != NO_KEY) entries[base + __popc(mask & lt)] = i | (d < 0 ? 0x80000000u : 0u);
+    }
+}
+
+// ---- exclusive scan (three kernels) ----
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* warp_tot, uint32_t& total) {
+    unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (unsigned)o) x += y;
+    }
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    unsigned nw = blockDim.x >> 5;
+    if (wid == 0) {
+        uint32_t t = lane < nw ? warp_tot[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= (unsigned)o) t += y;
+        }
+        if (lane < nw) warp_tot[lane] = t;
+    }
+    __syncthreads();
+    uint32_t before = wid ? warp_tot[wid - 1] : 0;
+    total = warp_tot[nw - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+// 1024 elements per block of 256 threads (4 consecutive each)
+__global__ void __launch_bounds__(256) k_scan_blocks(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                     uint32_t len, uint32_t* __restrict__ block_sums) {
+    __shared__ uint32_t wt[32];
+    size_t base = (size_t)blockIdx.x * 1024 + threadIdx.x * 4;
+    uint32_t v[4], s = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        v[j] = base + j < len ? in[base + j] : 0;
+        s += v[j];
+    }
+    uint32_t total;
+    uint32_t pre = block_excl_scan(s, wt, total);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if (base + j < len) out[base + j] = pre;
+        pre += v[j];
+    }
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+// one block of 1024 threads scans nb block sums in place; writes the grand total
+__global__ void __launch_bounds__(1024) k_scan_top(uint32_t* __restrict__ sums, uint32_t nb,
+                                                   uint32_t* __restrict__ total_out) {
+    __shared__ uint32_t wt[32];
+    uint32_t per = (nb + 1023) / 1024;
+    uint32_t lo = threadIdx.x * per, hi = min(lo + per, nb);
+    uint32_t s = 0;
+    for (uint32_t j = lo; j < hi; j++) s += sums[j];
+    uint32_t total;
+    uint32_t pre = block_excl_scan(s, wt, total);
+    for (uint32_t j = lo; j < hi; j++) {
+        uint32_t x = sums[j];
+        sums[j] = pre;
+        pre += x;
+    }
+    if (threadIdx.x == 0) *total_out = total;
+}
+
+__global__ void __launch_bounds__(256) k_scan_add(uint32_t* __restrict__ out, uint32_t len,
+                                                  const uint32_t* __restrict__ sums,
+                                                  const uint32_t* __restrict__ total) {
+    size_t i = (size_t)blockIdx.x * 256 + threadIdx.x;
+    if (i < len) out[i] += sums[i / 1024];
+    if (i == 0) out[len] = *total;
+}
+
+__global__ void k_nseg(const uint32_t* __restrict__ offsets, uint32_t K, uint32_t L, uint32_t* __restrict__ nseg) {
+    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= K) return;
+    uint32_t lo = offsets[g], hi = offsets[g + 1];
+    nseg[g] = hi > lo ? ((hi - 1) / L - lo / L + 1) : 0;
+}
+
+__global__ void k_copy_u32(uint32_t* dst, const uint32_t* src, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[i];
+}
+
+// ---- accumulate: one thread per chunk of L sorted entries ----
+template <class F>
+__global__ void __launch_bounds__(128) k_accumulate(const uint32_t* __restrict__ entries,
+                                                    const uint32_t* __restrict__ offsets,
+                                                    const uint32_t* __restrict__ seg_base, uint32_t K,
+                                                    const uint32_t* __restrict__ d_M, uint32_t L,
+                                                    const uint4* __restrict__ bases, uint32_t base_offset,
+                                                    uint32_t n_bases, uint4* __restrict__ partials) {
+    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t M = *d_M;
+    size_t start = t * L;
+    if (start >= M) return;
+    size_t end = start + L < M ? start + L : M;
+    // last bucket g with offsets[g] <= start; then offsets[g+1] > start
+    uint32_t lo = 0, hi = K;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (offsets[mid] <= start) lo = mid; else hi = mid;
+    }
+    uint32_t g = lo;
+    uint32_t next = offsets[g + 1];
+    Xyzz<F> acc = Xyzz<F>::identity();
+    for (size_t k = start; k < end; k++) {
+        if (k == next) {
+            st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), acc);
+            acc = Xyzz<F>::identity();
+            do {
+                g++;
+                next = offsets[g + 1];
+            } while (next <= k);
+        }
+        uint32_t e = entries[k];
+        uint32_t idx = e & 0x7fffffffu;
+        if (idx >= base_offset && idx - base_offset < n_bases) {
+            Affine<F> p = ld_affine<F>(bases, idx - base_offset);
+            if (!p.is_inf()) {
+                if (e >> 31) p.y = neg(p.y);
+                acc = xyzz_add_affine(acc, p.x, p.y);
+            }
+        }
+    }
+    st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), acc);
+}
+
+// ---- bucket reduce: thread (w, p) folds buckets [p*m, (p+1)*m) of window w ----
+template <class F>
+__global__ void __launch_bounds__(128) k_bucket_reduce(const uint4* __restrict__ partials,
+                                                       const uint32_t* __restrict__ offsets,
+                                                       const uint32_t* __restrict__ seg_base, uint32_t L, uint32_t B,
+                                                       uint32_t W, uint32_t m, uint32_t P,
+                                                       uint4* __restrict__ seg_out) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= W * P) return;
+    uint32_t w = t / P, p = t % P;
+    Xyzz<F> run = Xyzz<F>::identity(), tot = Xyzz<F>::identity();
+    for (int j = (int)m - 1; j >= 0; j--) {
+        uint32_t g = w * B + p * m + (uint32_t)j;
+        uint32_t lo = offsets[g], hi = offsets[g + 1];
+        if (hi > lo) {
+            uint32_t ns = (hi - 1) / L - lo / L + 1, b0 = seg_base[g];
+            for (uint32_t s = 0; s < ns; s++) run = xyzz_add(run, ld_xyzz<F>(partials, b0 + s));
+        }
+        tot = xyzz_add(tot, run);
+    }
+    // segment weight offset: buckets here carry weight (b - p m + 1) in tot; add p m * run
+    uint32_t k = p * m;
+    Xyzz<F> acc = Xyzz<F>::identity();
+    if (k) {
+        for (int bit = 31 - __clz(k); bit >= 0; bit--) {
+            acc = xyzz_dbl(acc);
+            if ((k >> bit) & 1u) acc = xyzz_add(acc, run);
+        }
+    }
+    st_xyzz<F>(seg_out, t, xyzz_add(tot, acc));
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) k_window_reduce(const uint4* __restrict__ seg_out, uint32_t P,
+                                                       uint4* __restrict__ windows) {
+    extern __shared__ uint4 smem[];
+    uint32_t w = blockIdx.x;
+    Xyzz<F> acc = Xyzz<F>::identity();
+    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) acc = xyzz_add(acc, ld_xyzz<F>(seg_out, (size_t)w * P + i));
+    st_xyzz<F>(smem, threadIdx.x, acc);
+    __syncthreads();
+    for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            acc = xyzz_add(acc, ld_xyzz<F>(smem, threadIdx.x + s));
+            st_xyzz<F>(smem, threadIdx.x, acc);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) st_xyzz<F>(windows, w, acc);
+}
+
+}  // namespace g16d
+
+namespace g16 {
+
+using namespace g16d;
+
+void MsmSort::release() {
+    cudaFree(d_scalars_std);
+    cudaFree(d_counts);
+    cudaFree(d_offsets);
+    cudaFree(d_cursor);
+    cudaFree(d_seg_base);
+    cudaFree(d_scan_tmp);
+    cudaFree(d_entries);
+    cudaFree(d_total);
+    *this = MsmSort();
+}
+
+void MsmAccum::release() {
+    cudaFree(d_partials);
+    cudaFree(d_segments);
+    cudaFree(d_windows);
+    *this = MsmAccum();
+}
+
+int msm_window_bits(size_t m) {
+    // cost ~ windows * (m + 2 * buckets): bucket reduction runs fully parallel
+    // on the device, so buckets weigh less than the reference CPU model's 3
+    int best = 8;
+    double best_cost = 1e300;
+    for (int c = 8; c <= 18; c++) {
+        double windows = (255 + c - 1) / c;
+        double cost = windows * ((double)m + 2.0 * (double)(1u << (c - 1)));
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = c;
+        }
+    }
+    return best;
+}
+
+template <class T>
+static cudaError_t grow(T*& p, size_t& cap, size_t need_elems) {
+    if (need_elems <= cap && p) return cudaSuccess;
+    cudaFree(p);
+    p = nullptr;
+    size_t n = need_elems + need_elems / 8 + 64;
+    cudaError_t e = cudaMalloc((void**)&p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        cap = 0;
+        set_error("cudaMalloc of %zu bytes for MSM scratch failed: %s", n * sizeof(T), cudaGetErrorString(e));
+        return e;
+    }
+    cap = n;
+    return cudaSuccess;
+}
+
+static cudaError_t grow_bytes(void*& p, size_t& cap, size_t need) {
+    if (need <= cap && p) return cudaSuccess;
+    cudaFree(p);
+    p = nullptr;
+    size_t n = need + need / 8 + 256;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+        cap = 0;
+        set_error("cudaMalloc of %zu bytes for MSM scratch failed: %s", n, cudaGetErrorString(e));
+        return e;
+    }
+    cap = n;
+    return cudaSuccess;
+}
+
+// exclusive scan of in[0..len) into out[0..len] (out[len] = total); total also to *d_total
+static cudaError_t scan(const uint32_t* in, uint32_t* out, uint32_t len, uint32_t* tmp, uint32_t* d_total,
+                        cudaStream_t st) {
+    uint32_t nb = (len + 1023) / 1024;
+    if (nb == 0) nb = 1;
+    k_scan_blocks<<<nb, 256, 0, st>>>(in, out, len, tmp);
+    k_scan_top<<<1, 1024, 0, st>>>(tmp, nb, d_total);
+    k_scan_add<<<blocks_for(len ? len : 1, 256), 256, 0, st>>>(out, len, tmp, d_total);
+    return cudaGetLastError();
+}
+
+cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomery, int c, cudaStream_t st) {
+    if (n >= 0x80000000ull) {
+        set_error("MSM of %zu points exceeds the 2^31 point-index limit", n);
+        return cudaErrorInvalidValue;
+    }
+    if (c == 0) c = msm_window_bits(n);
+    s.c = c;
+    s.W = (255 + c - 1) / c;
+    s.B = 1u << (c - 1);
+    s.K = (uint32_t)s.W * s.B;
+    s.n = n;
+    size_t nn = n ? n : 1;
+    G16_CUDA(grow(s.d_scalars_std, s.cap_scalars, nn * 8));
+    size_t kk = (size_t)s.K + 1;
+    if (kk > s.cap_k || !s.d_counts) {
+        size_t cap = 0;
+        G16_CUDA(grow(s.d_counts, cap, kk));
+        cap = 0;
+        G16_CUDA(grow(s.d_offsets, cap, kk));
+        cap = 0;
+        G16_CUDA(grow(s.d_cursor, cap, kk));
+        cap = 0;
+        G16_CUDA(grow(s.d_seg_base, cap, kk));
+        s.cap_k = cap;
+    }
+    G16_CUDA(grow(s.d_scan_tmp, s.cap_tmp, kk / 1024 + 2));
+    G16_CUDA(grow(s.d_entries, s.cap_entries, nn * s.W));
+    if (!s.d_total) G16_CUDA(cudaMalloc((void**)&s.d_total, 4 * sizeof(uint32_t)));
+
+    G16_CUDA(cudaMemsetAsync(s.d_counts, 0, kk * sizeof(uint32_t), st));
+    G16_CUDA(cudaMemsetAsync(s.d_total, 0, 4 * sizeof(uint32_t), st));
+    if (n) {
+        TimedLaunch tl("msm_digits", st);
+        k_digits_count<<<blocks_for(n, 256), 256, 0, st>>>((const uint4*)d_scalars, montgomery ? 1 : 0, (uint32_t)n,
+                                                          c, s.W, s.B, (uint4*)s.d_scalars_std, s.d_counts);
+    }
+    G16_CUDA(cudaGetLastError());
+    {
+        TimedLaunch tl("msm_scan", st);
+        G16_CUDA(scan(s.d_counts, s.d_offsets, s.K, s.d_scan_tmp, s.d_total, st));
+    }
+    k_copy_u32<<<blocks_for(s.K, 256), 256, 0, st>>>(s.d_cursor, s.d_offsets, s.K);
+    if (n) {
+        TimedLaunch tl("msm_scatter", st);
+        k_scatter<<<blocks_for(n, 256), 256, 0, st>>>((const uint4*)s.d_scalars_std, (uint32_t)n, c, s.W, s.B,
+                                                     s.d_cursor, s.d_entries);
+    }
+    G16_CUDA(cudaGetLastError());
+    // per-bucket segment counts -> segment base (into counts, then scanned)
+    k_nseg<<<blocks_for(s.K, 256), 256, 0, st>>>(s.d_offsets, s.K, s.chunk, s.d_counts);
+    G16_CUDA(scan(s.d_counts, s.d_seg_base, s.K, s.d_scan_tmp, s.d_total + 1, st));
+    return cudaSuccess;
+}
+
+template <class F>
+static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bases, uint32_t base_offset,
+                              uint32_t n_bases, cudaStream_t st, size_t xyzz_bytes, const char* tag) {
+    size_t max_entries = (s.n ? s.n : 1) * (size_t)s.W;
+    size_t chunks = (max_entries + s.chunk - 1) / s.chunk;
+    size_t max_partials = (size_t)s.K + chunks + 1;
+    G16_CUDA(grow_bytes(acc.d_partials, acc.cap_partials, max_partials * xyzz_bytes));
+    uint32_t m = s.B < 16 ? s.B : 16;
+    uint32_t P = s.B / m;
+    acc.segs_per_window = P;
+    G16_CUDA(grow_bytes(acc.d_segments, acc.cap_segments, (size_t)s.W * P * xyzz_bytes));
+    G16_CUDA(grow_bytes(acc.d_windows, acc.cap_windows, (size_t)s.W * xyzz_bytes));
+    {
+        TimedLaunch tl(tag, st);
+        k_accumulate<F><<<blocks_for(chunks, 128), 128, 0, st>>>(s.d_entries, s.d_offsets, s.d_seg_base, s.K,
+                                                                  s.d_total, s.chunk, (const uint4*)d_bases,
+                                                                  base_offset, n_bases, (uint4*)acc.d_partials);
+    }
+    G16_CUDA(cudaGetLastError());
+    {
+        TimedLaunch tl("msm_bucket_reduce", st);
+        k_bucket_reduce<F><<<blocks_for((size_t)s.W * P, 128), 128, 0, st>>>(
+            (const uint4*)acc.d_partials, s.d_offsets, s.d_seg_base, s.chunk, s.B, s.W, m, P,
+            (uint4*)acc.d_segments);
+    }
+    G16_CUDA(cudaGetLastError());
+    {
+        TimedLaunch tl("msm_window_reduce", st);
+        k_window_reduce<F><<<s.W, 128, 128 * xyzz_bytes, st>>>((const uint4*)acc.d_segments, P,
+                                                                 (uint4*)acc.d_windows);
+    }
+    G16_CUDA(cudaGetLastError());
+    return cudaSuccess;
+}
+
+cudaError_t msm_accumulate_g1(const MsmSort& s, MsmAccum& acc, const void* d_bases, uint32_t base_offset,
+                              uint32_t n_bases, cudaStream_t st) {
+    return accumulate<g16d::Fq>(s, acc, d_bases, base_offset, n_bases, st, XYZZ_G1_BYTES, "msm_accumulate_g1");
+}
+
+cudaError_t msm_accumulate_g2(const MsmSort& s, MsmAccum& acc, const void* d_bases, uint32_t base_offset,
+                              uint32_t n_bases, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_window_reduce<g16d::Fq2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 256);
+        attr = true;
+    }
+    return accumulate<g16d::Fq2>(s, acc, d_bases, base_offset, n_bases, st, XYZZ_G2_BYTES, "msm_accumulate_g2");
+}
+
+// ---- host: window sums -> Horner ----
+static Fq fq_at(const uint8_t* p) {
+    uint64_t v[4];
+    std::memcpy(v, p, 32);
+    return Fq::raw(v);
+}
+
+template <class F>
+static F read_coord(const uint8_t* p);
+template <>
+Fq read_coord<Fq>(const uint8_t* p) { return fq_at(p); }
+template <>
+Fq2 read_coord<Fq2>(const uint8_t* p) { return {fq_at(p), fq_at(p + 32)}; }
+
+template <class F>
+static Jac<F> combine(const uint8_t* w, int W, int c) {
+    const size_t cs = sizeof(F) == sizeof(Fq) ? 32 : 64;   // coordinate bytes
+    std::vector<F> zz(W), zzz(W);
+    std::vector<F> X(W), Y(W);
+    std::vector<char> inf(W);
+    for (int i = 0; i < W; i++) {
+        const uint8_t* p = w + (size_t)i * 4 * cs;
+        X[i] = read_coord<F>(p);
+        Y[i] = read_coord<F>(p + cs);
+        zz[i] = read_coord<F>(p + 2 * cs);
+        zzz[i] = read_coord<F>(p + 3 * cs);
+        inf[i] = zz[i].is_zero();
+    }
+    // batch inversion of every nonzero zz and zzz
+    std::vector<F> vals, pref;
+    for (int i = 0; i < W; i++)
+        if (!inf[i]) {
+            vals.push_back(zz[i]);
+            vals.push_back(zzz[i]);
+        }
+    std::vector<F> invs(vals.size());
+    if (!vals.empty()) {
+        pref.resize(vals.size());
+        F run = F::one();
+        for (size_t k = 0; k < vals.size(); k++) {
+            pref[k] = run;
+            run = run * vals[k];
+        }
+        F iv = run.inv();
+        for (size_t k = vals.size(); k-- > 0;) {
+            invs[k] = iv * pref[k];
+            iv = iv * vals[k];
+        }
+    }
+    std::vector<Affine<F>> aff(W);
+    size_t k = 0;
+    for (int i = 0; i < W; i++) {
+        if (inf[i]) {
+            aff[i].x = F::zero();
+            aff[i].y = F::zero();
+            aff[i].inf = true;
+            continue;
+        }
+        aff[i].x = X[i] * invs[k];
+        aff[i].y = Y[i] * invs[k + 1];
+        aff[i].inf = false;
+        k += 2;
+    }
+    Jac<F> acc = Jac<F>::from_affine(aff[W - 1]);
+    for (int i = W - 2; i >= 0; i--) {
+        for (int j = 0; j < c; j++) acc = acc.dbl();
+        acc = acc.add_affine(aff[i]);
+    }
+    return acc;
+}
+
+G1J msm_combine_g1(const uint8_t* windows_xyzz, int W, int c) { return combine<Fq>(windows_xyzz, W, c); }
+G2J msm_combine_g2(const uint8_t* windows_xyzz, int W, int c) { return combine<Fq2>(windows_xyzz, W, c); }
+
+}  // namespace g16

@@ -1,0 +1,87 @@
+// Pippenger MSM engine for BN254 G1 / G2 on sm_100a (host interface).
+//
+// Replaces the reference's CUDA MSM (crates/cuda/src/msm.rs + kernels/msm.cu:
+// count / scan / scatter / segmented accumulate / merge / reduce, host
+// Horner at msm.rs:3976-4010) and implements the MsmBackend contract of
+// crates/msm/src/lib.rs:52-82: sum_i k_i P_i, scalars in standard or
+// Montgomery form, infinity bases and zero scalars contribute nothing.
+//
+// Pipeline, all on one stream, no host synchronisation until the window
+// sums are read back:
+//   1. digits: signed c-bit digits over 255 bits (carry-free recoding, the
+//      same digit set as crates/msm/src/lib.rs:319-333), per-(window,bucket)
+//      histogram with warp-aggregated atomics;
+//   2. exclusive scan -> bucket offsets; scatter of (point index | sign) into
+//      bucket order: a counting sort of (window, bucket, point) keys;
+//   3. accumulate: the sorted list is cut into fixed-length chunks, one
+//      thread per chunk adds its points into XYZZ partial bucket sums, so a
+//      fat bucket (a repeated witness value) is spread over many threads;
+//   4. bucket reduce: per window, segments of buckets fold their partials
+//      and run the running-sum reduction sum_b (b+1) S_b;
+//   5. window reduce: one block per window sums the segment results;
+//   6. host: Horner over the W window sums (c doublings between windows).
+// One sort serves every base vector that shares the scalars: the prover
+// sorts the witness once and accumulates A, B1, L (G1) and B2 (G2) from it.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "host_bn254.hpp"
+
+namespace g16 {
+
+struct MsmSort {
+    // parameters
+    int c = 0, W = 0;
+    uint32_t B = 0;        // buckets per window, 2^(c-1)
+    uint32_t K = 0;        // W * B
+    size_t n = 0;          // scalars sorted
+    uint32_t chunk = 16;   // accumulate chunk length
+    // device buffers (capacities in elements)
+    uint32_t* d_scalars_std = nullptr;  size_t cap_scalars = 0;   // 8 u32 per scalar
+    uint32_t* d_counts = nullptr;       size_t cap_k = 0;         // K + 1
+    uint32_t* d_offsets = nullptr;                                // K + 1
+    uint32_t* d_cursor = nullptr;                                 // K
+    uint32_t* d_seg_base = nullptr;                               // K + 1
+    uint32_t* d_scan_tmp = nullptr;     size_t cap_tmp = 0;
+    uint32_t* d_entries = nullptr;      size_t cap_entries = 0;
+    uint32_t* d_total = nullptr;                                  // [0] = M, [1] = S
+    void release();
+};
+
+struct MsmAccum {
+    void* d_partials = nullptr;    size_t cap_partials = 0;   // bytes
+    void* d_segments = nullptr;    size_t cap_segments = 0;   // bytes
+    void* d_windows = nullptr;     size_t cap_windows = 0;    // bytes
+    uint32_t segs_per_window = 0;
+    void release();
+};
+
+// Window width for m scalars that reach the buckets.  The reference CPU model
+// (crates/msm/src/lib.rs:160-172) with the GPU's cheaper bucket reduction.
+int msm_window_bits(size_t m);
+
+// Sort n device-resident scalars (32 bytes each; montgomery != 0 converts
+// from Montgomery form first).  c = 0 picks msm_window_bits(n).
+cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomery, int c, cudaStream_t st);
+
+// Accumulate bases against a sorted scalar set and reduce to W window sums
+// (XYZZ, device, in acc.d_windows).  Entry i uses base i - base_offset; entries
+// below base_offset or at/after base_offset + n_bases are skipped.
+cudaError_t msm_accumulate_g1(const MsmSort& s, MsmAccum& acc, const void* d_bases, uint32_t base_offset,
+                              uint32_t n_bases, cudaStream_t st);
+cudaError_t msm_accumulate_g2(const MsmSort& s, MsmAccum& acc, const void* d_bases, uint32_t base_offset,
+                              uint32_t n_bases, cudaStream_t st);
+
+// Host side: W XYZZ window sums (as copied back) -> Horner -> Jacobian.
+G1J msm_combine_g1(const uint8_t* windows_xyzz, int W, int c);
+G2J msm_combine_g2(const uint8_t* windows_xyzz, int W, int c);
+
+constexpr size_t XYZZ_G1_BYTES = 128;
+constexpr size_t XYZZ_G2_BYTES = 256;
+
+// kernel-time accounting hook (events around each kernel class), optional
+struct KernelTimer;
+void msm_set_timer(KernelTimer* t);
+
+}  // namespace g16

@@ -1,0 +1,395 @@
+// Radix-2 Fr NTT kernels (see ntt.cuh).
+#include "common.cuh"
+#include "field.cuh"
+#include "host_bn254.hpp"
+#include "ntt.cuh"
+#include <vector>
+
+namespace g16d {
+
+struct Vec3 {
+    uint4* p[3];
+};
+
+__device__ __forceinline__ Fr ld_s(const uint4* sm, uint32_t e) {
+    uint4 a = sm[2 * e], b = sm[2 * e + 1];
+    Fr r;
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+    r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+    return r;
+}
+__device__ __forceinline__ void st_s(uint4* sm, uint32_t e, const Fr& x) {
+    sm[2 * e] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
+    sm[2 * e + 1] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
+}
+__device__ __forceinline__ Fr ld_g(const uint4* g, size_t i) {
+    uint4 a = __ldg(g + 2 * i), b = __ldg(g + 2 * i + 1);
+    Fr r;
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+    r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+    return r;
+}
+__device__ __forceinline__ Fr ld_rw(const uint4* g, size_t i) {
+    uint4 a = g[2 * i], b = g[2 * i + 1];
+    Fr r;
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+    r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+    return r;
+}
+__device__ __forceinline__ void st_g(uint4* g, size_t i, const Fr& x) {
+    g[2 * i] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
+    g[2 * i + 1] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
+}
+
+// One radix-2 stage on a shared-memory tile.  The tile holds elements
+// i = hi*2^(s_lo+k) + mid*2^s_lo + (lo0 + l) at smem slot mid*L + l; stage
+// s = s_lo + j pairs mid values differing in bit j.  The butterfly's
+// position inside its 2^(s+1) block is (mid mod 2^j)*2^s_lo + lo0 + l and
+// its twiddle omega_{2^(s+1)}^pos = tw[pos << (log_n - s - 1)].
+template <bool DIF>
+__device__ __forceinline__ void run_stage(uint4* sm, uint32_t j, uint32_t s_lo, uint32_t log_L, uint32_t lo0,
+                                          uint32_t log_n, uint32_t half_tile, const uint4* __restrict__ tw) {
+    const uint32_t L = 1u << log_L;
+    const uint32_t s = s_lo + j;
+    const uint32_t jmask = (1u << j) - 1u;
+    for (uint32_t q = threadIdx.x; q < half_tile; q += blockDim.x) {
+        uint32_t l = q & (L - 1u);
+        uint32_t mq = q >> log_L;
+        uint32_t mid_a = ((mq >> j) << (j + 1)) | (mq & jmask);
+        uint32_t ea = (mid_a << log_L) | l;
+        uint32_t eb = ea + (1u << (j + log_L));
+        uint32_t pos = ((mid_a & jmask) << s_lo) | (lo0 + l);
+        Fr a = ld_s(sm, ea), b = ld_s(sm, eb);
+        if (DIF) {
+            Fr d = sub(a, b);
+            a = add(a, b);
+            b = pos ? mul(d, ld_g(tw, (size_t)pos << (log_n - s - 1))) : d;
+        } else {
+            Fr t = pos ? mul(b, ld_g(tw, (size_t)pos << (log_n - s - 1))) : b;
+            b = sub(a, t);
+            a = add(a, t);
+        }
+        st_s(sm, ea, a);
+        st_s(sm, eb, b);
+    }
+}
+
+// Stages [s_lo, s_lo + k) of 2^log_n, one tile of (2^k)*L elements per block;
+// blockIdx.y selects the vector.  Optional epilogues: multiply by *scale,
+// or write h = join_a * join_b - x to join_out instead of storing x.
+template <bool DIF>
+__global__ void __launch_bounds__(256) k_ntt_pass(Vec3 vecs, uint32_t log_n, uint32_t s_lo, uint32_t k,
+                                                  uint32_t log_L, const uint4* __restrict__ tw,
+                                                  const uint4* __restrict__ scale, const uint4* __restrict__ join_a,
+                                                  const uint4* __restrict__ join_b, uint4* __restrict__ join_out) {
+    extern __shared__ uint4 sm[];
+    uint4* data = vecs.p[blockIdx.y];
+    const uint32_t L = 1u << log_L;
+    const uint32_t tile = (1u << k) << log_L;
+    const uint32_t bph = s_lo - log_L;
+    const size_t hi = blockIdx.x >> bph;
+    const uint32_t lo0 = (blockIdx.x & ((1u << bph) - 1u)) << log_L;
+    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
+        uint32_t mid = e >> log_L, l = e & (L - 1u);
+        size_t gi = (hi << (s_lo + k)) | ((size_t)mid << s_lo) | (lo0 + l);
+        sm[2 * e] = data[2 * gi];
+        sm[2 * e + 1] = data[2 * gi + 1];
+    }
+    __syncthreads();
+    for (uint32_t jj = 0; jj < k; jj++) {
+        uint32_t j = DIF ? k - 1 - jj : jj;
+        run_stage<DIF>(sm, j, s_lo, log_L, lo0, log_n, tile / 2, tw);
+        __syncthreads();
+    }
+    Fr sc;
+    if (scale) sc = ld_g(scale, 0);
+    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
+        uint32_t mid = e >> log_L, l = e & (L - 1u);
+        size_t gi = (hi << (s_lo + k)) | ((size_t)mid << s_lo) | (lo0 + l);
+        Fr x = ld_s(sm, e);
+        if (scale) x = mul(x, sc);
+        if (join_out) {
+            Fr h = sub(mul(ld_rw(join_a, gi), ld_rw(join_b, gi)), x);
+            st_g(join_out, gi, h);
+        } else {
+            st_g(data, gi, x);
+        }
+    }
+}
+
+// The fused middle of iNTT -> coset -> NTT: DIF stages [0, k) with inverse
+// twiddles, a[p] *= coset[p], DIT stages [0, k) with forward twiddles, on
+// contiguous tiles of 2^k.  Optional h = join_a * join_b - x epilogue for a
+// transform that has no outer passes.
+__global__ void __launch_bounds__(256) k_ntt_mid(Vec3 vecs, uint32_t log_n, uint32_t k, const uint4* __restrict__ tw,
+                                                 const uint4* __restrict__ tw_inv, const uint4* __restrict__ coset,
+                                                 const uint4* __restrict__ join_a, const uint4* __restrict__ join_b,
+                                                 uint4* __restrict__ join_out) {
+    extern __shared__ uint4 sm[];
+    uint4* data = vecs.p[blockIdx.y];
+    const uint32_t tile = 1u << k;
+    const size_t base = (size_t)blockIdx.x << k;
+    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
+        sm[2 * e] = data[2 * (base + e)];
+        sm[2 * e + 1] = data[2 * (base + e) + 1];
+    }
+    __syncthreads();
+    for (int j = (int)k - 1; j >= 0; j--) {
+        run_stage<true>(sm, (uint32_t)j, 0, 0, 0, log_n, tile / 2, tw_inv);
+        __syncthreads();
+    }
+    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) st_s(sm, e, mul(ld_s(sm, e), ld_g(coset, base + e)));
+    __syncthreads();
+    for (uint32_t j = 0; j < k; j++) {
+        run_stage<false>(sm, j, 0, 0, 0, log_n, tile / 2, tw);
+        __syncthreads();
+    }
+    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
+        Fr x = ld_s(sm, e);
+        if (join_out) {
+            st_g(join_out, base + e, sub(mul(ld_rw(join_a, base + e), ld_rw(join_b, base + e)), x));
+        } else {
+            st_g(data, base + e, x);
+        }
+    }
+}
+
+__device__ __forceinline__ Fr fr_pow_u64(Fr b, uint64_t e) {
+    Fr acc = Fr::one();
+    while (e) {
+        if (e & 1) acc = mul(acc, b);
+        b = mul(b, b);
+        e >>= 1;
+    }
+    return acc;
+}
+
+// out[i or bitrev(i)] = scale * base^i for i < count, 16 per thread
+__global__ void k_powers(uint4* out, Fr base, Fr scale, uint64_t count, uint32_t bitrev_log) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t i0 = t * 16;
+    if (i0 >= count) return;
+    Fr p = mul(scale, fr_pow_u64(base, i0));
+    for (uint64_t i = i0; i < i0 + 16 && i < count; i++) {
+        size_t dst = bitrev_log ? (size_t)(__brevll(i) >> (64 - bitrev_log)) : (size_t)i;
+        st_g(out, dst, p);
+        p = mul(p, base);
+    }
+}
+
+// a[i] *= shift^i, 16 per thread
+__global__ void k_distribute(uint4* a, Fr shift, uint64_t n) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t i0 = t * 16;
+    if (i0 >= n) return;
+    Fr p = fr_pow_u64(shift, i0);
+    for (uint64_t i = i0; i < i0 + 16 && i < n; i++) {
+        st_g(a, i, mul(ld_rw(a, i), p));
+        p = mul(p, shift);
+    }
+}
+
+__global__ void k_bitrev(uint4* a, uint32_t log_n, uint64_t n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t j = __brevll(i) >> (64 - log_n);
+    if (j > i) {
+        Fr x = ld_rw(a, i), y = ld_rw(a, j);
+        st_g(a, i, y);
+        st_g(a, j, x);
+    }
+}
+
+__global__ void k_join(const uint4* a, const uint4* b, const uint4* c, uint4* h, uint64_t n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    st_g(h, i, sub(mul(ld_rw(a, i), ld_rw(b, i)), ld_rw(c, i)));
+}
+
+}  // namespace g16d
+
+namespace g16 {
+
+using namespace g16d;
+
+static constexpr uint32_t TILE_LOG = 11;    // 2048 elements, 64 KiB of shared memory
+static constexpr uint32_t OUTER_LOG_L = 2;  // 4 consecutive columns (128 B) per tile row
+
+void NttTables::release() {
+    cudaFree(d_tw);
+    cudaFree(d_tw_inv);
+    cudaFree(d_coset);
+    d_tw = d_tw_inv = d_coset = nullptr;
+    log_n = -1;
+}
+
+static g16d::Fr to_dev(const g16::Fr& x) {
+    g16d::Fr r;
+    std::memcpy(r.v, x.x.v, 32);
+    return r;
+}
+
+cudaError_t ntt_tables(NttTables& t, int log_n, cudaStream_t st) {
+    if (t.log_n == log_n) return cudaSuccess;
+    if (log_n < 1 || log_n > 27) {
+        set_error("NTT size 2^%d outside [2^1, 2^27]", log_n);
+        return cudaErrorInvalidValue;
+    }
+    host_init();
+    t.release();
+    size_t n = (size_t)1 << log_n;
+    G16_CUDA(cudaMalloc(&t.d_tw, (n / 2) * 32));
+    G16_CUDA(cudaMalloc(&t.d_tw_inv, (n / 2) * 32));
+    G16_CUDA(cudaMalloc(&t.d_coset, n * 32 + 32));   // + one slot holding 1/n for the scale epilogue
+    g16::Fr w = domain_root(log_n), wi = w.inv();
+    g16::Fr ninv = g16::Fr::from_u64(n).inv();
+    g16::Fr shift = domain_root(log_n + 1);
+    std::memcpy(t.n_inv, ninv.x.v, 32);
+    std::memcpy(t.shift, shift.x.v, 32);
+    g16d::Fr d_one;
+    std::memcpy(d_one.v, g16::Fr::one().x.v, 32);
+    k_powers<<<blocks_for((n / 2 + 15) / 16, 128), 128, 0, st>>>((uint4*)t.d_tw, to_dev(w), d_one, n / 2, 0);
+    k_powers<<<blocks_for((n / 2 + 15) / 16, 128), 128, 0, st>>>((uint4*)t.d_tw_inv, to_dev(wi), d_one, n / 2, 0);
+    k_powers<<<blocks_for((n + 15) / 16, 128), 128, 0, st>>>((uint4*)t.d_coset, to_dev(shift), to_dev(ninv), n,
+                                                              (uint32_t)log_n);
+    G16_CUDA(cudaMemcpyAsync((uint8_t*)t.d_coset + n * 32, ninv.x.v, 32, cudaMemcpyHostToDevice, st));
+    G16_CUDA(cudaGetLastError());
+    G16_CUDA(cudaStreamSynchronize(st));
+    t.log_n = log_n;
+    return cudaSuccess;
+}
+
+struct Pass {
+    uint32_t s_lo, k, log_L;
+};
+
+// outer passes covering stages [k0, log_n), in increasing s_lo
+static std::vector<Pass> outer_passes(uint32_t log_n, uint32_t k0) {
+    std::vector<Pass> v;
+    uint32_t rem = log_n - k0;
+    if (!rem) return v;
+    uint32_t kmax = TILE_LOG - OUTER_LOG_L;
+    uint32_t np = (rem + kmax - 1) / kmax;
+    uint32_t s = k0;
+    for (uint32_t i = 0; i < np; i++) {
+        uint32_t k = rem / np + (i < rem % np ? 1 : 0);
+        uint32_t ll = OUTER_LOG_L < s ? OUTER_LOG_L : s;
+        v.push_back({s, k, ll});
+        s += k;
+    }
+    return v;
+}
+
+static bool attrs_done = false;
+static void set_attrs() {
+    if (attrs_done) return;
+    size_t smem = ((size_t)1 << TILE_LOG) * 32;
+    cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_ntt_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attrs_done = true;
+}
+
+static cudaError_t launch_pass(bool dif, Vec3 v, int nv, uint32_t log_n, const Pass& p, const void* tw,
+                               const void* scale, const void* ja, const void* jb, void* jo, cudaStream_t st) {
+    uint32_t tile = (1u << p.k) << p.log_L;
+    size_t n = (size_t)1 << log_n;
+    dim3 grid((unsigned)(n / tile), nv);
+    unsigned threads = tile / 2 < 256 ? tile / 2 : 256;
+    size_t smem = (size_t)tile * 32;
+    TimedLaunch tl(dif ? "ntt_pass_dif" : "ntt_pass_dit", st);
+    if (dif)
+        k_ntt_pass<true><<<grid, threads, smem, st>>>(v, log_n, p.s_lo, p.k, p.log_L, (const uint4*)tw,
+                                                       (const uint4*)scale, (const uint4*)ja, (const uint4*)jb,
+                                                       (uint4*)jo);
+    else
+        k_ntt_pass<false><<<grid, threads, smem, st>>>(v, log_n, p.s_lo, p.k, p.log_L, (const uint4*)tw,
+                                                        (const uint4*)scale, (const uint4*)ja, (const uint4*)jb,
+                                                        (uint4*)jo);
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_mid(Vec3 v, int nv, const NttTables& t, const void* ja, const void* jb, void* jo,
+                              cudaStream_t st) {
+    uint32_t log_n = (uint32_t)t.log_n;
+    uint32_t k0 = log_n < TILE_LOG ? log_n : TILE_LOG;
+    uint32_t tile = 1u << k0;
+    size_t n = (size_t)1 << log_n;
+    dim3 grid((unsigned)(n / tile), nv);
+    unsigned threads = tile / 2 < 256 ? tile / 2 : 256;
+    TimedLaunch tl("ntt_mid_fused", st);
+    k_ntt_mid<<<grid, threads, (size_t)tile * 32, st>>>(v, log_n, k0, (const uint4*)t.d_tw, (const uint4*)t.d_tw_inv,
+                                                         (const uint4*)t.d_coset, (const uint4*)ja, (const uint4*)jb,
+                                                         (uint4*)jo);
+    return cudaGetLastError();
+}
+
+cudaError_t ntt_h_pipeline(const NttTables& t, void* a, void* b, void* c, void* h, cudaStream_t st) {
+    set_attrs();
+    uint32_t log_n = (uint32_t)t.log_n;
+    uint32_t k0 = log_n < TILE_LOG ? log_n : TILE_LOG;
+    auto outer = outer_passes(log_n, k0);
+    Vec3 abc = {{(uint4*)a, (uint4*)b, (uint4*)c}};
+    // inverse, DIF, top stages first
+    for (size_t i = outer.size(); i-- > 0;)
+        G16_CUDA(launch_pass(true, abc, 3, log_n, outer[i], t.d_tw_inv, nullptr, nullptr, nullptr, nullptr, st));
+    if (outer.empty()) {
+        G16_CUDA(launch_mid(abc, 2, t, nullptr, nullptr, nullptr, st));
+        Vec3 cc = {{(uint4*)c, nullptr, nullptr}};
+        return launch_mid(cc, 1, t, a, b, h, st);
+    }
+    G16_CUDA(launch_mid(abc, 3, t, nullptr, nullptr, nullptr, st));
+    for (size_t i = 0; i + 1 < outer.size(); i++)
+        G16_CUDA(launch_pass(false, abc, 3, log_n, outer[i], t.d_tw, nullptr, nullptr, nullptr, nullptr, st));
+    G16_CUDA(launch_pass(false, abc, 2, log_n, outer.back(), t.d_tw, nullptr, nullptr, nullptr, nullptr, st));
+    Vec3 cc = {{(uint4*)c, nullptr, nullptr}};
+    return launch_pass(false, cc, 1, log_n, outer.back(), t.d_tw, nullptr, a, b, h, st);
+}
+
+cudaError_t ntt_intt_coset_ntt(const NttTables& t, void* a, cudaStream_t st) {
+    set_attrs();
+    uint32_t log_n = (uint32_t)t.log_n;
+    uint32_t k0 = log_n < TILE_LOG ? log_n : TILE_LOG;
+    auto outer = outer_passes(log_n, k0);
+    Vec3 v = {{(uint4*)a, nullptr, nullptr}};
+    for (size_t i = outer.size(); i-- > 0;)
+        G16_CUDA(launch_pass(true, v, 1, log_n, outer[i], t.d_tw_inv, nullptr, nullptr, nullptr, nullptr, st));
+    G16_CUDA(launch_mid(v, 1, t, nullptr, nullptr, nullptr, st));
+    for (auto& p : outer)
+        G16_CUDA(launch_pass(false, v, 1, log_n, p, t.d_tw, nullptr, nullptr, nullptr, nullptr, st));
+    return cudaSuccess;
+}
+
+static cudaError_t dit_natural(const NttTables& t, void* a, const void* tw, const void* scale, cudaStream_t st) {
+    set_attrs();
+    uint32_t log_n = (uint32_t)t.log_n;
+    size_t n = (size_t)1 << log_n;
+    k_bitrev<<<blocks_for(n, 256), 256, 0, st>>>((uint4*)a, log_n, n);
+    G16_CUDA(cudaGetLastError());
+    uint32_t k0 = log_n < TILE_LOG ? log_n : TILE_LOG;
+    auto outer = outer_passes(log_n, k0);
+    Vec3 v = {{(uint4*)a, nullptr, nullptr}};
+    Pass inner = {0, k0, 0};
+    G16_CUDA(launch_pass(false, v, 1, log_n, inner, tw, outer.empty() ? scale : nullptr, nullptr, nullptr, nullptr,
+                         st));
+    for (size_t i = 0; i < outer.size(); i++)
+        G16_CUDA(launch_pass(false, v, 1, log_n, outer[i], tw, i + 1 == outer.size() ? scale : nullptr, nullptr,
+                             nullptr, nullptr, st));
+    return cudaSuccess;
+}
+
+cudaError_t ntt_forward(const NttTables& t, void* a, cudaStream_t st) { return dit_natural(t, a, t.d_tw, nullptr, st); }
+
+cudaError_t ntt_inverse(const NttTables& t, void* a, cudaStream_t st) {
+    size_t n = (size_t)1 << t.log_n;
+    return dit_natural(t, a, t.d_tw_inv, (const uint8_t*)t.d_coset + n * 32, st);
+}
+
+cudaError_t ntt_distribute_powers(void* a, size_t n, const uint64_t* shift_mont, cudaStream_t st) {
+    g16d::Fr s;
+    std::memcpy(s.v, shift_mont, 32);
+    k_distribute<<<blocks_for((n + 15) / 16, 128), 128, 0, st>>>((uint4*)a, s, n);
+    return cudaGetLastError();
+}
+
+}  // namespace g16

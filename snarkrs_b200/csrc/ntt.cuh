@@ -1,0 +1,51 @@
+// Radix-2 Fr NTT on sm_100a (host interface).
+//
+// Replaces the reference's CUDA stages 1-3 (crates/cuda/src/kernels/ntt.cu:
+// g16_ntt_head / g16_ntt_tail) and the CPU CpuNtt API
+// (crates/ntt/src/lib.rs:415-584).  Values are fixed by the mathematics (a
+// DFT over omega_n = TWO_ADIC_ROOT^(2^(28 - log n)), crates/field/src/lib.rs:46-84),
+// so outputs are bit-identical to the CPU's whatever the pass structure.
+//
+// Structure: a transform of 2^log_n is cut into shared-memory passes.  The
+// inner pass covers stages [0, k0) on contiguous tiles of 2^k0 elements; the
+// outer passes cover the remaining stages on tiles gathered with stride
+// 2^s_lo (L consecutive columns per tile for 128-byte segments).  The
+// prover's iNTT -> coset -> NTT chain runs DIF (natural -> bit-reversed) for
+// the inverse and DIT (bit-reversed -> natural) for the forward, so the two
+// inner passes and the coset multiply in between fuse into one kernel and no
+// bit-reversal pass exists; the forward's last pass of C also fuses
+// H = A*B - C (crates/groth16/src/cpu.rs:230-246, no division by Z).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace g16 {
+
+struct NttTables {
+    int log_n = -1;
+    void* d_tw = nullptr;       // omega^i, i < n/2 (Montgomery Fr)
+    void* d_tw_inv = nullptr;   // omega^-i, i < n/2
+    void* d_coset = nullptr;    // shift^bitrev(p) / n, p < n (the proving coset shift omega_2n)
+    uint64_t n_inv[4];          // 1/n, Montgomery
+    uint64_t shift[4];          // omega_2n, Montgomery
+    void release();
+};
+
+// Build (or keep) the tables for 2^log_n on the device, log_n in [1, 27].
+cudaError_t ntt_tables(NttTables& t, int log_n, cudaStream_t st);
+
+// The prover's stages 1-4 on device vectors of n = 2^log_n: A, B, C each go
+// iNTT -> * shift^i/n -> NTT (natural order in and out, in place) and
+// h = A*B - C is written to h (may alias none of A, B, C).
+cudaError_t ntt_h_pipeline(const NttTables& t, void* a, void* b, void* c, void* h, cudaStream_t st);
+
+// One vector through the same chain (the reference's intt_coset_ntt).
+cudaError_t ntt_intt_coset_ntt(const NttTables& t, void* a, cudaStream_t st);
+
+// Standalone transforms, natural order in and out.
+cudaError_t ntt_forward(const NttTables& t, void* a, cudaStream_t st);
+cudaError_t ntt_inverse(const NttTables& t, void* a, cudaStream_t st);   // includes the 1/n scale
+// a[i] *= shift^i (crates/ntt/src/lib.rs:582), shift Montgomery
+cudaError_t ntt_distribute_powers(void* a, size_t n, const uint64_t* shift_mont, cudaStream_t st);
+
+}  // namespace g16

@@ -1,0 +1,837 @@
+// Groth16 prover orchestration and the extern "C" boundary (include/g16b200.h).
+//
+// Mirrors the reference's CUDA backend split (crates/cuda/src/backend.rs:
+// CudaBackend / CudaCircuit; stages.rs: stages 0-4; msm.rs: stages 5-9) and
+// the PreparedCircuit contract (crates/groth16/src/lib.rs:371-455):
+//   prepare      upload CSR, bases and domain tables once (backend.rs:325-457)
+//   stage 0      gather A.w and B.w over the CSR rows, C = A*B (cpu.rs:140-174, 316-341)
+//   stages 1-4   iNTT -> coset -> NTT for A, B, C, H = A*B - C (cpu.rs:191-252)
+//   stages 5-9   five MSMs: A, B1, L in G1 and B2 in G2 from one sort of the
+//                witness, H in G1 (cpu.rs:477-632)
+//   stage 11     blinding and assembly on the host (prove.rs:335-430), the
+//                four key-only products computed on a side thread while the
+//                device runs, as blinded_with does (prove.rs:201-229).
+#include <atomic>
+#include <cstdarg>
+#include <chrono>
+#include <future>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+#include "common.cuh"
+#include "curve.cuh"
+#include "field.cuh"
+#include "formats.hpp"
+#include "g16b200.h"
+#include "host_bn254.hpp"
+#include "msm.cuh"
+#include "ntt.cuh"
+
+namespace g16 {
+
+static thread_local std::string g_err;
+
+void set_error(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+
+KernelTimer& timer() {
+    static KernelTimer t;
+    return t;
+}
+
+}  // namespace g16
+
+using namespace g16;
+
+// ---------------------------------------------------------------- kernels
+namespace g16d {
+
+// Stage 0: one thread per constraint row.  Zero witness values are skipped
+// and ones added without a multiply, which is exact either way
+// (crates/groth16/src/cpu.rs:150-170).
+__global__ void __launch_bounds__(256) k_gather(const uint32_t* __restrict__ rpa, const uint32_t* __restrict__ siga,
+                                                const uint32_t* __restrict__ vida, const uint32_t* __restrict__ rpb,
+                                                const uint32_t* __restrict__ sigb, const uint32_t* __restrict__ vidb,
+                                                const uint4* __restrict__ values, const uint4* __restrict__ w,
+                                                uint32_t n, uint4* __restrict__ A, uint4* __restrict__ B,
+                                                uint4* __restrict__ C) {
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= n) return;
+    Fr acc[2];
+    const uint32_t* rp[2] = {rpa, rpb};
+    const uint32_t* sg[2] = {siga, sigb};
+    const uint32_t* vd[2] = {vida, vidb};
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+        Fr a = Fr::zero();
+        for (uint32_t k = rp[m][row]; k < rp[m][row + 1]; k++) {
+            Fr wv = load32(reinterpret_cast<const Fr*>(w) + sg[m][k]);
+            if (wv.is_zero()) continue;
+            Fr v = load32(reinterpret_cast<const Fr*>(values) + vd[m][k]);
+            a = add(a, wv.is_one() ? v : mul(v, wv));
+        }
+        acc[m] = a;
+    }
+    store32(reinterpret_cast<Fr*>(A) + row, acc[0]);
+    store32(reinterpret_cast<Fr*>(B) + row, acc[1]);
+    store32(reinterpret_cast<Fr*>(C) + row, mul(acc[0], acc[1]));
+}
+
+}  // namespace g16d
+
+// ---------------------------------------------------------------- handles
+struct g16_backend {
+    int ordinal = 0;
+    uint64_t vram_limit = 0;
+    std::atomic<uint64_t> vram_used{0};
+    cudaStream_t stream = nullptr;
+    std::mutex mu;   // primitives share the scratch below
+    MsmSort sort;
+    MsmAccum acc;
+    void* d_in = nullptr;
+    size_t cap_in = 0;
+    void* d_in2 = nullptr;
+    size_t cap_in2 = 0;
+    std::vector<std::unique_ptr<NttTables>> ntt;   // by log_n
+    uint8_t* h_pinned = nullptr;                   // window sums readback
+    size_t cap_pinned = 0;
+};
+
+struct g16_circuit {
+    g16_backend* be = nullptr;
+    uint32_t n_vars = 0, n_public = 0, n = 0;
+    int log_n = 0;
+    // resident key
+    uint32_t *d_rp[2] = {nullptr, nullptr}, *d_sig[2] = {nullptr, nullptr}, *d_vid[2] = {nullptr, nullptr};
+    void* d_values = nullptr;
+    void *d_a = nullptr, *d_b1 = nullptr, *d_b2 = nullptr, *d_l = nullptr, *d_h = nullptr;
+    NttTables ntt;
+    G1A alpha1, beta1, delta1;
+    G2A beta2, delta2;
+    // per-proof scratch
+    void* d_w = nullptr;
+    void* d_abc = nullptr;   // A | B | C, n each
+    void* d_hpoly = nullptr;
+    MsmSort sort_w, sort_h;
+    MsmAccum acc[5];
+    uint8_t* h_win = nullptr;   // pinned, 5 * 20 windows * 256 B
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::mutex mu;
+    g16_stage_timings t = {0, 0, 0, 0, 0, 0};
+    uint64_t device_bytes = 0;
+    std::vector<void*> allocs;
+};
+
+struct g16_hpoly {
+    g16_circuit* owner = nullptr;
+    void* d_h = nullptr;
+    uint32_t n = 0;
+};
+
+struct g16_zkey {
+    ZkeyHost k;
+};
+
+namespace {
+
+int fail(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    set_error("%s", buf);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation) return fail(G16_ERR_DEVICE_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+    std::string prev = [] {
+        char b[512];
+        g16_last_error(b, sizeof b);
+        return std::string(b);
+    }();
+    return fail(G16_ERR_DEVICE, "%s: %s (%s)", what, cudaGetErrorString(e), prev.c_str());
+}
+
+#define CK(call, what)                                  \
+    do {                                                \
+        cudaError_t e__ = (call);                       \
+        if (e__ != cudaSuccess) return cuda_fail(e__, what); \
+    } while (0)
+
+cudaError_t circuit_alloc(g16_circuit* c, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 32);
+    if (e == cudaSuccess) {
+        c->allocs.push_back(*p);
+        c->device_bytes += bytes;
+        c->be->vram_used += bytes;
+    }
+    return e;
+}
+
+bool is_one_mont(const uint8_t* w0) {
+    host_init();
+    return std::memcmp(w0, FR_P.one.v, 32) == 0;
+}
+
+template <class A>
+bool unpack_checked(A& a, const uint8_t* p) {
+    return unpack(a, p);
+}
+
+// r * P for a standard-form scalar given as Montgomery Fr
+G1J g1_mul(const G1J& p, const g16::Fr& k) {
+    uint64_t s[4];
+    k.to_std(s);
+    return p.mul(s);
+}
+G2J g2_mul(const G2J& p, const g16::Fr& k) {
+    uint64_t s[4];
+    k.to_std(s);
+    return p.mul(s);
+}
+
+struct BlinderTerms {
+    G1J d1r, d1s, d1rs;
+    G2J d2s;
+};
+
+BlinderTerms blinder_terms(const g16_circuit* c, const g16::Fr& r, const g16::Fr& s) {
+    BlinderTerms t;
+    G1J d1 = G1J::from_affine(c->delta1);
+    t.d1r = g1_mul(d1, r);
+    t.d1s = g1_mul(d1, s);
+    t.d1rs = g1_mul(d1, r * s);
+    t.d2s = g2_mul(G2J::from_affine(c->delta2), s);
+    return t;
+}
+
+struct MsmJac {
+    G1J a, b1, l, h;
+    G2J b2;
+};
+
+void assemble(const g16_circuit* c, const MsmJac& m, const BlinderTerms& t, const g16::Fr& r, const g16::Fr& s,
+              g16_proof* out) {
+    G1J pi_a = m.a.add_affine(c->alpha1) + t.d1r;
+    G2J pi_b = m.b2.add_affine(c->beta2) + t.d2s;
+    G1J pib1 = m.b1.add_affine(c->beta1) + t.d1s;
+    G1J pi_c = m.l + m.h + g1_mul(pi_a, s) + g1_mul(pib1, r) + t.d1rs.neg();
+    G1J g1s[2] = {pi_a, pi_c};
+    G1A g1a[2];
+    batch_to_affine(g1s, g1a, 2);
+    G2A g2a = pi_b.to_affine();
+    pack(out->a, g1a[0]);
+    pack(out->b, g2a);
+    pack(out->c, g1a[1]);
+}
+
+void to_outputs(const MsmJac& m, g16_msm_outputs* o) {
+    G1J g1s[4] = {m.a, m.b1, m.l, m.h};
+    G1A a[4];
+    batch_to_affine(g1s, a, 4);
+    pack(o->a_g1, a[0]);
+    pack(o->b_g1, a[1]);
+    pack(o->l_g1, a[2]);
+    pack(o->h_g1, a[3]);
+    pack(o->b_g2, m.b2.to_affine());
+}
+
+int check_witness(const g16_circuit* c, size_t n, const uint8_t* w_host) {
+    if (n != c->n_vars)
+        return fail(G16_ERR_WITNESS_LENGTH, "witness has %zu values, the circuit has %u wires", n, c->n_vars);
+    if (w_host && !is_one_mont(w_host)) return fail(G16_ERR_CONSTANT_WIRE, "witness[0] is not 1");
+    return G16_OK;
+}
+
+uint64_t elapsed_us(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) return 0;
+    return (uint64_t)(ms * 1000.0);
+}
+
+// stages 0-4 on the device witness; H left in h_out (device)
+int run_h(g16_circuit* c, const void* d_w, void* h_out) {
+    cudaStream_t st = c->stream;
+    uint8_t* abc = (uint8_t*)c->d_abc;
+    size_t vb = (size_t)c->n * 32;
+    CK(cudaEventRecord(c->ev[0], st), "event");
+    {
+        TimedLaunch tl("gather", st);
+        g16d::k_gather<<<blocks_for(c->n, 256), 256, 0, st>>>(
+            c->d_rp[0], c->d_sig[0], c->d_vid[0], c->d_rp[1], c->d_sig[1], c->d_vid[1], (const uint4*)c->d_values,
+            (const uint4*)d_w, c->n, (uint4*)abc, (uint4*)(abc + vb), (uint4*)(abc + 2 * vb));
+    }
+    CK(cudaGetLastError(), "gather launch");
+    CK(cudaEventRecord(c->ev[1], st), "event");
+    CK(ntt_h_pipeline(c->ntt, abc, abc + vb, abc + 2 * vb, h_out, st), "NTT pipeline");
+    CK(cudaEventRecord(c->ev[2], st), "event");
+    return G16_OK;
+}
+
+// stages 5-9: five MSMs, window sums read back, Horner on the host
+int run_msms(g16_circuit* c, const void* d_w, const void* d_h, MsmJac& out) {
+    cudaStream_t st = c->stream;
+    CK(msm_sort(c->sort_h, d_h, c->n, true, 0, st), "H sort");
+    CK(msm_accumulate_g1(c->sort_h, c->acc[4], c->d_h, 0, c->n, st), "H accumulate");
+    CK(msm_sort(c->sort_w, d_w, c->n_vars, true, 0, st), "witness sort");
+    CK(msm_accumulate_g1(c->sort_w, c->acc[0], c->d_a, 0, c->n_vars, st), "A accumulate");
+    CK(msm_accumulate_g1(c->sort_w, c->acc[2], c->d_b1, 0, c->n_vars, st), "B1 accumulate");
+    uint32_t off = c->n_public + 1;
+    CK(msm_accumulate_g1(c->sort_w, c->acc[3], c->d_l, off, c->n_vars - off, st), "L accumulate");
+    CK(msm_accumulate_g2(c->sort_w, c->acc[1], c->d_b2, 0, c->n_vars, st), "B2 accumulate");
+    // readback: slot i holds up to 32 windows of 256 bytes
+    const size_t slot = 32 * 256;
+    for (int i = 0; i < 5; i++) {
+        const MsmSort& s = (i == 4) ? c->sort_h : c->sort_w;
+        size_t bytes = (size_t)s.W * (i == 1 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES);
+        CK(cudaMemcpyAsync(c->h_win + i * slot, c->acc[i].d_windows, bytes, cudaMemcpyDeviceToHost, st),
+           "window readback");
+    }
+    CK(cudaEventRecord(c->ev[3], st), "event");
+    CK(cudaStreamSynchronize(st), "MSM stages");
+    timer().collect();
+    out.a = msm_combine_g1(c->h_win + 0 * slot, c->sort_w.W, c->sort_w.c);
+    out.b2 = msm_combine_g2(c->h_win + 1 * slot, c->sort_w.W, c->sort_w.c);
+    out.b1 = msm_combine_g1(c->h_win + 2 * slot, c->sort_w.W, c->sort_w.c);
+    out.l = msm_combine_g1(c->h_win + 3 * slot, c->sort_w.W, c->sort_w.c);
+    out.h = msm_combine_g1(c->h_win + 4 * slot, c->sort_h.W, c->sort_h.c);
+    return G16_OK;
+}
+
+int prove_on_device(g16_circuit* c, const void* d_w, const uint8_t* r_mont, const uint8_t* s_mont, g16_proof* out) {
+    g16::Fr r = g16::Fr::raw((const uint64_t*)r_mont), s = g16::Fr::raw((const uint64_t*)s_mont);
+    uint64_t rr[4], ss[4];
+    std::memcpy(rr, r_mont, 32);
+    std::memcpy(ss, s_mont, 32);
+    if (!g16::Fr::canonical(rr) || !g16::Fr::canonical(ss)) return fail(G16_ERR_INVALID_ARGUMENT, "r or s not below r");
+    auto terms = std::async(std::launch::async, [&] { return blinder_terms(c, r, s); });
+    int rc = run_h(c, d_w, c->d_hpoly);
+    MsmJac m;
+    if (rc == G16_OK) rc = run_msms(c, d_w, c->d_hpoly, m);
+    BlinderTerms t = terms.get();
+    if (rc != G16_OK) return rc;
+    auto t0 = std::chrono::steady_clock::now();
+    assemble(c, m, t, r, s, out);
+    auto t1 = std::chrono::steady_clock::now();
+    c->t.gather_us += elapsed_us(c->ev[0], c->ev[1]);
+    c->t.ntt_us += elapsed_us(c->ev[1], c->ev[2]);
+    c->t.msm_us += elapsed_us(c->ev[2], c->ev[3]);
+    c->t.assemble_us += (uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(t1 - t0).count();
+    return G16_OK;
+}
+
+int upload_witness(g16_circuit* c, const uint8_t* w, size_t n) {
+    CK(cudaMemcpyAsync(c->d_w, w, n * 32, cudaMemcpyHostToDevice, c->stream), "witness upload");
+    return G16_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- C ABI
+extern "C" {
+
+size_t g16_last_error(char* buf, size_t len) {
+    const std::string& e = g_err;
+    if (buf && len) {
+        size_t k = e.size() < len - 1 ? e.size() : len - 1;
+        std::memcpy(buf, e.data(), k);
+        buf[k] = 0;
+    }
+    return e.size();
+}
+
+int g16_backend_open(int ordinal, uint64_t vram_limit, g16_backend** out) {
+    if (!out) return fail(G16_ERR_INVALID_ARGUMENT, "null output handle");
+    host_init();
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        return fail(G16_ERR_DEVICE, "no CUDA device: %s", e != cudaSuccess ? cudaGetErrorString(e) : "count is 0");
+    if (ordinal < 0 || ordinal >= count) return fail(G16_ERR_DEVICE, "CUDA device %d of %d", ordinal, count);
+    CK(cudaSetDevice(ordinal), "cudaSetDevice");
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, ordinal), "cudaGetDeviceProperties");
+    if (prop.major < 10) return fail(G16_ERR_DEVICE, "device %d is sm_%d%d; this build targets sm_100a", ordinal, prop.major, prop.minor);
+    auto b = std::make_unique<g16_backend>();
+    b->ordinal = ordinal;
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    b->vram_limit = vram_limit ? vram_limit : (uint64_t)free_b;
+    CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream");
+    *out = b.release();
+    return G16_OK;
+}
+
+void g16_backend_free(g16_backend* b) {
+    if (!b) return;
+    cudaSetDevice(b->ordinal);
+    cudaStreamSynchronize(b->stream);
+    b->sort.release();
+    b->acc.release();
+    cudaFree(b->d_in);
+    cudaFree(b->d_in2);
+    for (auto& t : b->ntt)
+        if (t) t->release();
+    cudaFreeHost(b->h_pinned);
+    cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+const char* g16_backend_name(const g16_backend*) { return "cuda-b200"; }
+uint64_t g16_backend_vram_used(const g16_backend* b) { return b ? b->vram_used.load() : 0; }
+
+// ---- formats ----
+int g16_zkey_parse(const uint8_t* bytes, size_t len, int check_points, g16_zkey** out) {
+    if (!bytes || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    auto z = std::make_unique<g16_zkey>();
+    int rc = zkey_parse(bytes, len, check_points != 0, z->k);
+    if (rc != G16_OK) return rc;
+    *out = z.release();
+    return G16_OK;
+}
+
+int g16_zkey_view_get(const g16_zkey* k, g16_zkey_view* out) {
+    if (!k || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    zkey_view(k->k, *out);
+    return G16_OK;
+}
+
+void g16_zkey_free(g16_zkey* k) { delete k; }
+
+int g16_wtns_parse(const uint8_t* bytes, size_t len, uint8_t* out_mont, size_t cap, size_t* n_out) {
+    if (!bytes || !n_out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    std::vector<uint8_t> w;
+    int rc = wtns_parse(bytes, len, w);
+    if (rc != G16_OK) return rc;
+    *n_out = w.size() / 32;
+    if (!out_mont) return G16_OK;
+    if (cap < *n_out) return fail(G16_ERR_INVALID_ARGUMENT, "witness buffer holds %zu of %zu values", cap, *n_out);
+    std::memcpy(out_mont, w.data(), w.size());
+    return G16_OK;
+}
+
+int g16_wtns_write(const uint8_t* w_mont, size_t n, uint8_t* out, size_t cap, size_t* len_out) {
+    if (!w_mont || !len_out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    std::vector<uint8_t> b = wtns_write(w_mont, n);
+    *len_out = b.size();
+    if (!out) return G16_OK;
+    if (cap < b.size()) return fail(G16_ERR_INVALID_ARGUMENT, "buffer too small");
+    std::memcpy(out, b.data(), b.size());
+    return G16_OK;
+}
+
+// ---- prepare ----
+int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
+    if (!b || !k || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    uint32_t n = k->domain_size;
+    if (n < 2 || (n & (n - 1)) || n > (1u << 27)) return fail(G16_ERR_BACKEND, "domain size %u is not a power of two in [2, 2^27]", n);
+    if ((uint64_t)k->n_public + 1 > k->n_vars) return fail(G16_ERR_BACKEND, "n_public %u exceeds n_vars %u", k->n_public, k->n_vars);
+    if (k->n_vars >= 0x80000000u || n >= 0x80000000u) return fail(G16_ERR_BACKEND, "more than 2^31 wires");
+    // CSR structure (Coefficients::check_structure, formats/src/lib.rs:185-270)
+    for (int m = 0; m < 2; m++) {
+        const uint32_t* rp = k->row_ptr[m];
+        if (!rp || rp[0] != 0 || rp[n] != k->nnz[m]) return fail(G16_ERR_BACKEND, "matrix %d row_ptr is malformed", m);
+        for (uint32_t i = 0; i < n; i++)
+            if (rp[i + 1] < rp[i]) return fail(G16_ERR_BACKEND, "matrix %d row_ptr is not monotone at row %u", m, i);
+        for (uint32_t i = 0; i < k->nnz[m]; i++) {
+            if (k->signal[m][i] >= k->n_vars) return fail(G16_ERR_BACKEND, "matrix %d nonzero %u references signal %u", m, i, k->signal[m][i]);
+            if (k->value_id[m][i] >= k->n_values) return fail(G16_ERR_BACKEND, "matrix %d nonzero %u references value %u", m, i, k->value_id[m][i]);
+        }
+    }
+    uint64_t nv = k->n_vars, nl = nv - k->n_public - 1;
+    // memory budget, refused before any allocation (backend.rs:367-381)
+    uint64_t key_bytes = 4ull * (n + 1) * 2 + 8ull * (k->nnz[0] + k->nnz[1]) + 32ull * k->n_values + nv * 64 * 2 +
+                         nv * 128 + nl * 64 + (uint64_t)n * 64 + (uint64_t)n * 32 * 2 + 32;
+    uint64_t scratch = nv * 32 + (uint64_t)n * 32 * 4 + ((uint64_t)n + nv) * 32 + ((uint64_t)n + nv) * 16 * 4 +
+                       ((uint64_t)n + nv) * 16 / 16 * 256 * 2 + (64ull << 20);
+    if (b->vram_used + key_bytes + scratch > b->vram_limit)
+        return fail(G16_ERR_DEVICE_MEMORY, "circuit needs about %llu MiB of device memory, %llu MiB of the %llu MiB budget are free",
+                    (unsigned long long)((key_bytes + scratch) >> 20),
+                    (unsigned long long)((b->vram_limit - std::min<uint64_t>(b->vram_limit, b->vram_used)) >> 20),
+                    (unsigned long long)(b->vram_limit >> 20));
+    // header points
+    auto c = std::make_unique<g16_circuit>();
+    c->be = b;
+    c->n_vars = k->n_vars;
+    c->n_public = k->n_public;
+    c->n = n;
+    while ((1u << c->log_n) < n) c->log_n++;
+    if (!unpack(c->alpha1, k->alpha_g1) || !unpack(c->beta1, k->beta_g1) || !unpack(c->delta1, k->delta_g1) ||
+        !unpack(c->beta2, k->beta_g2) || !unpack(c->delta2, k->delta_g2))
+        return fail(G16_ERR_BACKEND, "non-canonical header point");
+    if (c->alpha1.inf || c->beta1.inf || c->delta1.inf || c->beta2.inf || c->delta2.inf)
+        return fail(G16_ERR_BACKEND, "a header point is the point at infinity");
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+    for (auto& e : c->ev) CK(cudaEventCreate(&e), "event");
+    struct Up {
+        void** dst;
+        const void* src;
+        size_t bytes;
+    } ups[] = {
+        {(void**)&c->d_rp[0], k->row_ptr[0], 4ull * (n + 1)},
+        {(void**)&c->d_rp[1], k->row_ptr[1], 4ull * (n + 1)},
+        {(void**)&c->d_sig[0], k->signal[0], 4ull * k->nnz[0]},
+        {(void**)&c->d_sig[1], k->signal[1], 4ull * k->nnz[1]},
+        {(void**)&c->d_vid[0], k->value_id[0], 4ull * k->nnz[0]},
+        {(void**)&c->d_vid[1], k->value_id[1], 4ull * k->nnz[1]},
+        {&c->d_values, k->values, 32ull * k->n_values},
+        {&c->d_a, k->a_query, 64ull * nv},
+        {&c->d_b1, k->b_g1_query, 64ull * nv},
+        {&c->d_b2, k->b_g2_query, 128ull * nv},
+        {&c->d_l, k->l_query, 64ull * nl},
+        {&c->d_h, k->h_query, 64ull * n},
+    };
+    g16_circuit* cp = c.get();
+    auto cleanup = [&] { g16_circuit_free(c.release()); };
+    for (auto& u : ups) {
+        cudaError_t e = circuit_alloc(cp, u.dst, u.bytes);
+        if (e == cudaSuccess && u.bytes) e = cudaMemcpyAsync(*u.dst, u.src, u.bytes, cudaMemcpyHostToDevice, cp->stream);
+        if (e != cudaSuccess) {
+            int rc = cuda_fail(e, "key upload");
+            cleanup();
+            return rc;
+        }
+    }
+    cudaError_t e = circuit_alloc(cp, &cp->d_w, 32ull * nv);
+    if (e == cudaSuccess) e = circuit_alloc(cp, &cp->d_abc, 32ull * n * 3);
+    if (e == cudaSuccess) e = circuit_alloc(cp, &cp->d_hpoly, 32ull * n);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&cp->h_win, 5 * 32 * 256);
+    if (e == cudaSuccess) e = ntt_tables(cp->ntt, cp->log_n, cp->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cp->stream);
+    if (e != cudaSuccess) {
+        int rc = cuda_fail(e, "prepare");
+        cleanup();
+        return rc;
+    }
+    cp->device_bytes += 3ull * 32 * n / 2 * 2;
+    *out = c.release();
+    return G16_OK;
+}
+
+void g16_circuit_free(g16_circuit* c) {
+    if (!c) return;
+    cudaSetDevice(c->be->ordinal);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void* p : c->allocs) cudaFree(p);
+    c->be->vram_used -= std::min<uint64_t>(c->be->vram_used, c->device_bytes);
+    c->ntt.release();
+    c->sort_w.release();
+    c->sort_h.release();
+    for (auto& a : c->acc) a.release();
+    if (c->h_win) cudaFreeHost(c->h_win);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+uint32_t g16_circuit_n_vars(const g16_circuit* c) { return c ? c->n_vars : 0; }
+uint32_t g16_circuit_n_public(const g16_circuit* c) { return c ? c->n_public : 0; }
+uint32_t g16_circuit_domain_size(const g16_circuit* c) { return c ? c->n : 0; }
+uint64_t g16_circuit_device_bytes(const g16_circuit* c) { return c ? c->device_bytes : 0; }
+
+// ---- stages ----
+int g16_compute_h(g16_circuit* c, const uint8_t* w, size_t n, g16_hpoly** out) {
+    if (!c || !w || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    int rc = check_witness(c, n, w);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
+    auto h = std::make_unique<g16_hpoly>();
+    h->owner = c;
+    h->n = c->n;
+    CK(cudaMalloc(&h->d_h, 32ull * c->n), "H allocation");
+    if ((rc = upload_witness(c, w, n))) return rc;
+    if ((rc = run_h(c, c->d_w, h->d_h))) {
+        cudaFree(h->d_h);
+        return rc;
+    }
+    CK(cudaStreamSynchronize(c->stream), "stages 0-4");
+    timer().collect();
+    c->t.gather_us += elapsed_us(c->ev[0], c->ev[1]);
+    c->t.ntt_us += elapsed_us(c->ev[1], c->ev[2]);
+    *out = h.release();
+    return G16_OK;
+}
+
+int g16_h_to_host(const g16_hpoly* h, uint8_t* out, size_t cap) {
+    if (!h || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    if (cap < h->n) return fail(G16_ERR_INVALID_ARGUMENT, "buffer holds %zu of %u values", cap, h->n);
+    CK(cudaSetDevice(h->owner->be->ordinal), "cudaSetDevice");
+    CK(cudaMemcpy(out, h->d_h, 32ull * h->n, cudaMemcpyDeviceToHost), "H readback");
+    return G16_OK;
+}
+
+void g16_hpoly_free(g16_hpoly* h) {
+    if (!h) return;
+    cudaFree(h->d_h);
+    delete h;
+}
+
+int g16_msms(g16_circuit* c, const uint8_t* w, size_t n, const g16_hpoly* h, g16_msm_outputs* out) {
+    if (!c || !w || !h || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    if (h->owner != c) return fail(G16_ERR_BACKEND, "H handle was computed by another circuit");
+    int rc = check_witness(c, n, w);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
+    if ((rc = upload_witness(c, w, n))) return rc;
+    CK(cudaEventRecord(c->ev[2], c->stream), "event");
+    MsmJac m;
+    if ((rc = run_msms(c, c->d_w, h->d_h, m))) return rc;
+    c->t.msm_us += elapsed_us(c->ev[2], c->ev[3]);
+    to_outputs(m, out);
+    return G16_OK;
+}
+
+int g16_h_and_msms(g16_circuit* c, const uint8_t* w, size_t n, g16_msm_outputs* out) {
+    if (!c || !w || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    int rc = check_witness(c, n, w);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
+    if ((rc = upload_witness(c, w, n))) return rc;
+    if ((rc = run_h(c, c->d_w, c->d_hpoly))) return rc;
+    MsmJac m;
+    if ((rc = run_msms(c, c->d_w, c->d_hpoly, m))) return rc;
+    c->t.gather_us += elapsed_us(c->ev[0], c->ev[1]);
+    c->t.ntt_us += elapsed_us(c->ev[1], c->ev[2]);
+    c->t.msm_us += elapsed_us(c->ev[2], c->ev[3]);
+    to_outputs(m, out);
+    return G16_OK;
+}
+
+int g16_prove_with_blinders(g16_circuit* c, const uint8_t* w, size_t n, const uint8_t* r, const uint8_t* s,
+                            g16_proof* out) {
+    if (!c || !w || !r || !s || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    int rc = check_witness(c, n, w);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
+    if ((rc = upload_witness(c, w, n))) return rc;
+    return prove_on_device(c, c->d_w, r, s, out);
+}
+
+int g16_prove_with_blinders_device(g16_circuit* c, const void* d_w, size_t n, const uint8_t* r, const uint8_t* s,
+                                   g16_proof* out) {
+    if (!c || !d_w || !r || !s || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    int rc = check_witness(c, n, nullptr);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(c->mu);
+    CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
+    return prove_on_device(c, d_w, r, s, out);
+}
+
+int g16_stage_timings_get(const g16_circuit* c, g16_stage_timings* out) {
+    if (!c || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    *out = c->t;
+    return G16_OK;
+}
+
+int g16_prove_batch(g16_backend* b, size_t count, g16_circuit* const* circuits, const uint8_t* const* witnesses,
+                    const size_t* lens, const uint8_t* r, const uint8_t* s, g16_proof* out) {
+    if (!b || (count && (!circuits || !witnesses || !lens || !r || !s || !out)))
+        return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    for (size_t i = 0; i < count; i++) {
+        int rc = g16_prove_with_blinders(circuits[i], witnesses[i], lens[i], r + 32 * i, s + 32 * i, out + i);
+        if (rc) return rc;
+    }
+    return G16_OK;
+}
+
+// ---- primitives ----
+static int grow_dev(void*& p, size_t& cap, size_t need) {
+    if (need <= cap && p) return G16_OK;
+    cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    CK(cudaMalloc(&p, need ? need : 32), "scratch allocation");
+    cap = need;
+    return G16_OK;
+}
+
+static int msm_device_impl(g16_backend* b, const void* d_bases, const void* d_scalars, size_t n, int form, bool g2,
+                           uint8_t* out) {
+    if (form != G16_SCALARS_STANDARD && form != G16_SCALARS_MONTGOMERY)
+        return fail(G16_ERR_INVALID_ARGUMENT, "unknown scalar form %d", form);
+    if (n == 0) {
+        std::memset(out, 0, g2 ? 128 : 64);
+        return G16_OK;
+    }
+    cudaStream_t st = b->stream;
+    CK(msm_sort(b->sort, d_scalars, n, form == G16_SCALARS_MONTGOMERY, 0, st), "MSM sort");
+    if (g2) CK(msm_accumulate_g2(b->sort, b->acc, d_bases, 0, (uint32_t)n, st), "MSM accumulate");
+    else CK(msm_accumulate_g1(b->sort, b->acc, d_bases, 0, (uint32_t)n, st), "MSM accumulate");
+    size_t bytes = (size_t)b->sort.W * (g2 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES);
+    if (bytes > b->cap_pinned) {
+        cudaFreeHost(b->h_pinned);
+        b->h_pinned = nullptr;
+        CK(cudaMallocHost((void**)&b->h_pinned, 32 * 256), "pinned buffer");
+        b->cap_pinned = 32 * 256;
+    }
+    CK(cudaMemcpyAsync(b->h_pinned, b->acc.d_windows, bytes, cudaMemcpyDeviceToHost, st), "window readback");
+    CK(cudaStreamSynchronize(st), "MSM");
+    timer().collect();
+    if (g2) pack(out, msm_combine_g2(b->h_pinned, b->sort.W, b->sort.c).to_affine());
+    else pack(out, msm_combine_g1(b->h_pinned, b->sort.W, b->sort.c).to_affine());
+    return G16_OK;
+}
+
+static int msm_host_impl(g16_backend* b, const uint8_t* bases, const uint8_t* scalars, size_t n, int form, bool g2,
+                         uint8_t* out) {
+    if (!b || (n && (!bases || !scalars)) || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> g(b->mu);
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    if (n == 0) {
+        std::memset(out, 0, g2 ? 128 : 64);
+        return G16_OK;
+    }
+    size_t bb = n * (g2 ? 128 : 64);
+    int rc;
+    if ((rc = grow_dev(b->d_in, b->cap_in, bb))) return rc;
+    if ((rc = grow_dev(b->d_in2, b->cap_in2, n * 32))) return rc;
+    CK(cudaMemcpyAsync(b->d_in, bases, bb, cudaMemcpyHostToDevice, b->stream), "bases upload");
+    CK(cudaMemcpyAsync(b->d_in2, scalars, n * 32, cudaMemcpyHostToDevice, b->stream), "scalars upload");
+    return msm_device_impl(b, b->d_in, b->d_in2, n, form, g2, out);
+}
+
+int g16_msm_g1(g16_backend* b, const uint8_t* bases, const uint8_t* scalars, size_t n, int form, uint8_t* out64) {
+    return msm_host_impl(b, bases, scalars, n, form, false, out64);
+}
+int g16_msm_g2(g16_backend* b, const uint8_t* bases, const uint8_t* scalars, size_t n, int form, uint8_t* out128) {
+    return msm_host_impl(b, bases, scalars, n, form, true, out128);
+}
+int g16_msm_g1_device(g16_backend* b, const void* d_bases, const void* d_scalars, size_t n, int form, uint8_t* out64) {
+    if (!b || !out64) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> g(b->mu);
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    return msm_device_impl(b, d_bases, d_scalars, n, form, false, out64);
+}
+int g16_msm_g2_device(g16_backend* b, const void* d_bases, const void* d_scalars, size_t n, int form, uint8_t* out128) {
+    if (!b || !out128) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> g(b->mu);
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    return msm_device_impl(b, d_bases, d_scalars, n, form, true, out128);
+}
+
+static int ntt_device_impl(g16_backend* b, int mode, uint32_t log_n, void* d, const uint8_t* shift_mont) {
+    if (log_n < 1 || log_n > 27) return fail(G16_ERR_INVALID_ARGUMENT, "log_n %u outside [1, 27]", log_n);
+    if (b->ntt.size() <= log_n) b->ntt.resize(log_n + 1);
+    if (!b->ntt[log_n]) b->ntt[log_n] = std::make_unique<NttTables>();
+    NttTables& t = *b->ntt[log_n];
+    CK(ntt_tables(t, (int)log_n, b->stream), "NTT tables");
+    cudaStream_t st = b->stream;
+    size_t n = (size_t)1 << log_n;
+    uint64_t shift[4];
+    if (shift_mont) std::memcpy(shift, shift_mont, 32);
+    else std::memcpy(shift, t.shift, 32);
+    switch (mode) {
+        case G16_NTT_FORWARD: CK(ntt_forward(t, d, st), "NTT"); break;
+        case G16_NTT_INVERSE: CK(ntt_inverse(t, d, st), "iNTT"); break;
+        case G16_NTT_INTT_COSET_NTT:
+            if (shift_mont && std::memcmp(shift_mont, t.shift, 32) != 0)
+                return fail(G16_ERR_INVALID_ARGUMENT, "intt_coset_ntt runs on the proving coset only");
+            CK(ntt_intt_coset_ntt(t, d, st), "iNTT-coset-NTT");
+            break;
+        case G16_NTT_COSET_FORWARD:
+            CK(ntt_distribute_powers(d, n, shift, st), "distribute powers");
+            CK(ntt_forward(t, d, st), "NTT");
+            break;
+        case G16_NTT_COSET_INVERSE: {
+            g16::Fr si = g16::Fr::raw(shift).inv();
+            CK(ntt_inverse(t, d, st), "iNTT");
+            CK(ntt_distribute_powers(d, n, si.x.v, st), "distribute powers");
+            break;
+        }
+        default: return fail(G16_ERR_INVALID_ARGUMENT, "unknown NTT mode %d", mode);
+    }
+    return G16_OK;
+}
+
+int g16_ntt(g16_backend* b, int mode, uint32_t log_n, uint8_t* data, const uint8_t* shift_mont) {
+    if (!b || !data) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> g(b->mu);
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    if (log_n < 1 || log_n > 27) return fail(G16_ERR_INVALID_ARGUMENT, "log_n %u outside [1, 27]", log_n);
+    size_t bytes = ((size_t)1 << log_n) * 32;
+    int rc;
+    if ((rc = grow_dev(b->d_in, b->cap_in, bytes))) return rc;
+    CK(cudaMemcpyAsync(b->d_in, data, bytes, cudaMemcpyHostToDevice, b->stream), "NTT upload");
+    if ((rc = ntt_device_impl(b, mode, log_n, b->d_in, shift_mont))) return rc;
+    CK(cudaMemcpyAsync(data, b->d_in, bytes, cudaMemcpyDeviceToHost, b->stream), "NTT readback");
+    CK(cudaStreamSynchronize(b->stream), "NTT");
+    timer().collect();
+    return G16_OK;
+}
+
+int g16_ntt_device(g16_backend* b, int mode, uint32_t log_n, void* d, const uint8_t* shift_mont) {
+    if (!b || !d) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> g(b->mu);
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    int rc = ntt_device_impl(b, mode, log_n, d, shift_mont);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(b->stream), "NTT");
+    timer().collect();
+    return G16_OK;
+}
+
+// ---- timing ----
+void g16_kernel_timing_enable(int on) { timer().enabled = on != 0; }
+void g16_kernel_timing_reset(void) { timer().reset(); }
+size_t g16_kernel_timing_report(char* buf, size_t len) {
+    timer().collect();
+    std::string s;
+    {
+        std::lock_guard<std::mutex> g(timer().mu);
+        for (auto& kv : timer().totals) {
+            char line[256];
+            snprintf(line, sizeof line, "%s %.6f %ld\n", kv.first.c_str(), kv.second.first, kv.second.second);
+            s += line;
+        }
+    }
+    if (buf && len) {
+        size_t k = s.size() < len - 1 ? s.size() : len - 1;
+        std::memcpy(buf, s.data(), k);
+        buf[k] = 0;
+    }
+    return s.size();
+}
+
+// ---- device memory helpers ----
+int g16_device_alloc(g16_backend* b, size_t bytes, void** d_out) {
+    if (!b || !d_out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    CK(cudaMalloc(d_out, bytes ? bytes : 32), "device allocation");
+    return G16_OK;
+}
+int g16_device_free(g16_backend* b, void* d) {
+    if (!b) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    CK(cudaFree(d), "device free");
+    return G16_OK;
+}
+int g16_device_upload(g16_backend* b, void* d_dst, const void* src, size_t bytes) {
+    if (!b || !d_dst || !src) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    CK(cudaMemcpy(d_dst, src, bytes, cudaMemcpyHostToDevice), "upload");
+    return G16_OK;
+}
+int g16_device_sync(g16_backend* b) {
+    if (!b) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    CK(cudaDeviceSynchronize(), "device synchronize");
+    return G16_OK;
+}
+
+}  // extern "C"
