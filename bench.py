@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""Groth16 / BN254 prove throughput on B200 (proofs/s), one JSON line.
+
+Workload: one plain Groth16 prove of a seeded synthetic R1CS with 1,100,000
+constraints (domain 2^21, 1,100,257 wires), the witness-value mix of the
+configs (about 60% in {0,1}, 20% below 2^32, 20% uniform), a key written from
+seeded toxic waste, seeded blinders r and s.  A step is one full proof:
+stages 0-11 (gather, iNTT -> coset -> NTT of A, B, C, H = A*B - C, the five
+MSMs, blinding and assembly).  Every step proves a different witness.
+
+  value   proofs/s over K steps with the K witnesses already resident in HBM,
+          timed between CUDA events with a barrier and synchronize on both
+          sides, max over ranks (N GPUs run N independent replicas: weak).
+  e2e     the same through the reference-facing C ABI call with host buffers:
+          each step copies its witness from pinned host memory to the device
+          and reads the MSM window sums back; p50/p99 per-proof latency too.
+  roofline  the dominant kernel (most device time in the timed region), its
+          algorithmic work per launch / its average launch duration (CUDA
+          events on its own stream) against the measured peak.
+  cpu_baseline  the CPU oracle (a C restatement of the reference's CPU
+          prover) proving the same circuit on this host's cores.
+
+`--impl reference` times that CPU restatement alone (the reference is Rust
+and cannot be built on this image), rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CONSTRAINTS = 1_100_000
+N_INPUTS, N_PUBLIC = 256, 16
+CIRCUIT_SEED, TOXIC_SEED = 21, 0x5EED
+FQ_MUL_IMAD = 264            # 8x32-bit CIOS Montgomery product: 32-bit multiply-adds
+MADD_FQ_MULS = {"msm_accumulate_g1": 10, "msm_accumulate_g2": 30}   # madd-2008-s: 8M + 2S (Fq2 = 3 Fq)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--constraints", type=int, default=N_CONSTRAINTS)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def workload_name(nc, domain, n_vars):
+    return "groth16 prove, synthetic R1CS %d constraints (domain 2^%d, %d wires), BN254" % (
+        nc, domain.bit_length() - 1, n_vars)
+
+
+def blinders(i):
+    import random
+    import snarkrs_b200 as S
+    rng = random.Random(1000 + i)
+    return S.fr_to_mont_bytes(rng.randrange(1, S.R_MOD)), S.fr_to_mont_bytes(rng.randrange(1, S.R_MOD))
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def synth_key(sc, nc):
+    """The workload's .zkey; cached under /tmp so repeated runs on one host skip the key generation."""
+    path = os.path.join(os.environ.get("G16_BENCH_CACHE", "/tmp"), "g16b200_bench_%d_%d_%d.zkey" % (
+        CIRCUIT_SEED, nc, TOXIC_SEED))
+    try:
+        with open(path, "rb") as f:
+            return f.read()
+    except OSError:
+        pass
+    zk = sc.zkey(TOXIC_SEED)
+    try:
+        with open(path + ".tmp", "wb") as f:
+            f.write(zk)
+        os.replace(path + ".tmp", path)
+    except OSError:
+        pass
+    return zk
+
+
+def cpu_prove_rate(zk, sc, n_proofs):
+    """The oracle proving n_proofs different witnesses of the same circuit, all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    ok = O.Zkey(zk)
+    threads = O.max_threads()
+    times = []
+    for i in range(n_proofs):
+        w = sc.witness(10_000 + i)
+        r, s = blinders(10_000 + i)
+        t0 = time.perf_counter()
+        ok.prove(w, O.from_bytes(r), O.from_bytes(s))
+        times.append(time.perf_counter() - t0)
+    ok.close()
+    return times, threads
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    import snarkrs_b200 as S
+    sc = S.SynthCircuit(CIRCUIT_SEED, args.constraints, N_INPUTS, N_PUBLIC)
+    zk = synth_key(sc, args.constraints)
+    times, threads = cpu_prove_rate(zk, sc, args.warmup + args.steps)
+    timed = times[args.warmup:]
+    value = len(timed) / sum(timed)
+    line = {
+        "impl": "reference", "metric": "proofs/s", "value": value, "unit": "proofs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(timed) / len(timed),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (BN254 Montgomery, exact)",
+        "data": "synthetic",
+        "config": {"workload": workload_name(args.constraints, sc.domain_size, sc.n_vars),
+                   "n_constraints": args.constraints, "domain": sc.domain_size, "n_vars": sc.n_vars},
+        "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "port",
+                         "sample": "%d full proofs of the workload (after %d warm-up), C restatement of the "
+                                   "reference CPU prover, OpenMP over all host threads" % (len(timed), args.warmup)},
+        "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "p50_ms": 1e3 * statistics.median(timed),
+        "note": "the reference is Rust (ark-* 0.5 not vendored, no cargo here); this arm times the C restatement",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import snarkrs_b200 as S
+    rank, local_rank, world = dist_env()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    torch.cuda.set_device(local_rank)
+    backend = S.CudaBackend(local_rank)
+    sc = S.SynthCircuit(CIRCUIT_SEED, args.constraints, N_INPUTS, N_PUBLIC)
+    zk = synth_key(sc, args.constraints) if rank == 0 or world == 1 else None
+    if world > 1:
+        barrier()
+        zk = synth_key(sc, args.constraints)
+    pk = S.ProvingKey.from_bytes(zk, check_points=False)
+    circ = backend.prepare(pk)
+    K, W = args.steps, args.warmup
+    nbytes = 32 * sc.n_vars
+    # per-step witnesses (different seeds per rank and step), in pinned host memory
+    wits = []
+    for i in range(W + K):
+        t = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        t.numpy()[:] = memoryview(sc.witness(rank * 1_000_000 + i))
+        wits.append(t)
+    bl = [blinders(rank * 1_000_000 + i) for i in range(W + K)]
+    # device-resident copies for the kernel-side number
+    dwit = [torch.empty(nbytes, dtype=torch.uint8, device="cuda") for _ in range(W + K)]
+    for d, h in zip(dwit, wits):
+        d.copy_(h)
+    torch.cuda.synchronize()
+
+    # ---- value: inputs resident in HBM ----
+    for i in range(W):
+        circ.prove_with_blinders_device(dwit[i].data_ptr(), sc.n_vars, *bl[i])
+    S.kernel_timing_reset()
+    S.kernel_timing(True)
+    clocks = Clocks(local_rank)
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = S.launch_count()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(W, W + K):
+        circ.prove_with_blinders_device(dwit[i].data_ptr(), sc.n_vars, *bl[i])
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    launches = int(S.launch_count() - launches0)
+    S.kernel_timing(False)
+    kern = S.kernel_timing_report()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * K / (ms / 1e3)
+
+    # ---- e2e: host buffers through the C ABI, pinned witness copied every step ----
+    lat = []
+    barrier()
+    torch.cuda.synchronize()
+    t_all = time.perf_counter()
+    for i in range(W, W + K):
+        t0 = time.perf_counter()
+        circ.prove_with_blinders(wits[i].numpy(), *bl[i])
+        lat.append(time.perf_counter() - t0)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t_all)
+    e2e_value = world * K / e2e_s
+    readback = int(circ.readback_bytes())
+
+    if rank != 0:
+        barrier()
+        return
+
+    # ---- roofline of the dominant kernel ----
+    peaks, peak_kind = measured_peaks()
+    imad_peak = S.imad_peak(backend)
+    dom = max(kern.items(), key=lambda kv: kv[1][0])
+    name, (tot_ms, n_launch, units) = dom[0], dom[1]
+    roof = {"kernel": name, "launches": n_launch, "avg_ms": tot_ms / max(n_launch, 1)}
+    if name in MADD_FQ_MULS:
+        imad_per_launch = units / max(n_launch, 1) * MADD_FQ_MULS[name] * FQ_MUL_IMAD
+        achieved = imad_per_launch / (roof["avg_ms"] / 1e3)
+        roof.update({"bound": "imad", "achieved": achieved / 1e12, "peak": imad_peak / 1e12, "unit": "TIMAD/s",
+                     "frac": achieved / imad_peak, "peak_source": "measured in this run by the mad.lo/mad.hi "
+                                                                    "issue-rate probe (g16_imad_peak)",
+                     "work_per_launch": "%.0f mixed additions x %d Fq products x %d IMAD" % (
+                         units / max(n_launch, 1), MADD_FQ_MULS[name], FQ_MUL_IMAD)})
+    roof["traffic"] = traffic_for(name)
+    share = {k: round(v[0] / sum(x[0] for x in kern.values()), 4) for k, v in kern.items()}
+    t = circ.stage_timings()
+
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        times, threads = cpu_prove_rate(zk, sc, 1)
+        cpu = {"value": 1 / times[0], "unit": "proofs/s", "cores": threads, "kind": "port",
+               "sample": "1 full proof of the same workload by the C restatement of the reference CPU prover "
+                         "(OpenMP, all host threads), %.1f s" % times[0]}
+    line = {
+        "metric": "proofs/s", "value": value, "unit": "proofs/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32 (BN254 Fq/Fr Montgomery limbs, exact)", "data": "synthetic",
+        "config": {"workload": workload_name(args.constraints, sc.domain_size, sc.n_vars),
+                   "n_constraints": args.constraints, "domain": sc.domain_size, "n_vars": sc.n_vars,
+                   "l2": "no flush: the resident key (%.0f MB) and per-step witnesses exceed the 126 MB L2" %
+                         (circ.device_bytes() / 1e6),
+                   "replicas": world},
+        "e2e": {"value": e2e_value, "unit": "proofs/s", "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": readback, "p50_ms": 1e3 * statistics.median(lat),
+                "p99_ms": 1e3 * sorted(lat)[min(len(lat) - 1, int(0.99 * len(lat)))]},
+        "roofline": roof,
+        "kernel_share": share,
+        "stage_us_total": t,
+        "gpu_launches": launches,
+        "clocks": clk,
+        "hbm_peak_gbs": peaks.get("hbm_gbs"), "hbm_peak_source": peak_kind,
+        "reference_published": "T4 warm CUDA prove at domain 2^21: 1263 ms (bench/results/cuda-size-sweep-2026-11-10.md:26)",
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    if dist:
+        barrier()
+
+
+def traffic_for(name):
+    """DRAM bytes per launch from the committed ncu summary, when one exists for this kernel."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(name)
+    except OSError:
+        return None
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

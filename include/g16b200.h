@@ -184,8 +184,16 @@ int g16_ntt_device(g16_backend *b, int mode, uint32_t log_n, void *d_data_mont, 
 /* ---------------- kernel timing (CUDA events on the launching stream) ---------------- */
 void g16_kernel_timing_enable(int on);
 void g16_kernel_timing_reset(void);
-/* Writes "name ms launches\n" lines; returns the full length. */
+/* Writes "name total_ms launches work_units\n" lines; returns the full length.
+ * work_units: mixed additions for the MSM accumulate kernels, else 0. */
 size_t g16_kernel_timing_report(char *buf, size_t len);
+/* Kernels launched by this library since load (every launch site counts). */
+uint64_t g16_launch_count(void);
+/* Device-to-host bytes the last proof on this circuit read back. */
+uint64_t g16_circuit_readback_bytes(const g16_circuit *c);
+/* Measured issue rate of 32-bit mad.lo/mad.hi on this device (per second):
+ * the peak of the integer-multiply roofline the field kernels run against. */
+int g16_imad_peak(g16_backend *b, double *imad_per_s);
 
 /* ---------------- device memory helpers (for callers without a CUDA runtime) ---------------- */
 int g16_device_alloc(g16_backend *b, size_t bytes, void **d_out);

@@ -337,6 +337,10 @@ class CudaCircuit:
                                                    bytes(r_mont), bytes(s_mont), ctypes.byref(p)))
         return Proof(p.a, p.b, p.c)
 
+    def readback_bytes(self):
+        lib().g16_circuit_readback_bytes.restype = ctypes.c_uint64
+        return lib().g16_circuit_readback_bytes(self._h)
+
     def stage_timings(self):
         t = StageTimings()
         check(lib().g16_stage_timings_get(self._h, ctypes.byref(t)))
@@ -549,14 +553,29 @@ def kernel_timing_reset():
 
 
 def kernel_timing_report():
-    """{kernel class: (total ms, launches)} from CUDA events on the launching stream."""
+    """{kernel class: (total ms, launches, work units)} from CUDA events on the launching stream.
+
+    Work units are the mixed additions performed, for the MSM accumulate kernels."""
     buf = ctypes.create_string_buffer(1 << 16)
     lib().g16_kernel_timing_report(buf, 1 << 16)
     out = {}
     for line in buf.value.decode().splitlines():
-        name, ms, cnt = line.split()
-        out[name] = (float(ms), int(cnt))
+        name, ms, cnt, units = line.split()
+        out[name] = (float(ms), int(cnt), float(units))
     return out
+
+
+def launch_count():
+    """Kernels this library has launched since it was loaded."""
+    lib().g16_launch_count.restype = ctypes.c_uint64
+    return lib().g16_launch_count()
+
+
+def imad_peak(backend):
+    """Measured 32-bit mad.lo/mad.hi issue rate of the device (per second)."""
+    v = ctypes.c_double()
+    check(lib().g16_imad_peak(backend._h, ctypes.byref(v)))
+    return v.value
 
 
 def fr_to_mont_bytes(x):

@@ -1,6 +1,7 @@
 // Shared host-side plumbing: error capture and optional per-kernel event timing.
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdio>
 #include <map>
 #include <mutex>
@@ -34,7 +35,15 @@ struct KernelTimer {
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> pool;
     std::map<std::string, std::pair<double, long>> totals;   // ms, launches
+    std::map<std::string, double> units;                     // algorithmic work, per kernel class
+    std::atomic<uint64_t> launches{0};                        // every kernel this library launched
     std::mutex mu;
+
+    void add_units(const char* name, double u) {
+        if (!enabled) return;
+        std::lock_guard<std::mutex> g(mu);
+        units[name] += u;
+    }
 
     cudaEvent_t take() {
         if (!pool.empty()) {
@@ -79,6 +88,7 @@ struct KernelTimer {
         collect();
         std::lock_guard<std::mutex> g(mu);
         totals.clear();
+        units.clear();
     }
 };
 
@@ -86,7 +96,10 @@ KernelTimer& timer();
 
 struct TimedLaunch {
     cudaStream_t s;
-    TimedLaunch(const char* name, cudaStream_t st) : s(st) { timer().begin(name, st); }
+    TimedLaunch(const char* name, cudaStream_t st) : s(st) {
+        timer().launches.fetch_add(1, std::memory_order_relaxed);
+        timer().begin(name, st);
+    }
     ~TimedLaunch() { timer().end(s); }
 };
 

@@ -182,7 +182,8 @@ __global__ void __launch_bounds__(128) k_accumulate(const uint32_t* __restrict__
                                                     const uint32_t* __restrict__ seg_base, uint32_t K,
                                                     const uint32_t* __restrict__ d_M, uint32_t L,
                                                     const uint4* __restrict__ bases, uint32_t base_offset,
-                                                    uint32_t n_bases, uint4* __restrict__ partials) {
+                                                    uint32_t n_bases, uint4* __restrict__ partials,
+                                                    unsigned long long* __restrict__ work) {
     size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t M = *d_M;
     size_t start = t * L;
@@ -197,6 +198,7 @@ __global__ void __launch_bounds__(128) k_accumulate(const uint32_t* __restrict__
     uint32_t g = lo;
     uint32_t next = offsets[g + 1];
     Xyzz<F> acc = Xyzz<F>::identity();
+    unsigned adds = 0;
     for (size_t k = start; k < end; k++) {
         if (k == next) {
             st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), acc);
@@ -213,10 +215,15 @@ __global__ void __launch_bounds__(128) k_accumulate(const uint32_t* __restrict__
             if (!p.is_inf()) {
                 if (e >> 31) p.y = neg(p.y);
                 acc = xyzz_add_affine(acc, p.x, p.y);
+                adds++;
             }
         }
     }
     st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), acc);
+    // mixed additions performed, one atomic per converged group of lanes
+    unsigned mask = __activemask();
+    unsigned total = __reduce_add_sync(mask, adds);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1)) atomicAdd(work, (unsigned long long)total);
 }
 
 // ---- bucket reduce: thread (w, p) folds buckets [p*m, (p+1)*m) of window w ----
@@ -289,6 +296,7 @@ void MsmSort::release() {
 }
 
 void MsmAccum::release() {
+    cudaFree(d_work);
     cudaFree(d_partials);
     cudaFree(d_segments);
     cudaFree(d_windows);
@@ -347,9 +355,18 @@ static cudaError_t scan(const uint32_t* in, uint32_t* out, uint32_t len, uint32_
                         cudaStream_t st) {
     uint32_t nb = (len + 1023) / 1024;
     if (nb == 0) nb = 1;
-    k_scan_blocks<<<nb, 256, 0, st>>>(in, out, len, tmp);
-    k_scan_top<<<1, 1024, 0, st>>>(tmp, nb, d_total);
-    k_scan_add<<<blocks_for(len ? len : 1, 256), 256, 0, st>>>(out, len, tmp, d_total);
+    {
+        TimedLaunch tl("msm_scan", st);
+        k_scan_blocks<<<nb, 256, 0, st>>>(in, out, len, tmp);
+    }
+    {
+        TimedLaunch tl("msm_scan", st);
+        k_scan_top<<<1, 1024, 0, st>>>(tmp, nb, d_total);
+    }
+    {
+        TimedLaunch tl("msm_scan", st);
+        k_scan_add<<<blocks_for(len ? len : 1, 256), 256, 0, st>>>(out, len, tmp, d_total);
+    }
     return cudaGetLastError();
 }
 
@@ -390,11 +407,11 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
                                                           c, s.W, s.B, (uint4*)s.d_scalars_std, s.d_counts);
     }
     G16_CUDA(cudaGetLastError());
+    G16_CUDA(scan(s.d_counts, s.d_offsets, s.K, s.d_scan_tmp, s.d_total, st));
     {
-        TimedLaunch tl("msm_scan", st);
-        G16_CUDA(scan(s.d_counts, s.d_offsets, s.K, s.d_scan_tmp, s.d_total, st));
+        TimedLaunch tl("msm_copy", st);
+        k_copy_u32<<<blocks_for(s.K, 256), 256, 0, st>>>(s.d_cursor, s.d_offsets, s.K);
     }
-    k_copy_u32<<<blocks_for(s.K, 256), 256, 0, st>>>(s.d_cursor, s.d_offsets, s.K);
     if (n) {
         TimedLaunch tl("msm_scatter", st);
         k_scatter<<<blocks_for(n, 256), 256, 0, st>>>((const uint4*)s.d_scalars_std, (uint32_t)n, c, s.W, s.B,
@@ -402,7 +419,10 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
     }
     G16_CUDA(cudaGetLastError());
     // per-bucket segment counts -> segment base (into counts, then scanned)
-    k_nseg<<<blocks_for(s.K, 256), 256, 0, st>>>(s.d_offsets, s.K, s.chunk, s.d_counts);
+    {
+        TimedLaunch tl("msm_nseg", st);
+        k_nseg<<<blocks_for(s.K, 256), 256, 0, st>>>(s.d_offsets, s.K, s.chunk, s.d_counts);
+    }
     G16_CUDA(scan(s.d_counts, s.d_seg_base, s.K, s.d_scan_tmp, s.d_total + 1, st));
     return cudaSuccess;
 }
@@ -419,11 +439,14 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     acc.segs_per_window = P;
     G16_CUDA(grow_bytes(acc.d_segments, acc.cap_segments, (size_t)s.W * P * xyzz_bytes));
     G16_CUDA(grow_bytes(acc.d_windows, acc.cap_windows, (size_t)s.W * xyzz_bytes));
+    if (!acc.d_work) G16_CUDA(cudaMalloc((void**)&acc.d_work, sizeof(unsigned long long)));
+    G16_CUDA(cudaMemsetAsync(acc.d_work, 0, sizeof(unsigned long long), st));
     {
         TimedLaunch tl(tag, st);
         k_accumulate<F><<<blocks_for(chunks, 128), 128, 0, st>>>(s.d_entries, s.d_offsets, s.d_seg_base, s.K,
                                                                   s.d_total, s.chunk, (const uint4*)d_bases,
-                                                                  base_offset, n_bases, (uint4*)acc.d_partials);
+                                                                  base_offset, n_bases, (uint4*)acc.d_partials,
+                                                                  acc.d_work);
     }
     G16_CUDA(cudaGetLastError());
     {

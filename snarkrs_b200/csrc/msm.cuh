@@ -53,6 +53,7 @@ struct MsmAccum {
     void* d_partials = nullptr;    size_t cap_partials = 0;   // bytes
     void* d_segments = nullptr;    size_t cap_segments = 0;   // bytes
     void* d_windows = nullptr;     size_t cap_windows = 0;    // bytes
+    unsigned long long* d_work = nullptr;                      // mixed additions performed
     uint32_t segs_per_window = 0;
     void release();
 };

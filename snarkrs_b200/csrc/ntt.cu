@@ -248,10 +248,20 @@ cudaError_t ntt_tables(NttTables& t, int log_n, cudaStream_t st) {
     std::memcpy(t.shift, shift.x.v, 32);
     g16d::Fr d_one;
     std::memcpy(d_one.v, g16::Fr::one().x.v, 32);
-    k_powers<<<blocks_for((n / 2 + 15) / 16, 128), 128, 0, st>>>((uint4*)t.d_tw, to_dev(w), d_one, n / 2, 0);
-    k_powers<<<blocks_for((n / 2 + 15) / 16, 128), 128, 0, st>>>((uint4*)t.d_tw_inv, to_dev(wi), d_one, n / 2, 0);
-    k_powers<<<blocks_for((n + 15) / 16, 128), 128, 0, st>>>((uint4*)t.d_coset, to_dev(shift), to_dev(ninv), n,
-                                                              (uint32_t)log_n);
+    {
+        TimedLaunch tl("ntt_tables", st);
+        k_powers<<<blocks_for((n / 2 + 15) / 16, 128), 128, 0, st>>>((uint4*)t.d_tw, to_dev(w), d_one, n / 2, 0);
+    }
+    {
+        TimedLaunch tl("ntt_tables", st);
+        k_powers<<<blocks_for((n / 2 + 15) / 16, 128), 128, 0, st>>>((uint4*)t.d_tw_inv, to_dev(wi), d_one, n / 2,
+                                                                      0);
+    }
+    {
+        TimedLaunch tl("ntt_tables", st);
+        k_powers<<<blocks_for((n + 15) / 16, 128), 128, 0, st>>>((uint4*)t.d_coset, to_dev(shift), to_dev(ninv), n,
+                                                                  (uint32_t)log_n);
+    }
     G16_CUDA(cudaMemcpyAsync((uint8_t*)t.d_coset + n * 32, ninv.x.v, 32, cudaMemcpyHostToDevice, st));
     G16_CUDA(cudaGetLastError());
     G16_CUDA(cudaStreamSynchronize(st));
@@ -364,7 +374,10 @@ static cudaError_t dit_natural(const NttTables& t, void* a, const void* tw, cons
     set_attrs();
     uint32_t log_n = (uint32_t)t.log_n;
     size_t n = (size_t)1 << log_n;
-    k_bitrev<<<blocks_for(n, 256), 256, 0, st>>>((uint4*)a, log_n, n);
+    {
+        TimedLaunch tl("ntt_bitrev", st);
+        k_bitrev<<<blocks_for(n, 256), 256, 0, st>>>((uint4*)a, log_n, n);
+    }
     G16_CUDA(cudaGetLastError());
     uint32_t k0 = log_n < TILE_LOG ? log_n : TILE_LOG;
     auto outer = outer_passes(log_n, k0);
@@ -388,6 +401,7 @@ cudaError_t ntt_inverse(const NttTables& t, void* a, cudaStream_t st) {
 cudaError_t ntt_distribute_powers(void* a, size_t n, const uint64_t* shift_mont, cudaStream_t st) {
     g16d::Fr s;
     std::memcpy(s.v, shift_mont, 32);
+    TimedLaunch tl("ntt_distribute", st);
     k_distribute<<<blocks_for((n + 15) / 16, 128), 128, 0, st>>>((uint4*)a, s, n);
     return cudaGetLastError();
 }

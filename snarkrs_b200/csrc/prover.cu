@@ -84,6 +84,40 @@ __global__ void __launch_bounds__(256) k_gather(const uint32_t* __restrict__ rpa
     store32(reinterpret_cast<Fr*>(C) + row, mul(acc[0], acc[1]));
 }
 
+// Throughput probe for the 32-bit multiply-add the field code is built from:
+// eight independent chains alternating mad.lo.u32 and mad.hi.u32, so the
+// issue rate, not latency, bounds it.  Gives the integer roofline's peak.
+__global__ void __launch_bounds__(256) k_imad_peak(uint32_t* out, uint32_t iters, uint32_t seed) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t x0 = t ^ seed, x1 = t + 1, x2 = t + 2, x3 = t + 3, x4 = t + 4, x5 = t + 5, x6 = t + 6, x7 = t + 7;
+    uint32_t b = 0x9e3779b9u ^ t, c = 0x7f4a7c15u + seed;
+    for (uint32_t i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            asm volatile(
+                "mad.lo.u32 %0, %0, %8, %9;\n\t"
+                "mad.lo.u32 %1, %1, %8, %9;\n\t"
+                "mad.lo.u32 %2, %2, %8, %9;\n\t"
+                "mad.lo.u32 %3, %3, %8, %9;\n\t"
+                "mad.lo.u32 %4, %4, %8, %9;\n\t"
+                "mad.lo.u32 %5, %5, %8, %9;\n\t"
+                "mad.lo.u32 %6, %6, %8, %9;\n\t"
+                "mad.lo.u32 %7, %7, %8, %9;\n\t"
+                "mad.hi.u32 %0, %0, %8, %9;\n\t"
+                "mad.hi.u32 %1, %1, %8, %9;\n\t"
+                "mad.hi.u32 %2, %2, %8, %9;\n\t"
+                "mad.hi.u32 %3, %3, %8, %9;\n\t"
+                "mad.hi.u32 %4, %4, %8, %9;\n\t"
+                "mad.hi.u32 %5, %5, %8, %9;\n\t"
+                "mad.hi.u32 %6, %6, %8, %9;\n\t"
+                "mad.hi.u32 %7, %7, %8, %9;"
+                : "+r"(x0), "+r"(x1), "+r"(x2), "+r"(x3), "+r"(x4), "+r"(x5), "+r"(x6), "+r"(x7)
+                : "r"(b), "r"(c));
+        }
+    }
+    out[t] = x0 ^ x1 ^ x2 ^ x3 ^ x4 ^ x5 ^ x6 ^ x7;
+}
+
 }  // namespace g16d
 
 // ---------------------------------------------------------------- handles
@@ -102,6 +136,7 @@ struct g16_backend {
     std::vector<std::unique_ptr<NttTables>> ntt;   // by log_n
     uint8_t* h_pinned = nullptr;                   // window sums readback
     size_t cap_pinned = 0;
+    unsigned long long* h_work = nullptr;
 };
 
 struct g16_circuit {
@@ -121,7 +156,9 @@ struct g16_circuit {
     void* d_hpoly = nullptr;
     MsmSort sort_w, sort_h;
     MsmAccum acc[5];
-    uint8_t* h_win = nullptr;   // pinned, 5 * 20 windows * 256 B
+    uint8_t* h_win = nullptr;   // pinned, 5 * 32 windows * 256 B
+    unsigned long long* h_work = nullptr;   // pinned, mixed additions per MSM
+    uint64_t readback_bytes = 0;            // device-to-host bytes of the last proof
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::mutex mu;
@@ -291,15 +328,23 @@ int run_msms(g16_circuit* c, const void* d_w, const void* d_h, MsmJac& out) {
     CK(msm_accumulate_g2(c->sort_w, c->acc[1], c->d_b2, 0, c->n_vars, st), "B2 accumulate");
     // readback: slot i holds up to 32 windows of 256 bytes
     const size_t slot = 32 * 256;
+    c->readback_bytes = 0;
     for (int i = 0; i < 5; i++) {
         const MsmSort& s = (i == 4) ? c->sort_h : c->sort_w;
         size_t bytes = (size_t)s.W * (i == 1 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES);
         CK(cudaMemcpyAsync(c->h_win + i * slot, c->acc[i].d_windows, bytes, cudaMemcpyDeviceToHost, st),
            "window readback");
+        c->readback_bytes += bytes;
+        if (timer().enabled)
+            CK(cudaMemcpyAsync(c->h_work + i, c->acc[i].d_work, 8, cudaMemcpyDeviceToHost, st), "work readback");
     }
     CK(cudaEventRecord(c->ev[3], st), "event");
     CK(cudaStreamSynchronize(st), "MSM stages");
     timer().collect();
+    if (timer().enabled) {
+        timer().add_units("msm_accumulate_g1", (double)(c->h_work[0] + c->h_work[2] + c->h_work[3] + c->h_work[4]));
+        timer().add_units("msm_accumulate_g2", (double)c->h_work[1]);
+    }
     out.a = msm_combine_g1(c->h_win + 0 * slot, c->sort_w.W, c->sort_w.c);
     out.b2 = msm_combine_g2(c->h_win + 1 * slot, c->sort_w.W, c->sort_w.c);
     out.b1 = msm_combine_g1(c->h_win + 2 * slot, c->sort_w.W, c->sort_w.c);
@@ -383,6 +428,7 @@ void g16_backend_free(g16_backend* b) {
     for (auto& t : b->ntt)
         if (t) t->release();
     cudaFreeHost(b->h_pinned);
+    if (b->h_work) cudaFreeHost(b->h_work);
     cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -507,6 +553,7 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
     if (e == cudaSuccess) e = circuit_alloc(cp, &cp->d_abc, 32ull * n * 3);
     if (e == cudaSuccess) e = circuit_alloc(cp, &cp->d_hpoly, 32ull * n);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&cp->h_win, 5 * 32 * 256);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&cp->h_work, 8 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = ntt_tables(cp->ntt, cp->log_n, cp->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(cp->stream);
     if (e != cudaSuccess) {
@@ -530,6 +577,7 @@ void g16_circuit_free(g16_circuit* c) {
     c->sort_h.release();
     for (auto& a : c->acc) a.release();
     if (c->h_win) cudaFreeHost(c->h_win);
+    if (c->h_work) cudaFreeHost(c->h_work);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -681,8 +729,13 @@ static int msm_device_impl(g16_backend* b, const void* d_bases, const void* d_sc
         b->cap_pinned = 32 * 256;
     }
     CK(cudaMemcpyAsync(b->h_pinned, b->acc.d_windows, bytes, cudaMemcpyDeviceToHost, st), "window readback");
+    if (timer().enabled) {
+        if (!b->h_work) CK(cudaMallocHost((void**)&b->h_work, sizeof(unsigned long long)), "pinned buffer");
+        CK(cudaMemcpyAsync(b->h_work, b->acc.d_work, 8, cudaMemcpyDeviceToHost, st), "work readback");
+    }
     CK(cudaStreamSynchronize(st), "MSM");
     timer().collect();
+    if (timer().enabled) timer().add_units(g2 ? "msm_accumulate_g2" : "msm_accumulate_g1", (double)*b->h_work);
     if (g2) pack(out, msm_combine_g2(b->h_pinned, b->sort.W, b->sort.c).to_affine());
     else pack(out, msm_combine_g1(b->h_pinned, b->sort.W, b->sort.c).to_affine());
     return G16_OK;
@@ -796,7 +849,9 @@ size_t g16_kernel_timing_report(char* buf, size_t len) {
         std::lock_guard<std::mutex> g(timer().mu);
         for (auto& kv : timer().totals) {
             char line[256];
-            snprintf(line, sizeof line, "%s %.6f %ld\n", kv.first.c_str(), kv.second.first, kv.second.second);
+            auto u = timer().units.find(kv.first);
+            snprintf(line, sizeof line, "%s %.6f %ld %.0f\n", kv.first.c_str(), kv.second.first, kv.second.second,
+                     u == timer().units.end() ? 0.0 : u->second);
             s += line;
         }
     }
@@ -806,6 +861,49 @@ size_t g16_kernel_timing_report(char* buf, size_t len) {
         buf[k] = 0;
     }
     return s.size();
+}
+
+uint64_t g16_launch_count(void) { return timer().launches.load(); }
+
+uint64_t g16_circuit_readback_bytes(const g16_circuit* c) { return c ? c->readback_bytes : 0; }
+
+int g16_imad_peak(g16_backend* b, double* imad_per_s) {
+    if (!b || !imad_per_s) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> g(b->mu);
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->ordinal), "attribute");
+    unsigned blocks = (unsigned)sms * 8, threads = 256;
+    uint32_t iters = 4096;
+    uint32_t* d = nullptr;
+    CK(cudaMalloc(&d, (size_t)blocks * threads * 4), "probe buffer");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {
+        cudaEventRecord(e0, b->stream);
+        {
+            TimedLaunch tl("imad_peak", b->stream);
+            g16d::k_imad_peak<<<blocks, threads, 0, b->stream>>>(d, iters, (uint32_t)rep);
+        }
+        cudaEventRecord(e1, b->stream);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) {
+            cudaFree(d);
+            return cuda_fail(e, "IMAD probe");
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep && ms < best) best = ms;   // first run is warm-up
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d);
+    // 8 chains x (mad.lo + mad.hi) x 4 unrolled per iteration
+    double ops = (double)blocks * threads * iters * 64.0;
+    *imad_per_s = ops / (best * 1e-3);
+    return G16_OK;
 }
 
 // ---- device memory helpers ----
