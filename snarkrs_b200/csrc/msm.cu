@@ -163,11 +163,20 @@ __global__ void __launch_bounds__(256) k_scan_add(uint32_t* __restrict__ out, ui
     if (i == 0) out[len] = *total;
 }
 
-__global__ void k_nseg(const uint32_t* __restrict__ offsets, uint32_t K, uint32_t L, uint32_t* __restrict__ nseg) {
+// Partial sums per bucket (one per chunk the bucket touches).  Buckets with
+// more than FAT_PARTIALS of them -- a repeated scalar, most often 1 -- go on
+// the fat list and are folded in parallel before the bucket sums.
+constexpr uint32_t FAT_PARTIALS = 8;
+constexpr uint32_t FAT_JOBS = 64;
+
+__global__ void k_nseg(const uint32_t* __restrict__ offsets, uint32_t K, uint32_t L, uint32_t* __restrict__ nseg,
+                       uint32_t* __restrict__ fat_list, uint32_t* __restrict__ fat_count) {
     uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= K) return;
     uint32_t lo = offsets[g], hi = offsets[g + 1];
-    nseg[g] = hi > lo ? ((hi - 1) / L - lo / L + 1) : 0;
+    uint32_t ns = hi > lo ? ((hi - 1) / L - lo / L + 1) : 0;
+    nseg[g] = ns;
+    if (ns > FAT_PARTIALS) fat_list[atomicAdd(fat_count, 1u)] = g;
 }
 
 __global__ void k_copy_u32(uint32_t* dst, const uint32_t* src, uint32_t n) {
@@ -226,28 +235,111 @@ __global__ void __launch_bounds__(128) k_accumulate(const uint32_t* __restrict__
     if ((threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1)) atomicAdd(work, (unsigned long long)total);
 }
 
-// ---- bucket reduce: thread (w, p) folds buckets [p*m, (p+1)*m) of window w ----
+__device__ __forceinline__ uint32_t n_partials(const uint32_t* offsets, uint32_t g, uint32_t L) {
+    uint32_t lo = offsets[g], hi = offsets[g + 1];
+    return hi > lo ? ((hi - 1) / L - lo / L + 1) : 0;
+}
+
+// Block-wide sum of one XYZZ point per thread through shared memory; the
+// result is valid in thread 0.
 template <class F>
-__global__ void __launch_bounds__(128) k_bucket_reduce(const uint4* __restrict__ partials,
-                                                       const uint32_t* __restrict__ offsets,
-                                                       const uint32_t* __restrict__ seg_base, uint32_t L, uint32_t B,
-                                                       uint32_t W, uint32_t m, uint32_t P,
-                                                       uint4* __restrict__ seg_out) {
+__device__ __forceinline__ Xyzz<F> block_sum(Xyzz<F> acc, uint4* smem) {
+    st_xyzz<F>(smem, threadIdx.x, acc);
+    __syncthreads();
+    for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            acc = xyzz_add(acc, ld_xyzz<F>(smem, threadIdx.x + s));
+            st_xyzz<F>(smem, threadIdx.x, acc);
+        }
+        __syncthreads();
+    }
+    return acc;
+}
+
+// Fat buckets, stage 1: each of a fat bucket's partials is assigned to one of
+// FAT_JOBS contiguous jobs; a block folds one job into the job's first slot.
+template <class F>
+__global__ void __launch_bounds__(128) k_fat_merge_jobs(uint4* __restrict__ partials,
+                                                        const uint32_t* __restrict__ offsets,
+                                                        const uint32_t* __restrict__ seg_base,
+                                                        const uint32_t* __restrict__ fat_list,
+                                                        const uint32_t* __restrict__ fat_count, uint32_t L) {
+    extern __shared__ uint4 smem[];
+    uint32_t items = *fat_count * FAT_JOBS;
+    for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
+        uint32_t g = fat_list[item / FAT_JOBS], j = item % FAT_JOBS;
+        uint32_t ns = n_partials(offsets, g, L), J = (ns + FAT_JOBS - 1) / FAT_JOBS;
+        uint32_t a = j * J;
+        if (a >= ns) continue;   // uniform across the block
+        uint32_t b = min(a + J, ns), base = seg_base[g];
+        Xyzz<F> acc = Xyzz<F>::identity();
+        for (uint32_t i = a + threadIdx.x; i < b; i += blockDim.x) acc = xyzz_add(acc, ld_xyzz<F>(partials, base + i));
+        acc = block_sum(acc, smem);
+        if (threadIdx.x == 0) st_xyzz<F>(partials, base + a, acc);
+        __syncthreads();
+    }
+}
+
+// Fat buckets, stage 2: fold the (at most FAT_JOBS) job results into the
+// bucket's first partial slot.
+template <class F>
+__global__ void __launch_bounds__(64) k_fat_merge_final(uint4* __restrict__ partials,
+                                                        const uint32_t* __restrict__ offsets,
+                                                        const uint32_t* __restrict__ seg_base,
+                                                        const uint32_t* __restrict__ fat_list,
+                                                        const uint32_t* __restrict__ fat_count, uint32_t L) {
+    extern __shared__ uint4 smem[];
+    uint32_t nf = *fat_count;
+    for (uint32_t f = blockIdx.x; f < nf; f += gridDim.x) {
+        uint32_t g = fat_list[f];
+        uint32_t ns = n_partials(offsets, g, L), J = (ns + FAT_JOBS - 1) / FAT_JOBS;
+        uint32_t base = seg_base[g];
+        uint32_t a = threadIdx.x * J;
+        Xyzz<F> acc = a < ns ? ld_xyzz<F>(partials, base + a) : Xyzz<F>::identity();
+        acc = block_sum(acc, smem);
+        if (threadIdx.x == 0) st_xyzz<F>(partials, base, acc);
+        __syncthreads();
+    }
+}
+
+// Bucket sums S_g: one thread per bucket folds its few partials (a fat
+// bucket's total already sits in its first slot).
+template <class F>
+__global__ void __launch_bounds__(128) k_bucket_sums(const uint4* __restrict__ partials,
+                                                     const uint32_t* __restrict__ offsets,
+                                                     const uint32_t* __restrict__ seg_base, uint32_t K, uint32_t L,
+                                                     uint4* __restrict__ buckets) {
+    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= K) return;
+    uint32_t ns = n_partials(offsets, g, L), base = seg_base[g];
+    Xyzz<F> acc = Xyzz<F>::identity();
+    if (ns > FAT_PARTIALS) {
+        acc = ld_xyzz<F>(partials, base);
+    } else {
+        for (uint32_t s = 0; s < ns; s++) acc = xyzz_add(acc, ld_xyzz<F>(partials, base + s));
+    }
+    st_xyzz<F>(buckets, g, acc);
+}
+
+// Segment (w, p) of SEG buckets: running sums give run = sum S_b and
+// tot = sum (b - p SEG + 1) S_b over the segment; the segment's share of
+// sum_b (b + 1) S_b is then tot + (p SEG) run.
+constexpr uint32_t SEG = 8;
+
+template <class F>
+__global__ void __launch_bounds__(128) k_segments(const uint4* __restrict__ buckets, uint32_t B, uint32_t W,
+                                                  uint32_t P, uint4* __restrict__ seg_out) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= W * P) return;
     uint32_t w = t / P, p = t % P;
     Xyzz<F> run = Xyzz<F>::identity(), tot = Xyzz<F>::identity();
-    for (int j = (int)m - 1; j >= 0; j--) {
-        uint32_t g = w * B + p * m + (uint32_t)j;
-        uint32_t lo = offsets[g], hi = offsets[g + 1];
-        if (hi > lo) {
-            uint32_t ns = (hi - 1) / L - lo / L + 1, b0 = seg_base[g];
-            for (uint32_t s = 0; s < ns; s++) run = xyzz_add(run, ld_xyzz<F>(partials, b0 + s));
-        }
+    size_t g0 = (size_t)w * B + (size_t)p * SEG;
+#pragma unroll 1
+    for (int j = SEG - 1; j >= 0; j--) {
+        run = xyzz_add(run, ld_xyzz<F>(buckets, g0 + j));
         tot = xyzz_add(tot, run);
     }
-    // segment weight offset: buckets here carry weight (b - p m + 1) in tot; add p m * run
-    uint32_t k = p * m;
+    uint32_t k = p * SEG;
     Xyzz<F> acc = Xyzz<F>::identity();
     if (k) {
         for (int bit = 31 - __clz(k); bit >= 0; bit--) {
@@ -258,23 +350,20 @@ __global__ void __launch_bounds__(128) k_bucket_reduce(const uint4* __restrict__
     st_xyzz<F>(seg_out, t, xyzz_add(tot, acc));
 }
 
+// Group sums: grid (blocks per group, groups); each block folds `per` items per
+// thread and writes one partial per block.
 template <class F>
-__global__ void __launch_bounds__(128) k_window_reduce(const uint4* __restrict__ seg_out, uint32_t P,
-                                                       uint4* __restrict__ windows) {
+__global__ void __launch_bounds__(128) k_group_sum(const uint4* __restrict__ in, uint32_t items_per_group,
+                                                   uint4* __restrict__ out) {
     extern __shared__ uint4 smem[];
-    uint32_t w = blockIdx.x;
+    uint32_t grp = blockIdx.y;
+    uint32_t chunk = (items_per_group + gridDim.x - 1) / gridDim.x;
+    uint32_t lo = blockIdx.x * chunk, hi = min(lo + chunk, items_per_group);
     Xyzz<F> acc = Xyzz<F>::identity();
-    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) acc = xyzz_add(acc, ld_xyzz<F>(seg_out, (size_t)w * P + i));
-    st_xyzz<F>(smem, threadIdx.x, acc);
-    __syncthreads();
-    for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) {
-            acc = xyzz_add(acc, ld_xyzz<F>(smem, threadIdx.x + s));
-            st_xyzz<F>(smem, threadIdx.x, acc);
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) st_xyzz<F>(windows, w, acc);
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
+        acc = xyzz_add(acc, ld_xyzz<F>(in, (size_t)grp * items_per_group + i));
+    acc = block_sum(acc, smem);
+    if (threadIdx.x == 0) st_xyzz<F>(out, (size_t)grp * gridDim.x + blockIdx.x, acc);
 }
 
 }  // namespace g16d
@@ -289,6 +378,7 @@ void MsmSort::release() {
     cudaFree(d_offsets);
     cudaFree(d_cursor);
     cudaFree(d_seg_base);
+    cudaFree(d_fat_list);
     cudaFree(d_scan_tmp);
     cudaFree(d_entries);
     cudaFree(d_total);
@@ -297,6 +387,7 @@ void MsmSort::release() {
 
 void MsmAccum::release() {
     cudaFree(d_work);
+    cudaFree(d_buckets);
     cudaFree(d_partials);
     cudaFree(d_segments);
     cudaFree(d_windows);
@@ -376,6 +467,10 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
         return cudaErrorInvalidValue;
     }
     if (c == 0) c = msm_window_bits(n);
+    if (c < 4 || c > 24) {
+        set_error("MSM window of %d bits outside [4, 24]", c);
+        return cudaErrorInvalidValue;
+    }
     s.c = c;
     s.W = (255 + c - 1) / c;
     s.B = 1u << (c - 1);
@@ -393,6 +488,8 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
         G16_CUDA(grow(s.d_cursor, cap, kk));
         cap = 0;
         G16_CUDA(grow(s.d_seg_base, cap, kk));
+        cap = 0;
+        G16_CUDA(grow(s.d_fat_list, cap, kk));
         s.cap_k = cap;
     }
     G16_CUDA(grow(s.d_scan_tmp, s.cap_tmp, kk / 1024 + 2));
@@ -421,7 +518,8 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
     // per-bucket segment counts -> segment base (into counts, then scanned)
     {
         TimedLaunch tl("msm_nseg", st);
-        k_nseg<<<blocks_for(s.K, 256), 256, 0, st>>>(s.d_offsets, s.K, s.chunk, s.d_counts);
+        k_nseg<<<blocks_for(s.K, 256), 256, 0, st>>>(s.d_offsets, s.K, s.chunk, s.d_counts, s.d_fat_list,
+                                                      s.d_total + 2);
     }
     G16_CUDA(scan(s.d_counts, s.d_seg_base, s.K, s.d_scan_tmp, s.d_total + 1, st));
     return cudaSuccess;
@@ -434,32 +532,51 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     size_t chunks = (max_entries + s.chunk - 1) / s.chunk;
     size_t max_partials = (size_t)s.K + chunks + 1;
     G16_CUDA(grow_bytes(acc.d_partials, acc.cap_partials, max_partials * xyzz_bytes));
-    uint32_t m = s.B < 16 ? s.B : 16;
-    uint32_t P = s.B / m;
+    const uint32_t P = s.B / SEG;                  // segments per window
+    const uint32_t G = (P + 511) / 512;            // group-sum blocks per window
     acc.segs_per_window = P;
-    G16_CUDA(grow_bytes(acc.d_segments, acc.cap_segments, (size_t)s.W * P * xyzz_bytes));
+    G16_CUDA(grow_bytes(acc.d_buckets, acc.cap_buckets, (size_t)s.K * xyzz_bytes));
+    G16_CUDA(grow_bytes(acc.d_segments, acc.cap_segments, ((size_t)s.W * P + (size_t)s.W * G) * xyzz_bytes));
     G16_CUDA(grow_bytes(acc.d_windows, acc.cap_windows, (size_t)s.W * xyzz_bytes));
     if (!acc.d_work) G16_CUDA(cudaMalloc((void**)&acc.d_work, sizeof(unsigned long long)));
     G16_CUDA(cudaMemsetAsync(acc.d_work, 0, sizeof(unsigned long long), st));
+    uint4* partials = (uint4*)acc.d_partials;
+    uint4* groups = (uint4*)((uint8_t*)acc.d_segments + (size_t)s.W * P * xyzz_bytes);
     {
         TimedLaunch tl(tag, st);
         k_accumulate<F><<<blocks_for(chunks, 128), 128, 0, st>>>(s.d_entries, s.d_offsets, s.d_seg_base, s.K,
                                                                   s.d_total, s.chunk, (const uint4*)d_bases,
-                                                                  base_offset, n_bases, (uint4*)acc.d_partials,
-                                                                  acc.d_work);
+                                                                  base_offset, n_bases, partials, acc.d_work);
     }
     G16_CUDA(cudaGetLastError());
     {
-        TimedLaunch tl("msm_bucket_reduce", st);
-        k_bucket_reduce<F><<<blocks_for((size_t)s.W * P, 128), 128, 0, st>>>(
-            (const uint4*)acc.d_partials, s.d_offsets, s.d_seg_base, s.chunk, s.B, s.W, m, P,
-            (uint4*)acc.d_segments);
+        TimedLaunch tl("msm_fat_merge", st);
+        k_fat_merge_jobs<F><<<296, 128, 128 * xyzz_bytes, st>>>(partials, s.d_offsets, s.d_seg_base, s.d_fat_list,
+                                                                s.d_total + 2, s.chunk);
+    }
+    {
+        TimedLaunch tl("msm_fat_merge", st);
+        k_fat_merge_final<F><<<148, 64, 64 * xyzz_bytes, st>>>(partials, s.d_offsets, s.d_seg_base, s.d_fat_list,
+                                                               s.d_total + 2, s.chunk);
     }
     G16_CUDA(cudaGetLastError());
     {
-        TimedLaunch tl("msm_window_reduce", st);
-        k_window_reduce<F><<<s.W, 128, 128 * xyzz_bytes, st>>>((const uint4*)acc.d_segments, P,
-                                                                 (uint4*)acc.d_windows);
+        TimedLaunch tl("msm_bucket_sums", st);
+        k_bucket_sums<F><<<blocks_for(s.K, 128), 128, 0, st>>>(partials, s.d_offsets, s.d_seg_base, s.K, s.chunk,
+                                                                (uint4*)acc.d_buckets);
+    }
+    {
+        TimedLaunch tl("msm_segments", st);
+        k_segments<F><<<blocks_for((size_t)s.W * P, 128), 128, 0, st>>>((const uint4*)acc.d_buckets, s.B, s.W, P,
+                                                                         (uint4*)acc.d_segments);
+    }
+    {
+        TimedLaunch tl("msm_window_sum", st);
+        k_group_sum<F><<<dim3(G, s.W), 128, 128 * xyzz_bytes, st>>>((const uint4*)acc.d_segments, P, groups);
+    }
+    {
+        TimedLaunch tl("msm_window_sum", st);
+        k_group_sum<F><<<dim3(1, s.W), 128, 128 * xyzz_bytes, st>>>(groups, G, (uint4*)acc.d_windows);
     }
     G16_CUDA(cudaGetLastError());
     return cudaSuccess;
@@ -472,11 +589,6 @@ cudaError_t msm_accumulate_g1(const MsmSort& s, MsmAccum& acc, const void* d_bas
 
 cudaError_t msm_accumulate_g2(const MsmSort& s, MsmAccum& acc, const void* d_bases, uint32_t base_offset,
                               uint32_t n_bases, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_window_reduce<g16d::Fq2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 256);
-        attr = true;
-    }
     return accumulate<g16d::Fq2>(s, acc, d_bases, base_offset, n_bases, st, XYZZ_G2_BYTES, "msm_accumulate_g2");
 }
 

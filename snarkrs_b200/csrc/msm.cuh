@@ -16,9 +16,13 @@
 //   3. accumulate: the sorted list is cut into fixed-length chunks, one
 //      thread per chunk adds its points into XYZZ partial bucket sums, so a
 //      fat bucket (a repeated witness value) is spread over many threads;
-//   4. bucket reduce: per window, segments of buckets fold their partials
-//      and run the running-sum reduction sum_b (b+1) S_b;
-//   5. window reduce: one block per window sums the segment results;
+//   4. fat buckets (more than a few partials, e.g. every scalar equal to 1)
+//      are folded by blocks in two tree stages; then one thread per bucket
+//      sums its partials into S_b;
+//   5. the running-sum reduction sum_b (b+1) S_b in segments of 8 buckets
+//      (two short dependent chains per thread), each segment weighted by its
+//      offset, then block tree sums per window: depth stays short because a
+//      dependent XYZZ addition costs microseconds of latency;
 //   6. host: Horner over the W window sums (c doublings between windows).
 // One sort serves every base vector that shares the scalars: the prover
 // sorts the witness once and accumulates A, B1, L (G1) and B2 (G2) from it.
@@ -43,14 +47,16 @@ struct MsmSort {
     uint32_t* d_offsets = nullptr;                                // K + 1
     uint32_t* d_cursor = nullptr;                                 // K
     uint32_t* d_seg_base = nullptr;                               // K + 1
+    uint32_t* d_fat_list = nullptr;                               // buckets with many partials
     uint32_t* d_scan_tmp = nullptr;     size_t cap_tmp = 0;
     uint32_t* d_entries = nullptr;      size_t cap_entries = 0;
-    uint32_t* d_total = nullptr;                                  // [0] = M, [1] = S
+    uint32_t* d_total = nullptr;                                  // [0] = M, [1] = S, [2] = fat buckets
     void release();
 };
 
 struct MsmAccum {
     void* d_partials = nullptr;    size_t cap_partials = 0;   // bytes
+    void* d_buckets = nullptr;     size_t cap_buckets = 0;    // bytes, one XYZZ sum per bucket
     void* d_segments = nullptr;    size_t cap_segments = 0;   // bytes
     void* d_windows = nullptr;     size_t cap_windows = 0;    // bytes
     unsigned long long* d_work = nullptr;                      // mixed additions performed
