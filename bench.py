@@ -50,6 +50,10 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--constraints", type=int, default=N_CONSTRAINTS)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="prove", choices=["prove", "msm-g1", "msm-g2", "ntt"],
+                   help="prove (default): full proofs; msm-g1/msm-g2/ntt: the standalone primitives")
+    p.add_argument("--log-n", type=int, default=20, help="primitive size 2^log_n")
+    p.add_argument("--dist", type=int, default=0, help="MSM scalars: 0 uniform, 1 = 70%% in {0,1}")
     return p.parse_args()
 
 
@@ -332,10 +336,96 @@ def traffic_for(name):
         return None
 
 
+def run_primitive(args):
+    """Standalone MSM (points/s) or NTT (elements/s) on device-resident inputs."""
+    import torch
+    import snarkrs_b200 as S
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    backend = S.CudaBackend(local_rank)
+    n = 1 << args.log_n
+    K, W = args.steps, args.warmup
+    g2 = args.workload == "msm-g2"
+    if args.workload.startswith("msm"):
+        bases = S.synth_points(2 if g2 else 1, 77 + rank, n)
+        scal = S.synth_scalars(78 + rank, n, args.dist)
+        d_b = torch.frombuffer(bytearray(bases), dtype=torch.uint8).cuda()
+        d_s = torch.frombuffer(bytearray(scal), dtype=torch.uint8).cuda()
+        msm = S.CudaMsm(backend)
+        fn = msm.msm_g2_device if g2 else msm.msm_g1_device
+        step = lambda: fn(d_b.data_ptr(), d_s.data_ptr(), n)
+        unit, what = "points/s", "%s MSM, N = 2^%d, %s scalars" % (
+            "G2" if g2 else "G1", args.log_n, "70% {0,1}" if args.dist else "uniform")
+        host = lambda: (msm.msm_g2 if g2 else msm.msm_g1)(bases, scal)
+        h2d = len(bases) + len(scal)
+    else:
+        data = S.synth_scalars(79 + rank, n, 0)
+        d = torch.frombuffer(bytearray(data), dtype=torch.uint8).cuda()
+        ntt = S.CudaNtt(backend)
+        step = lambda: ntt.ntt_device(S.NTT_INTT_COSET_NTT, args.log_n, d.data_ptr())
+        unit, what = "elements/s", "Fr iNTT -> coset -> NTT (intt_coset_ntt), n = 2^%d" % args.log_n
+        host = lambda: ntt.intt_coset_ntt(data)
+        h2d = len(data)
+    for _ in range(W):
+        step()
+    S.kernel_timing_reset()
+    S.kernel_timing(True)
+    torch.cuda.synchronize()
+    l0 = S.launch_count()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(K):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    S.kernel_timing(False)
+    kern = S.kernel_timing_report()
+    ms = e0.elapsed_time(e1)
+    t0 = time.perf_counter()
+    for _ in range(K):
+        host()
+    e2e_s = time.perf_counter() - t0
+    line = {"metric": unit, "value": n * K / (ms / 1e3), "unit": unit, "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32 (BN254 Montgomery limbs, exact)", "data": "synthetic", "config": {"workload": what},
+            "e2e": {"value": n * K / e2e_s, "unit": unit, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": (128 if g2 else 64) if args.workload.startswith("msm") else h2d},
+            "gpu_launches": int(S.launch_count() - l0), "clocks": clk,
+            "kernel_share": {k: round(v[0] / sum(x[0] for x in kern.values()), 4) for k, v in kern.items()}}
+    dom = max(kern.items(), key=lambda kv: kv[1][0])
+    name, (tot_ms, n_launch, units) = dom[0], dom[1]
+    roof = {"kernel": name, "launches": n_launch, "avg_ms": tot_ms / max(n_launch, 1)}
+    if name in MADD_FQ_MULS:
+        peak = S.imad_peak(backend)
+        achieved = units / max(n_launch, 1) * MADD_FQ_MULS[name] * FQ_MUL_IMAD / (roof["avg_ms"] / 1e3)
+        roof.update({"bound": "imad", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TIMAD/s",
+                     "frac": achieved / peak})
+    roof["traffic"] = traffic_for(name)
+    line["roofline"] = roof
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        O.build()
+        t0 = time.perf_counter()
+        if args.workload.startswith("msm"):
+            (O.msm_g2 if g2 else O.msm_g1)(bases, scal)
+        else:
+            O.ntt(args.log_n, O.NTT_INTT_COSET_NTT, data)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": n / dt, "unit": unit, "cores": O.max_threads(), "kind": "port",
+                                "sample": "1 run of the same input on the C restatement, %.2f s" % dt}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload != "prove":
+        run_primitive(args)
     else:
         run_ours(args)
 

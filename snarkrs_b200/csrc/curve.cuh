@@ -43,42 +43,42 @@ typedef Xyzz<Fq> G1Xyzz;
 typedef Xyzz<Fq2> G2Xyzz;
 
 // 2 * (x, y) for an affine point (mdbl-2008-s-1)
-template <class F>
+template <class F, bool INL = true>
 __device__ __forceinline__ Xyzz<F> xyzz_dbl_affine(const F& x, const F& y) {
     F u = dbl(y);
-    F v = sqr(u);
-    F w = mul(u, v);
-    F s = mul(x, v);
-    F xx = sqr(x);
+    F v = fsqr<INL>(u);
+    F w = fmul<INL>(u, v);
+    F s = fmul<INL>(x, v);
+    F xx = fsqr<INL>(x);
     F m = add(dbl(xx), xx);
     Xyzz<F> r;
-    r.x = sub(sqr(m), dbl(s));
-    r.y = sub(mul(m, sub(s, r.x)), mul(w, y));
+    r.x = sub(fsqr<INL>(m), dbl(s));
+    r.y = sub(fmul<INL>(m, sub(s, r.x)), fmul<INL>(w, y));
     r.zz = v;
     r.zzz = w;
     return r;
 }
 
 // 2 * p (dbl-2008-s-1)
-template <class F>
+template <class F, bool INL = true>
 __device__ __forceinline__ Xyzz<F> xyzz_dbl(const Xyzz<F>& p) {
     if (p.is_inf()) return p;
     F u = dbl(p.y);
-    F v = sqr(u);
-    F w = mul(u, v);
-    F s = mul(p.x, v);
-    F xx = sqr(p.x);
+    F v = fsqr<INL>(u);
+    F w = fmul<INL>(u, v);
+    F s = fmul<INL>(p.x, v);
+    F xx = fsqr<INL>(p.x);
     F m = add(dbl(xx), xx);
     Xyzz<F> r;
-    r.x = sub(sqr(m), dbl(s));
-    r.y = sub(mul(m, sub(s, r.x)), mul(w, p.y));
-    r.zz = mul(v, p.zz);
-    r.zzz = mul(w, p.zzz);
+    r.x = sub(fsqr<INL>(m), dbl(s));
+    r.y = sub(fmul<INL>(m, sub(s, r.x)), fmul<INL>(w, p.y));
+    r.zz = fmul<INL>(v, p.zz);
+    r.zzz = fmul<INL>(w, p.zzz);
     return r;
 }
 
 // p + (x2, y2) for a finite affine point (madd-2008-s)
-template <class F>
+template <class F, bool INL = true>
 __device__ __forceinline__ Xyzz<F> xyzz_add_affine(const Xyzz<F>& p, const F& x2, const F& y2) {
     if (p.is_inf()) {
         Xyzz<F> r;
@@ -88,48 +88,48 @@ __device__ __forceinline__ Xyzz<F> xyzz_add_affine(const Xyzz<F>& p, const F& x2
         r.zzz = F::one();
         return r;
     }
-    F u2 = mul(x2, p.zz);
-    F s2 = mul(y2, p.zzz);
+    F u2 = fmul<INL>(x2, p.zz);
+    F s2 = fmul<INL>(y2, p.zzz);
     F pp_ = sub(u2, p.x);
     F rr = sub(s2, p.y);
     if (pp_.is_zero()) {
-        if (rr.is_zero()) return xyzz_dbl_affine(x2, y2);
+        if (rr.is_zero()) return xyzz_dbl_affine<F, INL>(x2, y2);
         return Xyzz<F>::identity();
     }
-    F pp = sqr(pp_);
-    F ppp = mul(pp_, pp);
-    F q = mul(p.x, pp);
+    F pp = fsqr<INL>(pp_);
+    F ppp = fmul<INL>(pp_, pp);
+    F q = fmul<INL>(p.x, pp);
     Xyzz<F> r;
-    r.x = sub(sub(sqr(rr), ppp), dbl(q));
-    r.y = sub(mul(rr, sub(q, r.x)), mul(p.y, ppp));
-    r.zz = mul(p.zz, pp);
-    r.zzz = mul(p.zzz, ppp);
+    r.x = sub(sub(fsqr<INL>(rr), ppp), dbl(q));
+    r.y = sub(fmul<INL>(rr, sub(q, r.x)), fmul<INL>(p.y, ppp));
+    r.zz = fmul<INL>(p.zz, pp);
+    r.zzz = fmul<INL>(p.zzz, ppp);
     return r;
 }
 
 // p + q (add-2008-s)
-template <class F>
+template <class F, bool INL = true>
 __device__ __forceinline__ Xyzz<F> xyzz_add(const Xyzz<F>& p, const Xyzz<F>& q) {
     if (p.is_inf()) return q;
     if (q.is_inf()) return p;
-    F u1 = mul(p.x, q.zz);
-    F u2 = mul(q.x, p.zz);
-    F s1 = mul(p.y, q.zzz);
-    F s2 = mul(q.y, p.zzz);
+    F u1 = fmul<INL>(p.x, q.zz);
+    F u2 = fmul<INL>(q.x, p.zz);
+    F s1 = fmul<INL>(p.y, q.zzz);
+    F s2 = fmul<INL>(q.y, p.zzz);
     F pp_ = sub(u2, u1);
     F rr = sub(s2, s1);
     if (pp_.is_zero()) {
-        if (rr.is_zero()) return xyzz_dbl(p);
+        if (rr.is_zero()) return xyzz_dbl<F, INL>(p);
         return Xyzz<F>::identity();
     }
-    F pp = sqr(pp_);
-    F ppp = mul(pp_, pp);
-    F qq = mul(u1, pp);
+    F pp = fsqr<INL>(pp_);
+    F ppp = fmul<INL>(pp_, pp);
+    F qq = fmul<INL>(u1, pp);
     Xyzz<F> r;
-    r.x = sub(sub(sqr(rr), ppp), dbl(qq));
-    r.y = sub(mul(rr, sub(qq, r.x)), mul(s1, ppp));
-    r.zz = mul(mul(p.zz, q.zz), pp);
-    r.zzz = mul(mul(p.zzz, q.zzz), ppp);
+    r.x = sub(sub(fsqr<INL>(rr), ppp), dbl(qq));
+    r.y = sub(fmul<INL>(rr, sub(qq, r.x)), fmul<INL>(s1, ppp));
+    r.zz = fmul<INL>(fmul<INL>(p.zz, q.zz), pp);
+    r.zzz = fmul<INL>(fmul<INL>(p.zzz, q.zzz), ppp);
     return r;
 }
 

@@ -279,6 +279,40 @@ __device__ __forceinline__ Fq2 sqr(const Fq2& a) {
     return {p, dbl(q)};
 }
 
+// ---- product policy: inlined, or one out-of-line copy ----
+// Latency-bound kernels (bucket reduction) run long dependent chains of point
+// operations; inlining ~14 CIOS bodies per point operation, several operations
+// per kernel, overflows the instruction cache.  They call a single
+// out-of-line copy instead (operands by value, so they stay in registers).
+// The throughput kernels keep every product inlined.
+template <class Params>
+__device__ __noinline__ Fp<Params> mul_ool(Fp<Params> a, Fp<Params> b) {
+    return mul(a, b);
+}
+
+template <bool INL, class Params>
+__device__ __forceinline__ Fp<Params> fmul(const Fp<Params>& a, const Fp<Params>& b) {
+    if constexpr (INL) return mul(a, b);
+    else return mul_ool(a, b);
+}
+template <bool INL, class Params>
+__device__ __forceinline__ Fp<Params> fsqr(const Fp<Params>& a) {
+    return fmul<INL>(a, a);
+}
+template <bool INL>
+__device__ __forceinline__ Fq2 fmul(const Fq2& a, const Fq2& b) {
+    Fq t0 = fmul<INL>(a.c0, b.c0);
+    Fq t1 = fmul<INL>(a.c1, b.c1);
+    Fq m = fmul<INL>(add(a.c0, a.c1), add(b.c0, b.c1));
+    return {sub(t0, t1), sub(sub(m, t0), t1)};
+}
+template <bool INL>
+__device__ __forceinline__ Fq2 fsqr(const Fq2& a) {
+    Fq p = fmul<INL>(add(a.c0, a.c1), sub(a.c0, a.c1));
+    Fq q = fmul<INL>(a.c0, a.c1);
+    return {p, dbl(q)};
+}
+
 // ---- 128-bit vector loads / stores of 32-byte elements ----
 template <class T>
 __device__ __forceinline__ T load32(const T* p) {

@@ -248,7 +248,7 @@ __device__ __forceinline__ Xyzz<F> block_sum(Xyzz<F> acc, uint4* smem) {
     __syncthreads();
     for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
         if (threadIdx.x < s) {
-            acc = xyzz_add(acc, ld_xyzz<F>(smem, threadIdx.x + s));
+            acc = xyzz_add<F, false>(acc, ld_xyzz<F>(smem, threadIdx.x + s));
             st_xyzz<F>(smem, threadIdx.x, acc);
         }
         __syncthreads();
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(128) k_fat_merge_jobs(uint4* __restrict__ part
         if (a >= ns) continue;   // uniform across the block
         uint32_t b = min(a + J, ns), base = seg_base[g];
         Xyzz<F> acc = Xyzz<F>::identity();
-        for (uint32_t i = a + threadIdx.x; i < b; i += blockDim.x) acc = xyzz_add(acc, ld_xyzz<F>(partials, base + i));
+        for (uint32_t i = a + threadIdx.x; i < b; i += blockDim.x) acc = xyzz_add<F, false>(acc, ld_xyzz<F>(partials, base + i));
         acc = block_sum(acc, smem);
         if (threadIdx.x == 0) st_xyzz<F>(partials, base + a, acc);
         __syncthreads();
@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(128) k_bucket_sums(const uint4* __restrict__ p
     if (ns > FAT_PARTIALS) {
         acc = ld_xyzz<F>(partials, base);
     } else {
-        for (uint32_t s = 0; s < ns; s++) acc = xyzz_add(acc, ld_xyzz<F>(partials, base + s));
+        for (uint32_t s = 0; s < ns; s++) acc = xyzz_add<F, false>(acc, ld_xyzz<F>(partials, base + s));
     }
     st_xyzz<F>(buckets, g, acc);
 }
@@ -336,18 +336,18 @@ __global__ void __launch_bounds__(128) k_segments(const uint4* __restrict__ buck
     size_t g0 = (size_t)w * B + (size_t)p * SEG;
 #pragma unroll 1
     for (int j = SEG - 1; j >= 0; j--) {
-        run = xyzz_add(run, ld_xyzz<F>(buckets, g0 + j));
-        tot = xyzz_add(tot, run);
+        run = xyzz_add<F, false>(run, ld_xyzz<F>(buckets, g0 + j));
+        tot = xyzz_add<F, false>(tot, run);
     }
     uint32_t k = p * SEG;
     Xyzz<F> acc = Xyzz<F>::identity();
     if (k) {
         for (int bit = 31 - __clz(k); bit >= 0; bit--) {
-            acc = xyzz_dbl(acc);
-            if ((k >> bit) & 1u) acc = xyzz_add(acc, run);
+            acc = xyzz_dbl<F, false>(acc);
+            if ((k >> bit) & 1u) acc = xyzz_add<F, false>(acc, run);
         }
     }
-    st_xyzz<F>(seg_out, t, xyzz_add(tot, acc));
+    st_xyzz<F>(seg_out, t, xyzz_add<F, false>(tot, acc));
 }
 
 // Group sums: grid (blocks per group, groups); each block folds `per` items per
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(128) k_group_sum(const uint4* __restrict__ in,
     uint32_t lo = blockIdx.x * chunk, hi = min(lo + chunk, items_per_group);
     Xyzz<F> acc = Xyzz<F>::identity();
     for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
-        acc = xyzz_add(acc, ld_xyzz<F>(in, (size_t)grp * items_per_group + i));
+        acc = xyzz_add<F, false>(acc, ld_xyzz<F>(in, (size_t)grp * items_per_group + i));
     acc = block_sum(acc, smem);
     if (threadIdx.x == 0) st_xyzz<F>(out, (size_t)grp * gridDim.x + blockIdx.x, acc);
 }
