@@ -183,6 +183,14 @@ __device__ __forceinline__ Affine<F> ld_affine(const uint4* base, size_t i) {
 }
 
 template <class F>
+__device__ __forceinline__ void st_affine(uint4* base, size_t i, const F& x, const F& y) {
+    constexpr int U = Codec<F>::U4;
+    uint4* p = base + i * (2 * U);
+    Codec<F>::st(p, x);
+    Codec<F>::st(p + U, y);
+}
+
+template <class F>
 __device__ __forceinline__ void st_xyzz(uint4* base, size_t i, const Xyzz<F>& x) {
     constexpr int U = Codec<F>::U4;
     uint4* p = base + i * (4 * U);

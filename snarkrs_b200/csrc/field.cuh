@@ -313,6 +313,29 @@ __device__ __forceinline__ Fq2 fsqr(const Fq2& a) {
     return {p, dbl(q)};
 }
 
+// a^(p-2) by right-to-left square-and-multiply (Fermat); 0 maps to 0.  Used
+// off the hot path (table building), so it calls the out-of-line product.
+template <class Params>
+__device__ Fp<Params> inv(const Fp<Params>& a) {
+    Fp<Params> r = Fp<Params>::one(), b = a;
+#pragma unroll
+    for (int limb = 0; limb < 8; limb++) {
+        uint32_t e = Params::P(limb) - (limb == 0 ? 2u : 0u);
+        for (int bit = 0; bit < 32; bit++) {
+            if (e & 1u) r = mul_ool(r, b);
+            b = mul_ool(b, b);
+            e >>= 1;
+        }
+    }
+    return r;
+}
+
+// 1/(c0 + c1 u) = (c0 - c1 u) / (c0^2 + c1^2)
+__device__ __forceinline__ Fq2 inv(const Fq2& a) {
+    Fq n = inv(add(mul_ool(a.c0, a.c0), mul_ool(a.c1, a.c1)));
+    return {mul_ool(a.c0, n), neg(mul_ool(a.c1, n))};
+}
+
 // ---- 128-bit vector loads / stores of 32-byte elements ----
 template <class T>
 __device__ __forceinline__ T load32(const T* p) {

@@ -32,8 +32,10 @@ __device__ __forceinline__ int signed_digit(const uint32_t* s, int w, int c) {
 
 constexpr uint32_t NO_KEY = 0xffffffffu;
 
+// kw: key stride per window (B when every window has its own buckets, 0 when
+// all windows share one bucket set over window-shifted bases)
 __global__ void __launch_bounds__(256) k_digits_count(const uint4* __restrict__ scalars, int mont, uint32_t n, int c,
-                                                      int W, uint32_t B, uint4* __restrict__ scalars_std,
+                                                      int W, uint32_t kw, uint4* __restrict__ scalars_std,
                                                       uint32_t* __restrict__ counts) {
     __shared__ uint32_t sh[256 * 9];
     uint32_t i = blockIdx.x * 256 + threadIdx.x;
@@ -53,14 +55,16 @@ __global__ void __launch_bounds__(256) k_digits_count(const uint4* __restrict__ 
     unsigned lane = threadIdx.x & 31;
     for (int w = 0; w < W; w++) {
         int d = signed_digit(row, w, c);
-        uint32_t key = (valid && d != 0) ? (uint32_t)w * B + (uint32_t)(d < 0 ? -d : d) - 1u : NO_KEY;
+        uint32_t key = (valid && d != 0) ? (uint32_t)w * kw + (uint32_t)(d < 0 ? -d : d) - 1u : NO_KEY;
         unsigned mask = __match_any_sync(0xffffffffu, key);
         if (key != NO_KEY && lane == (unsigned)(__ffs(mask) - 1)) atomicAdd(&counts[key], (uint32_t)__popc(mask));
     }
 }
 
+// ew: entry-index stride per window (0, or n for window-shifted bases: entry
+// w*n + i names base 2^(c w) P_i)
 __global__ void __launch_bounds__(256) k_scatter(const uint4* __restrict__ scalars_std, uint32_t n, int c, int W,
-                                                 uint32_t B, uint32_t* __restrict__ cursor,
+                                                 uint32_t kw, uint32_t ew, uint32_t* __restrict__ cursor,
                                                  uint32_t* __restrict__ entries) {
     __shared__ uint32_t sh[256 * 9];
     uint32_t i = blockIdx.x * 256 + threadIdx.x;
@@ -78,13 +82,13 @@ __global__ void __launch_bounds__(256) k_scatter(const uint4* __restrict__ scala
     unsigned lt = (1u << lane) - 1u;
     for (int w = 0; w < W; w++) {
         int d = signed_digit(row, w, c);
-        uint32_t key = (valid && d != 0) ? (uint32_t)w * B + (uint32_t)(d < 0 ? -d : d) - 1u : NO_KEY;
+        uint32_t key = (valid && d != 0) ? (uint32_t)w * kw + (uint32_t)(d < 0 ? -d : d) - 1u : NO_KEY;
         unsigned mask = __match_any_sync(0xffffffffu, key);
         int leader = __ffs(mask) - 1;
         uint32_t base = 0;
         if (key != NO_KEY && (int)lane == leader) base = atomicAdd(&cursor[key], (uint32_t)__popc(mask));
         base = __shfl_sync(0xffffffffu, base, leader);
-        if (key != NO_KEY) entries[base + __popc(mask & lt)] = i | (d < 0 ? 0x80000000u : 0u);
+        if (key != NO_KEY) entries[base + __popc(mask & lt)] = ((uint32_t)w * ew + i) | (d < 0 ? 0x80000000u : 0u);
     }
 }
 
@@ -366,6 +370,39 @@ __global__ void __launch_bounds__(128) k_group_sum(const uint4* __restrict__ in,
     if (threadIdx.x == 0) st_xyzz<F>(out, (size_t)grp * gridDim.x + blockIdx.x, acc);
 }
 
+// Window-shifted base table: out[w n + i] = 2^(c w) P_i (affine), one thread per
+// point, c doublings per window and one inversion per output.  Table building
+// runs once per prepared key.
+template <class F>
+__global__ void __launch_bounds__(128) k_window_table(const uint4* __restrict__ in, uint32_t n, uint32_t skip, int c,
+                                                      int W, uint4* __restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Affine<F> p;
+    bool inf = i < skip;
+    if (!inf) {
+        p = ld_affine<F>(in, i - skip);
+        inf = p.is_inf();
+    }
+    if (inf) {
+        for (int w = 0; w < W; w++) st_affine<F>(out, (size_t)w * n + i, F::zero(), F::zero());
+        return;
+    }
+    st_affine<F>(out, i, p.x, p.y);
+    Xyzz<F> acc;
+    acc.x = p.x;
+    acc.y = p.y;
+    acc.zz = F::one();
+    acc.zzz = F::one();
+    for (int w = 1; w < W; w++) {
+        for (int j = 0; j < c; j++) acc = xyzz_dbl<F, false>(acc);
+        F zi = inv(fmul<false>(acc.zz, acc.zzz));   // 1 / (ZZ ZZZ)
+        F x = fmul<false>(fmul<false>(acc.x, acc.zzz), zi);
+        F y = fmul<false>(fmul<false>(acc.y, acc.zz), zi);
+        st_affine<F>(out, (size_t)w * n + i, x, y);
+    }
+}
+
 }  // namespace g16d
 
 namespace g16 {
@@ -392,6 +429,33 @@ void MsmAccum::release() {
     cudaFree(d_segments);
     cudaFree(d_windows);
     *this = MsmAccum();
+}
+
+int msm_shared_window_bits(size_t m) {
+    int best = 8;
+    double best_cost = 1e300;
+    for (int c = 8; c <= 22; c++) {
+        double cost = (double)m * msm_windows(c) + 3.0 * (double)(1u << (c - 1));
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = c;
+        }
+    }
+    return best;
+}
+
+cudaError_t msm_window_table_g1(const void* d_in, size_t n, uint32_t skip, int c, void* d_out, cudaStream_t st) {
+    TimedLaunch tl("msm_window_table", st);
+    k_window_table<g16d::Fq><<<blocks_for(n, 128), 128, 0, st>>>((const uint4*)d_in, (uint32_t)n, skip, c,
+                                                                 msm_windows(c), (uint4*)d_out);
+    return cudaGetLastError();
+}
+
+cudaError_t msm_window_table_g2(const void* d_in, size_t n, uint32_t skip, int c, void* d_out, cudaStream_t st) {
+    TimedLaunch tl("msm_window_table", st);
+    k_window_table<g16d::Fq2><<<blocks_for(n, 128), 128, 0, st>>>((const uint4*)d_in, (uint32_t)n, skip, c,
+                                                                  msm_windows(c), (uint4*)d_out);
+    return cudaGetLastError();
 }
 
 int msm_window_bits(size_t m) {
@@ -461,11 +525,8 @@ static cudaError_t scan(const uint32_t* in, uint32_t* out, uint32_t len, uint32_
     return cudaGetLastError();
 }
 
-cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomery, int c, cudaStream_t st) {
-    if (n >= 0x80000000ull) {
-        set_error("MSM of %zu points exceeds the 2^31 point-index limit", n);
-        return cudaErrorInvalidValue;
-    }
+cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomery, int c, cudaStream_t st,
+                     bool shared_windows) {
     if (c == 0) c = msm_window_bits(n);
     if (c < 4 || c > 24) {
         set_error("MSM window of %d bits outside [4, 24]", c);
@@ -474,8 +535,20 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
     s.c = c;
     s.W = (255 + c - 1) / c;
     s.B = 1u << (c - 1);
-    s.K = (uint32_t)s.W * s.B;
+    s.shared = shared_windows;
+    s.K = shared_windows ? s.B : (uint32_t)s.W * s.B;
     s.n = n;
+    if ((shared_windows ? n * (size_t)s.W : n) >= 0x80000000ull) {
+        set_error("MSM of %zu points x %d windows exceeds the 2^31 entry-index limit", n, s.W);
+        return cudaErrorInvalidValue;
+    }
+    // about eight entries per partial sum on average, at least 16 per chunk
+    s.chunk = 16;
+    if (shared_windows) {
+        size_t per_bucket = n * (size_t)s.W / s.K;
+        while (s.chunk < 256 && (size_t)s.chunk * 4 < per_bucket) s.chunk <<= 1;
+    }
+    const uint32_t kw = shared_windows ? 0u : s.B, ew = shared_windows ? (uint32_t)n : 0u;
     size_t nn = n ? n : 1;
     G16_CUDA(grow(s.d_scalars_std, s.cap_scalars, nn * 8));
     size_t kk = (size_t)s.K + 1;
@@ -501,7 +574,7 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
     if (n) {
         TimedLaunch tl("msm_digits", st);
         k_digits_count<<<blocks_for(n, 256), 256, 0, st>>>((const uint4*)d_scalars, montgomery ? 1 : 0, (uint32_t)n,
-                                                          c, s.W, s.B, (uint4*)s.d_scalars_std, s.d_counts);
+                                                          c, s.W, kw, (uint4*)s.d_scalars_std, s.d_counts);
     }
     G16_CUDA(cudaGetLastError());
     G16_CUDA(scan(s.d_counts, s.d_offsets, s.K, s.d_scan_tmp, s.d_total, st));
@@ -511,7 +584,7 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
     }
     if (n) {
         TimedLaunch tl("msm_scatter", st);
-        k_scatter<<<blocks_for(n, 256), 256, 0, st>>>((const uint4*)s.d_scalars_std, (uint32_t)n, c, s.W, s.B,
+        k_scatter<<<blocks_for(n, 256), 256, 0, st>>>((const uint4*)s.d_scalars_std, (uint32_t)n, c, s.W, kw, ew,
                                                      s.d_cursor, s.d_entries);
     }
     G16_CUDA(cudaGetLastError());
@@ -534,14 +607,15 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     G16_CUDA(grow_bytes(acc.d_partials, acc.cap_partials, max_partials * xyzz_bytes));
     const uint32_t P = s.B / SEG;                  // segments per window
     const uint32_t G = (P + 511) / 512;            // group-sum blocks per window
+    const uint32_t Wr = s.shared ? 1u : (uint32_t)s.W;   // bucket sets to reduce
     acc.segs_per_window = P;
     G16_CUDA(grow_bytes(acc.d_buckets, acc.cap_buckets, (size_t)s.K * xyzz_bytes));
-    G16_CUDA(grow_bytes(acc.d_segments, acc.cap_segments, ((size_t)s.W * P + (size_t)s.W * G) * xyzz_bytes));
-    G16_CUDA(grow_bytes(acc.d_windows, acc.cap_windows, (size_t)s.W * xyzz_bytes));
+    G16_CUDA(grow_bytes(acc.d_segments, acc.cap_segments, ((size_t)Wr * P + (size_t)Wr * G) * xyzz_bytes));
+    G16_CUDA(grow_bytes(acc.d_windows, acc.cap_windows, (size_t)Wr * xyzz_bytes));
     if (!acc.d_work) G16_CUDA(cudaMalloc((void**)&acc.d_work, sizeof(unsigned long long)));
     G16_CUDA(cudaMemsetAsync(acc.d_work, 0, sizeof(unsigned long long), st));
     uint4* partials = (uint4*)acc.d_partials;
-    uint4* groups = (uint4*)((uint8_t*)acc.d_segments + (size_t)s.W * P * xyzz_bytes);
+    uint4* groups = (uint4*)((uint8_t*)acc.d_segments + (size_t)Wr * P * xyzz_bytes);
     {
         TimedLaunch tl(tag, st);
         k_accumulate<F><<<blocks_for(chunks, 128), 128, 0, st>>>(s.d_entries, s.d_offsets, s.d_seg_base, s.K,
@@ -567,16 +641,16 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     }
     {
         TimedLaunch tl("msm_segments", st);
-        k_segments<F><<<blocks_for((size_t)s.W * P, 128), 128, 0, st>>>((const uint4*)acc.d_buckets, s.B, s.W, P,
-                                                                         (uint4*)acc.d_segments);
+        k_segments<F><<<blocks_for((size_t)Wr * P, 128), 128, 0, st>>>((const uint4*)acc.d_buckets, s.B, Wr, P,
+                                                                        (uint4*)acc.d_segments);
     }
     {
         TimedLaunch tl("msm_window_sum", st);
-        k_group_sum<F><<<dim3(G, s.W), 128, 128 * xyzz_bytes, st>>>((const uint4*)acc.d_segments, P, groups);
+        k_group_sum<F><<<dim3(G, Wr), 128, 128 * xyzz_bytes, st>>>((const uint4*)acc.d_segments, P, groups);
     }
     {
         TimedLaunch tl("msm_window_sum", st);
-        k_group_sum<F><<<dim3(1, s.W), 128, 128 * xyzz_bytes, st>>>(groups, G, (uint4*)acc.d_windows);
+        k_group_sum<F><<<dim3(1, Wr), 128, 128 * xyzz_bytes, st>>>(groups, G, (uint4*)acc.d_windows);
     }
     G16_CUDA(cudaGetLastError());
     return cudaSuccess;

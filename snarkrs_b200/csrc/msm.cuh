@@ -38,7 +38,8 @@ struct MsmSort {
     // parameters
     int c = 0, W = 0;
     uint32_t B = 0;        // buckets per window, 2^(c-1)
-    uint32_t K = 0;        // W * B
+    uint32_t K = 0;        // W * B, or B when the windows share one bucket set
+    bool shared = false;   // entries index window-shifted bases (w * n + i), one bucket set
     size_t n = 0;          // scalars sorted
     uint32_t chunk = 16;   // accumulate chunk length
     // device buffers (capacities in elements)
@@ -70,7 +71,22 @@ int msm_window_bits(size_t m);
 
 // Sort n device-resident scalars (32 bytes each; montgomery != 0 converts
 // from Montgomery form first).  c = 0 picks msm_window_bits(n).
-cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomery, int c, cudaStream_t st);
+// shared_windows: the bases are the window-shifted table 2^(c w) P_i laid out
+// at w * n + i (msm_window_table); all windows then fall into one bucket set
+// and the result needs no Horner step.
+cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomery, int c, cudaStream_t st,
+                     bool shared_windows = false);
+
+// Window count for c-bit signed digits over 255 bits.
+inline int msm_windows(int c) { return (255 + c - 1) / c; }
+// Window width for window-shifted bases: the cost is ~m * ceil(255/c) mixed
+// additions plus a single bucket reduction over 2^(c-1) buckets.
+int msm_shared_window_bits(size_t m);
+
+// Build the window-shifted base table: out[w * n + i] = 2^(c w) P_i, affine,
+// for i < n, where P_i = in[i - skip] for i >= skip and infinity below skip.
+cudaError_t msm_window_table_g1(const void* d_in, size_t n, uint32_t skip, int c, void* d_out, cudaStream_t st);
+cudaError_t msm_window_table_g2(const void* d_in, size_t n, uint32_t skip, int c, void* d_out, cudaStream_t st);
 
 // Accumulate bases against a sorted scalar set and reduce to W window sums
 // (XYZZ, device, in acc.d_windows).  Entry i uses base i - base_offset; entries

@@ -147,6 +147,9 @@ struct g16_circuit {
     uint32_t *d_rp[2] = {nullptr, nullptr}, *d_sig[2] = {nullptr, nullptr}, *d_vid[2] = {nullptr, nullptr};
     void* d_values = nullptr;
     void *d_a = nullptr, *d_b1 = nullptr, *d_b2 = nullptr, *d_l = nullptr, *d_h = nullptr;
+    // window-shifted base tables 2^(c w) P_i at w * N + i (msm_window_table)
+    void *t_a = nullptr, *t_b1 = nullptr, *t_b2 = nullptr, *t_l = nullptr, *t_h = nullptr;
+    int c_w = 0, c_h = 0;   // window bits of the witness and H MSMs
     NttTables ntt;
     G1A alpha1, beta1, delta1;
     G2A beta2, delta2;
@@ -318,20 +321,19 @@ int run_h(g16_circuit* c, const void* d_w, void* h_out) {
 // stages 5-9: five MSMs, window sums read back, Horner on the host
 int run_msms(g16_circuit* c, const void* d_w, const void* d_h, MsmJac& out) {
     cudaStream_t st = c->stream;
-    CK(msm_sort(c->sort_h, d_h, c->n, true, 0, st), "H sort");
-    CK(msm_accumulate_g1(c->sort_h, c->acc[4], c->d_h, 0, c->n, st), "H accumulate");
-    CK(msm_sort(c->sort_w, d_w, c->n_vars, true, 0, st), "witness sort");
-    CK(msm_accumulate_g1(c->sort_w, c->acc[0], c->d_a, 0, c->n_vars, st), "A accumulate");
-    CK(msm_accumulate_g1(c->sort_w, c->acc[2], c->d_b1, 0, c->n_vars, st), "B1 accumulate");
-    uint32_t off = c->n_public + 1;
-    CK(msm_accumulate_g1(c->sort_w, c->acc[3], c->d_l, off, c->n_vars - off, st), "L accumulate");
-    CK(msm_accumulate_g2(c->sort_w, c->acc[1], c->d_b2, 0, c->n_vars, st), "B2 accumulate");
+    const uint32_t nh = c->n * (uint32_t)msm_windows(c->c_h), nw = c->n_vars * (uint32_t)msm_windows(c->c_w);
+    CK(msm_sort(c->sort_h, d_h, c->n, true, c->c_h, st, true), "H sort");
+    CK(msm_accumulate_g1(c->sort_h, c->acc[4], c->t_h, 0, nh, st), "H accumulate");
+    CK(msm_sort(c->sort_w, d_w, c->n_vars, true, c->c_w, st, true), "witness sort");
+    CK(msm_accumulate_g1(c->sort_w, c->acc[0], c->t_a, 0, nw, st), "A accumulate");
+    CK(msm_accumulate_g1(c->sort_w, c->acc[2], c->t_b1, 0, nw, st), "B1 accumulate");
+    CK(msm_accumulate_g1(c->sort_w, c->acc[3], c->t_l, 0, nw, st), "L accumulate");
+    CK(msm_accumulate_g2(c->sort_w, c->acc[1], c->t_b2, 0, nw, st), "B2 accumulate");
     // readback: slot i holds up to 32 windows of 256 bytes
     const size_t slot = 32 * 256;
     c->readback_bytes = 0;
     for (int i = 0; i < 5; i++) {
-        const MsmSort& s = (i == 4) ? c->sort_h : c->sort_w;
-        size_t bytes = (size_t)s.W * (i == 1 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES);
+        size_t bytes = i == 1 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES;   // one shared window per MSM
         CK(cudaMemcpyAsync(c->h_win + i * slot, c->acc[i].d_windows, bytes, cudaMemcpyDeviceToHost, st),
            "window readback");
         c->readback_bytes += bytes;
@@ -345,11 +347,11 @@ int run_msms(g16_circuit* c, const void* d_w, const void* d_h, MsmJac& out) {
         timer().add_units("msm_accumulate_g1", (double)(c->h_work[0] + c->h_work[2] + c->h_work[3] + c->h_work[4]));
         timer().add_units("msm_accumulate_g2", (double)c->h_work[1]);
     }
-    out.a = msm_combine_g1(c->h_win + 0 * slot, c->sort_w.W, c->sort_w.c);
-    out.b2 = msm_combine_g2(c->h_win + 1 * slot, c->sort_w.W, c->sort_w.c);
-    out.b1 = msm_combine_g1(c->h_win + 2 * slot, c->sort_w.W, c->sort_w.c);
-    out.l = msm_combine_g1(c->h_win + 3 * slot, c->sort_w.W, c->sort_w.c);
-    out.h = msm_combine_g1(c->h_win + 4 * slot, c->sort_h.W, c->sort_h.c);
+    out.a = msm_combine_g1(c->h_win + 0 * slot, 1, c->c_w);
+    out.b2 = msm_combine_g2(c->h_win + 1 * slot, 1, c->c_w);
+    out.b1 = msm_combine_g1(c->h_win + 2 * slot, 1, c->c_w);
+    out.l = msm_combine_g1(c->h_win + 3 * slot, 1, c->c_w);
+    out.h = msm_combine_g1(c->h_win + 4 * slot, 1, c->c_h);
     return G16_OK;
 }
 
@@ -499,6 +501,11 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
     // memory budget, refused before any allocation (backend.rs:367-381)
     uint64_t key_bytes = 4ull * (n + 1) * 2 + 8ull * (k->nnz[0] + k->nnz[1]) + 32ull * k->n_values + nv * 64 * 2 +
                          nv * 128 + nl * 64 + (uint64_t)n * 64 + (uint64_t)n * 32 * 2 + 32;
+    const int c_w = msm_shared_window_bits(nv / 2 + 1), c_h = msm_shared_window_bits(n);
+    const uint64_t Ww = (uint64_t)msm_windows(c_w), Wh = (uint64_t)msm_windows(c_h);
+    if (nv * Ww >= 0x80000000ull || (uint64_t)n * Wh >= 0x80000000ull)
+        return fail(G16_ERR_BACKEND, "circuit too large for 31-bit MSM entry indices");
+    key_bytes += nv * Ww * (64 * 3 + 128) + (uint64_t)n * Wh * 64;
     uint64_t scratch = nv * 32 + (uint64_t)n * 32 * 4 + ((uint64_t)n + nv) * 32 + ((uint64_t)n + nv) * 16 * 4 +
                        ((uint64_t)n + nv) * 16 / 16 * 256 * 2 + (64ull << 20);
     if (b->vram_used + key_bytes + scratch > b->vram_limit)
@@ -562,6 +569,27 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
         return rc;
     }
     cp->device_bytes += 3ull * 32 * n / 2 * 2;
+    // window-shifted base tables; the plain bases are their window-0 slice
+    cp->c_w = c_w;
+    cp->c_h = c_h;
+    {
+        cudaError_t e2 = circuit_alloc(cp, &cp->t_a, 64ull * nv * Ww);
+        if (e2 == cudaSuccess) e2 = circuit_alloc(cp, &cp->t_b1, 64ull * nv * Ww);
+        if (e2 == cudaSuccess) e2 = circuit_alloc(cp, &cp->t_l, 64ull * nv * Ww);
+        if (e2 == cudaSuccess) e2 = circuit_alloc(cp, &cp->t_b2, 128ull * nv * Ww);
+        if (e2 == cudaSuccess) e2 = circuit_alloc(cp, &cp->t_h, 64ull * n * Wh);
+        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_a, nv, 0, c_w, cp->t_a, cp->stream);
+        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_b1, nv, 0, c_w, cp->t_b1, cp->stream);
+        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_l, nv, k->n_public + 1, c_w, cp->t_l, cp->stream);
+        if (e2 == cudaSuccess) e2 = msm_window_table_g2(cp->d_b2, nv, 0, c_w, cp->t_b2, cp->stream);
+        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_h, n, 0, c_h, cp->t_h, cp->stream);
+        if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(cp->stream);
+        if (e2 != cudaSuccess) {
+            int rc = cuda_fail(e2, "window tables");
+            cleanup();
+            return rc;
+        }
+    }
     *out = c.release();
     return G16_OK;
 }
