@@ -170,8 +170,14 @@ __global__ void __launch_bounds__(256) k_scan_add(uint32_t* __restrict__ out, ui
 // Partial sums per bucket (one per chunk the bucket touches).  Buckets with
 // more than FAT_PARTIALS of them -- a repeated scalar, most often 1 -- go on
 // the fat list and are folded in parallel before the bucket sums.
-constexpr uint32_t FAT_PARTIALS = 8;
+constexpr uint32_t FAT_PARTIALS = 32;
 constexpr uint32_t FAT_JOBS = 64;
+
+// partials per job of a fat bucket: at least FAT_PARTIALS, at most FAT_JOBS jobs
+__device__ __forceinline__ uint32_t fat_job_len(uint32_t ns) {
+    uint32_t j = (ns + FAT_JOBS - 1) / FAT_JOBS;
+    return j < FAT_PARTIALS ? FAT_PARTIALS : j;
+}
 
 __global__ void k_nseg(const uint32_t* __restrict__ offsets, uint32_t K, uint32_t L, uint32_t* __restrict__ nseg,
                        uint32_t* __restrict__ fat_list, uint32_t* __restrict__ fat_count) {
@@ -272,7 +278,7 @@ __global__ void __launch_bounds__(128) k_fat_merge_jobs(uint4* __restrict__ part
     uint32_t items = *fat_count * FAT_JOBS;
     for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
         uint32_t g = fat_list[item / FAT_JOBS], j = item % FAT_JOBS;
-        uint32_t ns = n_partials(offsets, g, L), J = (ns + FAT_JOBS - 1) / FAT_JOBS;
+        uint32_t ns = n_partials(offsets, g, L), J = fat_job_len(ns);
         uint32_t a = j * J;
         if (a >= ns) continue;   // uniform across the block
         uint32_t b = min(a + J, ns), base = seg_base[g];
@@ -296,7 +302,7 @@ __global__ void __launch_bounds__(64) k_fat_merge_final(uint4* __restrict__ part
     uint32_t nf = *fat_count;
     for (uint32_t f = blockIdx.x; f < nf; f += gridDim.x) {
         uint32_t g = fat_list[f];
-        uint32_t ns = n_partials(offsets, g, L), J = (ns + FAT_JOBS - 1) / FAT_JOBS;
+        uint32_t ns = n_partials(offsets, g, L), J = fat_job_len(ns);
         uint32_t base = seg_base[g];
         uint32_t a = threadIdx.x * J;
         Xyzz<F> acc = a < ns ? ld_xyzz<F>(partials, base + a) : Xyzz<F>::identity();
