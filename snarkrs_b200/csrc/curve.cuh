@@ -93,7 +93,7 @@ __device__ __forceinline__ Xyzz<F> xyzz_add_affine(const Xyzz<F>& p, const F& x2
     F pp_ = sub(u2, p.x);
     F rr = sub(s2, p.y);
     if (pp_.is_zero()) {
-        if (rr.is_zero()) return xyzz_dbl_affine<F, INL>(x2, y2);
+        if (rr.is_zero()) return xyzz_dbl_affine<F, false>(x2, y2);   // rare: keep it out of the hot code
         return Xyzz<F>::identity();
     }
     F pp = fsqr<INL>(pp_);
@@ -119,7 +119,7 @@ __device__ __forceinline__ Xyzz<F> xyzz_add(const Xyzz<F>& p, const Xyzz<F>& q) 
     F pp_ = sub(u2, u1);
     F rr = sub(s2, s1);
     if (pp_.is_zero()) {
-        if (rr.is_zero()) return xyzz_dbl<F, INL>(p);
+        if (rr.is_zero()) return xyzz_dbl<F, false>(p);   // rare: keep it out of the hot code
         return Xyzz<F>::identity();
     }
     F pp = fsqr<INL>(pp_);

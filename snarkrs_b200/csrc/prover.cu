@@ -162,8 +162,10 @@ struct g16_circuit {
     uint8_t* h_win = nullptr;   // pinned, 5 * 32 windows * 256 B
     unsigned long long* h_work = nullptr;   // pinned, mixed additions per MSM
     uint64_t readback_bytes = 0;            // device-to-host bytes of the last proof
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;   // gather -> NTT -> H MSM, and the join
+    cudaStream_t s2 = nullptr, s3 = nullptr;   // witness MSMs: A, L on s2; B1, B2 on s3
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_sort = nullptr, ev_s2 = nullptr, ev_s3 = nullptr;
     std::mutex mu;
     g16_stage_timings t = {0, 0, 0, 0, 0, 0};
     uint64_t device_bytes = 0;
@@ -318,41 +320,72 @@ int run_h(g16_circuit* c, const void* d_w, void* h_out) {
     return G16_OK;
 }
 
-// stages 5-9: five MSMs, window sums read back, Horner on the host
-int run_msms(g16_circuit* c, const void* d_w, const void* d_h, MsmJac& out) {
-    cudaStream_t st = c->stream;
-    const uint32_t nh = c->n * (uint32_t)msm_windows(c->c_h), nw = c->n_vars * (uint32_t)msm_windows(c->c_w);
-    CK(msm_sort(c->sort_h, d_h, c->n, true, c->c_h, st, true), "H sort");
-    CK(msm_accumulate_g1(c->sort_h, c->acc[4], c->t_h, 0, nh, st), "H accumulate");
-    CK(msm_sort(c->sort_w, d_w, c->n_vars, true, c->c_w, st, true), "witness sort");
-    CK(msm_accumulate_g1(c->sort_w, c->acc[0], c->t_a, 0, nw, st), "A accumulate");
-    CK(msm_accumulate_g1(c->sort_w, c->acc[2], c->t_b1, 0, nw, st), "B1 accumulate");
-    CK(msm_accumulate_g1(c->sort_w, c->acc[3], c->t_l, 0, nw, st), "L accumulate");
-    CK(msm_accumulate_g2(c->sort_w, c->acc[1], c->t_b2, 0, nw, st), "B2 accumulate");
-    // readback: slot i holds up to 32 windows of 256 bytes
-    const size_t slot = 32 * 256;
-    c->readback_bytes = 0;
-    for (int i = 0; i < 5; i++) {
+// Stages 5-9.  The witness sort and the A, B1, L, B2 accumulations depend only
+// on the witness, so they run on two side streams (ordered after the witness
+// upload) while the main stream does gather -> NTT -> H sort -> H accumulate;
+// the main stream joins them before the window sums are read back.
+constexpr size_t WIN_SLOT = 32 * 256;
+
+int enqueue_witness_msms(g16_circuit* c, const void* d_w) {
+    const uint32_t nw = c->n_vars * (uint32_t)msm_windows(c->c_w);
+    CK(cudaEventRecord(c->ev_fork, c->stream), "event");
+    CK(cudaStreamWaitEvent(c->s2, c->ev_fork, 0), "stream wait");
+    CK(msm_sort(c->sort_w, d_w, c->n_vars, true, c->c_w, c->s2, true), "witness sort");
+    CK(cudaEventRecord(c->ev_sort, c->s2), "event");
+    CK(cudaStreamWaitEvent(c->s3, c->ev_sort, 0), "stream wait");
+    CK(msm_accumulate_g1(c->sort_w, c->acc[0], c->t_a, 0, nw, c->s2), "A accumulate");
+    CK(msm_accumulate_g1(c->sort_w, c->acc[2], c->t_b1, 0, nw, c->s3), "B1 accumulate");
+    CK(msm_accumulate_g1(c->sort_w, c->acc[3], c->t_l, 0, nw, c->s2), "L accumulate");
+    CK(msm_accumulate_g2(c->sort_w, c->acc[1], c->t_b2, 0, nw, c->s3), "B2 accumulate");
+    for (int i = 0; i < 4; i++) {
+        cudaStream_t st = (i == 0 || i == 3) ? c->s2 : c->s3;
         size_t bytes = i == 1 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES;   // one shared window per MSM
-        CK(cudaMemcpyAsync(c->h_win + i * slot, c->acc[i].d_windows, bytes, cudaMemcpyDeviceToHost, st),
+        CK(cudaMemcpyAsync(c->h_win + i * WIN_SLOT, c->acc[i].d_windows, bytes, cudaMemcpyDeviceToHost, st),
            "window readback");
-        c->readback_bytes += bytes;
         if (timer().enabled)
             CK(cudaMemcpyAsync(c->h_work + i, c->acc[i].d_work, 8, cudaMemcpyDeviceToHost, st), "work readback");
     }
+    CK(cudaEventRecord(c->ev_s2, c->s2), "event");
+    CK(cudaEventRecord(c->ev_s3, c->s3), "event");
+    return G16_OK;
+}
+
+int enqueue_h_msm(g16_circuit* c, const void* d_h) {
+    cudaStream_t st = c->stream;
+    const uint32_t nh = c->n * (uint32_t)msm_windows(c->c_h);
+    CK(msm_sort(c->sort_h, d_h, c->n, true, c->c_h, st, true), "H sort");
+    CK(msm_accumulate_g1(c->sort_h, c->acc[4], c->t_h, 0, nh, st), "H accumulate");
+    CK(cudaMemcpyAsync(c->h_win + 4 * WIN_SLOT, c->acc[4].d_windows, XYZZ_G1_BYTES, cudaMemcpyDeviceToHost, st),
+       "window readback");
+    if (timer().enabled) CK(cudaMemcpyAsync(c->h_work + 4, c->acc[4].d_work, 8, cudaMemcpyDeviceToHost, st), "work readback");
+    return G16_OK;
+}
+
+int finish_msms(g16_circuit* c, MsmJac& out) {
+    cudaStream_t st = c->stream;
+    CK(cudaStreamWaitEvent(st, c->ev_s2, 0), "stream wait");
+    CK(cudaStreamWaitEvent(st, c->ev_s3, 0), "stream wait");
     CK(cudaEventRecord(c->ev[3], st), "event");
     CK(cudaStreamSynchronize(st), "MSM stages");
     timer().collect();
+    c->readback_bytes = 3 * XYZZ_G1_BYTES + XYZZ_G2_BYTES + XYZZ_G1_BYTES;
     if (timer().enabled) {
         timer().add_units("msm_accumulate_g1", (double)(c->h_work[0] + c->h_work[2] + c->h_work[3] + c->h_work[4]));
         timer().add_units("msm_accumulate_g2", (double)c->h_work[1]);
     }
-    out.a = msm_combine_g1(c->h_win + 0 * slot, 1, c->c_w);
-    out.b2 = msm_combine_g2(c->h_win + 1 * slot, 1, c->c_w);
-    out.b1 = msm_combine_g1(c->h_win + 2 * slot, 1, c->c_w);
-    out.l = msm_combine_g1(c->h_win + 3 * slot, 1, c->c_w);
-    out.h = msm_combine_g1(c->h_win + 4 * slot, 1, c->c_h);
+    out.a = msm_combine_g1(c->h_win + 0 * WIN_SLOT, 1, c->c_w);
+    out.b2 = msm_combine_g2(c->h_win + 1 * WIN_SLOT, 1, c->c_w);
+    out.b1 = msm_combine_g1(c->h_win + 2 * WIN_SLOT, 1, c->c_w);
+    out.l = msm_combine_g1(c->h_win + 3 * WIN_SLOT, 1, c->c_w);
+    out.h = msm_combine_g1(c->h_win + 4 * WIN_SLOT, 1, c->c_h);
     return G16_OK;
+}
+
+int run_msms(g16_circuit* c, const void* d_w, const void* d_h, MsmJac& out) {
+    int rc = enqueue_witness_msms(c, d_w);
+    if (rc == G16_OK) rc = enqueue_h_msm(c, d_h);
+    if (rc == G16_OK) rc = finish_msms(c, out);
+    return rc;
 }
 
 int prove_on_device(g16_circuit* c, const void* d_w, const uint8_t* r_mont, const uint8_t* s_mont, g16_proof* out) {
@@ -362,9 +395,11 @@ int prove_on_device(g16_circuit* c, const void* d_w, const uint8_t* r_mont, cons
     std::memcpy(ss, s_mont, 32);
     if (!g16::Fr::canonical(rr) || !g16::Fr::canonical(ss)) return fail(G16_ERR_INVALID_ARGUMENT, "r or s not below r");
     auto terms = std::async(std::launch::async, [&] { return blinder_terms(c, r, s); });
-    int rc = run_h(c, d_w, c->d_hpoly);
+    int rc = enqueue_witness_msms(c, d_w);
+    if (rc == G16_OK) rc = run_h(c, d_w, c->d_hpoly);
+    if (rc == G16_OK) rc = enqueue_h_msm(c, c->d_hpoly);
     MsmJac m;
-    if (rc == G16_OK) rc = run_msms(c, d_w, c->d_hpoly, m);
+    if (rc == G16_OK) rc = finish_msms(c, m);
     BlinderTerms t = terms.get();
     if (rc != G16_OK) return rc;
     auto t0 = std::chrono::steady_clock::now();
@@ -526,7 +561,11 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
     if (c->alpha1.inf || c->beta1.inf || c->delta1.inf || c->beta2.inf || c->delta2.inf)
         return fail(G16_ERR_BACKEND, "a header point is the point at infinity");
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+    CK(cudaStreamCreateWithFlags(&c->s2, cudaStreamNonBlocking), "stream");
+    CK(cudaStreamCreateWithFlags(&c->s3, cudaStreamNonBlocking), "stream");
     for (auto& e : c->ev) CK(cudaEventCreate(&e), "event");
+    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_sort, &c->ev_s2, &c->ev_s3})
+        CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "event");
     struct Up {
         void** dst;
         const void* src;
@@ -597,7 +636,8 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
 void g16_circuit_free(g16_circuit* c) {
     if (!c) return;
     cudaSetDevice(c->be->ordinal);
-    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (cudaStream_t s : {c->stream, c->s2, c->s3})
+        if (s) cudaStreamSynchronize(s);
     for (void* p : c->allocs) cudaFree(p);
     c->be->vram_used -= std::min<uint64_t>(c->be->vram_used, c->device_bytes);
     c->ntt.release();
@@ -608,6 +648,10 @@ void g16_circuit_free(g16_circuit* c) {
     if (c->h_work) cudaFreeHost(c->h_work);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {c->ev_fork, c->ev_sort, c->ev_s2, c->ev_s3})
+        if (e) cudaEventDestroy(e);
+    if (c->s2) cudaStreamDestroy(c->s2);
+    if (c->s3) cudaStreamDestroy(c->s3);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
