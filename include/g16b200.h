@@ -189,6 +189,10 @@ void g16_kernel_timing_reset(void);
 size_t g16_kernel_timing_report(char *buf, size_t len);
 /* Kernels launched by this library since load (every launch site counts). */
 uint64_t g16_launch_count(void);
+/* serial != 0 runs every stage of this circuit's proofs on one stream (no
+ * overlap), so per-kernel event times do not include concurrent work: for
+ * profiling.  Results are identical either way. */
+int g16_circuit_set_serial(g16_circuit *c, int serial);
 /* Device-to-host bytes the last proof on this circuit read back. */
 uint64_t g16_circuit_readback_bytes(const g16_circuit *c);
 /* Measured issue rate of 32-bit mad.lo/mad.hi on this device (per second):

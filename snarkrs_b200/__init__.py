@@ -337,6 +337,10 @@ class CudaCircuit:
                                                    bytes(r_mont), bytes(s_mont), ctypes.byref(p)))
         return Proof(p.a, p.b, p.c)
 
+    def set_serial(self, serial=True):
+        """Run every stage on one stream (profiling); results are identical."""
+        check(lib().g16_circuit_set_serial(self._h, int(bool(serial))))
+
     def readback_bytes(self):
         lib().g16_circuit_readback_bytes.restype = ctypes.c_uint64
         return lib().g16_circuit_readback_bytes(self._h)

@@ -164,6 +164,7 @@ struct g16_circuit {
     uint64_t readback_bytes = 0;            // device-to-host bytes of the last proof
     cudaStream_t stream = nullptr;   // gather -> NTT -> H MSM, and the join
     cudaStream_t s2 = nullptr, s3 = nullptr;   // witness MSMs: A, L on s2; B1, B2 on s3
+    bool serial = false;                        // everything on `stream` (profiling)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_sort = nullptr, ev_s2 = nullptr, ev_s3 = nullptr;
     std::mutex mu;
@@ -328,25 +329,26 @@ constexpr size_t WIN_SLOT = 32 * 256;
 
 int enqueue_witness_msms(g16_circuit* c, const void* d_w) {
     const uint32_t nw = c->n_vars * (uint32_t)msm_windows(c->c_w);
+    cudaStream_t s2 = c->serial ? c->stream : c->s2, s3 = c->serial ? c->stream : c->s3;
     CK(cudaEventRecord(c->ev_fork, c->stream), "event");
-    CK(cudaStreamWaitEvent(c->s2, c->ev_fork, 0), "stream wait");
-    CK(msm_sort(c->sort_w, d_w, c->n_vars, true, c->c_w, c->s2, true), "witness sort");
-    CK(cudaEventRecord(c->ev_sort, c->s2), "event");
-    CK(cudaStreamWaitEvent(c->s3, c->ev_sort, 0), "stream wait");
-    CK(msm_accumulate_g1(c->sort_w, c->acc[0], c->t_a, 0, nw, c->s2), "A accumulate");
-    CK(msm_accumulate_g1(c->sort_w, c->acc[2], c->t_b1, 0, nw, c->s3), "B1 accumulate");
-    CK(msm_accumulate_g1(c->sort_w, c->acc[3], c->t_l, 0, nw, c->s2), "L accumulate");
-    CK(msm_accumulate_g2(c->sort_w, c->acc[1], c->t_b2, 0, nw, c->s3), "B2 accumulate");
+    CK(cudaStreamWaitEvent(s2, c->ev_fork, 0), "stream wait");
+    CK(msm_sort(c->sort_w, d_w, c->n_vars, true, c->c_w, s2, true), "witness sort");
+    CK(cudaEventRecord(c->ev_sort, s2), "event");
+    CK(cudaStreamWaitEvent(s3, c->ev_sort, 0), "stream wait");
+    CK(msm_accumulate_g1(c->sort_w, c->acc[0], c->t_a, 0, nw, s2), "A accumulate");
+    CK(msm_accumulate_g1(c->sort_w, c->acc[2], c->t_b1, 0, nw, s3), "B1 accumulate");
+    CK(msm_accumulate_g1(c->sort_w, c->acc[3], c->t_l, 0, nw, s2), "L accumulate");
+    CK(msm_accumulate_g2(c->sort_w, c->acc[1], c->t_b2, 0, nw, s3), "B2 accumulate");
     for (int i = 0; i < 4; i++) {
-        cudaStream_t st = (i == 0 || i == 3) ? c->s2 : c->s3;
+        cudaStream_t st = (i == 0 || i == 3) ? s2 : s3;
         size_t bytes = i == 1 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES;   // one shared window per MSM
         CK(cudaMemcpyAsync(c->h_win + i * WIN_SLOT, c->acc[i].d_windows, bytes, cudaMemcpyDeviceToHost, st),
            "window readback");
         if (timer().enabled)
             CK(cudaMemcpyAsync(c->h_work + i, c->acc[i].d_work, 8, cudaMemcpyDeviceToHost, st), "work readback");
     }
-    CK(cudaEventRecord(c->ev_s2, c->s2), "event");
-    CK(cudaEventRecord(c->ev_s3, c->s3), "event");
+    CK(cudaEventRecord(c->ev_s2, s2), "event");
+    CK(cudaEventRecord(c->ev_s3, s3), "event");
     return G16_OK;
 }
 
@@ -938,6 +940,13 @@ size_t g16_kernel_timing_report(char* buf, size_t len) {
 uint64_t g16_launch_count(void) { return timer().launches.load(); }
 
 uint64_t g16_circuit_readback_bytes(const g16_circuit* c) { return c ? c->readback_bytes : 0; }
+
+int g16_circuit_set_serial(g16_circuit* c, int serial) {
+    if (!c) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> g(c->mu);
+    c->serial = serial != 0;
+    return G16_OK;
+}
 
 int g16_imad_peak(g16_backend* b, double* imad_per_s) {
     if (!b || !imad_per_s) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
