@@ -174,6 +174,21 @@ int g16_msm_g1_device(g16_backend *b, const void *d_bases, const void *d_scalars
 int g16_msm_g2_device(g16_backend *b, const void *d_bases, const void *d_scalars, size_t n, int scalars_form,
                       uint8_t *out128);
 
+/* A G1 MSM that allocates no memory -- no counterpart in the reference.
+ * For callers that cannot call cudaMalloc: their device memory belongs to
+ * another allocator, or an allocation (and its implicit device
+ * synchronisation) is not acceptable in their request path.  Same result as
+ * g16_msm_g1_device, computed inside one fixed scratch array (about 12 MiB)
+ * that is part of the library image and that every GPU which loads the
+ * library holds until the process exits.  At most 16384 points (larger n is
+ * refused with G16_ERR_INVALID_ARGUMENT); runs on `device`'s legacy default
+ * stream and returns with the result on the host.  The first call on a device
+ * looks up the array's address (make it before any stream capture).  All
+ * calls share the array: calls whose device work overlaps race and must be
+ * serialised by the caller.  Kernel timing must be off. */
+int g16_msm_g1_device_noalloc(int device, const void *d_bases, const void *d_scalars, size_t n, int scalars_form,
+                              uint8_t *out64);
+
 /* ---------------- NTT (CpuNtt API, crates/ntt/src/lib.rs:415-584) ---------------- */
 /* In place on 2^log_n Montgomery Fr in host memory.  shift_mont is the coset
  * shift for the COSET modes (NULL = the proving coset shift omega_2n). */

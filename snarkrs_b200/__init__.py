@@ -366,6 +366,7 @@ class CudaBackend:
     """Backend (crates/groth16/src/lib.rs:371-380) over one B200: name() and prepare()."""
 
     def __init__(self, ordinal=0, vram_limit=0):
+        self.ordinal = int(ordinal)
         h = ctypes.c_void_p()
         check(lib().g16_backend_open(int(ordinal), ctypes.c_uint64(vram_limit), ctypes.byref(h)))
         self._h = h
@@ -451,6 +452,13 @@ class CudaMsm:
         out = ctypes.create_string_buffer(64)
         check(lib().g16_msm_g1_device(self.backend._h, ctypes.c_void_p(d_bases), ctypes.c_void_p(d_scalars),
                                       ctypes.c_size_t(n), int(form), out))
+        return out.raw
+
+    def msm_g1_device_noalloc(self, d_bases, d_scalars, n, form=SCALARS_STANDARD):
+        """G1 MSM that allocates nothing (fixed library scratch, at most 16384 points)."""
+        out = ctypes.create_string_buffer(64)
+        check(lib().g16_msm_g1_device_noalloc(ctypes.c_int(self.backend.ordinal), ctypes.c_void_p(d_bases),
+                                              ctypes.c_void_p(d_scalars), ctypes.c_size_t(n), int(form), out))
         return out.raw
 
     def msm_g2_device(self, d_bases, d_scalars, n, form=SCALARS_STANDARD):

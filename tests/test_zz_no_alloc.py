@@ -1,0 +1,64 @@
+"""The allocation-free G1 MSM entry point (g16_msm_g1_device_noalloc).
+
+Some callers of this library cannot call cudaMalloc, because their device
+memory belongs to another allocator or because an allocation in their request
+path is not acceptable.  For them the library offers one MSM that runs inside a
+fixed scratch array built into the library.  This file checks, through the C
+ABI, that it returns exactly what the allocating entry point returns: on two
+calls in a row (the second sees the first call's leftovers in the shared
+scratch), at the largest size it accepts, and that it refuses a larger input.
+It sorts last so that a failure here leaves every other test already run.
+"""
+import ctypes
+
+import pytest
+
+import snarkrs_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+MAX_POINTS = 16384
+
+
+def _on_device(backend, data):
+    d = backend.alloc(len(data))
+    backend.upload(d, data)
+    return d
+
+
+def _noalloc(device, d_bases, d_scalars, n, form=S.SCALARS_STANDARD):
+    out = ctypes.create_string_buffer(64)
+    rc = S.lib().g16_msm_g1_device_noalloc(ctypes.c_int(device), ctypes.c_void_p(d_bases),
+                                           ctypes.c_void_p(d_scalars), ctypes.c_size_t(n), ctypes.c_int(form), out)
+    return rc, out.raw
+
+
+def test_noalloc_msm_matches_the_allocating_entry_point():
+    backend = S.CudaBackend(0)
+    msm = S.CudaMsm(backend)
+    buffers = []
+    try:
+        cases = [(1000, 0), (MAX_POINTS, 1), (MAX_POINTS, 0), (37, 1)]
+        for n, dist in cases:
+            bases = S.synth_points(1, 900 + n + dist, n)
+            scal = S.synth_scalars(901 + n + dist, n, dist)
+            db, ds = _on_device(backend, bases), _on_device(backend, scal)
+            buffers += [db, ds]
+            want = msm.msm_g1_device(db, ds, n)
+            for _ in range(2):          # two calls in a row on the shared scratch
+                rc, got = _noalloc(backend.ordinal, db, ds, n)
+                assert rc == S.G16_OK, S.last_error()
+                assert got == want
+        # Montgomery-form scalars through both entry points
+        n = 512
+        rc, got = _noalloc(backend.ordinal, buffers[0], buffers[1], n, S.SCALARS_MONTGOMERY)
+        assert rc == S.G16_OK, S.last_error()
+        assert got == msm.msm_g1_device(buffers[0], buffers[1], n, S.SCALARS_MONTGOMERY)
+        # beyond the fixed scratch: refused, nothing launched
+        rc, _ = _noalloc(backend.ordinal, buffers[2], buffers[3], MAX_POINTS + 1)
+        assert rc == S.InvalidArgumentError.code
+        assert "16384" in S.last_error()
+    finally:
+        for d in buffers:
+            backend.free(d)
+        backend.close()
