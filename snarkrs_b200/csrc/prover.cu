@@ -14,10 +14,14 @@
 #include <atomic>
 #include <cstdarg>
 #include <chrono>
+#include <condition_variable>
+#include <cstdlib>
+#include <cstring>
 #include <future>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 #include "common.cuh"
 #include "curve.cuh"
@@ -139,6 +143,68 @@ struct g16_backend {
     unsigned long long* h_work = nullptr;
 };
 
+namespace {
+
+// The device state of one proof in flight.  A prepared circuit keeps a pool of
+// these, so several proofs of the same circuit overlap on the GPU, each on its
+// own three streams with its own scratch.
+struct Workspace {
+    void* d_w = nullptr;       // witness, n_vars Fr
+    void* d_abc = nullptr;     // A | B | C, n Fr each
+    void* d_hpoly = nullptr;   // H, n Fr
+    MsmSort sort_w, sort_h;
+    MsmAccum acc[5];           // A, B2, B1, L, H
+    uint8_t* h_win = nullptr;  // pinned readback of the MSM results
+    unsigned long long* h_work = nullptr;
+    cudaStream_t stream = nullptr;             // gather -> NTT -> H MSM, and the join
+    cudaStream_t s2 = nullptr, s3 = nullptr;   // witness MSMs: A, L on s2; B1, B2 on s3
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_sort = nullptr, ev_s2 = nullptr, ev_s3 = nullptr;
+    cudaGraphExec_t graph = nullptr;   // stages 0-9 captured once, replayed per proof
+    uint64_t graph_kernels = 0;
+    uint64_t proofs = 0;
+    uint64_t bytes = 0;                // fixed device buffers
+
+    cudaError_t init(uint32_t n_vars, uint32_t n) {
+        cudaError_t e = cudaMalloc(&d_w, 32ull * n_vars);
+        if (e == cudaSuccess) e = cudaMalloc(&d_abc, 32ull * n * 3);
+        if (e == cudaSuccess) e = cudaMalloc(&d_hpoly, 32ull * n);
+        if (e == cudaSuccess) e = cudaMallocHost((void**)&h_win, 5 * 32 * 256);
+        if (e == cudaSuccess) e = cudaMallocHost((void**)&h_work, 8 * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s3, cudaStreamNonBlocking);
+        for (auto& x : ev)
+            if (e == cudaSuccess) e = cudaEventCreate(&x);
+        for (cudaEvent_t* x : {&ev_fork, &ev_sort, &ev_s2, &ev_s3})
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(x, cudaEventDisableTiming);
+        bytes = 32ull * n_vars + 32ull * n * 4;
+        return e;
+    }
+    void release() {
+        for (cudaStream_t s : {stream, s2, s3})
+            if (s) cudaStreamSynchronize(s);
+        if (graph) cudaGraphExecDestroy(graph);
+        cudaFree(d_w);
+        cudaFree(d_abc);
+        cudaFree(d_hpoly);
+        sort_w.release();
+        sort_h.release();
+        for (auto& a : acc) a.release();
+        if (h_win) cudaFreeHost(h_win);
+        if (h_work) cudaFreeHost(h_work);
+        for (auto& x : ev)
+            if (x) cudaEventDestroy(x);
+        for (cudaEvent_t x : {ev_fork, ev_sort, ev_s2, ev_s3})
+            if (x) cudaEventDestroy(x);
+        for (cudaStream_t s : {s2, s3, stream})
+            if (s) cudaStreamDestroy(s);
+        *this = Workspace();
+    }
+};
+
+}  // namespace
+
 struct g16_circuit {
     g16_backend* be = nullptr;
     uint32_t n_vars = 0, n_public = 0, n = 0;
@@ -153,22 +219,17 @@ struct g16_circuit {
     NttTables ntt;
     G1A alpha1, beta1, delta1;
     G2A beta2, delta2;
-    // per-proof scratch
-    void* d_w = nullptr;
-    void* d_abc = nullptr;   // A | B | C, n each
-    void* d_hpoly = nullptr;
-    MsmSort sort_w, sort_h;
-    MsmAccum acc[5];
-    uint8_t* h_win = nullptr;   // pinned, 5 * 32 windows * 256 B
-    unsigned long long* h_work = nullptr;   // pinned, mixed additions per MSM
-    uint64_t readback_bytes = 0;            // device-to-host bytes of the last proof
-    cudaStream_t stream = nullptr;   // gather -> NTT -> H MSM, and the join
-    cudaStream_t s2 = nullptr, s3 = nullptr;   // witness MSMs: A, L on s2; B1, B2 on s3
-    bool serial = false;                        // everything on `stream` (profiling)
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaEvent_t ev_fork = nullptr, ev_sort = nullptr, ev_s2 = nullptr, ev_s3 = nullptr;
+    // workspaces: one per proof in flight
     std::mutex mu;
+    std::condition_variable cv;
+    std::vector<std::unique_ptr<Workspace>> pool;
+    std::vector<Workspace*> idle;
+    uint32_t max_workspaces = 8;
+    uint64_t ws_estimate = 0;          // device bytes of one workspace, scratch included
+    bool serial = false;               // every stage on one stream (profiling)
+    bool graphs = true;                // replay proofs as captured CUDA graphs
     g16_stage_timings t = {0, 0, 0, 0, 0, 0};
+    uint64_t readback_bytes = 0;       // device-to-host bytes of the last proof
     uint64_t device_bytes = 0;
     std::vector<void*> allocs;
 };
@@ -221,14 +282,56 @@ cudaError_t circuit_alloc(g16_circuit* c, void** p, size_t bytes) {
     return e;
 }
 
+// Take an idle workspace, or build one while the pool is below its cap and the
+// backend's device-memory budget has room; otherwise wait for one to come back.
+int acquire(g16_circuit* c, Workspace** out) {
+    std::unique_lock<std::mutex> lk(c->mu);
+    for (;;) {
+        if (!c->idle.empty()) {
+            *out = c->idle.back();
+            c->idle.pop_back();
+            return G16_OK;
+        }
+        bool room = c->be->vram_used + c->ws_estimate <= c->be->vram_limit;
+        if (c->pool.size() < c->max_workspaces && (room || c->pool.empty())) {
+            auto ws = std::make_unique<Workspace>();
+            cudaError_t e = ws->init(c->n_vars, c->n);
+            if (e == cudaSuccess) {
+                c->device_bytes += c->ws_estimate;
+                c->be->vram_used += c->ws_estimate;
+                *out = ws.get();
+                c->pool.push_back(std::move(ws));
+                return G16_OK;
+            }
+            ws->release();
+            cudaGetLastError();
+            if (c->pool.empty()) return cuda_fail(e, "workspace allocation");
+            c->max_workspaces = (uint32_t)c->pool.size();   // out of memory: stop growing the pool
+        }
+        c->cv.wait(lk);
+    }
+}
+
+void release(g16_circuit* c, Workspace* ws) {
+    {
+        std::lock_guard<std::mutex> g(c->mu);
+        c->idle.push_back(ws);
+    }
+    c->cv.notify_one();
+}
+
+struct WsGuard {
+    g16_circuit* c;
+    Workspace* ws = nullptr;
+    explicit WsGuard(g16_circuit* cc) : c(cc) {}
+    ~WsGuard() {
+        if (ws) release(c, ws);
+    }
+};
+
 bool is_one_mont(const uint8_t* w0) {
     host_init();
     return std::memcmp(w0, FR_P.one.v, 32) == 0;
-}
-
-template <class A>
-bool unpack_checked(A& a, const uint8_t* p) {
-    return unpack(a, p);
 }
 
 // r * P for a standard-form scalar given as Montgomery Fr
@@ -303,11 +406,11 @@ uint64_t elapsed_us(cudaEvent_t a, cudaEvent_t b) {
 }
 
 // stages 0-4 on the device witness; H left in h_out (device)
-int run_h(g16_circuit* c, const void* d_w, void* h_out) {
-    cudaStream_t st = c->stream;
-    uint8_t* abc = (uint8_t*)c->d_abc;
+int run_h(g16_circuit* c, Workspace* ws, const void* d_w, void* h_out) {
+    cudaStream_t st = ws->stream;
+    uint8_t* abc = (uint8_t*)ws->d_abc;
     size_t vb = (size_t)c->n * 32;
-    CK(cudaEventRecord(c->ev[0], st), "event");
+    CK(cudaEventRecord(ws->ev[0], st), "event");
     {
         TimedLaunch tl("gather", st);
         g16d::k_gather<<<blocks_for(c->n, 256), 256, 0, st>>>(
@@ -315,107 +418,158 @@ int run_h(g16_circuit* c, const void* d_w, void* h_out) {
             (const uint4*)d_w, c->n, (uint4*)abc, (uint4*)(abc + vb), (uint4*)(abc + 2 * vb));
     }
     CK(cudaGetLastError(), "gather launch");
-    CK(cudaEventRecord(c->ev[1], st), "event");
+    CK(cudaEventRecord(ws->ev[1], st), "event");
     CK(ntt_h_pipeline(c->ntt, abc, abc + vb, abc + 2 * vb, h_out, st), "NTT pipeline");
-    CK(cudaEventRecord(c->ev[2], st), "event");
+    CK(cudaEventRecord(ws->ev[2], st), "event");
     return G16_OK;
 }
 
 // Stages 5-9.  The witness sort and the A, B1, L, B2 accumulations depend only
 // on the witness, so they run on two side streams (ordered after the witness
 // upload) while the main stream does gather -> NTT -> H sort -> H accumulate;
-// the main stream joins them before the window sums are read back.
+// the main stream joins them before the results are read back.
 constexpr size_t WIN_SLOT = 32 * 256;
 
-int enqueue_witness_msms(g16_circuit* c, const void* d_w) {
+int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
     const uint32_t nw = c->n_vars * (uint32_t)msm_windows(c->c_w);
-    cudaStream_t s2 = c->serial ? c->stream : c->s2, s3 = c->serial ? c->stream : c->s3;
-    CK(cudaEventRecord(c->ev_fork, c->stream), "event");
-    CK(cudaStreamWaitEvent(s2, c->ev_fork, 0), "stream wait");
-    CK(msm_sort(c->sort_w, d_w, c->n_vars, true, c->c_w, s2, true), "witness sort");
-    CK(cudaEventRecord(c->ev_sort, s2), "event");
-    CK(cudaStreamWaitEvent(s3, c->ev_sort, 0), "stream wait");
-    CK(msm_accumulate_g1(c->sort_w, c->acc[0], c->t_a, 0, nw, s2), "A accumulate");
-    CK(msm_accumulate_g1(c->sort_w, c->acc[2], c->t_b1, 0, nw, s3), "B1 accumulate");
-    CK(msm_accumulate_g1(c->sort_w, c->acc[3], c->t_l, 0, nw, s2), "L accumulate");
-    CK(msm_accumulate_g2(c->sort_w, c->acc[1], c->t_b2, 0, nw, s3), "B2 accumulate");
+    cudaStream_t s2 = c->serial ? ws->stream : ws->s2, s3 = c->serial ? ws->stream : ws->s3;
+    CK(cudaEventRecord(ws->ev_fork, ws->stream), "event");
+    CK(cudaStreamWaitEvent(s2, ws->ev_fork, 0), "stream wait");
+    CK(msm_sort(ws->sort_w, d_w, c->n_vars, true, c->c_w, s2, true), "witness sort");
+    CK(cudaEventRecord(ws->ev_sort, s2), "event");
+    CK(cudaStreamWaitEvent(s3, ws->ev_sort, 0), "stream wait");
+    CK(msm_accumulate_g1(ws->sort_w, ws->acc[0], c->t_a, 0, nw, s2), "A accumulate");
+    CK(msm_accumulate_g1(ws->sort_w, ws->acc[2], c->t_b1, 0, nw, s3), "B1 accumulate");
+    CK(msm_accumulate_g1(ws->sort_w, ws->acc[3], c->t_l, 0, nw, s2), "L accumulate");
+    CK(msm_accumulate_g2(ws->sort_w, ws->acc[1], c->t_b2, 0, nw, s3), "B2 accumulate");
     for (int i = 0; i < 4; i++) {
         cudaStream_t st = (i == 0 || i == 3) ? s2 : s3;
         size_t bytes = i == 1 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES;   // one shared window per MSM
-        CK(cudaMemcpyAsync(c->h_win + i * WIN_SLOT, c->acc[i].d_windows, bytes, cudaMemcpyDeviceToHost, st),
+        CK(cudaMemcpyAsync(ws->h_win + i * WIN_SLOT, ws->acc[i].d_windows, bytes, cudaMemcpyDeviceToHost, st),
            "window readback");
         if (timer().enabled)
-            CK(cudaMemcpyAsync(c->h_work + i, c->acc[i].d_work, 8, cudaMemcpyDeviceToHost, st), "work readback");
+            CK(cudaMemcpyAsync(ws->h_work + i, ws->acc[i].d_work, 8, cudaMemcpyDeviceToHost, st), "work readback");
     }
-    CK(cudaEventRecord(c->ev_s2, s2), "event");
-    CK(cudaEventRecord(c->ev_s3, s3), "event");
+    CK(cudaEventRecord(ws->ev_s2, s2), "event");
+    CK(cudaEventRecord(ws->ev_s3, s3), "event");
     return G16_OK;
 }
 
-int enqueue_h_msm(g16_circuit* c, const void* d_h) {
-    cudaStream_t st = c->stream;
+int enqueue_h_msm(g16_circuit* c, Workspace* ws, const void* d_h) {
+    cudaStream_t st = ws->stream;
     const uint32_t nh = c->n * (uint32_t)msm_windows(c->c_h);
-    CK(msm_sort(c->sort_h, d_h, c->n, true, c->c_h, st, true), "H sort");
-    CK(msm_accumulate_g1(c->sort_h, c->acc[4], c->t_h, 0, nh, st), "H accumulate");
-    CK(cudaMemcpyAsync(c->h_win + 4 * WIN_SLOT, c->acc[4].d_windows, XYZZ_G1_BYTES, cudaMemcpyDeviceToHost, st),
+    CK(msm_sort(ws->sort_h, d_h, c->n, true, c->c_h, st, true), "H sort");
+    CK(msm_accumulate_g1(ws->sort_h, ws->acc[4], c->t_h, 0, nh, st), "H accumulate");
+    CK(cudaMemcpyAsync(ws->h_win + 4 * WIN_SLOT, ws->acc[4].d_windows, XYZZ_G1_BYTES, cudaMemcpyDeviceToHost, st),
        "window readback");
-    if (timer().enabled) CK(cudaMemcpyAsync(c->h_work + 4, c->acc[4].d_work, 8, cudaMemcpyDeviceToHost, st), "work readback");
+    if (timer().enabled)
+        CK(cudaMemcpyAsync(ws->h_work + 4, ws->acc[4].d_work, 8, cudaMemcpyDeviceToHost, st), "work readback");
     return G16_OK;
 }
 
-int finish_msms(g16_circuit* c, MsmJac& out) {
-    cudaStream_t st = c->stream;
-    CK(cudaStreamWaitEvent(st, c->ev_s2, 0), "stream wait");
-    CK(cudaStreamWaitEvent(st, c->ev_s3, 0), "stream wait");
-    CK(cudaEventRecord(c->ev[3], st), "event");
-    CK(cudaStreamSynchronize(st), "MSM stages");
+int enqueue_join(Workspace* ws) {
+    CK(cudaStreamWaitEvent(ws->stream, ws->ev_s2, 0), "stream wait");
+    CK(cudaStreamWaitEvent(ws->stream, ws->ev_s3, 0), "stream wait");
+    CK(cudaEventRecord(ws->ev[3], ws->stream), "event");
+    return G16_OK;
+}
+
+int collect_msms(g16_circuit* c, Workspace* ws, MsmJac& out) {
+    CK(cudaStreamSynchronize(ws->stream), "MSM stages");
     timer().collect();
-    c->readback_bytes = 3 * XYZZ_G1_BYTES + XYZZ_G2_BYTES + XYZZ_G1_BYTES;
-    if (timer().enabled) {
-        timer().add_units("msm_accumulate_g1", (double)(c->h_work[0] + c->h_work[2] + c->h_work[3] + c->h_work[4]));
-        timer().add_units("msm_accumulate_g2", (double)c->h_work[1]);
+    {
+        std::lock_guard<std::mutex> g(c->mu);
+        c->readback_bytes = 3 * XYZZ_G1_BYTES + XYZZ_G2_BYTES + XYZZ_G1_BYTES;
     }
-    out.a = msm_combine_g1(c->h_win + 0 * WIN_SLOT, 1, c->c_w);
-    out.b2 = msm_combine_g2(c->h_win + 1 * WIN_SLOT, 1, c->c_w);
-    out.b1 = msm_combine_g1(c->h_win + 2 * WIN_SLOT, 1, c->c_w);
-    out.l = msm_combine_g1(c->h_win + 3 * WIN_SLOT, 1, c->c_w);
-    out.h = msm_combine_g1(c->h_win + 4 * WIN_SLOT, 1, c->c_h);
+    if (timer().enabled) {
+        timer().add_units("msm_accumulate_g1",
+                          (double)(ws->h_work[0] + ws->h_work[2] + ws->h_work[3] + ws->h_work[4]));
+        timer().add_units("msm_accumulate_g2", (double)ws->h_work[1]);
+    }
+    out.a = msm_combine_g1(ws->h_win + 0 * WIN_SLOT, 1, c->c_w);
+    out.b2 = msm_combine_g2(ws->h_win + 1 * WIN_SLOT, 1, c->c_w);
+    out.b1 = msm_combine_g1(ws->h_win + 2 * WIN_SLOT, 1, c->c_w);
+    out.l = msm_combine_g1(ws->h_win + 3 * WIN_SLOT, 1, c->c_w);
+    out.h = msm_combine_g1(ws->h_win + 4 * WIN_SLOT, 1, c->c_h);
     return G16_OK;
 }
 
-int run_msms(g16_circuit* c, const void* d_w, const void* d_h, MsmJac& out) {
-    int rc = enqueue_witness_msms(c, d_w);
-    if (rc == G16_OK) rc = enqueue_h_msm(c, d_h);
-    if (rc == G16_OK) rc = finish_msms(c, out);
+// stages 0-9 for a witness already in device memory, enqueued on ws's streams
+int enqueue_proof(g16_circuit* c, Workspace* ws, const void* d_w) {
+    int rc = enqueue_witness_msms(c, ws, d_w);
+    if (rc == G16_OK) rc = run_h(c, ws, d_w, ws->d_hpoly);
+    if (rc == G16_OK) rc = enqueue_h_msm(c, ws, ws->d_hpoly);
+    if (rc == G16_OK) rc = enqueue_join(ws);
     return rc;
 }
 
-int prove_on_device(g16_circuit* c, const void* d_w, const uint8_t* r_mont, const uint8_t* s_mont, g16_proof* out) {
+// Stages 0-9.  From the second proof on a workspace (when every scratch buffer
+// has reached its size) the whole enqueue sequence is captured once as a CUDA
+// graph over the workspace's three streams and replayed, one launch per proof.
+int run_proof(g16_circuit* c, Workspace* ws, const void* d_w, MsmJac& out) {
+    bool use_graph = c->graphs && !c->serial && !timer().enabled && ws->proofs > 0;
+    if (use_graph) {
+        if (d_w != ws->d_w)
+            CK(cudaMemcpyAsync(ws->d_w, d_w, 32ull * c->n_vars, cudaMemcpyDeviceToDevice, ws->stream), "witness copy");
+        if (!ws->graph) {
+            uint64_t k0 = timer().launches.load();
+            CK(cudaStreamBeginCapture(ws->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+            int rc = enqueue_proof(c, ws, ws->d_w);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(ws->stream, &g);
+            if (rc != G16_OK) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            CK(e, "graph capture");
+            e = cudaGraphInstantiate(&ws->graph, g, 0);
+            cudaGraphDestroy(g);
+            CK(e, "graph instantiate");
+            ws->graph_kernels = timer().launches.load() - k0;
+            timer().launches.fetch_sub(ws->graph_kernels);   // counted when replayed
+        }
+        CK(cudaGraphLaunch(ws->graph, ws->stream), "graph launch");
+        timer().launches.fetch_add(ws->graph_kernels);
+    } else {
+        int rc = enqueue_proof(c, ws, d_w);
+        if (rc != G16_OK) return rc;
+    }
+    int rc = collect_msms(c, ws, out);
+    if (rc == G16_OK) ws->proofs++;
+    return rc;
+}
+
+void add_timings(g16_circuit* c, Workspace* ws, bool h, bool msm, uint64_t assemble_us) {
+    std::lock_guard<std::mutex> g(c->mu);
+    if (h) {
+        c->t.gather_us += elapsed_us(ws->ev[0], ws->ev[1]);
+        c->t.ntt_us += elapsed_us(ws->ev[1], ws->ev[2]);
+    }
+    if (msm) c->t.msm_us += elapsed_us(ws->ev[2], ws->ev[3]);
+    c->t.assemble_us += assemble_us;
+}
+
+int prove_on_device(g16_circuit* c, Workspace* ws, const void* d_w, const uint8_t* r_mont, const uint8_t* s_mont,
+                    g16_proof* out) {
     g16::Fr r = g16::Fr::raw((const uint64_t*)r_mont), s = g16::Fr::raw((const uint64_t*)s_mont);
     uint64_t rr[4], ss[4];
     std::memcpy(rr, r_mont, 32);
     std::memcpy(ss, s_mont, 32);
     if (!g16::Fr::canonical(rr) || !g16::Fr::canonical(ss)) return fail(G16_ERR_INVALID_ARGUMENT, "r or s not below r");
     auto terms = std::async(std::launch::async, [&] { return blinder_terms(c, r, s); });
-    int rc = enqueue_witness_msms(c, d_w);
-    if (rc == G16_OK) rc = run_h(c, d_w, c->d_hpoly);
-    if (rc == G16_OK) rc = enqueue_h_msm(c, c->d_hpoly);
     MsmJac m;
-    if (rc == G16_OK) rc = finish_msms(c, m);
+    int rc = run_proof(c, ws, d_w, m);
     BlinderTerms t = terms.get();
     if (rc != G16_OK) return rc;
     auto t0 = std::chrono::steady_clock::now();
     assemble(c, m, t, r, s, out);
     auto t1 = std::chrono::steady_clock::now();
-    c->t.gather_us += elapsed_us(c->ev[0], c->ev[1]);
-    c->t.ntt_us += elapsed_us(c->ev[1], c->ev[2]);
-    c->t.msm_us += elapsed_us(c->ev[2], c->ev[3]);
-    c->t.assemble_us += (uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(t1 - t0).count();
+    add_timings(c, ws, true, true, (uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(t1 - t0).count());
     return G16_OK;
 }
 
-int upload_witness(g16_circuit* c, const uint8_t* w, size_t n) {
-    CK(cudaMemcpyAsync(c->d_w, w, n * 32, cudaMemcpyHostToDevice, c->stream), "witness upload");
+int upload_witness(Workspace* ws, const uint8_t* w, size_t n) {
+    CK(cudaMemcpyAsync(ws->d_w, w, n * 32, cudaMemcpyHostToDevice, ws->stream), "witness upload");
     return G16_OK;
 }
 
@@ -515,6 +669,7 @@ int g16_wtns_write(const uint8_t* w_mont, size_t n, uint8_t* out, size_t cap, si
     return G16_OK;
 }
 
+
 // ---- prepare ----
 int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
     if (!b || !k || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
@@ -543,31 +698,30 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
     if (nv * Ww >= 0x80000000ull || (uint64_t)n * Wh >= 0x80000000ull)
         return fail(G16_ERR_BACKEND, "circuit too large for 31-bit MSM entry indices");
     key_bytes += nv * Ww * (64 * 3 + 128) + (uint64_t)n * Wh * 64;
-    uint64_t scratch = nv * 32 + (uint64_t)n * 32 * 4 + ((uint64_t)n + nv) * 32 + ((uint64_t)n + nv) * 16 * 4 +
-                       ((uint64_t)n + nv) * 16 / 16 * 256 * 2 + (64ull << 20);
-    if (b->vram_used + key_bytes + scratch > b->vram_limit)
+    // one workspace: witness, A|B|C, H, and the MSM scratch (entries, partials, buckets)
+    const uint64_t Kw = 1ull << (c_w - 1), Kh = 1ull << (c_h - 1);
+    uint64_t ws_bytes = nv * 32 + (uint64_t)n * 32 * 4;
+    ws_bytes += nv * 32 + nv * Ww * 4 + 24 * (Kw + 1) + (uint64_t)n * 32 + (uint64_t)n * Wh * 4 + 24 * (Kh + 1);
+    ws_bytes += 3 * 128 * (Kw * 2 + nv * Ww / 16 + 1) + 256 * (Kw * 2 + nv * Ww / 16 + 1);
+    ws_bytes += 128 * (Kh * 2 + (uint64_t)n * Wh / 16 + 1) + (16ull << 20);
+    if (b->vram_used + key_bytes + ws_bytes > b->vram_limit)
         return fail(G16_ERR_DEVICE_MEMORY, "circuit needs about %llu MiB of device memory, %llu MiB of the %llu MiB budget are free",
-                    (unsigned long long)((key_bytes + scratch) >> 20),
+                    (unsigned long long)((key_bytes + ws_bytes) >> 20),
                     (unsigned long long)((b->vram_limit - std::min<uint64_t>(b->vram_limit, b->vram_used)) >> 20),
                     (unsigned long long)(b->vram_limit >> 20));
-    // header points
     auto c = std::make_unique<g16_circuit>();
     c->be = b;
     c->n_vars = k->n_vars;
     c->n_public = k->n_public;
     c->n = n;
+    c->ws_estimate = ws_bytes;
+    if (const char* g = std::getenv("G16_CUDA_GRAPHS")) c->graphs = std::strcmp(g, "0") != 0;
     while ((1u << c->log_n) < n) c->log_n++;
     if (!unpack(c->alpha1, k->alpha_g1) || !unpack(c->beta1, k->beta_g1) || !unpack(c->delta1, k->delta_g1) ||
         !unpack(c->beta2, k->beta_g2) || !unpack(c->delta2, k->delta_g2))
         return fail(G16_ERR_BACKEND, "non-canonical header point");
     if (c->alpha1.inf || c->beta1.inf || c->delta1.inf || c->beta2.inf || c->delta2.inf)
         return fail(G16_ERR_BACKEND, "a header point is the point at infinity");
-    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
-    CK(cudaStreamCreateWithFlags(&c->s2, cudaStreamNonBlocking), "stream");
-    CK(cudaStreamCreateWithFlags(&c->s3, cudaStreamNonBlocking), "stream");
-    for (auto& e : c->ev) CK(cudaEventCreate(&e), "event");
-    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_sort, &c->ev_s2, &c->ev_s3})
-        CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "event");
     struct Up {
         void** dst;
         const void* src;
@@ -587,23 +741,20 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
         {&c->d_h, k->h_query, 64ull * n},
     };
     g16_circuit* cp = c.get();
+    cudaStream_t st = b->stream;
+    std::lock_guard<std::mutex> bg(b->mu);   // the backend stream does the uploads
     auto cleanup = [&] { g16_circuit_free(c.release()); };
     for (auto& u : ups) {
         cudaError_t e = circuit_alloc(cp, u.dst, u.bytes);
-        if (e == cudaSuccess && u.bytes) e = cudaMemcpyAsync(*u.dst, u.src, u.bytes, cudaMemcpyHostToDevice, cp->stream);
+        if (e == cudaSuccess && u.bytes) e = cudaMemcpyAsync(*u.dst, u.src, u.bytes, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) {
             int rc = cuda_fail(e, "key upload");
             cleanup();
             return rc;
         }
     }
-    cudaError_t e = circuit_alloc(cp, &cp->d_w, 32ull * nv);
-    if (e == cudaSuccess) e = circuit_alloc(cp, &cp->d_abc, 32ull * n * 3);
-    if (e == cudaSuccess) e = circuit_alloc(cp, &cp->d_hpoly, 32ull * n);
-    if (e == cudaSuccess) e = cudaMallocHost((void**)&cp->h_win, 5 * 32 * 256);
-    if (e == cudaSuccess) e = cudaMallocHost((void**)&cp->h_work, 8 * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = ntt_tables(cp->ntt, cp->log_n, cp->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(cp->stream);
+    cudaError_t e = ntt_tables(cp->ntt, cp->log_n, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         int rc = cuda_fail(e, "prepare");
         cleanup();
@@ -619,12 +770,12 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
         if (e2 == cudaSuccess) e2 = circuit_alloc(cp, &cp->t_l, 64ull * nv * Ww);
         if (e2 == cudaSuccess) e2 = circuit_alloc(cp, &cp->t_b2, 128ull * nv * Ww);
         if (e2 == cudaSuccess) e2 = circuit_alloc(cp, &cp->t_h, 64ull * n * Wh);
-        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_a, nv, 0, c_w, cp->t_a, cp->stream);
-        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_b1, nv, 0, c_w, cp->t_b1, cp->stream);
-        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_l, nv, k->n_public + 1, c_w, cp->t_l, cp->stream);
-        if (e2 == cudaSuccess) e2 = msm_window_table_g2(cp->d_b2, nv, 0, c_w, cp->t_b2, cp->stream);
-        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_h, n, 0, c_h, cp->t_h, cp->stream);
-        if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(cp->stream);
+        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_a, nv, 0, c_w, cp->t_a, st);
+        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_b1, nv, 0, c_w, cp->t_b1, st);
+        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_l, nv, k->n_public + 1, c_w, cp->t_l, st);
+        if (e2 == cudaSuccess) e2 = msm_window_table_g2(cp->d_b2, nv, 0, c_w, cp->t_b2, st);
+        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_h, n, 0, c_h, cp->t_h, st);
+        if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(st);
         if (e2 != cudaSuccess) {
             int rc = cuda_fail(e2, "window tables");
             cleanup();
@@ -638,23 +789,12 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
 void g16_circuit_free(g16_circuit* c) {
     if (!c) return;
     cudaSetDevice(c->be->ordinal);
-    for (cudaStream_t s : {c->stream, c->s2, c->s3})
-        if (s) cudaStreamSynchronize(s);
+    for (auto& ws : c->pool) ws->release();
+    c->pool.clear();
+    c->idle.clear();
     for (void* p : c->allocs) cudaFree(p);
     c->be->vram_used -= std::min<uint64_t>(c->be->vram_used, c->device_bytes);
     c->ntt.release();
-    c->sort_w.release();
-    c->sort_h.release();
-    for (auto& a : c->acc) a.release();
-    if (c->h_win) cudaFreeHost(c->h_win);
-    if (c->h_work) cudaFreeHost(c->h_work);
-    for (auto& e : c->ev)
-        if (e) cudaEventDestroy(e);
-    for (cudaEvent_t e : {c->ev_fork, c->ev_sort, c->ev_s2, c->ev_s3})
-        if (e) cudaEventDestroy(e);
-    if (c->s2) cudaStreamDestroy(c->s2);
-    if (c->s3) cudaStreamDestroy(c->s3);
-    if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
 
@@ -668,21 +808,20 @@ int g16_compute_h(g16_circuit* c, const uint8_t* w, size_t n, g16_hpoly** out) {
     if (!c || !w || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
-    std::lock_guard<std::mutex> g(c->mu);
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
+    WsGuard g(c);
+    if ((rc = acquire(c, &g.ws))) return rc;
     auto h = std::make_unique<g16_hpoly>();
     h->owner = c;
     h->n = c->n;
     CK(cudaMalloc(&h->d_h, 32ull * c->n), "H allocation");
-    if ((rc = upload_witness(c, w, n))) return rc;
-    if ((rc = run_h(c, c->d_w, h->d_h))) {
+    if ((rc = upload_witness(g.ws, w, n)) || (rc = run_h(c, g.ws, g.ws->d_w, h->d_h))) {
         cudaFree(h->d_h);
         return rc;
     }
-    CK(cudaStreamSynchronize(c->stream), "stages 0-4");
+    CK(cudaStreamSynchronize(g.ws->stream), "stages 0-4");
     timer().collect();
-    c->t.gather_us += elapsed_us(c->ev[0], c->ev[1]);
-    c->t.ntt_us += elapsed_us(c->ev[1], c->ev[2]);
+    add_timings(c, g.ws, true, false, 0);
     *out = h.release();
     return G16_OK;
 }
@@ -706,13 +845,16 @@ int g16_msms(g16_circuit* c, const uint8_t* w, size_t n, const g16_hpoly* h, g16
     if (h->owner != c) return fail(G16_ERR_BACKEND, "H handle was computed by another circuit");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
-    std::lock_guard<std::mutex> g(c->mu);
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
-    if ((rc = upload_witness(c, w, n))) return rc;
-    CK(cudaEventRecord(c->ev[2], c->stream), "event");
+    WsGuard g(c);
+    if ((rc = acquire(c, &g.ws))) return rc;
+    if ((rc = upload_witness(g.ws, w, n))) return rc;
+    CK(cudaEventRecord(g.ws->ev[2], g.ws->stream), "event");
     MsmJac m;
-    if ((rc = run_msms(c, c->d_w, h->d_h, m))) return rc;
-    c->t.msm_us += elapsed_us(c->ev[2], c->ev[3]);
+    if ((rc = enqueue_witness_msms(c, g.ws, g.ws->d_w)) || (rc = enqueue_h_msm(c, g.ws, h->d_h)) ||
+        (rc = enqueue_join(g.ws)) || (rc = collect_msms(c, g.ws, m)))
+        return rc;
+    add_timings(c, g.ws, false, true, 0);
     to_outputs(m, out);
     return G16_OK;
 }
@@ -721,15 +863,13 @@ int g16_h_and_msms(g16_circuit* c, const uint8_t* w, size_t n, g16_msm_outputs* 
     if (!c || !w || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
-    std::lock_guard<std::mutex> g(c->mu);
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
-    if ((rc = upload_witness(c, w, n))) return rc;
-    if ((rc = run_h(c, c->d_w, c->d_hpoly))) return rc;
+    WsGuard g(c);
+    if ((rc = acquire(c, &g.ws))) return rc;
+    if ((rc = upload_witness(g.ws, w, n))) return rc;
     MsmJac m;
-    if ((rc = run_msms(c, c->d_w, c->d_hpoly, m))) return rc;
-    c->t.gather_us += elapsed_us(c->ev[0], c->ev[1]);
-    c->t.ntt_us += elapsed_us(c->ev[1], c->ev[2]);
-    c->t.msm_us += elapsed_us(c->ev[2], c->ev[3]);
+    if ((rc = run_proof(c, g.ws, g.ws->d_w, m))) return rc;
+    add_timings(c, g.ws, true, true, 0);
     to_outputs(m, out);
     return G16_OK;
 }
@@ -739,10 +879,11 @@ int g16_prove_with_blinders(g16_circuit* c, const uint8_t* w, size_t n, const ui
     if (!c || !w || !r || !s || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
-    std::lock_guard<std::mutex> g(c->mu);
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
-    if ((rc = upload_witness(c, w, n))) return rc;
-    return prove_on_device(c, c->d_w, r, s, out);
+    WsGuard g(c);
+    if ((rc = acquire(c, &g.ws))) return rc;
+    if ((rc = upload_witness(g.ws, w, n))) return rc;
+    return prove_on_device(c, g.ws, g.ws->d_w, r, s, out);
 }
 
 int g16_prove_with_blinders_device(g16_circuit* c, const void* d_w, size_t n, const uint8_t* r, const uint8_t* s,
@@ -750,9 +891,10 @@ int g16_prove_with_blinders_device(g16_circuit* c, const void* d_w, size_t n, co
     if (!c || !d_w || !r || !s || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, nullptr);
     if (rc) return rc;
-    std::lock_guard<std::mutex> g(c->mu);
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
-    return prove_on_device(c, d_w, r, s, out);
+    WsGuard g(c);
+    if ((rc = acquire(c, &g.ws))) return rc;
+    return prove_on_device(c, g.ws, d_w, r, s, out);
 }
 
 int g16_stage_timings_get(const g16_circuit* c, g16_stage_timings* out) {
@@ -761,16 +903,44 @@ int g16_stage_timings_get(const g16_circuit* c, g16_stage_timings* out) {
     return G16_OK;
 }
 
+// Several proofs in flight at once: `lanes` host threads each take the next job
+// and prove it on a workspace of its circuit, so the jobs' kernels, copies and
+// host-side assembly overlap.  Each result is the same as a single call's.
 int g16_prove_batch(g16_backend* b, size_t count, g16_circuit* const* circuits, const uint8_t* const* witnesses,
                     const size_t* lens, const uint8_t* r, const uint8_t* s, g16_proof* out) {
     if (!b || (count && (!circuits || !witnesses || !lens || !r || !s || !out)))
         return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     for (size_t i = 0; i < count; i++) {
-        int rc = g16_prove_with_blinders(circuits[i], witnesses[i], lens[i], r + 32 * i, s + 32 * i, out + i);
+        if (!circuits[i] || !witnesses[i]) return fail(G16_ERR_INVALID_ARGUMENT, "null job %zu", i);
+        if (circuits[i]->be != b) return fail(G16_ERR_INVALID_ARGUMENT, "job %zu belongs to another backend", i);
+        int rc = check_witness(circuits[i], lens[i], witnesses[i]);
         if (rc) return rc;
     }
+    size_t lanes = 8;
+    if (const char* e = std::getenv("G16_BATCH_LANES")) lanes = (size_t)std::max(1, std::atoi(e));
+    lanes = std::min(lanes, count);
+    std::atomic<size_t> next{0};
+    std::vector<int> rcs(count, G16_OK);
+    std::vector<std::string> errs(count);
+    auto work = [&] {
+        cudaSetDevice(b->ordinal);
+        for (size_t i; (i = next.fetch_add(1)) < count;) {
+            rcs[i] = g16_prove_with_blinders(circuits[i], witnesses[i], lens[i], r + 32 * i, s + 32 * i, out + i);
+            if (rcs[i]) errs[i] = g_err;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < lanes; t++) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    for (size_t i = 0; i < count; i++)
+        if (rcs[i]) {
+            set_error("job %zu: %s", i, errs[i].c_str());
+            return rcs[i];
+        }
     return G16_OK;
 }
+
 
 // ---- primitives ----
 static int grow_dev(void*& p, size_t& cap, size_t need) {
