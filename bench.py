@@ -54,6 +54,7 @@ def parse():
                    help="prove (default): full proofs; msm-g1/msm-g2/ntt: the standalone primitives")
     p.add_argument("--log-n", type=int, default=20, help="primitive size 2^log_n")
     p.add_argument("--dist", type=int, default=0, help="MSM scalars: 0 uniform, 1 = 70%% in {0,1}")
+    p.add_argument("--lanes", type=int, default=4, help="served proving: concurrent proofs")
     return p.parse_args()
 
 
@@ -123,16 +124,16 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def synth_key(sc, nc):
+def synth_key(sc, nc, seed=CIRCUIT_SEED, toxic=TOXIC_SEED):
     """The workload's .zkey; cached under /tmp so repeated runs on one host skip the key generation."""
     path = os.path.join(os.environ.get("G16_BENCH_CACHE", "/tmp"), "g16b200_bench_%d_%d_%d.zkey" % (
-        CIRCUIT_SEED, nc, TOXIC_SEED))
+        seed, nc, toxic))
     try:
         with open(path, "rb") as f:
             return f.read()
     except OSError:
         pass
-    zk = sc.zkey(TOXIC_SEED)
+    zk = sc.zkey(toxic)
     try:
         with open(path + ".tmp", "wb") as f:
             f.write(zk)
@@ -496,10 +497,110 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+# Circuits labelled 2^k constraints have domain 2^k and about 0.52 * 2^k active
+# rows, the convention of the 2^21-constraint prove (1.1M rows, domain 2^21);
+# the largest one is that very circuit.
+SERVE_LOGS = [14, 16, 17, 18, 20, 21]
+SERVE_WEIGHTS = [30, 25, 20, 12, 8, 5]
+
+
+def serve_circuits():
+    out = []
+    for k in SERVE_LOGS:
+        if k == 21:
+            out.append((CIRCUIT_SEED, N_CONSTRAINTS))
+        else:
+            out.append((700 + k, (N_CONSTRAINTS << k) >> 21))
+    return out
+
+
+def run_serve(args):
+    """Poisson arrivals over six circuits; continuous batching vs plain FIFO, p50/p99."""
+    import random
+    import statistics as st
+    import snarkrs_b200 as S
+    import torch
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    backend = S.CudaBackend(local_rank)
+    keys, wits = [], []
+    for seed, nc in serve_circuits():
+        sc = S.SynthCircuit(seed, nc, N_INPUTS, N_PUBLIC)
+        keys.append(synth_key(sc, nc, seed))
+        wits.append([sc.witness(7000 + 10 * len(wits) + j) for j in range(2)])
+    budget = 120 << 30
+
+    def run(lanes, rate, n_req, seed):
+        rng = random.Random(seed)
+        srv = S.ProofServer(backend, budget, lanes)
+        for i, k in enumerate(keys):
+            srv.register_key(i, k)
+        # warm every key outside the measurement: prepare, one workspace per
+        # lane and its CUDA graph (captured on a workspace's second proof)
+        for i in range(len(keys)):
+            for _ in range(2):
+                r, s_ = blinders(i)
+                for t in [srv.submit(i, wits[i][0], r, s_) for _ in range(lanes)]:
+                    srv.wait(t)
+        reqs = []
+        t = 0.0
+        for j in range(n_req):
+            t += rng.expovariate(rate)
+            i = rng.choices(range(len(keys)), weights=SERVE_WEIGHTS)[0]
+            reqs.append((t, i, j))
+        tickets = []
+        t0 = time.perf_counter()
+        for (ta, i, j) in reqs:
+            delay = t0 + ta - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            r, s_ = blinders(10_000 + j)
+            tickets.append((srv.submit(i, wits[i][j % 2], r, s_), i, j))
+        lat, proofs = [], {}
+        for tk, i, j in tickets:
+            p, q, l = srv.wait(tk)
+            lat.append(l)
+            proofs[j] = p
+        t_end = time.perf_counter()
+        stats = srv.stats()
+        srv.close()
+        lat.sort()
+        return {"lanes": lanes, "offered_rate": rate, "requests": n_req,
+                "throughput": n_req / (t_end - t0), "p50_ms": lat[len(lat) // 2],
+                "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))], "mean_ms": st.mean(lat),
+                "stats": stats}, proofs
+
+    # plain capacity: mean service time over the mix, one request at a time
+    calib, _ = run(1, 1e6, 60, 1)     # back-to-back arrivals = saturated FIFO
+    cap = calib["throughput"]
+    n_req = max(100, args.steps * 40)
+    results = []
+    mix_ok = True
+    for frac in (0.5, 0.9, 1.5):
+        rate = frac * cap
+        plain, pp = run(1, rate, n_req, 42 + int(frac * 10))
+        served, sp = run(args.lanes, rate, n_req, 42 + int(frac * 10))
+        mix_ok &= all(pp[j] == sp[j] for j in pp)
+        results.append({"offered_fraction_of_plain_capacity": frac, "plain_fifo": plain, "served": served})
+    top = results[-1]["served"]
+    line = {"metric": "proofs/s", "value": top["throughput"], "unit": "proofs/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": 2, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32 (BN254 Montgomery limbs, exact)", "data": "synthetic",
+            "config": {"workload": "served prove: Poisson arrivals over 6 synthetic circuits of 2^14, 2^16, 2^17, "
+                                   "2^18, 2^20, 2^21 constraints, mix 30/25/20/12/8/5%, 120 GB key budget",
+                       "active_rows": [nc for _, nc in serve_circuits()], "lanes": args.lanes,
+                       "plain_capacity_proofs_s": cap},
+            "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"],
+            "sweep": results, "results_identical_alone_and_in_mix": mix_ok}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     if args.impl == "reference":
         run_reference(args)
     elif args.workload != "prove":

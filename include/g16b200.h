@@ -162,6 +162,32 @@ int g16_stage_timings_get(const g16_circuit *c, g16_stage_timings *out);
 int g16_prove_batch(g16_backend *b, size_t count, g16_circuit *const *circuits, const uint8_t *const *witnesses,
                     const size_t *lens, const uint8_t *r_mont, const uint8_t *s_mont, g16_proof *out);
 
+/* Served proving (no reference counterpart; the reference proves one request
+ * per call).  A request loop with continuous batching: `lanes` workers take
+ * queued requests as soon as they are free, so proofs of different circuits
+ * and sizes overlap on the device.  Registered keys are prepared on first use
+ * and stay resident in HBM while their device bytes fit key_budget_bytes
+ * (0 = unlimited); a key that does not fit evicts least recently used idle
+ * keys.  A proof starts when its circuit can hand out a workspace within the
+ * backend's device-memory budget.  Results equal single g16_prove_with_blinders
+ * calls. */
+typedef struct g16_server g16_server;
+typedef struct {
+    uint64_t submitted, completed, prepared, evicted, resident_keys, resident_bytes, queued;
+} g16_server_stats;
+int g16_server_new(g16_backend *b, uint64_t key_budget_bytes, int lanes, g16_server **out);
+/* Keeps a host copy of the .zkey bytes; the key is prepared when first needed. */
+int g16_server_register_key(g16_server *s, uint32_t key_id, const uint8_t *zkey, size_t len);
+/* Copies the witness (n Montgomery Fr) and the blinders; returns a ticket. */
+int g16_server_submit(g16_server *s, uint32_t key_id, const uint8_t *witness_mont, size_t n, const uint8_t *r_mont,
+                      const uint8_t *s_mont, uint64_t *ticket);
+/* Blocks until the ticket's proof is done.  queue_ms: submit to start;
+ * latency_ms: submit to finish.  Each ticket can be waited for once. */
+int g16_server_wait(g16_server *s, uint64_t ticket, g16_proof *out, double *queue_ms, double *latency_ms);
+int g16_server_stats_get(g16_server *s, g16_server_stats *out);
+/* Finishes the queued requests, then frees every resident key. */
+void g16_server_free(g16_server *s);
+
 /* ---------------- primitives (MsmBackend, crates/msm/src/lib.rs:52-82) ---------------- */
 /* sum_i scalars[i] * bases[i]; host buffers; result affine packed. */
 int g16_msm_g1(g16_backend *b, const uint8_t *bases, const uint8_t *scalars, size_t n, int scalars_form,

@@ -92,6 +92,7 @@ def lib():
         L.g16_circuit_free.argtypes = [vp]
         L.g16_hpoly_free.argtypes = [vp]
         L.g16_synth_free.argtypes = [vp]
+        L.g16_server_free.argtypes = [vp]
         for f in ("g16_circuit_n_vars", "g16_circuit_n_public", "g16_circuit_domain_size",
                   "g16_synth_n_vars", "g16_synth_domain_size"):
             getattr(L, f).restype = ctypes.c_uint32
@@ -413,6 +414,56 @@ class CudaBackend:
     def close(self):
         if self._h:
             lib().g16_backend_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in
+                ("submitted", "completed", "prepared", "evicted", "resident_keys", "resident_bytes", "queued")]
+
+
+class ProofServer:
+    """Served proving with continuous batching over a set of registered keys."""
+
+    def __init__(self, backend, key_budget_bytes=0, lanes=4):
+        h = ctypes.c_void_p()
+        check(lib().g16_server_new(backend._h, ctypes.c_uint64(key_budget_bytes), int(lanes), ctypes.byref(h)))
+        self._h = h
+        self.backend = backend
+
+    def register_key(self, key_id, zkey_bytes):
+        check(lib().g16_server_register_key(self._h, ctypes.c_uint32(key_id), bytes(zkey_bytes),
+                                            ctypes.c_size_t(len(zkey_bytes))))
+
+    def submit(self, key_id, witness_mont, r_mont, s_mont):
+        t = ctypes.c_uint64()
+        check(lib().g16_server_submit(self._h, ctypes.c_uint32(key_id), _buf(witness_mont),
+                                      ctypes.c_size_t(_nbytes(witness_mont) // 32), bytes(r_mont), bytes(s_mont),
+                                      ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket):
+        """(Proof, queue_ms, latency_ms)."""
+        p = _Proof()
+        q, lat = ctypes.c_double(), ctypes.c_double()
+        check(lib().g16_server_wait(self._h, ctypes.c_uint64(ticket), ctypes.byref(p), ctypes.byref(q),
+                                    ctypes.byref(lat)))
+        return Proof(p.a, p.b, p.c), q.value, lat.value
+
+    def stats(self):
+        st = _ServerStats()
+        check(lib().g16_server_stats_get(self._h, ctypes.byref(st)))
+        return {n: getattr(st, n) for n, _ in st._fields_}
+
+    def close(self):
+        if self._h:
+            lib().g16_server_free(self._h)
             self._h = None
 
     def __del__(self):

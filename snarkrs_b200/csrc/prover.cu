@@ -401,8 +401,22 @@ int check_witness(const g16_circuit* c, size_t n, const uint8_t* w_host) {
 
 uint64_t elapsed_us(cudaEvent_t a, cudaEvent_t b) {
     float ms = 0;
-    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) return 0;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        (void)cudaGetLastError();   // an unrecorded stage event is not a launch failure
+        return 0;
+    }
     return (uint64_t)(ms * 1000.0);
+}
+
+// Stage boundary event.  Inside a stream capture a plain record only orders
+// the captured work; the external flag turns it into an event-record node, so
+// that every graph replay records it and the stage timings stay live.
+cudaError_t stage_event(cudaEvent_t e, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t err = cudaStreamIsCapturing(st, &cs);
+    if (err != cudaSuccess) return err;
+    return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(e, st, cudaEventRecordExternal)
+                                               : cudaEventRecord(e, st);
 }
 
 // stages 0-4 on the device witness; H left in h_out (device)
@@ -410,7 +424,7 @@ int run_h(g16_circuit* c, Workspace* ws, const void* d_w, void* h_out) {
     cudaStream_t st = ws->stream;
     uint8_t* abc = (uint8_t*)ws->d_abc;
     size_t vb = (size_t)c->n * 32;
-    CK(cudaEventRecord(ws->ev[0], st), "event");
+    CK(stage_event(ws->ev[0], st), "event");
     {
         TimedLaunch tl("gather", st);
         g16d::k_gather<<<blocks_for(c->n, 256), 256, 0, st>>>(
@@ -418,9 +432,9 @@ int run_h(g16_circuit* c, Workspace* ws, const void* d_w, void* h_out) {
             (const uint4*)d_w, c->n, (uint4*)abc, (uint4*)(abc + vb), (uint4*)(abc + 2 * vb));
     }
     CK(cudaGetLastError(), "gather launch");
-    CK(cudaEventRecord(ws->ev[1], st), "event");
+    CK(stage_event(ws->ev[1], st), "event");
     CK(ntt_h_pipeline(c->ntt, abc, abc + vb, abc + 2 * vb, h_out, st), "NTT pipeline");
-    CK(cudaEventRecord(ws->ev[2], st), "event");
+    CK(stage_event(ws->ev[2], st), "event");
     return G16_OK;
 }
 
@@ -470,7 +484,7 @@ int enqueue_h_msm(g16_circuit* c, Workspace* ws, const void* d_h) {
 int enqueue_join(Workspace* ws) {
     CK(cudaStreamWaitEvent(ws->stream, ws->ev_s2, 0), "stream wait");
     CK(cudaStreamWaitEvent(ws->stream, ws->ev_s3, 0), "stream wait");
-    CK(cudaEventRecord(ws->ev[3], ws->stream), "event");
+    CK(stage_event(ws->ev[3], ws->stream), "event");
     return G16_OK;
 }
 
