@@ -155,6 +155,27 @@ int g16_prove_with_blinders_device(g16_circuit *c, const void *d_witness_mont, s
                                    const uint8_t *s_mont, g16_proof *out);
 int g16_stage_timings_get(const g16_circuit *c, g16_stage_timings *out);
 
+/* ---------------- per-instance tuning (no reference counterpart) ----------------
+ * The MSM window sizes and the NTT tiling of a prepared circuit.  g16_prepare
+ * picks them from a cost model; g16_autotune times candidates on the device
+ * with one of the circuit's witnesses and keeps the fastest (the proof's
+ * values do not depend on them).  Window-size changes rebuild the circuit's
+ * window-shifted base tables. */
+typedef struct {
+    int32_t msm_window_bits_witness; /* c of the A, B1, L, B2 MSMs */
+    int32_t msm_window_bits_h;       /* c of the H MSM */
+    int32_t ntt_tile_log;            /* inner NTT pass: tiles of 2^ntt_tile_log elements (2..12) */
+    int32_t ntt_outer_log_l;         /* outer passes: 2^ntt_outer_log_l columns per tile row */
+    double model_ms;                 /* stages 0-9 device time with the cost model's choice (autotune only) */
+    double tuned_ms;                 /* the same with the kept choice (autotune only) */
+} g16_tuning;
+int g16_tuning_get(const g16_circuit *c, g16_tuning *out);
+/* Applies explicit choices (window bits 8..20); no proof may be in flight on c. */
+int g16_tuning_set(g16_circuit *c, const g16_tuning *t);
+/* Times the candidates with one witness (n Montgomery Fr) and keeps the
+ * fastest; no proof may be in flight on c.  out may be NULL. */
+int g16_autotune(g16_circuit *c, const uint8_t *witness_mont, size_t n, g16_tuning *out);
+
 /* ---------------- batched and served proving ---------------- */
 /* Proves count independent jobs (circuits may repeat or differ) in one
  * submission; outputs are bit-identical to count single calls.

@@ -140,6 +140,15 @@ class _Proof(ctypes.Structure):
     _fields_ = [("a", ctypes.c_uint8 * 64), ("b", ctypes.c_uint8 * 128), ("c", ctypes.c_uint8 * 64)]
 
 
+class _Tuning(ctypes.Structure):
+    _fields_ = [("msm_window_bits_witness", ctypes.c_int32), ("msm_window_bits_h", ctypes.c_int32),
+                ("ntt_tile_log", ctypes.c_int32), ("ntt_outer_log_l", ctypes.c_int32),
+                ("model_ms", ctypes.c_double), ("tuned_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class _MsmOutputs(ctypes.Structure):
     _fields_ = [("a_g1", ctypes.c_uint8 * 64), ("b_g2", ctypes.c_uint8 * 128), ("b_g1", ctypes.c_uint8 * 64),
                 ("l_g1", ctypes.c_uint8 * 64), ("h_g1", ctypes.c_uint8 * 64)]
@@ -349,6 +358,23 @@ class CudaCircuit:
     def stage_timings(self):
         t = StageTimings()
         check(lib().g16_stage_timings_get(self._h, ctypes.byref(t)))
+        return t.as_dict()
+
+    def tuning(self):
+        """MSM window bits and NTT tiling in use (cost model, autotuner or set_tuning)."""
+        t = _Tuning()
+        check(lib().g16_tuning_get(self._h, ctypes.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, msm_window_bits_witness, msm_window_bits_h, ntt_tile_log, ntt_outer_log_l):
+        t = _Tuning(msm_window_bits_witness, msm_window_bits_h, ntt_tile_log, ntt_outer_log_l, 0.0, 0.0)
+        check(lib().g16_tuning_set(self._h, ctypes.byref(t)))
+
+    def autotune(self, witness_mont):
+        """Time window sizes and NTT tilings with this witness on the device; keep the fastest."""
+        t = _Tuning()
+        check(lib().g16_autotune(self._h, _buf(witness_mont), ctypes.c_size_t(_nbytes(witness_mont) // 32),
+                                 ctypes.byref(t)))
         return t.as_dict()
 
     def close(self):
@@ -615,17 +641,23 @@ def kernel_timing_reset():
     lib().g16_kernel_timing_reset()
 
 
+def _timing_lines():
+    buf = ctypes.create_string_buffer(1 << 16)
+    lib().g16_kernel_timing_report(buf, 1 << 16)
+    return [line.split() for line in buf.value.decode().splitlines()]
+
+
 def kernel_timing_report():
     """{kernel class: (total ms, launches, work units)} from CUDA events on the launching stream.
 
-    Work units are the mixed additions performed, for the MSM accumulate kernels."""
-    buf = ctypes.create_string_buffer(1 << 16)
-    lib().g16_kernel_timing_report(buf, 1 << 16)
-    out = {}
-    for line in buf.value.decode().splitlines():
-        name, ms, cnt, units = line.split()
-        out[name] = (float(ms), int(cnt), float(units))
-    return out
+    Work units are the mixed additions performed, for the MSM accumulate kernels,
+    and the Fr products, for the NTT passes."""
+    return {f[0]: (float(f[1]), int(f[2]), float(f[3])) for f in _timing_lines()}
+
+
+def kernel_timing_bytes():
+    """{kernel class: algorithmic HBM bytes} over the same launches (NTT passes, MSM sort)."""
+    return {f[0]: float(f[4]) for f in _timing_lines() if float(f[4]) > 0}
 
 
 def launch_count():

@@ -36,6 +36,7 @@ struct KernelTimer {
     std::vector<cudaEvent_t> pool;
     std::map<std::string, std::pair<double, long>> totals;   // ms, launches
     std::map<std::string, double> units;                     // algorithmic work, per kernel class
+    std::map<std::string, double> bytes;                     // algorithmic HBM bytes, per kernel class
     std::atomic<uint64_t> launches{0};                        // every kernel this library launched
     std::mutex mu;
 
@@ -43,6 +44,11 @@ struct KernelTimer {
         if (!enabled) return;
         std::lock_guard<std::mutex> g(mu);
         units[name] += u;
+    }
+    void add_bytes(const char* name, double b) {
+        if (!enabled) return;
+        std::lock_guard<std::mutex> g(mu);
+        bytes[name] += b;
     }
 
     cudaEvent_t take() {
@@ -89,6 +95,7 @@ struct KernelTimer {
         std::lock_guard<std::mutex> g(mu);
         totals.clear();
         units.clear();
+        bytes.clear();
     }
 };
 

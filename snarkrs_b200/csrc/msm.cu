@@ -578,6 +578,7 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
     G16_CUDA(cudaMemsetAsync(s.d_counts, 0, kk * sizeof(uint32_t), st));
     G16_CUDA(cudaMemsetAsync(s.d_total, 0, 4 * sizeof(uint32_t), st));
     if (n) {
+        timer().add_bytes("msm_digits", 64.0 * n);   // scalars in, standard-form copy out
         TimedLaunch tl("msm_digits", st);
         k_digits_count<<<blocks_for(n, 256), 256, 0, st>>>((const uint4*)d_scalars, montgomery ? 1 : 0, (uint32_t)n,
                                                           c, s.W, kw, (uint4*)s.d_scalars_std, s.d_counts);

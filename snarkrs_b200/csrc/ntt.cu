@@ -212,8 +212,9 @@ namespace g16 {
 
 using namespace g16d;
 
-static constexpr uint32_t TILE_LOG = 11;    // 2048 elements, 64 KiB of shared memory
-static constexpr uint32_t OUTER_LOG_L = 2;  // 4 consecutive columns (128 B) per tile row
+bool ntt_tiling_valid(const NttTiling& t) {
+    return t.tile_log >= 2 && t.tile_log <= NTT_MAX_TILE_LOG && t.outer_log_l < t.tile_log && t.outer_log_l <= 4;
+}
 
 void NttTables::release() {
     cudaFree(d_tw);
@@ -273,17 +274,20 @@ struct Pass {
     uint32_t s_lo, k, log_L;
 };
 
+// the inner pass's stage count
+static uint32_t inner_k(const NttTiling& tl, uint32_t log_n) { return log_n < tl.tile_log ? log_n : tl.tile_log; }
+
 // outer passes covering stages [k0, log_n), in increasing s_lo
-static std::vector<Pass> outer_passes(uint32_t log_n, uint32_t k0) {
+static std::vector<Pass> outer_passes(const NttTiling& tl, uint32_t log_n, uint32_t k0) {
     std::vector<Pass> v;
     uint32_t rem = log_n - k0;
     if (!rem) return v;
-    uint32_t kmax = TILE_LOG - OUTER_LOG_L;
+    uint32_t kmax = tl.tile_log - tl.outer_log_l;
     uint32_t np = (rem + kmax - 1) / kmax;
     uint32_t s = k0;
     for (uint32_t i = 0; i < np; i++) {
         uint32_t k = rem / np + (i < rem % np ? 1 : 0);
-        uint32_t ll = OUTER_LOG_L < s ? OUTER_LOG_L : s;
+        uint32_t ll = tl.outer_log_l < s ? tl.outer_log_l : s;
         v.push_back({s, k, ll});
         s += k;
     }
@@ -293,7 +297,7 @@ static std::vector<Pass> outer_passes(uint32_t log_n, uint32_t k0) {
 static bool attrs_done = false;
 static void set_attrs() {
     if (attrs_done) return;
-    size_t smem = ((size_t)1 << TILE_LOG) * 32;
+    size_t smem = ((size_t)1 << NTT_MAX_TILE_LOG) * 32;
     cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k_ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k_ntt_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -307,7 +311,12 @@ static cudaError_t launch_pass(bool dif, Vec3 v, int nv, uint32_t log_n, const P
     dim3 grid((unsigned)(n / tile), nv);
     unsigned threads = tile / 2 < 256 ? tile / 2 : 256;
     size_t smem = (size_t)tile * 32;
-    TimedLaunch tl(dif ? "ntt_pass_dif" : "ntt_pass_dit", st);
+    const char* name = dif ? "ntt_pass_dif" : "ntt_pass_dit";
+    // work: one Fr product per butterfly, plus the scale / join epilogue;
+    // bytes: each vector read and written once, the join also reads A and B
+    timer().add_units(name, (double)nv * (double)(n / 2) * p.k + (scale ? (double)nv * n : 0.0) + (jo ? (double)n : 0.0));
+    timer().add_bytes(name, 64.0 * nv * n + (jo ? 64.0 * n : 0.0));
+    TimedLaunch tl(name, st);
     if (dif)
         k_ntt_pass<true><<<grid, threads, smem, st>>>(v, log_n, p.s_lo, p.k, p.log_L, (const uint4*)tw,
                                                        (const uint4*)scale, (const uint4*)ja, (const uint4*)jb,
@@ -322,11 +331,13 @@ static cudaError_t launch_pass(bool dif, Vec3 v, int nv, uint32_t log_n, const P
 static cudaError_t launch_mid(Vec3 v, int nv, const NttTables& t, const void* ja, const void* jb, void* jo,
                               cudaStream_t st) {
     uint32_t log_n = (uint32_t)t.log_n;
-    uint32_t k0 = log_n < TILE_LOG ? log_n : TILE_LOG;
+    uint32_t k0 = inner_k(t.tiling, log_n);
     uint32_t tile = 1u << k0;
     size_t n = (size_t)1 << log_n;
     dim3 grid((unsigned)(n / tile), nv);
     unsigned threads = tile / 2 < 256 ? tile / 2 : 256;
+    timer().add_units("ntt_mid_fused", (double)nv * ((double)n * k0 + n) + (jo ? (double)n : 0.0));
+    timer().add_bytes("ntt_mid_fused", 64.0 * nv * n + (jo ? 64.0 * n : 0.0));
     TimedLaunch tl("ntt_mid_fused", st);
     k_ntt_mid<<<grid, threads, (size_t)tile * 32, st>>>(v, log_n, k0, (const uint4*)t.d_tw, (const uint4*)t.d_tw_inv,
                                                          (const uint4*)t.d_coset, (const uint4*)ja, (const uint4*)jb,
@@ -337,8 +348,8 @@ static cudaError_t launch_mid(Vec3 v, int nv, const NttTables& t, const void* ja
 cudaError_t ntt_h_pipeline(const NttTables& t, void* a, void* b, void* c, void* h, cudaStream_t st) {
     set_attrs();
     uint32_t log_n = (uint32_t)t.log_n;
-    uint32_t k0 = log_n < TILE_LOG ? log_n : TILE_LOG;
-    auto outer = outer_passes(log_n, k0);
+    uint32_t k0 = inner_k(t.tiling, log_n);
+    auto outer = outer_passes(t.tiling, log_n, k0);
     Vec3 abc = {{(uint4*)a, (uint4*)b, (uint4*)c}};
     // inverse, DIF, top stages first
     for (size_t i = outer.size(); i-- > 0;)
@@ -359,8 +370,8 @@ cudaError_t ntt_h_pipeline(const NttTables& t, void* a, void* b, void* c, void* 
 cudaError_t ntt_intt_coset_ntt(const NttTables& t, void* a, cudaStream_t st) {
     set_attrs();
     uint32_t log_n = (uint32_t)t.log_n;
-    uint32_t k0 = log_n < TILE_LOG ? log_n : TILE_LOG;
-    auto outer = outer_passes(log_n, k0);
+    uint32_t k0 = inner_k(t.tiling, log_n);
+    auto outer = outer_passes(t.tiling, log_n, k0);
     Vec3 v = {{(uint4*)a, nullptr, nullptr}};
     for (size_t i = outer.size(); i-- > 0;)
         G16_CUDA(launch_pass(true, v, 1, log_n, outer[i], t.d_tw_inv, nullptr, nullptr, nullptr, nullptr, st));
@@ -379,8 +390,8 @@ static cudaError_t dit_natural(const NttTables& t, void* a, const void* tw, cons
         k_bitrev<<<blocks_for(n, 256), 256, 0, st>>>((uint4*)a, log_n, n);
     }
     G16_CUDA(cudaGetLastError());
-    uint32_t k0 = log_n < TILE_LOG ? log_n : TILE_LOG;
-    auto outer = outer_passes(log_n, k0);
+    uint32_t k0 = inner_k(t.tiling, log_n);
+    auto outer = outer_passes(t.tiling, log_n, k0);
     Vec3 v = {{(uint4*)a, nullptr, nullptr}};
     Pass inner = {0, k0, 0};
     G16_CUDA(launch_pass(false, v, 1, log_n, inner, tw, outer.empty() ? scale : nullptr, nullptr, nullptr, nullptr,

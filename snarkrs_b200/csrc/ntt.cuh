@@ -21,8 +21,23 @@
 
 namespace g16 {
 
+// Tiling of the shared-memory passes: the inner pass works on contiguous
+// tiles of 2^tile_log elements, each outer pass on tiles of 2^k * 2^outer_log_l
+// elements with k <= tile_log - outer_log_l (2^outer_log_l consecutive
+// columns per tile row).  The values are the same for every tiling; only the
+// number of passes over HBM and the shared-memory footprint change.
+struct NttTiling {
+    uint32_t tile_log = 11;      // 2048 elements, 64 KiB of shared memory
+    uint32_t outer_log_l = 2;    // 4 columns = 128-byte rows
+};
+constexpr uint32_t NTT_MAX_TILE_LOG = 12;   // 128 KiB of shared memory
+
+// Is the tiling one the kernels accept?
+bool ntt_tiling_valid(const NttTiling& t);
+
 struct NttTables {
     int log_n = -1;
+    NttTiling tiling;
     void* d_tw = nullptr;       // omega^i, i < n/2 (Montgomery Fr)
     void* d_tw_inv = nullptr;   // omega^-i, i < n/2
     void* d_coset = nullptr;    // shift^bitrev(p) / n, p < n (the proving coset shift omega_2n)

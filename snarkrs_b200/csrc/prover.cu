@@ -228,6 +228,8 @@ struct g16_circuit {
     uint64_t ws_estimate = 0;          // device bytes of one workspace, scratch included
     bool serial = false;               // every stage on one stream (profiling)
     bool graphs = true;                // replay proofs as captured CUDA graphs
+    bool tuning = false;               // g16_autotune / g16_tuning_set running: no new proofs start
+    g16_tuning tuned = {0, 0, 0, 0, 0.0, 0.0};
     g16_stage_timings t = {0, 0, 0, 0, 0, 0};
     uint64_t readback_bytes = 0;       // device-to-host bytes of the last proof
     uint64_t device_bytes = 0;
@@ -282,11 +284,92 @@ cudaError_t circuit_alloc(g16_circuit* c, void** p, size_t bytes) {
     return e;
 }
 
+// Device bytes of one workspace: witness, A|B|C, H, and the MSM scratch
+// (sorted entries, partial sums, bucket sums) at window bits c_w and c_h.
+uint64_t workspace_estimate(uint64_t nv, uint64_t n, int c_w, int c_h) {
+    const uint64_t Ww = (uint64_t)msm_windows(c_w), Wh = (uint64_t)msm_windows(c_h);
+    const uint64_t Kw = 1ull << (c_w - 1), Kh = 1ull << (c_h - 1);
+    uint64_t b = nv * 32 + n * 32 * 4;
+    b += nv * 32 + nv * Ww * 4 + 24 * (Kw + 1) + n * 32 + n * Wh * 4 + 24 * (Kh + 1);
+    b += 3 * 128 * (Kw * 2 + nv * Ww / 16 + 1) + 256 * (Kw * 2 + nv * Ww / 16 + 1);
+    b += 128 * (Kh * 2 + n * Wh / 16 + 1) + (16ull << 20);
+    return b;
+}
+
+void circuit_free_alloc(g16_circuit* c, void* p, uint64_t bytes) {
+    if (!p) return;
+    for (size_t i = 0; i < c->allocs.size(); i++)
+        if (c->allocs[i] == p) {
+            c->allocs.erase(c->allocs.begin() + (long)i);
+            break;
+        }
+    cudaFree(p);
+    c->device_bytes -= std::min<uint64_t>(c->device_bytes, bytes);
+    c->be->vram_used -= std::min<uint64_t>(c->be->vram_used, bytes);
+}
+
+// (Re)build the window-shifted tables of the witness MSMs (A, B1, L, B2) for
+// window bits cw; the new tables replace the old ones only when all are built.
+int build_witness_tables(g16_circuit* c, int cw, cudaStream_t st) {
+    const uint64_t nv = c->n_vars, W = (uint64_t)msm_windows(cw);
+    if (nv * W >= 0x80000000ull) return fail(G16_ERR_BACKEND, "circuit too large for 31-bit MSM entry indices");
+    void *ta = nullptr, *tb1 = nullptr, *tl = nullptr, *tb2 = nullptr;
+    cudaError_t e = circuit_alloc(c, &ta, 64 * nv * W);
+    if (e == cudaSuccess) e = circuit_alloc(c, &tb1, 64 * nv * W);
+    if (e == cudaSuccess) e = circuit_alloc(c, &tl, 64 * nv * W);
+    if (e == cudaSuccess) e = circuit_alloc(c, &tb2, 128 * nv * W);
+    if (e == cudaSuccess) e = msm_window_table_g1(c->d_a, nv, 0, cw, ta, st);
+    if (e == cudaSuccess) e = msm_window_table_g1(c->d_b1, nv, 0, cw, tb1, st);
+    if (e == cudaSuccess) e = msm_window_table_g1(c->d_l, nv, c->n_public + 1, cw, tl, st);
+    if (e == cudaSuccess) e = msm_window_table_g2(c->d_b2, nv, 0, cw, tb2, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        int rc = cuda_fail(e, "window tables");
+        for (void* p : {ta, tb1, tl}) circuit_free_alloc(c, p, 64 * nv * W);
+        circuit_free_alloc(c, tb2, 128 * nv * W);
+        return rc;
+    }
+    if (c->c_w) {
+        const uint64_t Wo = (uint64_t)msm_windows(c->c_w);
+        for (void* p : {c->t_a, c->t_b1, c->t_l}) circuit_free_alloc(c, p, 64 * nv * Wo);
+        circuit_free_alloc(c, c->t_b2, 128 * nv * Wo);
+    }
+    c->t_a = ta;
+    c->t_b1 = tb1;
+    c->t_l = tl;
+    c->t_b2 = tb2;
+    c->c_w = cw;
+    return G16_OK;
+}
+
+// The same for the H MSM's table at window bits ch.
+int build_h_table(g16_circuit* c, int ch, cudaStream_t st) {
+    const uint64_t n = c->n, W = (uint64_t)msm_windows(ch);
+    if (n * W >= 0x80000000ull) return fail(G16_ERR_BACKEND, "domain too large for 31-bit MSM entry indices");
+    void* th = nullptr;
+    cudaError_t e = circuit_alloc(c, &th, 64 * n * W);
+    if (e == cudaSuccess) e = msm_window_table_g1(c->d_h, n, 0, ch, th, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        int rc = cuda_fail(e, "window tables");
+        circuit_free_alloc(c, th, 64 * n * W);
+        return rc;
+    }
+    if (c->c_h) circuit_free_alloc(c, c->t_h, 64 * n * (uint64_t)msm_windows(c->c_h));
+    c->t_h = th;
+    c->c_h = ch;
+    return G16_OK;
+}
+
 // Take an idle workspace, or build one while the pool is below its cap and the
 // backend's device-memory budget has room; otherwise wait for one to come back.
 int acquire(g16_circuit* c, Workspace** out) {
     std::unique_lock<std::mutex> lk(c->mu);
     for (;;) {
+        if (c->tuning) {
+            c->cv.wait(lk);
+            continue;
+        }
         if (!c->idle.empty()) {
             *out = c->idle.back();
             c->idle.pop_back();
@@ -587,6 +670,137 @@ int upload_witness(Workspace* ws, const uint8_t* w, size_t n) {
     return G16_OK;
 }
 
+// ---- per-instance tuning ----
+
+// Minimum over reps of the device time of enqueue() on ws->stream (after one
+// untimed run); negative on failure, with the error already set.
+template <class Fn>
+double time_on_stream(Workspace* ws, int reps, Fn&& enqueue) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        cuda_fail(cudaGetLastError(), "tuning events");
+        return -1.0;
+    }
+    double best = -1.0;
+    for (int i = 0; i <= reps; i++) {
+        cudaError_t e = cudaEventRecord(e0, ws->stream);
+        if (e != cudaSuccess) {
+            cuda_fail(e, "tuning");
+            best = -1.0;
+            break;
+        }
+        if (enqueue() != G16_OK) {
+            best = -1.0;
+            break;
+        }
+        e = cudaEventRecord(e1, ws->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) {
+            cuda_fail(e, "tuning");
+            best = -1.0;
+            break;
+        }
+        if (i > 0 && (best < 0 || ms < best)) best = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+}
+
+// Holds the circuit's proof path for tuning: the one workspace in ws is the
+// only one out of the pool, no other proof can start until release.
+struct TuningLock {
+    g16_circuit* c;
+    Workspace* ws = nullptr;
+    bool held = false;
+    explicit TuningLock(g16_circuit* cc) : c(cc) {}
+    int take() {
+        int rc = acquire(c, &ws);
+        if (rc) return rc;
+        std::lock_guard<std::mutex> g(c->mu);
+        if (c->idle.size() + 1 != c->pool.size())
+            return fail(G16_ERR_INVALID_ARGUMENT, "tuning needs a circuit with no proof in flight");
+        c->tuning = true;
+        held = true;
+        return G16_OK;
+    }
+    ~TuningLock() {
+        if (held) {
+            // captured graphs hold the old tables and launch shapes: capture again
+            for (auto& w : c->pool) {
+                if (w->graph) cudaGraphExecDestroy(w->graph);
+                w->graph = nullptr;
+                w->proofs = 0;
+            }
+            c->ws_estimate = workspace_estimate(c->n_vars, c->n, c->c_w, c->c_h);
+        }
+        if (ws) {
+            std::lock_guard<std::mutex> g(c->mu);
+            c->idle.push_back(ws);
+            c->tuning = false;
+        }
+        c->cv.notify_all();
+    }
+};
+
+bool window_bits_ok(int b) { return b >= 8 && b <= 20; }
+
+int apply_tuning(g16_circuit* c, Workspace* ws, const g16_tuning& t) {
+    NttTiling tl = {(uint32_t)t.ntt_tile_log, (uint32_t)t.ntt_outer_log_l};
+    if (!window_bits_ok(t.msm_window_bits_witness) || !window_bits_ok(t.msm_window_bits_h) || t.ntt_tile_log < 2 ||
+        t.ntt_outer_log_l < 0 || !ntt_tiling_valid(tl))
+        return fail(G16_ERR_INVALID_ARGUMENT, "tuning out of range: window bits %d/%d (8..20), NTT tile 2^%d, %d",
+                    t.msm_window_bits_witness, t.msm_window_bits_h, t.ntt_tile_log, t.ntt_outer_log_l);
+    int rc = G16_OK;
+    if (t.msm_window_bits_witness != c->c_w) rc = build_witness_tables(c, t.msm_window_bits_witness, ws->stream);
+    if (rc == G16_OK && t.msm_window_bits_h != c->c_h) rc = build_h_table(c, t.msm_window_bits_h, ws->stream);
+    if (rc == G16_OK) c->ntt.tiling = tl;
+    return rc;
+}
+
+g16_tuning current_tuning(const g16_circuit* c) {
+    g16_tuning t = c->tuned;
+    t.msm_window_bits_witness = c->c_w;
+    t.msm_window_bits_h = c->c_h;
+    t.ntt_tile_log = (int32_t)c->ntt.tiling.tile_log;
+    t.ntt_outer_log_l = (int32_t)c->ntt.tiling.outer_log_l;
+    return t;
+}
+
+// Hill-climb one window size: try the neighbours of the current value and keep
+// moving while the timed stage gets faster.
+template <class Build, class Time>
+int climb_window(int start, Build&& build, Time&& time_it, int* best_out) {
+    double t0 = time_it();
+    if (t0 < 0) return G16_ERR_DEVICE;
+    int best = start;
+    double best_t = t0;
+    for (int dir : {+1, -1}) {
+        int b = best + dir;
+        while (window_bits_ok(b) && b != start) {
+            int rc = build(b);
+            if (rc) return rc;
+            double t = time_it();
+            if (t < 0) return G16_ERR_DEVICE;
+            if (t < best_t * 0.99) {
+                best_t = t;
+                best = b;
+                b += dir;
+            } else {
+                break;
+            }
+        }
+        if (best != start) break;   // improved upward: do not try downward
+    }
+    int rc = build(best);
+    if (rc) return rc;
+    *best_out = best;
+    return G16_OK;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- C ABI
@@ -712,12 +926,7 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
     if (nv * Ww >= 0x80000000ull || (uint64_t)n * Wh >= 0x80000000ull)
         return fail(G16_ERR_BACKEND, "circuit too large for 31-bit MSM entry indices");
     key_bytes += nv * Ww * (64 * 3 + 128) + (uint64_t)n * Wh * 64;
-    // one workspace: witness, A|B|C, H, and the MSM scratch (entries, partials, buckets)
-    const uint64_t Kw = 1ull << (c_w - 1), Kh = 1ull << (c_h - 1);
-    uint64_t ws_bytes = nv * 32 + (uint64_t)n * 32 * 4;
-    ws_bytes += nv * 32 + nv * Ww * 4 + 24 * (Kw + 1) + (uint64_t)n * 32 + (uint64_t)n * Wh * 4 + 24 * (Kh + 1);
-    ws_bytes += 3 * 128 * (Kw * 2 + nv * Ww / 16 + 1) + 256 * (Kw * 2 + nv * Ww / 16 + 1);
-    ws_bytes += 128 * (Kh * 2 + (uint64_t)n * Wh / 16 + 1) + (16ull << 20);
+    const uint64_t ws_bytes = workspace_estimate(nv, n, c_w, c_h);
     if (b->vram_used + key_bytes + ws_bytes > b->vram_limit)
         return fail(G16_ERR_DEVICE_MEMORY, "circuit needs about %llu MiB of device memory, %llu MiB of the %llu MiB budget are free",
                     (unsigned long long)((key_bytes + ws_bytes) >> 20),
@@ -776,25 +985,11 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
     }
     cp->device_bytes += 3ull * 32 * n / 2 * 2;
     // window-shifted base tables; the plain bases are their window-0 slice
-    cp->c_w = c_w;
-    cp->c_h = c_h;
-    {
-        cudaError_t e2 = circuit_alloc(cp, &cp->t_a, 64ull * nv * Ww);
-        if (e2 == cudaSuccess) e2 = circuit_alloc(cp, &cp->t_b1, 64ull * nv * Ww);
-        if (e2 == cudaSuccess) e2 = circuit_alloc(cp, &cp->t_l, 64ull * nv * Ww);
-        if (e2 == cudaSuccess) e2 = circuit_alloc(cp, &cp->t_b2, 128ull * nv * Ww);
-        if (e2 == cudaSuccess) e2 = circuit_alloc(cp, &cp->t_h, 64ull * n * Wh);
-        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_a, nv, 0, c_w, cp->t_a, st);
-        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_b1, nv, 0, c_w, cp->t_b1, st);
-        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_l, nv, k->n_public + 1, c_w, cp->t_l, st);
-        if (e2 == cudaSuccess) e2 = msm_window_table_g2(cp->d_b2, nv, 0, c_w, cp->t_b2, st);
-        if (e2 == cudaSuccess) e2 = msm_window_table_g1(cp->d_h, n, 0, c_h, cp->t_h, st);
-        if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(st);
-        if (e2 != cudaSuccess) {
-            int rc = cuda_fail(e2, "window tables");
-            cleanup();
-            return rc;
-        }
+    int rc = build_witness_tables(cp, c_w, st);
+    if (rc == G16_OK) rc = build_h_table(cp, c_h, st);
+    if (rc != G16_OK) {
+        cleanup();
+        return rc;
     }
     *out = c.release();
     return G16_OK;
@@ -988,12 +1183,18 @@ static int msm_device_impl(g16_backend* b, const void* d_bases, const void* d_sc
     }
     CK(cudaMemcpyAsync(b->h_pinned, b->acc.d_windows, bytes, cudaMemcpyDeviceToHost, st), "window readback");
     if (timer().enabled) {
-        if (!b->h_work) CK(cudaMallocHost((void**)&b->h_work, sizeof(unsigned long long)), "pinned buffer");
+        // [0] mixed additions, [1] sorted entries (for the scatter's bytes)
+        if (!b->h_work) CK(cudaMallocHost((void**)&b->h_work, 2 * sizeof(unsigned long long)), "pinned buffer");
+        b->h_work[1] = 0;
         CK(cudaMemcpyAsync(b->h_work, b->acc.d_work, 8, cudaMemcpyDeviceToHost, st), "work readback");
+        CK(cudaMemcpyAsync(&b->h_work[1], b->sort.d_total, 4, cudaMemcpyDeviceToHost, st), "work readback");
     }
     CK(cudaStreamSynchronize(st), "MSM");
     timer().collect();
-    if (timer().enabled) timer().add_units(g2 ? "msm_accumulate_g2" : "msm_accumulate_g1", (double)*b->h_work);
+    if (timer().enabled) {
+        timer().add_units(g2 ? "msm_accumulate_g2" : "msm_accumulate_g1", (double)b->h_work[0]);
+        timer().add_bytes("msm_scatter", 32.0 * n + 4.0 * (double)b->h_work[1]);   // scalars in, entries out
+    }
     if (g2) pack(out, msm_combine_g2(b->h_pinned, b->sort.W, b->sort.c).to_affine());
     else pack(out, msm_combine_g1(b->h_pinned, b->sort.W, b->sort.c).to_affine());
     return G16_OK;
@@ -1108,8 +1309,9 @@ size_t g16_kernel_timing_report(char* buf, size_t len) {
         for (auto& kv : timer().totals) {
             char line[256];
             auto u = timer().units.find(kv.first);
-            snprintf(line, sizeof line, "%s %.6f %ld %.0f\n", kv.first.c_str(), kv.second.first, kv.second.second,
-                     u == timer().units.end() ? 0.0 : u->second);
+            auto by = timer().bytes.find(kv.first);
+            snprintf(line, sizeof line, "%s %.6f %ld %.0f %.0f\n", kv.first.c_str(), kv.second.first, kv.second.second,
+                     u == timer().units.end() ? 0.0 : u->second, by == timer().bytes.end() ? 0.0 : by->second);
             s += line;
         }
     }
@@ -1119,6 +1321,90 @@ size_t g16_kernel_timing_report(char* buf, size_t len) {
         buf[k] = 0;
     }
     return s.size();
+}
+
+int g16_tuning_get(const g16_circuit* c, g16_tuning* out) {
+    if (!c || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    *out = current_tuning(c);
+    return G16_OK;
+}
+
+int g16_tuning_set(g16_circuit* c, const g16_tuning* t) {
+    if (!c || !t) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
+    TuningLock lock(c);
+    int rc = lock.take();
+    if (rc) return rc;
+    return apply_tuning(c, lock.ws, *t);
+}
+
+int g16_autotune(g16_circuit* c, const uint8_t* w, size_t n, g16_tuning* out) {
+    if (!c || !w) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    int rc = check_witness(c, n, w);
+    if (rc) return rc;
+    CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
+    TuningLock lock(c);
+    if ((rc = lock.take())) return rc;
+    Workspace* ws = lock.ws;
+    const bool serial = c->serial;
+    if ((rc = upload_witness(ws, w, n))) return rc;
+    const int reps = 3;
+    auto whole = [&] { return time_on_stream(ws, reps, [&] { return enqueue_proof(c, ws, ws->d_w); }); };
+    const g16_tuning model = current_tuning(c);
+    double model_ms = whole();
+    if (model_ms < 0) return G16_ERR_DEVICE;
+    // 1. NTT tiling: gather + NTT chain alone
+    {
+        NttTiling best = c->ntt.tiling;
+        double best_t = -1;
+        for (uint32_t tl : {10u, 11u, 12u})
+            for (uint32_t ll : {1u, 2u, 3u}) {
+                if ((uint32_t)c->log_n <= 10 && !(tl == best.tile_log && ll == best.outer_log_l)) continue;
+                c->ntt.tiling = {tl, ll};
+                double t = time_on_stream(ws, reps, [&] { return run_h(c, ws, ws->d_w, ws->d_hpoly); });
+                if (t < 0) return G16_ERR_DEVICE;
+                if (best_t < 0 || t < best_t) {
+                    best_t = t;
+                    best = c->ntt.tiling;
+                }
+            }
+        c->ntt.tiling = best;
+    }
+    // 2. H MSM window (H from the tiling just chosen is in d_hpoly)
+    {
+        int best = c->c_h;
+        rc = climb_window(
+            c->c_h, [&](int b) { return b == c->c_h ? G16_OK : build_h_table(c, b, ws->stream); },
+            [&] { return time_on_stream(ws, reps, [&] { return enqueue_h_msm(c, ws, ws->d_hpoly); }); }, &best);
+        if (rc) return rc;
+    }
+    // 3. witness MSM window: the four MSMs serialised on one stream
+    {
+        c->serial = true;
+        int best = c->c_w;
+        rc = climb_window(
+            c->c_w, [&](int b) { return b == c->c_w ? G16_OK : build_witness_tables(c, b, ws->stream); },
+            [&] {
+                return time_on_stream(ws, reps, [&] {
+                    int r = enqueue_witness_msms(c, ws, ws->d_w);
+                    return r ? r : enqueue_join(ws);
+                });
+            },
+            &best);
+        c->serial = serial;
+        if (rc) return rc;
+    }
+    // 4. keep the tuned set only if the whole proof got faster
+    double tuned_ms = whole();
+    if (tuned_ms < 0) return G16_ERR_DEVICE;
+    if (tuned_ms > model_ms) {
+        if ((rc = apply_tuning(c, ws, model))) return rc;
+        tuned_ms = model_ms;
+    }
+    c->tuned.model_ms = model_ms;
+    c->tuned.tuned_ms = tuned_ms;
+    if (out) *out = current_tuning(c);
+    return G16_OK;
 }
 
 uint64_t g16_launch_count(void) { return timer().launches.load(); }
