@@ -336,6 +336,8 @@ def run_ours(args):
         "roofline": roof,
         "whole_proof_roofline": whole,
         "kernel_share": share,
+        "kernel_ms_per_step": {k: round(v[0] / K, 4) for k, v in kern.items()},
+        "kernel_launches_per_step": {k: v[1] / K for k, v in kern.items()},
         "kernel_rooflines": per_kernel,
         "stage_us_total": t,
         "gpu_launches": launches,

@@ -38,10 +38,11 @@ enum {
     G16_ERR_BACKEND = 3,          /* ProveError::Backend: malformed key or shape */
     G16_ERR_DEVICE = 4,           /* ProveError::Device: a CUDA call failed */
     G16_ERR_DEVICE_MEMORY = 5,    /* ProveError::DeviceMemory: refused before allocating */
-    G16_ERR_SELF_VERIFY = 6,      /* ProveError::SelfVerify (reserved) */
+    G16_ERR_SELF_VERIFY = 6,      /* ProveError::SelfVerify: g16_prove's proof failed its check */
     G16_ERR_TIMEOUT = 7,          /* a bounded device wait gave up */
     G16_ERR_INVALID_ARGUMENT = 8, /* null pointer, bad size, bad enum */
-    G16_ERR_FORMAT = 9            /* ZkeyError: malformed .zkey / .wtns bytes */
+    G16_ERR_FORMAT = 9,           /* ZkeyError: malformed .zkey / .wtns bytes */
+    G16_ERR_VERIFY = 10           /* verify::VerifyError: the proof does not verify */
 };
 
 /* Scalar encodings accepted by the MSM entry points. */
@@ -154,6 +155,28 @@ int g16_prove_with_blinders(g16_circuit *c, const uint8_t *witness_mont, size_t 
 int g16_prove_with_blinders_device(g16_circuit *c, const void *d_witness_mont, size_t n, const uint8_t *r_mont,
                                    const uint8_t *s_mont, g16_proof *out);
 int g16_stage_timings_get(const g16_circuit *c, g16_stage_timings *out);
+/* prove::prove (crates/groth16/src/prove.rs:34-92): r and s drawn from the
+ * operating system's CSPRNG, stages 0-11, then the proof is verified against
+ * the circuit's verifying key (timed as verify_us); G16_ERR_SELF_VERIFY when
+ * it does not verify. */
+int g16_prove(g16_circuit *c, const uint8_t *witness_mont, size_t n, g16_proof *out);
+
+/* ---------------- verification (crates/groth16/src/verify.rs:49-175) ----------------
+ * verify::verify on the host: key structure, proof elements (on the curve, B
+ * in the prime-order subgroup, none at infinity), then
+ * e(-A, B) e(alpha, beta) e(L, gamma) e(C, delta) = 1 with one final
+ * exponentiation.  public_mont: n_public Montgomery Fr (the witness's wires
+ * 1..n_public).  G16_OK when the proof verifies; G16_ERR_VERIFY when it does
+ * not or an element is invalid; G16_ERR_FORMAT for an unsafe key;
+ * G16_ERR_INVALID_ARGUMENT for a public-input count that does not match. */
+int g16_verify(const uint8_t *alpha_g1, const uint8_t *beta_g2, const uint8_t *gamma_g2, const uint8_t *delta_g2,
+               const uint8_t *ic, size_t n_ic, const uint8_t *public_mont, size_t n_public, const g16_proof *proof);
+/* The same against a prepared circuit's verifying key. */
+int g16_circuit_verify(const g16_circuit *c, const uint8_t *public_mont, size_t n_public, const g16_proof *proof);
+/* prod_i e(P_i, Q_i) == 1 for n packed affine pairs (G1 64 B, G2 128 B):
+ * returns 1, 0, or G16_ERR_INVALID_ARGUMENT (as a negative value) for
+ * non-canonical or off-curve input. */
+int g16_pairing_check(const uint8_t *g1_points, const uint8_t *g2_points, size_t n);
 
 /* ---------------- per-instance tuning (no reference counterpart) ----------------
  * The MSM window sizes and the NTT tiling of a prepared circuit.  g16_prepare

@@ -69,9 +69,14 @@ class FormatError(ProveError):
     code = 9
 
 
+class VerifyError(ProveError):
+    """verify::VerifyError (crates/groth16/src/verify.rs:17-33): the proof does not verify."""
+    code = 10
+
+
 _ERRORS = {c.code: c for c in (WitnessLengthError, ConstantWireError, BackendError, DeviceError,
                                 DeviceMemoryError, SelfVerifyError, TimeoutError_, InvalidArgumentError,
-                                FormatError)}
+                                FormatError, VerifyError)}
 
 _lib = None
 
@@ -170,6 +175,38 @@ class Proof:
         return "Proof(a=%s.., b=%s.., c=%s..)" % (self.a[:4].hex(), self.b[:4].hex(), self.c[:4].hex())
 
 
+def _proof_struct(proof):
+    raw = proof.to_bytes() if isinstance(proof, Proof) else bytes(proof)
+    if len(raw) != 256:
+        raise InvalidArgumentError("a proof is 256 bytes (A 64, B 128, C 64)")
+    p = _Proof()
+    ctypes.memmove(ctypes.addressof(p), raw, 256)
+    return p
+
+
+def verify(vk, public_mont, proof):
+    """verify::verify (crates/groth16/src/verify.rs:49-51) on the host.
+
+    vk = (alpha_g1, beta_g2, gamma_g2, delta_g2, [ic points]) packed bytes;
+    public_mont: the public inputs, Montgomery Fr.  Raises VerifyError,
+    FormatError (unsafe key) or InvalidArgumentError (count mismatch)."""
+    alpha, beta, gamma, delta, ic = vk
+    icb = b"".join(ic)
+    check(lib().g16_verify(bytes(alpha), bytes(beta), bytes(gamma), bytes(delta), icb, ctypes.c_size_t(len(ic)),
+                           bytes(public_mont), ctypes.c_size_t(len(public_mont) // 32),
+                           ctypes.byref(_proof_struct(proof))))
+
+
+def pairing_check(g1_points, g2_points):
+    """prod e(P_i, Q_i) == 1 over packed affine pairs."""
+    if len(g1_points) != len(g2_points):
+        raise InvalidArgumentError("pairing_check needs as many G1 as G2 points")
+    rc = lib().g16_pairing_check(b"".join(g1_points), b"".join(g2_points), ctypes.c_size_t(len(g1_points)))
+    if rc < 0:
+        check(-rc)
+    return rc == 1
+
+
 class MsmOutputs:
     """MsmOutputs (crates/groth16/src/lib.rs:311-318): five affine points, packed."""
 
@@ -240,6 +277,10 @@ class ProvingKey:
     def ic(self):
         raw = ctypes.string_at(self._view.ic, 64 * (self.n_public + 1))
         return [raw[64 * i:64 * i + 64] for i in range(self.n_public + 1)]
+
+    def verifying_key(self):
+        """(alpha_g1, beta_g2, gamma_g2, delta_g2, ic) packed, for verify()."""
+        return self.alpha_g1, self.beta_g2, self.gamma_g2, self.delta_g2, self.ic
 
     def close(self):
         if self._h:
@@ -359,6 +400,18 @@ class CudaCircuit:
         t = StageTimings()
         check(lib().g16_stage_timings_get(self._h, ctypes.byref(t)))
         return t.as_dict()
+
+    def prove(self, witness_mont):
+        """prove::prove (crates/groth16/src/prove.rs:34-92): fresh r, s, then the proof is checked."""
+        p = _Proof()
+        check(lib().g16_prove(self._h, _buf(witness_mont), ctypes.c_size_t(_nbytes(witness_mont) // 32),
+                              ctypes.byref(p)))
+        return Proof(p.a, p.b, p.c)
+
+    def verify(self, public_mont, proof):
+        """verify::verify against this circuit's key; raises VerifyError when the proof fails."""
+        check(lib().g16_circuit_verify(self._h, bytes(public_mont), ctypes.c_size_t(len(public_mont) // 32),
+                                       ctypes.byref(_proof_struct(proof))))
 
     def tuning(self):
         """MSM window bits and NTT tiling in use (cost model, autotuner or set_tuning)."""

@@ -5,28 +5,9 @@
 
 namespace g16 {
 
-FieldParams FR_P = {{0x43e1f593f0000001ULL, 0x2833e84879b97091ULL, 0xb85045b68181585dULL, 0x30644e72e131a029ULL},
-                    0, {{0}}, {{0}}};
-FieldParams FQ_P = {{0x3c208c16d87cfd47ULL, 0x97816a916871ca8dULL, 0xb85045b68181585dULL, 0x30644e72e131a029ULL},
-                    0, {{0}}, {{0}}};
-
 G1A G1_GENERATOR;
 G2A G2_GENERATOR;
 Fq2 TWIST_B;
-
-static void derive(FieldParams& f) {
-    uint64_t inv = 1;
-    for (int i = 0; i < 7; i++) inv *= 2 - f.p[0] * inv;
-    f.n0 = (uint64_t)0 - inv;
-    // R mod p and R^2 mod p by modular doubling
-    uint64_t x[4] = {1, 0, 0, 0};
-    for (int i = 0; i < 512; i++) {
-        if (i == 256) std::memcpy(f.one.v, x, 32);
-        uint64_t c = add4(x, x, x);
-        if (c || geq4(x, f.p)) sub4(x, x, f.p);
-    }
-    std::memcpy(f.r2.v, x, 32);
-}
 
 static Fq fq_dec(const char* s) {
     uint64_t v[4] = {0, 0, 0, 0};
@@ -44,8 +25,6 @@ static Fq fq_dec(const char* s) {
 void host_init() {
     static std::once_flag once;
     std::call_once(once, [] {
-        derive(FR_P);
-        derive(FQ_P);
         G1_GENERATOR.x = Fq::from_u64(1);
         G1_GENERATOR.y = Fq::from_u64(2);
         G1_GENERATOR.inf = false;

@@ -20,13 +20,52 @@ struct Fe {
 
 struct FieldParams {
     uint64_t p[4];
-    uint64_t n0;
-    Fe one;
-    Fe r2;
+    uint64_t n0;   // -p^-1 mod 2^64
+    Fe one;        // R mod p
+    Fe r2;         // R^2 mod p
 };
 
-extern FieldParams FR_P;
-extern FieldParams FQ_P;
+// n0, R and R^2 from the modulus, at compile time: R mod p and R^2 mod p by
+// 512 modular doublings of 1
+constexpr FieldParams make_field(uint64_t p0, uint64_t p1, uint64_t p2, uint64_t p3) {
+    FieldParams f{{p0, p1, p2, p3}, 0, {{0, 0, 0, 0}}, {{0, 0, 0, 0}}};
+    uint64_t inv = 1;
+    for (int i = 0; i < 7; i++) inv *= 2 - p0 * inv;
+    f.n0 = (uint64_t)0 - inv;
+    uint64_t x[4] = {1, 0, 0, 0};
+    for (int i = 0; i < 512; i++) {
+        if (i == 256)
+            for (int j = 0; j < 4; j++) f.one.v[j] = x[j];
+        uint64_t top = x[3] >> 63;
+        for (int j = 3; j > 0; j--) x[j] = (x[j] << 1) | (x[j - 1] >> 63);
+        x[0] <<= 1;
+        bool ge = top != 0;
+        if (!ge) {
+            ge = true;   // equal counts as >=
+            for (int j = 3; j >= 0; j--)
+                if (x[j] != f.p[j]) {
+                    ge = x[j] > f.p[j];
+                    break;
+                }
+        }
+        if (ge) {
+            uint64_t br = 0;
+            for (int j = 0; j < 4; j++) {
+                uint64_t a = x[j], b = f.p[j];
+                uint64_t d = a - b - br;
+                br = (a < b || a - b < br) ? 1 : 0;
+                x[j] = d;
+            }
+        }
+    }
+    for (int j = 0; j < 4; j++) f.r2.v[j] = x[j];
+    return f;
+}
+
+inline constexpr FieldParams FR_P =
+    make_field(0x43e1f593f0000001ULL, 0x2833e84879b97091ULL, 0xb85045b68181585dULL, 0x30644e72e131a029ULL);
+inline constexpr FieldParams FQ_P =
+    make_field(0x3c208c16d87cfd47ULL, 0x97816a916871ca8dULL, 0xb85045b68181585dULL, 0x30644e72e131a029ULL);
 void host_init();
 
 static inline bool geq4(const uint64_t* a, const uint64_t* p) {
@@ -63,46 +102,66 @@ struct Fp {
     bool is_zero() const { return (x.v[0] | x.v[1] | x.v[2] | x.v[3]) == 0; }
     bool operator==(const Fp& o) const { return std::memcmp(x.v, o.x.v, 32) == 0; }
     bool operator!=(const Fp& o) const { return !(*this == o); }
+    // Branch-free: both moduli are below 2^254, so a sum of two reduced
+    // values never carries out; the reduction is selected by a mask.
     Fp operator+(const Fp& o) const {
         Fp r;
-        uint64_t c = add4(r.x.v, x.v, o.x.v);
-        if (c || geq4(r.x.v, P.p)) sub4(r.x.v, r.x.v, P.p);
+        uint64_t s[4], d[4];
+        add4(s, x.v, o.x.v);
+        const uint64_t keep = (uint64_t)0 - sub4(d, s, P.p);   // all ones when s < p
+        for (int i = 0; i < 4; i++) r.x.v[i] = (s[i] & keep) | (d[i] & ~keep);
         return r;
     }
     Fp operator-(const Fp& o) const {
         Fp r;
-        if (sub4(r.x.v, x.v, o.x.v)) add4(r.x.v, r.x.v, P.p);
+        uint64_t d[4], pm[4];
+        const uint64_t mask = (uint64_t)0 - sub4(d, x.v, o.x.v);   // all ones on borrow
+        for (int i = 0; i < 4; i++) pm[i] = P.p[i] & mask;
+        add4(r.x.v, d, pm);
         return r;
     }
     Fp operator-() const { return is_zero() ? *this : zero() - *this; }
     Fp dbl() const { return *this + *this; }
+    // CIOS Montgomery product, unrolled over the constant modulus.  Both BN254
+    // moduli are below 2^254, so every partial result stays below 2p < 2^256
+    // and no fifth word survives a round.
     Fp operator*(const Fp& o) const {
-        uint64_t t[6] = {0, 0, 0, 0, 0, 0};
+        const uint64_t* a = x.v;
+        uint64_t t0 = 0, t1 = 0, t2 = 0, t3 = 0;
         for (int i = 0; i < 4; i++) {
-            uint64_t c = 0;
-            for (int j = 0; j < 4; j++) {
-                u128 uv = (u128)x.v[j] * o.x.v[i] + t[j] + c;
-                t[j] = (uint64_t)uv;
-                c = (uint64_t)(uv >> 64);
-            }
-            u128 s = (u128)t[4] + c;
-            t[4] = (uint64_t)s;
-            t[5] = (uint64_t)(s >> 64);
-            uint64_t m = t[0] * P.n0;
-            u128 uv = (u128)m * P.p[0] + t[0];
+            const uint64_t bi = o.x.v[i];
+            u128 uv = (u128)a[0] * bi + t0;
+            t0 = (uint64_t)uv;
+            uint64_t c = (uint64_t)(uv >> 64);
+            uv = (u128)a[1] * bi + t1 + c;
+            t1 = (uint64_t)uv;
             c = (uint64_t)(uv >> 64);
-            for (int j = 1; j < 4; j++) {
-                uv = (u128)m * P.p[j] + t[j] + c;
-                t[j - 1] = (uint64_t)uv;
-                c = (uint64_t)(uv >> 64);
-            }
-            s = (u128)t[4] + c;
-            t[3] = (uint64_t)s;
-            t[4] = t[5] + (uint64_t)(s >> 64);
+            uv = (u128)a[2] * bi + t2 + c;
+            t2 = (uint64_t)uv;
+            c = (uint64_t)(uv >> 64);
+            uv = (u128)a[3] * bi + t3 + c;
+            t3 = (uint64_t)uv;
+            const uint64_t t4 = (uint64_t)(uv >> 64);
+            const uint64_t m = t0 * P.n0;
+            uv = (u128)m * P.p[0] + t0;
+            c = (uint64_t)(uv >> 64);
+            uv = (u128)m * P.p[1] + t1 + c;
+            t0 = (uint64_t)uv;
+            c = (uint64_t)(uv >> 64);
+            uv = (u128)m * P.p[2] + t2 + c;
+            t1 = (uint64_t)uv;
+            c = (uint64_t)(uv >> 64);
+            uv = (u128)m * P.p[3] + t3 + c;
+            t2 = (uint64_t)uv;
+            t3 = t4 + (uint64_t)(uv >> 64);
         }
         Fp r;
-        std::memcpy(r.x.v, t, 32);
-        if (t[4] || geq4(r.x.v, P.p)) sub4(r.x.v, r.x.v, P.p);
+        r.x.v[0] = t0;
+        r.x.v[1] = t1;
+        r.x.v[2] = t2;
+        r.x.v[3] = t3;
+        uint64_t d[4];
+        if (!sub4(d, r.x.v, P.p)) std::memcpy(r.x.v, d, 32);
         return r;
     }
     Fp sqr() const { return *this * *this; }

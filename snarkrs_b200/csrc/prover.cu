@@ -31,6 +31,8 @@
 #include "host_bn254.hpp"
 #include "msm.cuh"
 #include "ntt.cuh"
+#include "pairing.hpp"
+#include <sys/random.h>
 
 namespace g16 {
 
@@ -218,7 +220,8 @@ struct g16_circuit {
     int c_w = 0, c_h = 0;   // window bits of the witness and H MSMs
     NttTables ntt;
     G1A alpha1, beta1, delta1;
-    G2A beta2, delta2;
+    G2A beta2, delta2, gamma2;
+    std::vector<G1A> ic;               // verifying key: constant wire, then the public inputs
     // workspaces: one per proof in flight
     std::mutex mu;
     std::condition_variable cv;
@@ -945,6 +948,13 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
         return fail(G16_ERR_BACKEND, "non-canonical header point");
     if (c->alpha1.inf || c->beta1.inf || c->delta1.inf || c->beta2.inf || c->delta2.inf)
         return fail(G16_ERR_BACKEND, "a header point is the point at infinity");
+    if (k->gamma_g2 && !unpack(c->gamma2, k->gamma_g2)) return fail(G16_ERR_BACKEND, "non-canonical gamma_g2");
+    if (!k->gamma_g2) c->gamma2.inf = true;
+    if (k->ic) {
+        c->ic.resize((size_t)k->n_public + 1);
+        for (size_t i = 0; i <= k->n_public; i++)
+            if (!unpack(c->ic[i], k->ic + 64 * i)) return fail(G16_ERR_BACKEND, "non-canonical IC point %zu", i);
+    }
     struct Up {
         void** dst;
         const void* src;
@@ -1104,6 +1114,105 @@ int g16_prove_with_blinders_device(g16_circuit* c, const void* d_w, size_t n, co
     WsGuard g(c);
     if ((rc = acquire(c, &g.ws))) return rc;
     return prove_on_device(c, g.ws, d_w, r, s, out);
+}
+
+int g16_prove(g16_circuit* c, const uint8_t* w, size_t n, g16_proof* out) {
+    if (!c || !w || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    // Fr::rand: uniform in [0, r) by rejection on 254-bit draws
+    uint8_t rs[2][32];
+    for (auto& x : rs) {
+        for (;;) {
+            uint64_t v[4];
+            size_t got = 0;
+            while (got < sizeof v) {
+                ssize_t k = getrandom((uint8_t*)v + got, sizeof v - got, 0);
+                if (k <= 0) return fail(G16_ERR_BACKEND, "getrandom failed");
+                got += (size_t)k;
+            }
+            v[3] &= (1ull << 62) - 1;
+            if (!g16::Fr::canonical(v)) continue;
+            if ((v[0] | v[1] | v[2] | v[3]) == 0) return fail(G16_ERR_BACKEND, "drew a zero blinder");
+            g16::Fr m = g16::Fr::from_std(v);
+            std::memcpy(x, m.x.v, 32);
+            break;
+        }
+    }
+    int rc = g16_prove_with_blinders(c, w, n, rs[0], rs[1], out);
+    if (rc) return rc;
+    auto t0 = std::chrono::steady_clock::now();
+    rc = g16_circuit_verify(c, w + 32, c->n_public, out);
+    uint64_t us = (uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(
+                      std::chrono::steady_clock::now() - t0).count();
+    {
+        std::lock_guard<std::mutex> g(c->mu);
+        c->t.verify_us += us;
+    }
+    if (rc == G16_ERR_VERIFY || rc == G16_ERR_FORMAT) {
+        std::string why = g_err;
+        return fail(G16_ERR_SELF_VERIFY, "the proof did not verify against its own key: %s", why.c_str());
+    }
+    return rc;
+}
+
+static int verify_status(VerifyResult v, const std::string& why) {
+    switch (v) {
+        case VerifyResult::Ok: return G16_OK;
+        case VerifyResult::PublicInputCount: return fail(G16_ERR_INVALID_ARGUMENT, "verify: %s", why.c_str());
+        case VerifyResult::EmptyKey:
+        case VerifyResult::UnsafeKey: return fail(G16_ERR_FORMAT, "verify: %s", why.c_str());
+        default: return fail(G16_ERR_VERIFY, "verify: %s", why.c_str());
+    }
+}
+
+int g16_verify(const uint8_t* alpha_g1, const uint8_t* beta_g2, const uint8_t* gamma_g2, const uint8_t* delta_g2,
+               const uint8_t* ic, size_t n_ic, const uint8_t* pub, size_t n_public, const g16_proof* proof) {
+    if (!alpha_g1 || !beta_g2 || !gamma_g2 || !delta_g2 || (n_ic && !ic) || (n_public && !pub) || !proof)
+        return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    host_init();
+    VerifyingKey vk;
+    std::vector<G1A> pts(n_ic);
+    if (!unpack(vk.alpha1, alpha_g1) || !unpack(vk.beta2, beta_g2) || !unpack(vk.gamma2, gamma_g2) ||
+        !unpack(vk.delta2, delta_g2))
+        return fail(G16_ERR_FORMAT, "verify: non-canonical verifying-key point");
+    for (size_t i = 0; i < n_ic; i++)
+        if (!unpack(pts[i], ic + 64 * i)) return fail(G16_ERR_FORMAT, "verify: non-canonical IC point %zu", i);
+    vk.ic = pts.data();
+    vk.n_ic = n_ic;
+    G1A a, c;
+    G2A b;
+    if (!unpack(a, proof->a) || !unpack(b, proof->b) || !unpack(c, proof->c))
+        return fail(G16_ERR_VERIFY, "verify: a proof coordinate is not below q");
+    for (size_t i = 0; i < n_public; i++) {
+        uint64_t v[4];
+        std::memcpy(v, pub + 32 * i, 32);
+        if (!g16::Fr::canonical(v)) return fail(G16_ERR_INVALID_ARGUMENT, "verify: public input %zu is not below r", i);
+    }
+    std::string why;
+    return verify_status(groth16_verify(vk, pub, n_public, a, b, c, &why), why);
+}
+
+int g16_circuit_verify(const g16_circuit* c, const uint8_t* pub, size_t n_public, const g16_proof* proof) {
+    if (!c || (n_public && !pub) || !proof) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    if (c->ic.empty()) return fail(G16_ERR_FORMAT, "verify: the key carried no IC section");
+    uint8_t alpha[64], beta[128], gamma[128], delta[128];
+    pack(alpha, c->alpha1);
+    pack(beta, c->beta2);
+    pack(gamma, c->gamma2);
+    pack(delta, c->delta2);
+    std::vector<uint8_t> ic(64 * c->ic.size());
+    for (size_t i = 0; i < c->ic.size(); i++) pack(ic.data() + 64 * i, c->ic[i]);
+    return g16_verify(alpha, beta, gamma, delta, ic.data(), c->ic.size(), pub, n_public, proof);
+}
+
+int g16_pairing_check(const uint8_t* g1, const uint8_t* g2, size_t n) {
+    if (n && (!g1 || !g2)) return -fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    host_init();
+    std::vector<G1A> p(n);
+    std::vector<G2A> q(n);
+    for (size_t i = 0; i < n; i++)
+        if (!unpack(p[i], g1 + 64 * i) || !unpack(q[i], g2 + 128 * i) || !on_curve(p[i]) || !on_curve(q[i]))
+            return -fail(G16_ERR_INVALID_ARGUMENT, "pairing input %zu is not a canonical curve point", i);
+    return pairing_product_is_one(p.data(), q.data(), n) ? 1 : 0;
 }
 
 int g16_stage_timings_get(const g16_circuit* c, g16_stage_timings* out) {
