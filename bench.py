@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--dist", type=int, default=0, help="MSM scalars: 0 uniform, 1 = 70%% in {0,1}")
     p.add_argument("--lanes", type=int, default=4, help="served proving: concurrent proofs")
     p.add_argument("--no-autotune", action="store_true", help="batched proving: keep the cost model's tuning")
+    p.add_argument("--no-mix", action="store_true",
+                   help="prove: skip the batched and served summaries attached to the plain-prove line")
     return p.parse_args()
 
 
@@ -347,6 +349,28 @@ def run_ours(args):
     }
     if cpu:
         line["cpu_baseline"] = cpu
+    if world == 1 and not args.no_mix:
+        circ.close()
+        # the metric's other half: batched and served proving against plain one-at-a-time
+        try:
+            b = run_batch(args, backend, emit=False, steps=min(args.steps, 3))
+            line["batched"] = {"workload": b["config"]["workload"], "value": b["value"], "unit": "proofs/s",
+                               "plain_value": b["plain"]["value"], "plain_p50_ms": b["plain"]["p50_ms"],
+                               "plain_p99_ms": b["plain"]["p99_ms"], "speedup_vs_plain": b["speedup_vs_plain"],
+                               "bit_exact_vs_plain": b["bit_exact_vs_plain"],
+                               "per_instance_tuning": b["config"]["per_instance_tuning"]}
+        except Exception as e:   # the plain-prove line above stands on its own
+            line["batched"] = {"error": repr(e)[:300]}
+        try:
+            v = run_serve(args, backend, emit=False, fracs=(1.5,), n_req=160)
+            top = v["sweep"][-1]
+            line["served"] = {"workload": v["config"]["workload"], "offered_fraction_of_plain_capacity": 1.5,
+                              "value": top["served"]["throughput"], "unit": "proofs/s",
+                              "p50_ms": top["served"]["p50_ms"], "p99_ms": top["served"]["p99_ms"],
+                              "plain_fifo": {k: top["plain_fifo"][k] for k in ("throughput", "p50_ms", "p99_ms")},
+                              "results_identical_alone_and_in_mix": v["results_identical_alone_and_in_mix"]}
+        except Exception as e:
+            line["served"] = {"error": repr(e)[:300]}
     print(json.dumps(line), flush=True)
     if dist:
         barrier()
@@ -482,6 +506,9 @@ def run_primitive(args):
     print(json.dumps(line), flush=True)
 
 
+BATCH_LANES = 8   # g16_prove_batch's default lane count (G16_BATCH_LANES)
+
+
 def batch_circuits(seed=3, count=8, lo=12, hi=18):
     """The batched workload's circuits: sizes log-uniform over 2^lo..2^hi constraints, seeded."""
     import random
@@ -489,13 +516,13 @@ def batch_circuits(seed=3, count=8, lo=12, hi=18):
     return sorted(int(2 ** rng.uniform(lo, hi)) for _ in range(count))
 
 
-def run_batch(args):
+def run_batch(args, backend=None, emit=True, steps=None):
     """64 proofs over 8 circuits of uneven size: one batched submission vs one at a time."""
     import snarkrs_b200 as S
     import torch
     rank, local_rank, world = dist_env()
     torch.cuda.set_device(local_rank)
-    backend = S.CudaBackend(local_rank)
+    backend = backend or S.CudaBackend(local_rank)
     sizes = batch_circuits()
     circs, wits, tunes = [], [], []
     t_tune = 0.0
@@ -504,8 +531,9 @@ def run_batch(args):
         circs.append(backend.prepare(S.ProvingKey.from_bytes(sc.zkey(TOXIC_SEED + i), check_points=False)))
         wits.append([sc.witness(1000 * i + j) for j in range(8)])
         if not args.no_autotune:
+            # the batched objective: as many proofs in flight as prove_batch has lanes
             t0 = time.perf_counter()
-            tunes.append(dict(circs[-1].autotune(wits[-1][0]), constraints=nc))
+            tunes.append(dict(circs[-1].autotune(wits[-1][0], concurrency=BATCH_LANES), constraints=nc))
             t_tune += time.perf_counter() - t0
         else:
             tunes.append(dict(circs[-1].tuning(), constraints=nc))
@@ -526,26 +554,32 @@ def run_batch(args):
         lat.append(time.perf_counter() - t1)
     t_plain = time.perf_counter() - t0
     best, out = None, None
-    for _ in range(max(1, args.steps)):
+    steps = steps or args.steps
+    for _ in range(max(1, steps)):
         t0 = time.perf_counter()
         out = backend.prove_batch(jobs)
         dt = time.perf_counter() - t0
         best = dt if best is None else min(best, dt)
     assert all(a == b for a, b in zip(out, plain)), "batched proofs differ from single proofs"
     lat.sort()
-    line = {"metric": "proofs/s", "value": len(jobs) / best, "unit": "proofs/s", "n_gpus": 1, "steps": args.steps,
+    line = {"metric": "proofs/s", "value": len(jobs) / best, "unit": "proofs/s", "n_gpus": 1, "steps": steps,
             "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32 (BN254 Montgomery limbs, exact)", "data": "synthetic",
             "config": {"workload": "batched prove: 64 proofs over 8 synthetic circuits, sizes log-uniform "
                                    "over 2^12..2^18 constraints, 8 witnesses each",
                        "constraints": sizes,
-                       "per_instance_tuning": "autotuner (g16_autotune, %.1f s for 8 circuits)" % t_tune
+                       "per_instance_tuning": "autotuner (g16_autotune, %d proofs in flight, %.1f s for 8 "
+                                              "circuits)" % (BATCH_LANES, t_tune)
                        if not args.no_autotune else "cost model", "tuning": tunes},
             "plain": {"value": len(jobs) / t_plain, "unit": "proofs/s", "p50_ms": 1e3 * lat[len(lat) // 2],
                       "p99_ms": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
             "batch_ms": 1e3 * best, "speedup_vs_plain": t_plain / best,
             "bit_exact_vs_plain": True}
-    print(json.dumps(line), flush=True)
+    for c in circs:
+        c.close()
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 # Circuits labelled 2^k constraints have domain 2^k and about 0.52 * 2^k active
@@ -565,7 +599,7 @@ def serve_circuits():
     return out
 
 
-def run_serve(args):
+def run_serve(args, backend=None, emit=True, fracs=(0.5, 0.9, 1.5), n_req=None):
     """Poisson arrivals over six circuits; continuous batching vs plain FIFO, p50/p99."""
     import random
     import statistics as st
@@ -573,7 +607,7 @@ def run_serve(args):
     import torch
     rank, local_rank, world = dist_env()
     torch.cuda.set_device(local_rank)
-    backend = S.CudaBackend(local_rank)
+    backend = backend or S.CudaBackend(local_rank)
     keys, wits = [], []
     for seed, nc in serve_circuits():
         sc = S.SynthCircuit(seed, nc, N_INPUTS, N_PUBLIC)
@@ -624,10 +658,10 @@ def run_serve(args):
     # plain capacity: mean service time over the mix, one request at a time
     calib, _ = run(1, 1e6, 60, 1)     # back-to-back arrivals = saturated FIFO
     cap = calib["throughput"]
-    n_req = max(100, args.steps * 40)
+    n_req = n_req or max(100, args.steps * 40)
     results = []
     mix_ok = True
-    for frac in (0.5, 0.9, 1.5):
+    for frac in fracs:
         rate = frac * cap
         plain, pp = run(1, rate, n_req, 42 + int(frac * 10))
         served, sp = run(args.lanes, rate, n_req, 42 + int(frac * 10))
@@ -643,7 +677,9 @@ def run_serve(args):
                        "plain_capacity_proofs_s": cap},
             "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"],
             "sweep": results, "results_identical_alone_and_in_mix": mix_ok}
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def main():

@@ -189,15 +189,19 @@ typedef struct {
     int32_t msm_window_bits_h;       /* c of the H MSM */
     int32_t ntt_tile_log;            /* inner NTT pass: tiles of 2^ntt_tile_log elements (2..12) */
     int32_t ntt_outer_log_l;         /* outer passes: 2^ntt_outer_log_l columns per tile row */
-    double model_ms;                 /* stages 0-9 device time with the cost model's choice (autotune only) */
+    double model_ms;                 /* device ms per proof with the cost model's choice (autotune only) */
     double tuned_ms;                 /* the same with the kept choice (autotune only) */
 } g16_tuning;
 int g16_tuning_get(const g16_circuit *c, g16_tuning *out);
 /* Applies explicit choices (window bits 8..20); no proof may be in flight on c. */
 int g16_tuning_set(g16_circuit *c, const g16_tuning *t);
 /* Times the candidates with one witness (n Montgomery Fr) and keeps the
- * fastest; no proof may be in flight on c.  out may be NULL. */
-int g16_autotune(g16_circuit *c, const uint8_t *witness_mont, size_t n, g16_tuning *out);
+ * fastest; no proof may be in flight on c.  concurrency 1 minimises one
+ * proof's latency (stage by stage); 2..8 minimises device time per proof
+ * with that many proofs in flight together on as many workspaces (the
+ * batched and served objective).  model_ms / tuned_ms are per proof.  out
+ * may be NULL. */
+int g16_autotune(g16_circuit *c, const uint8_t *witness_mont, size_t n, int concurrency, g16_tuning *out);
 
 /* ---------------- batched and served proving ---------------- */
 /* Proves count independent jobs (circuits may repeat or differ) in one

@@ -423,11 +423,14 @@ class CudaCircuit:
         t = _Tuning(msm_window_bits_witness, msm_window_bits_h, ntt_tile_log, ntt_outer_log_l, 0.0, 0.0)
         check(lib().g16_tuning_set(self._h, ctypes.byref(t)))
 
-    def autotune(self, witness_mont):
-        """Time window sizes and NTT tilings with this witness on the device; keep the fastest."""
+    def autotune(self, witness_mont, concurrency=1):
+        """Time window sizes and NTT tilings with this witness on the device; keep the fastest.
+
+        concurrency 1: one proof's latency; 2..8: device time per proof with
+        that many proofs in flight together (batched / served proving)."""
         t = _Tuning()
         check(lib().g16_autotune(self._h, _buf(witness_mont), ctypes.c_size_t(_nbytes(witness_mont) // 32),
-                                 ctypes.byref(t)))
+                                 int(concurrency), ctypes.byref(t)))
         return t.as_dict()
 
     def close(self):

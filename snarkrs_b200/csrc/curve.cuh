@@ -42,18 +42,23 @@ typedef Affine<Fq2> G2Affine;
 typedef Xyzz<Fq> G1Xyzz;
 typedef Xyzz<Fq2> G2Xyzz;
 
+// The formulas below group independent products per dependency level
+// (fmul2 / fmul3), which changes nothing in the values and lets the
+// out-of-line variant (INL = false) overlap their carry chains.
+
 // 2 * (x, y) for an affine point (mdbl-2008-s-1)
 template <class F, bool INL = true>
 __device__ __forceinline__ Xyzz<F> xyzz_dbl_affine(const F& x, const F& y) {
     F u = dbl(y);
-    F v = fsqr<INL>(u);
-    F w = fmul<INL>(u, v);
-    F s = fmul<INL>(x, v);
-    F xx = fsqr<INL>(x);
+    F v, xx, w, s, m2, t, wy;
+    fmul2<INL>(u, u, x, x, v, xx);      // V = U^2, X^2
+    fmul2<INL>(u, v, x, v, w, s);       // W = U V, S = X V
     F m = add(dbl(xx), xx);
+    m2 = fsqr<INL>(m);
     Xyzz<F> r;
-    r.x = sub(fsqr<INL>(m), dbl(s));
-    r.y = sub(fmul<INL>(m, sub(s, r.x)), fmul<INL>(w, y));
+    r.x = sub(m2, dbl(s));
+    fmul2<INL>(m, sub(s, r.x), w, y, t, wy);
+    r.y = sub(t, wy);
     r.zz = v;
     r.zzz = w;
     return r;
@@ -64,17 +69,27 @@ template <class F, bool INL = true>
 __device__ __forceinline__ Xyzz<F> xyzz_dbl(const Xyzz<F>& p) {
     if (p.is_inf()) return p;
     F u = dbl(p.y);
-    F v = fsqr<INL>(u);
-    F w = fmul<INL>(u, v);
-    F s = fmul<INL>(p.x, v);
-    F xx = fsqr<INL>(p.x);
+    F v, xx, w, s, m2, t, wy;
+    fmul2<INL>(u, u, p.x, p.x, v, xx);  // V = U^2, X^2
+    fmul2<INL>(u, v, p.x, v, w, s);     // W = U V, S = X V
     F m = add(dbl(xx), xx);
     Xyzz<F> r;
-    r.x = sub(fsqr<INL>(m), dbl(s));
-    r.y = sub(fmul<INL>(m, sub(s, r.x)), fmul<INL>(w, p.y));
-    r.zz = fmul<INL>(v, p.zz);
-    r.zzz = fmul<INL>(w, p.zzz);
+    fmul2<INL>(m, m, v, p.zz, m2, r.zz);     // M^2, ZZ3 = V ZZ1
+    r.x = sub(m2, dbl(s));
+    fmul3<INL>(m, sub(s, r.x), w, p.y, w, p.zzz, t, wy, r.zzz);   // ZZZ3 = W ZZZ1
+    r.y = sub(t, wy);
     return r;
+}
+
+// The doubling an addition falls into when both operands are equal: rare, so
+// one out-of-line copy keeps it (and its call arguments) out of the hot loops.
+template <class F>
+__device__ __noinline__ Xyzz<F> xyzz_dbl_affine_ool(F x, F y) {
+    return xyzz_dbl_affine<F, false>(x, y);
+}
+template <class F>
+__device__ __noinline__ Xyzz<F> xyzz_dbl_ool(Xyzz<F> p) {
+    return xyzz_dbl<F, false>(p);
 }
 
 // p + (x2, y2) for a finite affine point (madd-2008-s)
@@ -88,22 +103,34 @@ __device__ __forceinline__ Xyzz<F> xyzz_add_affine(const Xyzz<F>& p, const F& x2
         r.zzz = F::one();
         return r;
     }
-    F u2 = fmul<INL>(x2, p.zz);
-    F s2 = fmul<INL>(y2, p.zzz);
+    F u2, s2;
+    fmul2<INL>(x2, p.zz, y2, p.zzz, u2, s2);
     F pp_ = sub(u2, p.x);
     F rr = sub(s2, p.y);
     if (pp_.is_zero()) {
-        if (rr.is_zero()) return xyzz_dbl_affine<F, false>(x2, y2);   // rare: keep it out of the hot code
+        if (rr.is_zero()) return xyzz_dbl_affine_ool<F>(x2, y2);   // rare: keep it out of the hot code
         return Xyzz<F>::identity();
     }
-    F pp = fsqr<INL>(pp_);
-    F ppp = fmul<INL>(pp_, pp);
-    F q = fmul<INL>(p.x, pp);
     Xyzz<F> r;
-    r.x = sub(sub(fsqr<INL>(rr), ppp), dbl(q));
-    r.y = sub(fmul<INL>(rr, sub(q, r.x)), fmul<INL>(p.y, ppp));
-    r.zz = fmul<INL>(p.zz, pp);
-    r.zzz = fmul<INL>(p.zzz, ppp);
+    if constexpr (INL) {
+        // the accumulate kernel's inner loop: this order keeps the fewest
+        // values live (registers bound its occupancy)
+        F pp = sqr(pp_);
+        F ppp = mul(pp_, pp);
+        F q = mul(p.x, pp);
+        r.x = sub(sub(sqr(rr), ppp), dbl(q));
+        r.y = sub(mul(rr, sub(q, r.x)), mul(p.y, ppp));
+        r.zz = mul(p.zz, pp);
+        r.zzz = mul(p.zzz, ppp);
+    } else {
+        F pp, rr2, ppp, q, t, ypp;
+        fmul2<INL>(pp_, pp_, rr, rr, pp, rr2);
+        fmul2<INL>(pp_, pp, p.x, pp, ppp, q);
+        r.x = sub(sub(rr2, ppp), dbl(q));
+        fmul3<INL>(rr, sub(q, r.x), p.y, ppp, p.zzz, ppp, t, ypp, r.zzz);
+        r.y = sub(t, ypp);
+        r.zz = fmul<INL>(p.zz, pp);
+    }
     return r;
 }
 
@@ -112,24 +139,22 @@ template <class F, bool INL = true>
 __device__ __forceinline__ Xyzz<F> xyzz_add(const Xyzz<F>& p, const Xyzz<F>& q) {
     if (p.is_inf()) return q;
     if (q.is_inf()) return p;
-    F u1 = fmul<INL>(p.x, q.zz);
-    F u2 = fmul<INL>(q.x, p.zz);
-    F s1 = fmul<INL>(p.y, q.zzz);
-    F s2 = fmul<INL>(q.y, p.zzz);
+    F u1, u2, s1, s2, zz12, zzz12;
+    fmul3<INL>(p.x, q.zz, q.x, p.zz, p.zz, q.zz, u1, u2, zz12);
+    fmul3<INL>(p.y, q.zzz, q.y, p.zzz, p.zzz, q.zzz, s1, s2, zzz12);
     F pp_ = sub(u2, u1);
     F rr = sub(s2, s1);
     if (pp_.is_zero()) {
-        if (rr.is_zero()) return xyzz_dbl<F, false>(p);   // rare: keep it out of the hot code
+        if (rr.is_zero()) return xyzz_dbl_ool<F>(p);   // rare: keep it out of the hot code
         return Xyzz<F>::identity();
     }
-    F pp = fsqr<INL>(pp_);
-    F ppp = fmul<INL>(pp_, pp);
-    F qq = fmul<INL>(u1, pp);
+    F pp, rr2, ppp, qq, t, sppp;
+    fmul2<INL>(pp_, pp_, rr, rr, pp, rr2);
     Xyzz<F> r;
-    r.x = sub(sub(fsqr<INL>(rr), ppp), dbl(qq));
-    r.y = sub(fmul<INL>(rr, sub(qq, r.x)), fmul<INL>(s1, ppp));
-    r.zz = fmul<INL>(fmul<INL>(p.zz, q.zz), pp);
-    r.zzz = fmul<INL>(fmul<INL>(p.zzz, q.zzz), ppp);
+    fmul3<INL>(pp_, pp, u1, pp, zz12, pp, ppp, qq, r.zz);
+    r.x = sub(sub(rr2, ppp), dbl(qq));
+    fmul3<INL>(rr, sub(qq, r.x), s1, ppp, zzz12, ppp, t, sppp, r.zzz);
+    r.y = sub(t, sppp);
     return r;
 }
 

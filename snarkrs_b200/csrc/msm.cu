@@ -1,5 +1,6 @@
 // Pippenger MSM kernels and engine (see msm.cuh for the pipeline).
 #include "msm.cuh"
+#include <type_traits>
 #include "common.cuh"
 #include "curve.cuh"
 #include <algorithm>
@@ -233,7 +234,10 @@ __global__ void __launch_bounds__(128) k_accumulate(const uint32_t* __restrict__
             Affine<F> p = ld_affine<F>(bases, idx - base_offset);
             if (!p.is_inf()) {
                 if (e >> 31) p.y = neg(p.y);
-                acc = xyzz_add_affine(acc, p.x, p.y);
+                // G1 keeps its products inlined; the Fq2 body is large enough
+                // that one out-of-line Fq2 product (three Fq chains) runs
+                // faster than inlined code that misses the instruction cache
+                acc = xyzz_add_affine<F, !std::is_same<F, Fq2>::value>(acc, p.x, p.y);
                 adds++;
             }
         }
@@ -331,25 +335,26 @@ __global__ void __launch_bounds__(128) k_bucket_sums(const uint4* __restrict__ p
     st_xyzz<F>(buckets, g, acc);
 }
 
-// Segment (w, p) of SEG buckets: running sums give run = sum S_b and
-// tot = sum (b - p SEG + 1) S_b over the segment; the segment's share of
-// sum_b (b + 1) S_b is then tot + (p SEG) run.
-constexpr uint32_t SEG = 8;
+// Segment (w, p) of seg buckets: running sums give run = sum S_b and
+// tot = sum (b - p seg + 1) S_b over the segment; the segment's share of
+// sum_b (b + 1) S_b is then tot + (p seg) run.  seg is 1..8: short segments
+// when there are few buckets (more threads, a shorter dependent chain), up to
+// 8 when there are enough segments to fill the GPU anyway (msm_segment_len).
 
 template <class F>
 __global__ void __launch_bounds__(128) k_segments(const uint4* __restrict__ buckets, uint32_t B, uint32_t W,
-                                                  uint32_t P, uint4* __restrict__ seg_out) {
+                                                  uint32_t P, uint32_t seg, uint4* __restrict__ seg_out) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= W * P) return;
     uint32_t w = t / P, p = t % P;
     Xyzz<F> run = Xyzz<F>::identity(), tot = Xyzz<F>::identity();
-    size_t g0 = (size_t)w * B + (size_t)p * SEG;
+    size_t g0 = (size_t)w * B + (size_t)p * seg;
 #pragma unroll 1
-    for (int j = SEG - 1; j >= 0; j--) {
+    for (int j = (int)seg - 1; j >= 0; j--) {
         run = xyzz_add<F, false>(run, ld_xyzz<F>(buckets, g0 + j));
         tot = xyzz_add<F, false>(tot, run);
     }
-    uint32_t k = p * SEG;
+    uint32_t k = p * seg;
     Xyzz<F> acc = Xyzz<F>::identity();
     if (k) {
         for (int bit = 31 - __clz(k); bit >= 0; bit--) {
@@ -612,9 +617,10 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     size_t chunks = (max_entries + s.chunk - 1) / s.chunk;
     size_t max_partials = (size_t)s.K + chunks + 1;
     G16_CUDA(grow_bytes(acc.d_partials, acc.cap_partials, max_partials * xyzz_bytes));
-    const uint32_t P = s.B / SEG;                  // segments per window
-    const uint32_t G = (P + 511) / 512;            // group-sum blocks per window
     const uint32_t Wr = s.shared ? 1u : (uint32_t)s.W;   // bucket sets to reduce
+    const uint32_t seg = msm_segment_len(Wr, s.B);
+    const uint32_t P = s.B / seg;                  // segments per window
+    const uint32_t G = (uint32_t)msm_group_blocks(P);   // group-sum blocks per window
     acc.segs_per_window = P;
     G16_CUDA(grow_bytes(acc.d_buckets, acc.cap_buckets, (size_t)s.K * xyzz_bytes));
     G16_CUDA(grow_bytes(acc.d_segments, acc.cap_segments, ((size_t)Wr * P + (size_t)Wr * G) * xyzz_bytes));
@@ -648,7 +654,7 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     }
     {
         TimedLaunch tl("msm_segments", st);
-        k_segments<F><<<blocks_for((size_t)Wr * P, 128), 128, 0, st>>>((const uint4*)acc.d_buckets, s.B, Wr, P,
+        k_segments<F><<<blocks_for((size_t)Wr * P, 128), 128, 0, st>>>((const uint4*)acc.d_buckets, s.B, Wr, P, seg,
                                                                         (uint4*)acc.d_segments);
     }
     {

@@ -79,6 +79,20 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
 
 // Window count for c-bit signed digits over 255 bits.
 inline int msm_windows(int c) { return (255 + c - 1) / c; }
+// Buckets per running-sum segment (1..8) when bucket_sets sets of
+// buckets_per_set buckets are reduced.  A segment thread runs 2 seg additions
+// and a double-and-add of ~1.5 log2(buckets) operations, so short segments
+// shorten the dependent chain but multiply the total work.  Reductions of up
+// to 2048 buckets (small proofs, latency-bound) get one segment thread per
+// bucket; from 16384 buckets on, segments of 8 keep the work near 5 additions
+// per bucket.
+constexpr uint32_t msm_segment_len(uint64_t bucket_sets, uint64_t buckets_per_set) {
+    uint32_t seg = 1;
+    while (seg < 8 && bucket_sets * buckets_per_set / seg > 2048) seg *= 2;
+    return seg;
+}
+// Group-sum blocks per bucket set for P segments per set.
+constexpr uint64_t msm_group_blocks(uint64_t segs_per_set) { return (segs_per_set + 511) / 512; }
 // Window width for window-shifted bases: the cost is ~m * ceil(255/c) mixed
 // additions plus a single bucket reduction over 2^(c-1) buckets.
 int msm_shared_window_bits(size_t m);

@@ -43,7 +43,8 @@ constexpr int NOALLOC_W = (255 + NOALLOC_C - 1) / NOALLOC_C;      // 24 windows
 constexpr size_t NOALLOC_B = (size_t)1 << (NOALLOC_C - 1);        // 1024 buckets per window
 constexpr size_t NOALLOC_K = NOALLOC_W * NOALLOC_B;               // 24576 buckets in all
 constexpr size_t NOALLOC_CHUNK = 16;                              // entries per accumulate thread
-constexpr size_t NOALLOC_SEGS = NOALLOC_B / 8;                    // running-sum segments per window
+constexpr size_t NOALLOC_SEGS = NOALLOC_B / g16::msm_segment_len(NOALLOC_W, NOALLOC_B);   // segments per window
+constexpr size_t NOALLOC_GROUPS = g16::msm_group_blocks(NOALLOC_SEGS);                      // per window
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -66,7 +67,7 @@ constexpr size_t PARTIALS_BYTES =
 constexpr size_t OFF_BUCKETS = align256(OFF_PARTIALS + PARTIALS_BYTES);
 constexpr size_t BUCKETS_BYTES = g16::XYZZ_G1_BYTES * NOALLOC_K;
 constexpr size_t OFF_SEGMENTS = align256(OFF_BUCKETS + BUCKETS_BYTES);
-constexpr size_t SEGMENTS_BYTES = g16::XYZZ_G1_BYTES * (NOALLOC_W * NOALLOC_SEGS + NOALLOC_W);
+constexpr size_t SEGMENTS_BYTES = g16::XYZZ_G1_BYTES * (NOALLOC_W * NOALLOC_SEGS + NOALLOC_W * NOALLOC_GROUPS);
 constexpr size_t OFF_WINDOWS = align256(OFF_SEGMENTS + SEGMENTS_BYTES);
 constexpr size_t WINDOWS_BYTES = g16::XYZZ_G1_BYTES * NOALLOC_W;
 constexpr size_t OFF_WORK = align256(OFF_WINDOWS + WINDOWS_BYTES);

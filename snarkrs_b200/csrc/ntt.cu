@@ -63,9 +63,9 @@ __device__ __forceinline__ void run_stage(uint4* sm, uint32_t j, uint32_t s_lo, 
         if (DIF) {
             Fr d = sub(a, b);
             a = add(a, b);
-            b = pos ? mul(d, ld_g(tw, (size_t)pos << (log_n - s - 1))) : d;
+            b = pos ? mul_cc(d, ld_g(tw, (size_t)pos << (log_n - s - 1))) : d;
         } else {
-            Fr t = pos ? mul(b, ld_g(tw, (size_t)pos << (log_n - s - 1))) : b;
+            Fr t = pos ? mul_cc(b, ld_g(tw, (size_t)pos << (log_n - s - 1))) : b;
             b = sub(a, t);
             a = add(a, t);
         }
@@ -107,9 +107,9 @@ __global__ void __launch_bounds__(256) k_ntt_pass(Vec3 vecs, uint32_t log_n, uin
         uint32_t mid = e >> log_L, l = e & (L - 1u);
         size_t gi = (hi << (s_lo + k)) | ((size_t)mid << s_lo) | (lo0 + l);
         Fr x = ld_s(sm, e);
-        if (scale) x = mul(x, sc);
+        if (scale) x = mul_cc(x, sc);
         if (join_out) {
-            Fr h = sub(mul(ld_rw(join_a, gi), ld_rw(join_b, gi)), x);
+            Fr h = sub(mul_cc(ld_rw(join_a, gi), ld_rw(join_b, gi)), x);
             st_g(join_out, gi, h);
         } else {
             st_g(data, gi, x);
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(256) k_ntt_mid(Vec3 vecs, uint32_t log_n, uint
         run_stage<true>(sm, (uint32_t)j, 0, 0, 0, log_n, tile / 2, tw_inv);
         __syncthreads();
     }
-    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) st_s(sm, e, mul(ld_s(sm, e), ld_g(coset, base + e)));
+    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) st_s(sm, e, mul_cc(ld_s(sm, e), ld_g(coset, base + e)));
     __syncthreads();
     for (uint32_t j = 0; j < k; j++) {
         run_stage<false>(sm, j, 0, 0, 0, log_n, tile / 2, tw);
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(256) k_ntt_mid(Vec3 vecs, uint32_t log_n, uint
     for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
         Fr x = ld_s(sm, e);
         if (join_out) {
-            st_g(join_out, base + e, sub(mul(ld_rw(join_a, base + e), ld_rw(join_b, base + e)), x));
+            st_g(join_out, base + e, sub(mul_cc(ld_rw(join_a, base + e), ld_rw(join_b, base + e)), x));
         } else {
             st_g(data, base + e, x);
         }
@@ -157,8 +157,8 @@ __global__ void __launch_bounds__(256) k_ntt_mid(Vec3 vecs, uint32_t log_n, uint
 __device__ __forceinline__ Fr fr_pow_u64(Fr b, uint64_t e) {
     Fr acc = Fr::one();
     while (e) {
-        if (e & 1) acc = mul(acc, b);
-        b = mul(b, b);
+        if (e & 1) acc = mul_cc(acc, b);
+        b = mul_cc(b, b);
         e >>= 1;
     }
     return acc;
@@ -169,11 +169,11 @@ __global__ void k_powers(uint4* out, Fr base, Fr scale, uint64_t count, uint32_t
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     uint64_t i0 = t * 16;
     if (i0 >= count) return;
-    Fr p = mul(scale, fr_pow_u64(base, i0));
+    Fr p = mul_cc(scale, fr_pow_u64(base, i0));
     for (uint64_t i = i0; i < i0 + 16 && i < count; i++) {
         size_t dst = bitrev_log ? (size_t)(__brevll(i) >> (64 - bitrev_log)) : (size_t)i;
         st_g(out, dst, p);
-        p = mul(p, base);
+        p = mul_cc(p, base);
     }
 }
 
@@ -184,8 +184,8 @@ __global__ void k_distribute(uint4* a, Fr shift, uint64_t n) {
     if (i0 >= n) return;
     Fr p = fr_pow_u64(shift, i0);
     for (uint64_t i = i0; i < i0 + 16 && i < n; i++) {
-        st_g(a, i, mul(ld_rw(a, i), p));
-        p = mul(p, shift);
+        st_g(a, i, mul_cc(ld_rw(a, i), p));
+        p = mul_cc(p, shift);
     }
 }
 
@@ -203,7 +203,7 @@ __global__ void k_bitrev(uint4* a, uint32_t log_n, uint64_t n) {
 __global__ void k_join(const uint4* a, const uint4* b, const uint4* c, uint4* h, uint64_t n) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    st_g(h, i, sub(mul(ld_rw(a, i), ld_rw(b, i)), ld_rw(c, i)));
+    st_g(h, i, sub(mul_cc(ld_rw(a, i), ld_rw(b, i)), ld_rw(c, i)));
 }
 
 }  // namespace g16d

@@ -386,7 +386,7 @@ VerifyResult groth16_verify(const VerifyingKey& vk, const uint8_t* public_mont, 
         say("gamma_g2 equals delta_g2: the key had no phase-2 contribution");
         return VerifyResult::UnsafeKey;
     }
-    // check_proof (verify.rs:88-110)
+    // check_proof (crates/groth16/src/verify.rs:80-108)
     if (a.inf || b.inf || c.inf) {
         say(a.inf ? "A is the point at infinity" : b.inf ? "B is the point at infinity" : "C is the point at infinity");
         return VerifyResult::InvalidProof;
@@ -404,9 +404,9 @@ VerifyResult groth16_verify(const VerifyingKey& vk, const uint8_t* public_mont, 
         return VerifyResult::InvalidProof;
     }
     // B's subgroup check runs beside the pairing; an invalid B is refused
-    // whatever the pairing says (verify.rs:62-70)
+    // whatever the pairing says (crates/groth16/src/verify.rs:57-66)
     auto b_ok = std::async(std::launch::async, [&b] { return in_g2_subgroup(b); });
-    // aggregate_public (verify.rs:150-175)
+    // aggregate_public (crates/groth16/src/verify.rs:150-175)
     if (vk.n_ic == 0) {
         say("verifying key has an empty IC");
         b_ok.wait();

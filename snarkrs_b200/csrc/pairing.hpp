@@ -1,11 +1,11 @@
 // Host optimal-ate pairing over BN254 and the Groth16 verifier built on it.
 //
 // Replaces the reference's verify::verify / verify_unchecked / check_proof /
-// aggregate_public (crates/groth16/src/verify.rs:49-150), which prove::prove
+// aggregate_public (crates/groth16/src/verify.rs:49-175), which prove::prove
 // runs on every proof before returning it (crates/groth16/src/prove.rs:34-92).
-// A verification is four Miller loops sharing one accumulator and one final
-// exponentiation, about a millisecond on one host core; it never runs on the
-// device.
+// A verification is four Miller loops, one host thread each, whose product
+// goes through one final exponentiation, with B's subgroup check on a fifth
+// thread: a few milliseconds of host time.  It never runs on the device.
 //
 // Tower: Fq2 = Fq[u]/(u^2 + 1), Fq6 = Fq2[v]/(v^3 - xi) with xi = 9 + u,
 // Fq12 = Fq6[w]/(w^2 - v).  G2 lives on the D-type sextic twist

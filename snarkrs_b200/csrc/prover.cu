@@ -149,7 +149,7 @@ namespace {
 
 // The device state of one proof in flight.  A prepared circuit keeps a pool of
 // these, so several proofs of the same circuit overlap on the GPU, each on its
-// own three streams with its own scratch.
+// own five streams (the main one and one per witness MSM) with its own scratch.
 struct Workspace {
     void* d_w = nullptr;       // witness, n_vars Fr
     void* d_abc = nullptr;     // A | B | C, n Fr each
@@ -159,9 +159,10 @@ struct Workspace {
     uint8_t* h_win = nullptr;  // pinned readback of the MSM results
     unsigned long long* h_work = nullptr;
     cudaStream_t stream = nullptr;             // gather -> NTT -> H MSM, and the join
-    cudaStream_t s2 = nullptr, s3 = nullptr;   // witness MSMs: A, L on s2; B1, B2 on s3
+    cudaStream_t side[4] = {nullptr, nullptr, nullptr, nullptr};   // witness MSMs A, B1, L, B2, one each
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaEvent_t ev_fork = nullptr, ev_sort = nullptr, ev_s2 = nullptr, ev_s3 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_sort = nullptr;
+    cudaEvent_t ev_side[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaGraphExec_t graph = nullptr;   // stages 0-9 captured once, replayed per proof
     uint64_t graph_kernels = 0;
     uint64_t proofs = 0;
@@ -174,17 +175,17 @@ struct Workspace {
         if (e == cudaSuccess) e = cudaMallocHost((void**)&h_win, 5 * 32 * 256);
         if (e == cudaSuccess) e = cudaMallocHost((void**)&h_work, 8 * sizeof(unsigned long long));
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
-        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
-        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s3, cudaStreamNonBlocking);
+        for (auto& x : side)
+            if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
         for (auto& x : ev)
             if (e == cudaSuccess) e = cudaEventCreate(&x);
-        for (cudaEvent_t* x : {&ev_fork, &ev_sort, &ev_s2, &ev_s3})
+        for (cudaEvent_t* x : {&ev_fork, &ev_sort, &ev_side[0], &ev_side[1], &ev_side[2], &ev_side[3]})
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(x, cudaEventDisableTiming);
         bytes = 32ull * n_vars + 32ull * n * 4;
         return e;
     }
     void release() {
-        for (cudaStream_t s : {stream, s2, s3})
+        for (cudaStream_t s : {stream, side[0], side[1], side[2], side[3]})
             if (s) cudaStreamSynchronize(s);
         if (graph) cudaGraphExecDestroy(graph);
         cudaFree(d_w);
@@ -197,9 +198,9 @@ struct Workspace {
         if (h_work) cudaFreeHost(h_work);
         for (auto& x : ev)
             if (x) cudaEventDestroy(x);
-        for (cudaEvent_t x : {ev_fork, ev_sort, ev_s2, ev_s3})
+        for (cudaEvent_t x : {ev_fork, ev_sort, ev_side[0], ev_side[1], ev_side[2], ev_side[3]})
             if (x) cudaEventDestroy(x);
-        for (cudaStream_t s : {s2, s3, stream})
+        for (cudaStream_t s : {side[0], side[1], side[2], side[3], stream})
             if (s) cudaStreamDestroy(s);
         *this = Workspace();
     }
@@ -525,33 +526,37 @@ int run_h(g16_circuit* c, Workspace* ws, const void* d_w, void* h_out) {
 }
 
 // Stages 5-9.  The witness sort and the A, B1, L, B2 accumulations depend only
-// on the witness, so they run on two side streams (ordered after the witness
-// upload) while the main stream does gather -> NTT -> H sort -> H accumulate;
-// the main stream joins them before the results are read back.
+// on the witness, so they run on four side streams, one per MSM (ordered after
+// the witness upload; the sort on the first), while the main stream does
+// gather -> NTT -> H sort -> H accumulate; the main stream joins them before
+// the results are read back.
 constexpr size_t WIN_SLOT = 32 * 256;
 
 int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
     const uint32_t nw = c->n_vars * (uint32_t)msm_windows(c->c_w);
-    cudaStream_t s2 = c->serial ? ws->stream : ws->s2, s3 = c->serial ? ws->stream : ws->s3;
+    cudaStream_t st[4];
+    for (int i = 0; i < 4; i++) st[i] = c->serial ? ws->stream : ws->side[i];
     CK(cudaEventRecord(ws->ev_fork, ws->stream), "event");
-    CK(cudaStreamWaitEvent(s2, ws->ev_fork, 0), "stream wait");
-    CK(msm_sort(ws->sort_w, d_w, c->n_vars, true, c->c_w, s2, true), "witness sort");
-    CK(cudaEventRecord(ws->ev_sort, s2), "event");
-    CK(cudaStreamWaitEvent(s3, ws->ev_sort, 0), "stream wait");
-    CK(msm_accumulate_g1(ws->sort_w, ws->acc[0], c->t_a, 0, nw, s2), "A accumulate");
-    CK(msm_accumulate_g1(ws->sort_w, ws->acc[2], c->t_b1, 0, nw, s3), "B1 accumulate");
-    CK(msm_accumulate_g1(ws->sort_w, ws->acc[3], c->t_l, 0, nw, s2), "L accumulate");
-    CK(msm_accumulate_g2(ws->sort_w, ws->acc[1], c->t_b2, 0, nw, s3), "B2 accumulate");
+    CK(cudaStreamWaitEvent(st[0], ws->ev_fork, 0), "stream wait");
+    CK(msm_sort(ws->sort_w, d_w, c->n_vars, true, c->c_w, st[0], true), "witness sort");
+    CK(cudaEventRecord(ws->ev_sort, st[0]), "event");
+    for (int i = 1; i < 4; i++) CK(cudaStreamWaitEvent(st[i], ws->ev_sort, 0), "stream wait");
+    // acc slots: 0 A, 1 B2, 2 B1, 3 L (4 is H); one stream per MSM so that
+    // their latency-bound reduction tails run side by side
+    CK(msm_accumulate_g1(ws->sort_w, ws->acc[0], c->t_a, 0, nw, st[0]), "A accumulate");
+    CK(msm_accumulate_g1(ws->sort_w, ws->acc[2], c->t_b1, 0, nw, st[1]), "B1 accumulate");
+    CK(msm_accumulate_g1(ws->sort_w, ws->acc[3], c->t_l, 0, nw, st[2]), "L accumulate");
+    CK(msm_accumulate_g2(ws->sort_w, ws->acc[1], c->t_b2, 0, nw, st[3]), "B2 accumulate");
+    const int stream_of[4] = {0, 3, 1, 2};   // acc slot -> stream
     for (int i = 0; i < 4; i++) {
-        cudaStream_t st = (i == 0 || i == 3) ? s2 : s3;
+        cudaStream_t s_i = st[stream_of[i]];
         size_t bytes = i == 1 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES;   // one shared window per MSM
-        CK(cudaMemcpyAsync(ws->h_win + i * WIN_SLOT, ws->acc[i].d_windows, bytes, cudaMemcpyDeviceToHost, st),
+        CK(cudaMemcpyAsync(ws->h_win + i * WIN_SLOT, ws->acc[i].d_windows, bytes, cudaMemcpyDeviceToHost, s_i),
            "window readback");
         if (timer().enabled)
-            CK(cudaMemcpyAsync(ws->h_work + i, ws->acc[i].d_work, 8, cudaMemcpyDeviceToHost, st), "work readback");
+            CK(cudaMemcpyAsync(ws->h_work + i, ws->acc[i].d_work, 8, cudaMemcpyDeviceToHost, s_i), "work readback");
     }
-    CK(cudaEventRecord(ws->ev_s2, s2), "event");
-    CK(cudaEventRecord(ws->ev_s3, s3), "event");
+    for (int i = 0; i < 4; i++) CK(cudaEventRecord(ws->ev_side[i], st[i]), "event");
     return G16_OK;
 }
 
@@ -568,8 +573,7 @@ int enqueue_h_msm(g16_circuit* c, Workspace* ws, const void* d_h) {
 }
 
 int enqueue_join(Workspace* ws) {
-    CK(cudaStreamWaitEvent(ws->stream, ws->ev_s2, 0), "stream wait");
-    CK(cudaStreamWaitEvent(ws->stream, ws->ev_s3, 0), "stream wait");
+    for (int i = 0; i < 4; i++) CK(cudaStreamWaitEvent(ws->stream, ws->ev_side[i], 0), "stream wait");
     CK(stage_event(ws->ev[3], ws->stream), "event");
     return G16_OK;
 }
@@ -605,7 +609,7 @@ int enqueue_proof(g16_circuit* c, Workspace* ws, const void* d_w) {
 
 // Stages 0-9.  From the second proof on a workspace (when every scratch buffer
 // has reached its size) the whole enqueue sequence is captured once as a CUDA
-// graph over the workspace's three streams and replayed, one launch per proof.
+// graph over the workspace's five streams and replayed, one launch per proof.
 int run_proof(g16_circuit* c, Workspace* ws, const void* d_w, MsmJac& out) {
     bool use_graph = c->graphs && !c->serial && !timer().enabled && ws->proofs > 0;
     if (use_graph) {
@@ -717,17 +721,40 @@ double time_on_stream(Workspace* ws, int reps, Fn&& enqueue) {
 // only one out of the pool, no other proof can start until release.
 struct TuningLock {
     g16_circuit* c;
-    Workspace* ws = nullptr;
+    Workspace* ws = nullptr;            // the first workspace (also in all[0])
+    std::vector<Workspace*> all;        // every workspace the tuner holds
     bool held = false;
     explicit TuningLock(g16_circuit* cc) : c(cc) {}
-    int take() {
+    // Take one workspace; the circuit must have no proof in flight.  Then
+    // up to `want` workspaces in all (idle ones first, new ones while the
+    // memory budget allows), for the concurrent objective.
+    int take(int want = 1) {
         int rc = acquire(c, &ws);
         if (rc) return rc;
+        all.push_back(ws);
         std::lock_guard<std::mutex> g(c->mu);
         if (c->idle.size() + 1 != c->pool.size())
             return fail(G16_ERR_INVALID_ARGUMENT, "tuning needs a circuit with no proof in flight");
         c->tuning = true;
         held = true;
+        while ((int)all.size() < want) {
+            if (!c->idle.empty()) {
+                all.push_back(c->idle.back());
+                c->idle.pop_back();
+                continue;
+            }
+            if (c->pool.size() >= c->max_workspaces || c->be->vram_used + c->ws_estimate > c->be->vram_limit) break;
+            auto w = std::make_unique<Workspace>();
+            if (w->init(c->n_vars, c->n) != cudaSuccess) {
+                w->release();
+                cudaGetLastError();
+                break;
+            }
+            c->device_bytes += c->ws_estimate;
+            c->be->vram_used += c->ws_estimate;
+            all.push_back(w.get());
+            c->pool.push_back(std::move(w));
+        }
         return G16_OK;
     }
     ~TuningLock() {
@@ -740,14 +767,67 @@ struct TuningLock {
             }
             c->ws_estimate = workspace_estimate(c->n_vars, c->n, c->c_w, c->c_h);
         }
-        if (ws) {
+        {
             std::lock_guard<std::mutex> g(c->mu);
-            c->idle.push_back(ws);
-            c->tuning = false;
+            for (Workspace* w : all) c->idle.push_back(w);
+            if (held) c->tuning = false;
         }
         c->cv.notify_all();
     }
 };
+
+// Device time per proof with stages 0-9 of one proof on every workspace in
+// flight together (the batched / served objective): the minimum over reps of
+// (last workspace done - common start) / workspaces.  Negative on failure.
+double time_concurrent(g16_circuit* c, const std::vector<Workspace*>& all, int reps) {
+    std::vector<cudaEvent_t> ev(all.size() + 1, nullptr);
+    for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            for (auto& x : ev)
+                if (x) cudaEventDestroy(x);
+            cuda_fail(cudaGetLastError(), "tuning events");
+            return -1.0;
+        }
+    double best = -1.0;
+    for (int r = 0; r <= reps && best != -2.0; r++) {
+        cudaError_t e = cudaEventRecord(ev[0], all[0]->stream);
+        for (size_t i = 1; i < all.size() && e == cudaSuccess; i++) e = cudaStreamWaitEvent(all[i]->stream, ev[0], 0);
+        if (e != cudaSuccess) {
+            cuda_fail(e, "tuning");
+            best = -2.0;
+            break;
+        }
+        for (size_t i = 0; i < all.size(); i++) {
+            if (enqueue_proof(c, all[i], all[i]->d_w) != G16_OK) {
+                best = -2.0;
+                break;
+            }
+            e = cudaEventRecord(ev[i + 1], all[i]->stream);
+            if (e != cudaSuccess) {
+                cuda_fail(e, "tuning");
+                best = -2.0;
+                break;
+            }
+        }
+        if (best == -2.0) break;
+        float worst = 0;
+        for (size_t i = 0; i < all.size(); i++) {
+            float ms = 0;
+            e = cudaEventSynchronize(ev[i + 1]);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[0], ev[i + 1]);
+            if (e != cudaSuccess) {
+                cuda_fail(e, "tuning");
+                best = -2.0;
+                break;
+            }
+            worst = ms > worst ? ms : worst;
+        }
+        double per = worst / (double)all.size();
+        if (best != -2.0 && r > 0 && (best < 0 || per < best)) best = per;
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    return best == -2.0 ? -1.0 : best;
+}
 
 bool window_bits_ok(int b) { return b >= 8 && b <= 20; }
 
@@ -1447,22 +1527,29 @@ int g16_tuning_set(g16_circuit* c, const g16_tuning* t) {
     return apply_tuning(c, lock.ws, *t);
 }
 
-int g16_autotune(g16_circuit* c, const uint8_t* w, size_t n, g16_tuning* out) {
+int g16_autotune(g16_circuit* c, const uint8_t* w, size_t n, int concurrency, g16_tuning* out) {
     if (!c || !w) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    if (concurrency < 1 || concurrency > 8) return fail(G16_ERR_INVALID_ARGUMENT, "concurrency must be 1..8");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     TuningLock lock(c);
-    if ((rc = lock.take())) return rc;
+    if ((rc = lock.take(concurrency))) return rc;
     Workspace* ws = lock.ws;
     const bool serial = c->serial;
-    if ((rc = upload_witness(ws, w, n))) return rc;
+    for (Workspace* x : lock.all)
+        if ((rc = upload_witness(x, w, n))) return rc;
     const int reps = 3;
-    auto whole = [&] { return time_on_stream(ws, reps, [&] { return enqueue_proof(c, ws, ws->d_w); }); };
+    const bool together = lock.all.size() > 1;
+    // the objective: one proof alone, or stages 0-9 of every held workspace in flight together
+    auto whole = [&] {
+        return together ? time_concurrent(c, lock.all, reps)
+                        : time_on_stream(ws, reps, [&] { return enqueue_proof(c, ws, ws->d_w); });
+    };
     const g16_tuning model = current_tuning(c);
     double model_ms = whole();
     if (model_ms < 0) return G16_ERR_DEVICE;
-    // 1. NTT tiling: gather + NTT chain alone
+    // 1. NTT tiling: gather + NTT chain alone (or the concurrent objective)
     {
         NttTiling best = c->ntt.tiling;
         double best_t = -1;
@@ -1470,7 +1557,8 @@ int g16_autotune(g16_circuit* c, const uint8_t* w, size_t n, g16_tuning* out) {
             for (uint32_t ll : {1u, 2u, 3u}) {
                 if ((uint32_t)c->log_n <= 10 && !(tl == best.tile_log && ll == best.outer_log_l)) continue;
                 c->ntt.tiling = {tl, ll};
-                double t = time_on_stream(ws, reps, [&] { return run_h(c, ws, ws->d_w, ws->d_hpoly); });
+                double t = together ? whole()
+                                    : time_on_stream(ws, reps, [&] { return run_h(c, ws, ws->d_w, ws->d_hpoly); });
                 if (t < 0) return G16_ERR_DEVICE;
                 if (best_t < 0 || t < best_t) {
                     best_t = t;
@@ -1484,16 +1572,21 @@ int g16_autotune(g16_circuit* c, const uint8_t* w, size_t n, g16_tuning* out) {
         int best = c->c_h;
         rc = climb_window(
             c->c_h, [&](int b) { return b == c->c_h ? G16_OK : build_h_table(c, b, ws->stream); },
-            [&] { return time_on_stream(ws, reps, [&] { return enqueue_h_msm(c, ws, ws->d_hpoly); }); }, &best);
+            [&] {
+                return together ? whole()
+                                : time_on_stream(ws, reps, [&] { return enqueue_h_msm(c, ws, ws->d_hpoly); });
+            },
+            &best);
         if (rc) return rc;
     }
-    // 3. witness MSM window: the four MSMs serialised on one stream
+    // 3. witness MSM window: the four MSMs serialised on one stream (or the concurrent objective)
     {
-        c->serial = true;
+        c->serial = !together;
         int best = c->c_w;
         rc = climb_window(
             c->c_w, [&](int b) { return b == c->c_w ? G16_OK : build_witness_tables(c, b, ws->stream); },
             [&] {
+                if (together) return whole();
                 return time_on_stream(ws, reps, [&] {
                     int r = enqueue_witness_msms(c, ws, ws->d_w);
                     return r ? r : enqueue_join(ws);
@@ -1503,7 +1596,7 @@ int g16_autotune(g16_circuit* c, const uint8_t* w, size_t n, g16_tuning* out) {
         c->serial = serial;
         if (rc) return rc;
     }
-    // 4. keep the tuned set only if the whole proof got faster
+    // 4. keep the tuned set only if the objective got better
     double tuned_ms = whole();
     if (tuned_ms < 0) return G16_ERR_DEVICE;
     if (tuned_ms > model_ms) {

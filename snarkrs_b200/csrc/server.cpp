@@ -4,7 +4,7 @@
 // `lanes` worker threads each take the next request as soon as they are free,
 // so requests that arrive while others are on the GPU are admitted as lanes
 // free up and their kernels overlap on the device (each proof runs on its own
-// workspace: three streams, its own scratch).  Admission by device memory has
+// workspace: five streams, its own scratch).  Admission by device memory has
 // two levels:
 //   * proving keys are prepared on first use and stay resident in HBM while
 //     the sum of resident keys' device bytes fits the key budget; a key that

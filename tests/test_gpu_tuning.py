@@ -64,6 +64,21 @@ def test_autotune_keeps_results_and_reports(backend, circuit):
     circ.close()
 
 
+def test_concurrent_autotune_keeps_results(backend, circuit):
+    """The batched objective: four proofs in flight on four workspaces."""
+    sc, zk, ok = circuit
+    circ = backend.prepare(S.ProvingKey.from_bytes(zk))
+    t = circ.autotune(sc.witness(7), concurrency=4)
+    assert t["model_ms"] > 0 and 0 < t["tuned_ms"] <= t["model_ms"]
+    jobs = []
+    for j in (8, 9, 10, 11):
+        r, s = blinders(j)
+        jobs.append((circ, sc.witness(j), r, s))
+    for (c, w, r, s), p in zip(jobs, backend.prove_batch(jobs)):
+        assert p.to_bytes() == ok.prove(w, O.from_bytes(r), O.from_bytes(s))
+    circ.close()
+
+
 def test_tuning_refusals(backend, circuit):
     sc, zk, _ = circuit
     circ = backend.prepare(S.ProvingKey.from_bytes(zk))
@@ -72,4 +87,7 @@ def test_tuning_refusals(backend, circuit):
             circ.set_tuning(*bad)
     with pytest.raises(S.WitnessLengthError):
         circ.autotune(sc.witness(1)[:-32])
+    for bad in (0, 9):
+        with pytest.raises(S.InvalidArgumentError):
+            circ.autotune(sc.witness(1), concurrency=bad)
     circ.close()
