@@ -150,6 +150,18 @@ int g16_h_and_msms(g16_circuit *c, const uint8_t *witness_mont, size_t n, g16_ms
  * the caller's r and s (Montgomery Fr). */
 int g16_prove_with_blinders(g16_circuit *c, const uint8_t *witness_mont, size_t n, const uint8_t *r_mont,
                             const uint8_t *s_mont, g16_proof *out);
+/* PreparedCircuit::h_and_msms_from_rows (crates/groth16/src/lib.rs:425-444;
+ * the CPU backend's crates/groth16/src/cpu.rs:384-471) for a snarkjs-basis key:
+ * stage 0 handed over as a_rows[i] = A_i.w and b_rows[i] = B_i.w, rows <=
+ * domain_size Montgomery Fr each, every row past them zero.  The outputs
+ * equal g16_h_and_msms when the rows are the witness's own. */
+int g16_h_and_msms_from_rows(g16_circuit *c, const uint8_t *witness_mont, size_t n, const uint8_t *a_rows,
+                             const uint8_t *b_rows, size_t rows, g16_msm_outputs *out);
+/* Stages 0-11 of prove_from_rows (crates/groth16/src/prove.rs:93-117) with the
+ * caller's r and s; the self-check is g16_circuit_verify. */
+int g16_prove_with_blinders_from_rows(g16_circuit *c, const uint8_t *witness_mont, size_t n, const uint8_t *a_rows,
+                                      const uint8_t *b_rows, size_t rows, const uint8_t *r_mont,
+                                      const uint8_t *s_mont, g16_proof *out);
 /* The same with the witness already resident in device memory (a device
  * pointer to n Montgomery Fr); no host-to-device copy. */
 int g16_prove_with_blinders_device(g16_circuit *c, const void *d_witness_mont, size_t n, const uint8_t *r_mont,

@@ -4,7 +4,8 @@
  * Stages 0-11 of the reference CPU prover and its verifier:
  *   - stage 0, CpuCircuit::gather (crates/groth16/src/cpu.rs:140-174):
  *     A[c] = sum over CSR row c of coef * w[signal], same for B, C = A*B
- *     (cpu.rs:316-341);
+ *     (cpu.rs:316-341); or the caller's rows, zero padded, with C = A*B
+ *     (h_and_msms_from_rows, cpu.rs:384-425);
  *   - stages 1-4, coset_h (cpu.rs:191-252): intt_coset_ntt on A, B and C,
  *     then H = A*B - C with no division by Z (cpu.rs:230-246);
  *   - stages 5-9, msms_with (cpu.rs:477-632): A over a_query, B over
@@ -21,16 +22,10 @@
 
 #define R (&FR)
 
-int groth16_compute_h(const zkey_t *k, const fp_t *w, fp_t *h) {
+/* stage 0: A.w and B.w, one row per domain row (CpuCircuit::gather, cpu.rs:140-174) */
+void groth16_gather(const zkey_t *k, const fp_t *w, fp_t *a, fp_t *b) {
     size_t n = k->domain_size;
-    int log_n = 0;
-    while (((size_t)1 << log_n) < n) log_n++;
-    domain_t d;
-    if (domain_init(&d, log_n) != 0) return -1;
-    fp_t *ab[2];
-    ab[0] = h;
-    ab[1] = malloc(n * sizeof(fp_t));
-    fp_t *c = malloc(n * sizeof(fp_t));
+    fp_t *ab[2] = {a, b};
     for (int m = 0; m < 2; m++) {
         fp_t *out = ab[m];
 #pragma omp parallel for schedule(static)
@@ -44,6 +39,50 @@ int groth16_compute_h(const zkey_t *k, const fp_t *w, fp_t *h) {
             out[row] = acc;
         }
     }
+}
+
+/* stages 1-4 from the rows (h_and_msms_from_rows, cpu.rs:384-425): rows past
+ * n_rows are zero, C = A*B */
+int groth16_compute_h_from_rows(const zkey_t *k, const fp_t *a_rows, const fp_t *b_rows, size_t n_rows, fp_t *h) {
+    size_t n = k->domain_size;
+    if (n_rows > n) return -1;
+    int log_n = 0;
+    while (((size_t)1 << log_n) < n) log_n++;
+    domain_t d;
+    if (domain_init(&d, log_n) != 0) return -1;
+    fp_t *b = calloc(n, sizeof(fp_t));
+    fp_t *c = malloc(n * sizeof(fp_t));
+    memset(h, 0, n * sizeof(fp_t));
+    memcpy(h, a_rows, n_rows * sizeof(fp_t));
+    memcpy(b, b_rows, n_rows * sizeof(fp_t));
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)n; i++) fp_mul(R, &c[i], &h[i], &b[i]);
+    intt_coset_ntt(&d, h);
+    intt_coset_ntt(&d, b);
+    intt_coset_ntt(&d, c);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)n; i++) {
+        fp_t t;
+        fp_mul(R, &t, &h[i], &b[i]);
+        fp_sub(R, &h[i], &t, &c[i]);
+    }
+    free(b);
+    free(c);
+    domain_free(&d);
+    return 0;
+}
+
+int groth16_compute_h(const zkey_t *k, const fp_t *w, fp_t *h) {
+    size_t n = k->domain_size;
+    int log_n = 0;
+    while (((size_t)1 << log_n) < n) log_n++;
+    domain_t d;
+    if (domain_init(&d, log_n) != 0) return -1;
+    fp_t *ab[2];
+    ab[0] = h;
+    ab[1] = malloc(n * sizeof(fp_t));
+    fp_t *c = malloc(n * sizeof(fp_t));
+    groth16_gather(k, w, ab[0], ab[1]);
 #pragma omp parallel for schedule(static)
     for (long i = 0; i < (long)n; i++) fp_mul(R, &c[i], &ab[0][i], &ab[1][i]);
     intt_coset_ntt(&d, ab[0]);

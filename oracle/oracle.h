@@ -55,6 +55,8 @@ typedef struct { g1j_t a_g1; g2j_t b_g2; g1j_t b_g1, l_g1, h_g1; } msm_outputs_t
 
 /* witness in Montgomery form (the reference's &[Fr]), length n_vars */
 int  groth16_compute_h(const zkey_t *k, const fp_t *w, fp_t *h /* domain_size, Montgomery */);
+void groth16_gather(const zkey_t *k, const fp_t *w, fp_t *a, fp_t *b /* domain_size rows each */);
+int  groth16_compute_h_from_rows(const zkey_t *k, const fp_t *a_rows, const fp_t *b_rows, size_t n_rows, fp_t *h);
 int  groth16_msms(const zkey_t *k, const fp_t *w, const fp_t *h, msm_outputs_t *out);
 void groth16_assemble(const zkey_t *k, const msm_outputs_t *m, const fp_t *r, const fp_t *s, proof_t *p);
 int  groth16_prove(const zkey_t *k, const fp_t *w, const fp_t *r, const fp_t *s, proof_t *p);

@@ -233,6 +233,24 @@ class Zkey:
             raise ValueError("compute_h failed")
         return out.raw
 
+    def gather(self, witness_mont):
+        """Stage 0: (A.w, B.w), domain_size rows each, Montgomery bytes."""
+        a = ctypes.create_string_buffer(32 * self.domain_size)
+        b = ctypes.create_string_buffer(32 * self.domain_size)
+        rc = lib().oracle_gather(ctypes.c_void_p(self._h), bytes(witness_mont),
+                                 ctypes.c_size_t(len(witness_mont) // 32), a, b)
+        if rc != 0:
+            raise ValueError("gather failed")
+        return a.raw, b.raw
+
+    def compute_h_from_rows(self, a_rows, b_rows):
+        out = ctypes.create_string_buffer(32 * self.domain_size)
+        rc = lib().oracle_compute_h_from_rows(ctypes.c_void_p(self._h), bytes(a_rows), bytes(b_rows),
+                                              ctypes.c_size_t(len(a_rows) // 32), out)
+        if rc != 0:
+            raise ValueError("compute_h_from_rows failed")
+        return out.raw
+
     def msms(self, witness_mont, h_mont):
         out = ctypes.create_string_buffer(384)
         rc = lib().oracle_msms(ctypes.c_void_p(self._h), bytes(witness_mont),

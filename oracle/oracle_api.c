@@ -191,6 +191,18 @@ void oracle_zkey_info(const void *kv, uint32_t *out3) {
     out3[0] = k->n_vars; out3[1] = k->n_public; out3[2] = k->domain_size;
 }
 
+int oracle_gather(const void *kv, const uint8_t *w_mont, size_t n, uint8_t *a_out, uint8_t *b_out) {
+    const zkey_t *k = kv;
+    if (n != k->n_vars) return -1;
+    groth16_gather(k, (const fp_t *)w_mont, (fp_t *)a_out, (fp_t *)b_out);
+    return 0;
+}
+
+int oracle_compute_h_from_rows(const void *kv, const uint8_t *a_rows, const uint8_t *b_rows, size_t rows,
+                               uint8_t *h_out) {
+    return groth16_compute_h_from_rows(kv, (const fp_t *)a_rows, (const fp_t *)b_rows, rows, (fp_t *)h_out);
+}
+
 int oracle_compute_h(const void *kv, const uint8_t *w_mont, size_t n, uint8_t *h_out) {
     const zkey_t *k = kv;
     if (n != k->n_vars) return -1;

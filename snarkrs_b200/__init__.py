@@ -401,6 +401,26 @@ class CudaCircuit:
         check(lib().g16_stage_timings_get(self._h, ctypes.byref(t)))
         return t.as_dict()
 
+    def h_and_msms_from_rows(self, witness_mont, a_rows, b_rows):
+        """PreparedCircuit::h_and_msms_from_rows: stage 0 handed over as A.w and B.w rows."""
+        if _nbytes(a_rows) != _nbytes(b_rows):
+            raise BackendError("A.w and B.w must have the same number of rows")
+        o = _MsmOutputs()
+        check(lib().g16_h_and_msms_from_rows(self._h, _buf(witness_mont), ctypes.c_size_t(_nbytes(witness_mont) // 32),
+                                             _buf(a_rows), _buf(b_rows), ctypes.c_size_t(_nbytes(a_rows) // 32),
+                                             ctypes.byref(o)))
+        return MsmOutputs(o)
+
+    def prove_with_blinders_from_rows(self, witness_mont, a_rows, b_rows, r_mont, s_mont):
+        if _nbytes(a_rows) != _nbytes(b_rows):
+            raise BackendError("A.w and B.w must have the same number of rows")
+        p = _Proof()
+        check(lib().g16_prove_with_blinders_from_rows(self._h, _buf(witness_mont),
+                                                      ctypes.c_size_t(_nbytes(witness_mont) // 32), _buf(a_rows),
+                                                      _buf(b_rows), ctypes.c_size_t(_nbytes(a_rows) // 32),
+                                                      bytes(r_mont), bytes(s_mont), ctypes.byref(p)))
+        return Proof(p.a, p.b, p.c)
+
     def prove(self, witness_mont):
         """prove::prove (crates/groth16/src/prove.rs:34-92): fresh r, s, then the proof is checked."""
         p = _Proof()

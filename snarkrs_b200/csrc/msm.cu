@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(256) k_scan_add(uint32_t* __restrict__ out, ui
 // Partial sums per bucket (one per chunk the bucket touches).  Buckets with
 // more than FAT_PARTIALS of them -- a repeated scalar, most often 1 -- go on
 // the fat list and are folded in parallel before the bucket sums.
-constexpr uint32_t FAT_PARTIALS = 32;
+constexpr uint32_t FAT_PARTIALS = 16;
 constexpr uint32_t FAT_JOBS = 64;
 
 // partials per job of a fat bucket: at least FAT_PARTIALS, at most FAT_JOBS jobs

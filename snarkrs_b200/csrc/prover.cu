@@ -90,6 +90,16 @@ __global__ void __launch_bounds__(256) k_gather(const uint32_t* __restrict__ rpa
     store32(reinterpret_cast<Fr*>(C) + row, mul(acc[0], acc[1]));
 }
 
+// Stage 0 handed over (h_and_msms_from_rows): C = A * B on the caller's rows,
+// zero past them (crates/groth16/src/cpu.rs:409-425).
+__global__ void k_rows_c(const uint4* __restrict__ A, const uint4* __restrict__ B, uint4* __restrict__ C,
+                         uint32_t n) {
+    uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= n) return;
+    store32(reinterpret_cast<Fr*>(C) + row,
+            mul(load32(reinterpret_cast<const Fr*>(A) + row), load32(reinterpret_cast<const Fr*>(B) + row)));
+}
+
 // Throughput probe for the 32-bit multiply-add the field code is built from:
 // eight independent chains alternating mad.lo.u32 and mad.hi.u32, so the
 // issue rate, not latency, bounds it.  Gives the integer roofline's peak.
@@ -672,6 +682,45 @@ int prove_on_device(g16_circuit* c, Workspace* ws, const void* d_w, const uint8_
     return G16_OK;
 }
 
+// Stages 1-9 from the caller's A.w and B.w rows (stage 0 handed over): the
+// witness MSMs fork as in a proof, the main stream pads the rows to the
+// domain, forms C = A B and runs the NTT chain and the H MSM.
+int run_rows_proof(g16_circuit* c, Workspace* ws, const void* d_w, const uint8_t* a_rows, const uint8_t* b_rows,
+                   size_t rows, MsmJac& out) {
+    cudaStream_t st = ws->stream;
+    uint8_t* abc = (uint8_t*)ws->d_abc;
+    const size_t vb = (size_t)c->n * 32;
+    int rc = enqueue_witness_msms(c, ws, d_w);
+    if (rc) return rc;
+    CK(stage_event(ws->ev[0], st), "event");
+    for (int m = 0; m < 2; m++) {
+        uint8_t* dst = abc + m * vb;
+        if (rows) CK(cudaMemcpyAsync(dst, m ? b_rows : a_rows, rows * 32, cudaMemcpyHostToDevice, st), "rows upload");
+        if (rows < c->n) CK(cudaMemsetAsync(dst + rows * 32, 0, vb - rows * 32, st), "rows padding");
+    }
+    {
+        TimedLaunch tl("gather", st);
+        g16d::k_rows_c<<<blocks_for(c->n, 256), 256, 0, st>>>((const uint4*)abc, (const uint4*)(abc + vb),
+                                                               (uint4*)(abc + 2 * vb), c->n);
+    }
+    CK(cudaGetLastError(), "rows launch");
+    CK(stage_event(ws->ev[1], st), "event");
+    CK(ntt_h_pipeline(c->ntt, abc, abc + vb, abc + 2 * vb, ws->d_hpoly, st), "NTT pipeline");
+    CK(stage_event(ws->ev[2], st), "event");
+    if ((rc = enqueue_h_msm(c, ws, ws->d_hpoly)) || (rc = enqueue_join(ws))) return rc;
+    if ((rc = collect_msms(c, ws, out))) return rc;
+    ws->proofs++;
+    return G16_OK;
+}
+
+int check_rows(const g16_circuit* c, const uint8_t* a_rows, const uint8_t* b_rows, size_t rows) {
+    if (rows && (!a_rows || !b_rows)) return fail(G16_ERR_INVALID_ARGUMENT, "null rows");
+    if (rows > c->n)
+        return fail(G16_ERR_BACKEND, "A.w and B.w have %zu rows; both must be one per constraint, at most the domain "
+                                     "size %u", rows, c->n);
+    return G16_OK;
+}
+
 int upload_witness(Workspace* ws, const uint8_t* w, size_t n) {
     CK(cudaMemcpyAsync(ws->d_w, w, n * 32, cudaMemcpyHostToDevice, ws->stream), "witness upload");
     return G16_OK;
@@ -1170,6 +1219,49 @@ int g16_h_and_msms(g16_circuit* c, const uint8_t* w, size_t n, g16_msm_outputs* 
     if ((rc = run_proof(c, g.ws, g.ws->d_w, m))) return rc;
     add_timings(c, g.ws, true, true, 0);
     to_outputs(m, out);
+    return G16_OK;
+}
+
+int g16_h_and_msms_from_rows(g16_circuit* c, const uint8_t* w, size_t n, const uint8_t* a_rows,
+                             const uint8_t* b_rows, size_t rows, g16_msm_outputs* out) {
+    if (!c || !w || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    int rc = check_witness(c, n, w);
+    if (rc || (rc = check_rows(c, a_rows, b_rows, rows))) return rc;
+    CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
+    WsGuard g(c);
+    if ((rc = acquire(c, &g.ws))) return rc;
+    if ((rc = upload_witness(g.ws, w, n))) return rc;
+    MsmJac m;
+    if ((rc = run_rows_proof(c, g.ws, g.ws->d_w, a_rows, b_rows, rows, m))) return rc;
+    add_timings(c, g.ws, true, true, 0);
+    to_outputs(m, out);
+    return G16_OK;
+}
+
+int g16_prove_with_blinders_from_rows(g16_circuit* c, const uint8_t* w, size_t n, const uint8_t* a_rows,
+                                      const uint8_t* b_rows, size_t rows, const uint8_t* r_mont,
+                                      const uint8_t* s_mont, g16_proof* out) {
+    if (!c || !w || !r_mont || !s_mont || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    int rc = check_witness(c, n, w);
+    if (rc || (rc = check_rows(c, a_rows, b_rows, rows))) return rc;
+    uint64_t rr[4], ss[4];
+    std::memcpy(rr, r_mont, 32);
+    std::memcpy(ss, s_mont, 32);
+    if (!g16::Fr::canonical(rr) || !g16::Fr::canonical(ss)) return fail(G16_ERR_INVALID_ARGUMENT, "r or s not below r");
+    CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
+    WsGuard g(c);
+    if ((rc = acquire(c, &g.ws))) return rc;
+    if ((rc = upload_witness(g.ws, w, n))) return rc;
+    g16::Fr r = g16::Fr::raw(rr), s = g16::Fr::raw(ss);
+    auto terms = std::async(std::launch::async, [&] { return blinder_terms(c, r, s); });
+    MsmJac m;
+    rc = run_rows_proof(c, g.ws, g.ws->d_w, a_rows, b_rows, rows, m);
+    BlinderTerms t = terms.get();
+    if (rc) return rc;
+    auto t0 = std::chrono::steady_clock::now();
+    assemble(c, m, t, r, s, out);
+    auto t1 = std::chrono::steady_clock::now();
+    add_timings(c, g.ws, true, true, (uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(t1 - t0).count());
     return G16_OK;
 }
 

@@ -183,3 +183,22 @@ def test_gnark_toy_proof_verifies():
     assert not O.verify_vk(*args, bad, proof)
     swapped = P.pack_g1(c) + P.pack_g2(b) + P.pack_g1(a)
     assert not O.verify_vk(*args, pubm, swapped)
+
+
+def test_rows_path_restatement_matches_compute_h():
+    """h_and_msms_from_rows (crates/groth16/src/cpu.rs:384-425): the witness's own rows,
+    whole or cut after the last nonzero row, give the H of compute_h."""
+    import snarkrs_b200 as S
+    sc = S.SynthCircuit(seed=13, n_constraints=500, n_inputs=20, n_public=4)
+    ok = O.Zkey(sc.zkey(77))
+    w = sc.witness(2)
+    a, b = ok.gather(w)
+    h = ok.compute_h(w)
+    assert ok.compute_h_from_rows(a, b) == h
+    n = len(a) // 32
+    last = max(i for i in range(n) if any(a[32 * i:32 * i + 32]) or any(b[32 * i:32 * i + 32]))
+    assert ok.compute_h_from_rows(a[:32 * (last + 1)], b[:32 * (last + 1)]) == h
+    # rows that are not the witness's give another H
+    bad = bytearray(a)
+    bad[0] ^= 1
+    assert ok.compute_h_from_rows(bytes(bad), b) != h
