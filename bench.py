@@ -221,7 +221,9 @@ def run_ours(args):
         barrier()
         zk = synth_key(sc, args.constraints)
     pk = S.ProvingKey.from_bytes(zk, check_points=False)
+    t_prep = time.perf_counter()
     circ = backend.prepare(pk)
+    t_prep = time.perf_counter() - t_prep
     K, W = args.steps, args.warmup
     nbytes = 32 * sc.n_vars
     # per-step witnesses (different seeds per rank and step), in pinned host memory
@@ -303,7 +305,7 @@ def run_ours(args):
                                                                     "issue-rate probe (g16_imad_peak)",
                      "work_per_launch": "%.0f mixed additions x %d Fq products x %d IMAD" % (
                          units / max(n_launch, 1), MADD_FQ_MULS[name], FQ_MUL_IMAD)})
-    roof["traffic"] = traffic_for(name)
+    roof["traffic"] = traffic_for("prove-%d" % args.constraints, name)
     # whole-proof integer work: MSM mixed additions (measured counters) + the NTT chain
     n_dom = sc.domain_size
     log_n = n_dom.bit_length() - 1
@@ -331,7 +333,8 @@ def run_ours(args):
                    "n_constraints": args.constraints, "domain": sc.domain_size, "n_vars": sc.n_vars,
                    "l2": "no flush: the resident key (%.0f MB) and per-step witnesses exceed the 126 MB L2" %
                          (circ.device_bytes() / 1e6),
-                   "replicas": world},
+                   "replicas": world,
+                   "prepare_s": round(t_prep, 3)},
         "e2e": {"value": e2e_value, "unit": "proofs/s", "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": readback, "p50_ms": 1e3 * statistics.median(lat),
                 "p99_ms": 1e3 * sorted(lat)[min(len(lat) - 1, int(0.99 * len(lat)))]},
@@ -376,14 +379,15 @@ def run_ours(args):
         barrier()
 
 
-def traffic_for(name):
-    """DRAM bytes per launch from the committed ncu summary, when one exists for this kernel."""
+def traffic_for(workload, name):
+    """DRAM bytes per launch from the committed ncu summary for this workload and kernel, if any."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(p) as f:
-            return json.load(f).get(name)
-    except OSError:
+            entry = json.load(f).get(workload, {}).get(name)
+    except (OSError, ValueError, AttributeError):
         return None
+    return entry.get("bytes_per_launch") if isinstance(entry, dict) else None
 
 
 NTT_KERNELS = ("ntt_pass_dif", "ntt_pass_dit", "ntt_mid_fused")
@@ -488,7 +492,7 @@ def run_primitive(args):
     elif "hbm_frac" in r:
         roof.update({"bound": "hbm", "achieved": r["hbm_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": r["hbm_frac"], "peak_source": peak_kind})
-    roof["traffic"] = traffic_for(name)
+    roof["traffic"] = traffic_for("%s-2^%d" % (args.workload, args.log_n), name)
     line["roofline"] = roof
     line["kernel_rooflines"] = per_kernel
     if not args.no_cpu_baseline:

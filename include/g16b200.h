@@ -115,6 +115,14 @@ int g16_backend_open(int ordinal, uint64_t vram_limit, g16_backend **out);
 void g16_backend_free(g16_backend *b);
 const char *g16_backend_name(const g16_backend *b);   /* "cuda-b200" */
 uint64_t g16_backend_vram_used(const g16_backend *b);
+/* CudaBackend::constant_work (crates/cuda/src/backend.rs:100-118; the CPU
+ * MSM's Work::Constant, crates/msm/src/lib.rs:206-220): every MSM this backend
+ * runs afterwards (proofs, batches, servers, g16_msm_*) sends every window of
+ * every scalar through the buckets, zero digits into a bucket no reduction
+ * reads, so the sorted-entry count, launch sizes and additions follow the key
+ * and not the witness.  Results are unchanged.  Not for
+ * g16_msm_g1_device_noalloc. */
+int g16_backend_set_constant_work(g16_backend *b, int on);
 
 /* ---------------- .zkey / .wtns (crates/formats) ---------------- */
 /* ProvingKey::load (formats/src/lib.rs:430-505).  check_points != 0 also runs

@@ -468,11 +468,22 @@ class CudaCircuit:
 class CudaBackend:
     """Backend (crates/groth16/src/lib.rs:371-380) over one B200: name() and prepare()."""
 
-    def __init__(self, ordinal=0, vram_limit=0):
+    def __init__(self, ordinal=0, vram_limit=0, constant_work=False):
         self.ordinal = int(ordinal)
         h = ctypes.c_void_p()
         check(lib().g16_backend_open(int(ordinal), ctypes.c_uint64(vram_limit), ctypes.byref(h)))
         self._h = h
+        if constant_work:
+            self.set_constant_work(True)
+
+    @classmethod
+    def constant_work(cls, ordinal=0, vram_limit=0):
+        """CudaBackend::constant_work (crates/cuda/src/backend.rs:100-118)."""
+        return cls(ordinal, vram_limit, constant_work=True)
+
+    def set_constant_work(self, on=True):
+        """MSM cost follows the key, not the witness (results unchanged)."""
+        check(lib().g16_backend_set_constant_work(self._h, int(bool(on))))
 
     def name(self):
         return lib().g16_backend_name(self._h).decode()

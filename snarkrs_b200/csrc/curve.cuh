@@ -207,6 +207,14 @@ __device__ __forceinline__ Affine<F> ld_affine(const uint4* base, size_t i) {
     return {Codec<F>::ld(p), Codec<F>::ld(p + U)};
 }
 
+// for memory the same kernel also writes (no read-only cache path)
+template <class F>
+__device__ __forceinline__ Affine<F> ld_affine_rw(const uint4* base, size_t i) {
+    constexpr int U = Codec<F>::U4;
+    const uint4* p = base + i * (2 * U);
+    return {Codec<F>::ld_rw(p), Codec<F>::ld_rw(p + U)};
+}
+
 template <class F>
 __device__ __forceinline__ void st_affine(uint4* base, size_t i, const F& x, const F& y) {
     constexpr int U = Codec<F>::U4;

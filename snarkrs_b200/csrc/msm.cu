@@ -35,8 +35,9 @@ constexpr uint32_t NO_KEY = 0xffffffffu;
 
 // kw: key stride per window (B when every window has its own buckets, 0 when
 // all windows share one bucket set over window-shifted bases)
+// sink: the key of a zero digit (NO_KEY: not sorted; the constant-work sink bucket otherwise)
 __global__ void __launch_bounds__(256) k_digits_count(const uint4* __restrict__ scalars, int mont, uint32_t n, int c,
-                                                      int W, uint32_t kw, uint4* __restrict__ scalars_std,
+                                                      int W, uint32_t kw, uint32_t sink, uint4* __restrict__ scalars_std,
                                                       uint32_t* __restrict__ counts) {
     __shared__ uint32_t sh[256 * 9];
     uint32_t i = blockIdx.x * 256 + threadIdx.x;
@@ -56,7 +57,7 @@ __global__ void __launch_bounds__(256) k_digits_count(const uint4* __restrict__ 
     unsigned lane = threadIdx.x & 31;
     for (int w = 0; w < W; w++) {
         int d = signed_digit(row, w, c);
-        uint32_t key = (valid && d != 0) ? (uint32_t)w * kw + (uint32_t)(d < 0 ? -d : d) - 1u : NO_KEY;
+        uint32_t key = !valid ? NO_KEY : d != 0 ? (uint32_t)w * kw + (uint32_t)(d < 0 ? -d : d) - 1u : sink;
         unsigned mask = __match_any_sync(0xffffffffu, key);
         if (key != NO_KEY && lane == (unsigned)(__ffs(mask) - 1)) atomicAdd(&counts[key], (uint32_t)__popc(mask));
     }
@@ -65,7 +66,7 @@ __global__ void __launch_bounds__(256) k_digits_count(const uint4* __restrict__ 
 // ew: entry-index stride per window (0, or n for window-shifted bases: entry
 // w*n + i names base 2^(c w) P_i)
 __global__ void __launch_bounds__(256) k_scatter(const uint4* __restrict__ scalars_std, uint32_t n, int c, int W,
-                                                 uint32_t kw, uint32_t ew, uint32_t* __restrict__ cursor,
+                                                 uint32_t kw, uint32_t ew, uint32_t sink, uint32_t* __restrict__ cursor,
                                                  uint32_t* __restrict__ entries) {
     __shared__ uint32_t sh[256 * 9];
     uint32_t i = blockIdx.x * 256 + threadIdx.x;
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(256) k_scatter(const uint4* __restrict__ scala
     unsigned lt = (1u << lane) - 1u;
     for (int w = 0; w < W; w++) {
         int d = signed_digit(row, w, c);
-        uint32_t key = (valid && d != 0) ? (uint32_t)w * kw + (uint32_t)(d < 0 ? -d : d) - 1u : NO_KEY;
+        uint32_t key = !valid ? NO_KEY : d != 0 ? (uint32_t)w * kw + (uint32_t)(d < 0 ? -d : d) - 1u : sink;
         unsigned mask = __match_any_sync(0xffffffffu, key);
         int leader = __ffs(mask) - 1;
         uint32_t base = 0;
@@ -180,14 +181,31 @@ __device__ __forceinline__ uint32_t fat_job_len(uint32_t ns) {
     return j < FAT_PARTIALS ? FAT_PARTIALS : j;
 }
 
-__global__ void k_nseg(const uint32_t* __restrict__ offsets, uint32_t K, uint32_t L, uint32_t* __restrict__ nseg,
-                       uint32_t* __restrict__ fat_list, uint32_t* __restrict__ fat_count) {
+// Entries per accumulate thread, chosen on the device from the sorted count
+// M: at least L_min, and no more threads than ACC_THREADS, so that sparse
+// scalars (witnesses of zeros and ones) still spread over the whole GPU and
+// dense ones keep per-bucket partial counts low.
+constexpr uint32_t ACC_THREADS = 1u << 19;
+
+__device__ __forceinline__ uint32_t chunk_len(uint32_t M, uint32_t L_min) {
+    uint32_t L = (uint32_t)(((uint64_t)M + ACC_THREADS - 1) / ACC_THREADS);
+    return L > L_min ? L : L_min;
+}
+
+// partials per bucket for the Ks sorted buckets; only the K real ones can be
+// fat (the constant-work sink bucket K is accumulated but never reduced).
+// Also stores the chunk length L in total[3] for the kernels that follow.
+__global__ void k_nseg(const uint32_t* __restrict__ offsets, uint32_t Ks, uint32_t K, uint32_t L_min,
+                       uint32_t* __restrict__ nseg, uint32_t* __restrict__ fat_list, uint32_t* __restrict__ fat_count,
+                       uint32_t* __restrict__ total) {
     uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= K) return;
+    const uint32_t L = chunk_len(total[0], L_min);
+    if (g == 0) total[3] = L;
+    if (g >= Ks) return;
     uint32_t lo = offsets[g], hi = offsets[g + 1];
     uint32_t ns = hi > lo ? ((hi - 1) / L - lo / L + 1) : 0;
     nseg[g] = ns;
-    if (ns > FAT_PARTIALS) fat_list[atomicAdd(fat_count, 1u)] = g;
+    if (g < K && ns > FAT_PARTIALS) fat_list[atomicAdd(fat_count, 1u)] = g;
 }
 
 __global__ void k_copy_u32(uint32_t* dst, const uint32_t* src, uint32_t n) {
@@ -200,12 +218,12 @@ template <class F>
 __global__ void __launch_bounds__(128) k_accumulate(const uint32_t* __restrict__ entries,
                                                     const uint32_t* __restrict__ offsets,
                                                     const uint32_t* __restrict__ seg_base, uint32_t K,
-                                                    const uint32_t* __restrict__ d_M, uint32_t L,
+                                                    const uint32_t* __restrict__ d_M, const uint32_t* __restrict__ d_L,
                                                     const uint4* __restrict__ bases, uint32_t base_offset,
                                                     uint32_t n_bases, uint4* __restrict__ partials,
                                                     unsigned long long* __restrict__ work) {
     size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t M = *d_M;
+    const uint32_t M = *d_M, L = *d_L;
     size_t start = t * L;
     if (start >= M) return;
     size_t end = start + L < M ? start + L : M;
@@ -277,8 +295,10 @@ __global__ void __launch_bounds__(128) k_fat_merge_jobs(uint4* __restrict__ part
                                                         const uint32_t* __restrict__ offsets,
                                                         const uint32_t* __restrict__ seg_base,
                                                         const uint32_t* __restrict__ fat_list,
-                                                        const uint32_t* __restrict__ fat_count, uint32_t L) {
+                                                        const uint32_t* __restrict__ fat_count,
+                                                        const uint32_t* __restrict__ d_L) {
     extern __shared__ uint4 smem[];
+    const uint32_t L = *d_L;
     uint32_t items = *fat_count * FAT_JOBS;
     for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
         uint32_t g = fat_list[item / FAT_JOBS], j = item % FAT_JOBS;
@@ -301,8 +321,10 @@ __global__ void __launch_bounds__(64) k_fat_merge_final(uint4* __restrict__ part
                                                         const uint32_t* __restrict__ offsets,
                                                         const uint32_t* __restrict__ seg_base,
                                                         const uint32_t* __restrict__ fat_list,
-                                                        const uint32_t* __restrict__ fat_count, uint32_t L) {
+                                                        const uint32_t* __restrict__ fat_count,
+                                                        const uint32_t* __restrict__ d_L) {
     extern __shared__ uint4 smem[];
+    const uint32_t L = *d_L;
     uint32_t nf = *fat_count;
     for (uint32_t f = blockIdx.x; f < nf; f += gridDim.x) {
         uint32_t g = fat_list[f];
@@ -321,10 +343,11 @@ __global__ void __launch_bounds__(64) k_fat_merge_final(uint4* __restrict__ part
 template <class F>
 __global__ void __launch_bounds__(128) k_bucket_sums(const uint4* __restrict__ partials,
                                                      const uint32_t* __restrict__ offsets,
-                                                     const uint32_t* __restrict__ seg_base, uint32_t K, uint32_t L,
-                                                     uint4* __restrict__ buckets) {
+                                                     const uint32_t* __restrict__ seg_base, uint32_t K,
+                                                     const uint32_t* __restrict__ d_L, uint4* __restrict__ buckets) {
     uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= K) return;
+    const uint32_t L = *d_L;
     uint32_t ns = n_partials(offsets, g, L), base = seg_base[g];
     Xyzz<F> acc = Xyzz<F>::identity();
     if (ns > FAT_PARTIALS) {
@@ -381,12 +404,15 @@ __global__ void __launch_bounds__(128) k_group_sum(const uint4* __restrict__ in,
     if (threadIdx.x == 0) st_xyzz<F>(out, (size_t)grp * gridDim.x + blockIdx.x, acc);
 }
 
-// Window-shifted base table: out[w n + i] = 2^(c w) P_i (affine), one thread per
-// point, c doublings per window and one inversion per output.  Table building
-// runs once per prepared key.
+// Window-shifted base table: out[w n + i] = 2^(c w) P_i (affine).  Built once
+// per prepared key in two steps, so that the normalisations share inversions.
+//
+// Step 1, one thread per point: window 0 is P_i itself (written affine), and
+// the XYZZ multiples 2^(c w) P_i for w >= 1 (c doublings each) go to tmp at
+// (w - 1) n + i; a point at infinity (or below skip) gives zeros / identity.
 template <class F>
-__global__ void __launch_bounds__(128) k_window_table(const uint4* __restrict__ in, uint32_t n, uint32_t skip, int c,
-                                                      int W, uint4* __restrict__ out) {
+__global__ void __launch_bounds__(128) k_window_xyzz(const uint4* __restrict__ in, uint32_t n, uint32_t skip, int c,
+                                                     int W, uint4* __restrict__ out, uint4* __restrict__ tmp) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     Affine<F> p;
@@ -396,7 +422,8 @@ __global__ void __launch_bounds__(128) k_window_table(const uint4* __restrict__ 
         inf = p.is_inf();
     }
     if (inf) {
-        for (int w = 0; w < W; w++) st_affine<F>(out, (size_t)w * n + i, F::zero(), F::zero());
+        st_affine<F>(out, i, F::zero(), F::zero());
+        for (int w = 1; w < W; w++) st_xyzz<F>(tmp, (size_t)(w - 1) * n + i, Xyzz<F>::identity());
         return;
     }
     st_affine<F>(out, i, p.x, p.y);
@@ -407,10 +434,46 @@ __global__ void __launch_bounds__(128) k_window_table(const uint4* __restrict__ 
     acc.zzz = F::one();
     for (int w = 1; w < W; w++) {
         for (int j = 0; j < c; j++) acc = xyzz_dbl<F, false>(acc);
-        F zi = inv(fmul<false>(acc.zz, acc.zzz));   // 1 / (ZZ ZZZ)
-        F x = fmul<false>(fmul<false>(acc.x, acc.zzz), zi);
-        F y = fmul<false>(fmul<false>(acc.y, acc.zz), zi);
-        st_affine<F>(out, (size_t)w * n + i, x, y);
+        st_xyzz<F>(tmp, (size_t)(w - 1) * n + i, acc);
+    }
+}
+
+// Step 2, Montgomery's batch inversion over runs of NORM_RUN consecutive
+// entries: one inversion per run instead of one per entry.  With
+// d_j = ZZ_j ZZZ_j, x = X ZZZ / d and y = Y ZZ / d.  The output slots hold the
+// running products (x) and d_j (y) between the forward and the backward pass;
+// an identity entry (ZZ = 0) takes d = 1 and is written as zeros.
+constexpr uint32_t NORM_RUN = 32;
+
+template <class F>
+__global__ void __launch_bounds__(128) k_window_normalize(const uint4* __restrict__ tmp, size_t count,
+                                                          uint4* __restrict__ out) {
+    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    size_t a = t * NORM_RUN;
+    if (a >= count) return;
+    size_t b = a + NORM_RUN < count ? a + NORM_RUN : count;
+    F acc = F::one();
+    for (size_t j = a; j < b; j++) {
+        Xyzz<F> q = ld_xyzz<F>(tmp, j);
+        F d = q.zz.is_zero() ? F::one() : fmul<false>(q.zz, q.zzz);
+        acc = fmul<false>(acc, d);
+        st_affine<F>(out, j, acc, d);
+    }
+    F inv_acc = inv(acc);   // 1 / (d_a ... d_(b-1))
+    for (size_t j = b; j-- > a;) {
+        Affine<F> slot = ld_affine_rw<F>(out, j);   // (running product through j, d_j)
+        F before = j > a ? ld_affine_rw<F>(out, j - 1).x : F::one();
+        F inv_d = fmul<false>(inv_acc, before);   // 1 / d_j
+        inv_acc = fmul<false>(inv_acc, slot.y);   // 1 / (d_a ... d_(j-1))
+        Xyzz<F> q = ld_xyzz<F>(tmp, j);
+        if (q.zz.is_zero()) {
+            st_affine<F>(out, j, F::zero(), F::zero());
+        } else {
+            F x, y;
+            fmul2<false>(q.x, q.zzz, q.y, q.zz, x, y);
+            fmul2<false>(x, inv_d, y, inv_d, x, y);
+            st_affine<F>(out, j, x, y);
+        }
     }
 }
 
@@ -455,18 +518,38 @@ int msm_shared_window_bits(size_t m) {
     return best;
 }
 
+template <class F>
+static cudaError_t window_table(const void* d_in, size_t n, uint32_t skip, int c, void* d_out, cudaStream_t st,
+                                size_t xyzz_bytes) {
+    const int W = msm_windows(c);
+    const size_t count = n * (size_t)(W - 1);
+    void* tmp = nullptr;
+    G16_CUDA(cudaMalloc(&tmp, (count ? count : 1) * xyzz_bytes));
+    cudaError_t e = cudaSuccess;
+    {
+        TimedLaunch tl("msm_window_table", st);
+        k_window_xyzz<F><<<blocks_for(n, 128), 128, 0, st>>>((const uint4*)d_in, (uint32_t)n, skip, c, W,
+                                                            (uint4*)d_out, (uint4*)tmp);
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess && count) {
+        TimedLaunch tl("msm_window_table", st);
+        uint4* out1 = (uint4*)((uint8_t*)d_out + n * (xyzz_bytes / 2));   // window 1 onwards
+        k_window_normalize<F><<<blocks_for((count + NORM_RUN - 1) / NORM_RUN, 128), 128, 0, st>>>(
+            (const uint4*)tmp, count, out1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(tmp);
+    return e;
+}
+
 cudaError_t msm_window_table_g1(const void* d_in, size_t n, uint32_t skip, int c, void* d_out, cudaStream_t st) {
-    TimedLaunch tl("msm_window_table", st);
-    k_window_table<g16d::Fq><<<blocks_for(n, 128), 128, 0, st>>>((const uint4*)d_in, (uint32_t)n, skip, c,
-                                                                 msm_windows(c), (uint4*)d_out);
-    return cudaGetLastError();
+    return window_table<g16d::Fq>(d_in, n, skip, c, d_out, st, XYZZ_G1_BYTES);
 }
 
 cudaError_t msm_window_table_g2(const void* d_in, size_t n, uint32_t skip, int c, void* d_out, cudaStream_t st) {
-    TimedLaunch tl("msm_window_table", st);
-    k_window_table<g16d::Fq2><<<blocks_for(n, 128), 128, 0, st>>>((const uint4*)d_in, (uint32_t)n, skip, c,
-                                                                  msm_windows(c), (uint4*)d_out);
-    return cudaGetLastError();
+    return window_table<g16d::Fq2>(d_in, n, skip, c, d_out, st, XYZZ_G2_BYTES);
 }
 
 int msm_window_bits(size_t m) {
@@ -537,7 +620,7 @@ static cudaError_t scan(const uint32_t* in, uint32_t* out, uint32_t len, uint32_
 }
 
 cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomery, int c, cudaStream_t st,
-                     bool shared_windows) {
+                     bool shared_windows, bool constant_work) {
     if (c == 0) c = msm_window_bits(n);
     if (c < 4 || c > 24) {
         set_error("MSM window of %d bits outside [4, 24]", c);
@@ -548,21 +631,21 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
     s.B = 1u << (c - 1);
     s.shared = shared_windows;
     s.K = shared_windows ? s.B : (uint32_t)s.W * s.B;
+    s.constant_work = constant_work;
+    s.Ks = s.K + (constant_work ? 1u : 0u);
     s.n = n;
     if ((shared_windows ? n * (size_t)s.W : n) >= 0x80000000ull) {
         set_error("MSM of %zu points x %d windows exceeds the 2^31 entry-index limit", n, s.W);
         return cudaErrorInvalidValue;
     }
-    // about eight entries per partial sum on average, at least 16 per chunk
+    // the smallest chunk the accumulate may use (buffers are sized for it);
+    // the one it does use is chosen on the device from the entry count (k_nseg)
     s.chunk = 16;
-    if (shared_windows) {
-        size_t per_bucket = n * (size_t)s.W / s.K;
-        while (s.chunk < 256 && (size_t)s.chunk * 4 < per_bucket) s.chunk <<= 1;
-    }
     const uint32_t kw = shared_windows ? 0u : s.B, ew = shared_windows ? (uint32_t)n : 0u;
+    const uint32_t sink = constant_work ? s.K : NO_KEY;
     size_t nn = n ? n : 1;
     G16_CUDA(grow(s.d_scalars_std, s.cap_scalars, nn * 8));
-    size_t kk = (size_t)s.K + 1;
+    size_t kk = (size_t)s.Ks + 1;
     if (kk > s.cap_k || !s.d_counts) {
         size_t cap = 0;
         G16_CUDA(grow(s.d_counts, cap, kk));
@@ -586,27 +669,27 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
         timer().add_bytes("msm_digits", 64.0 * n);   // scalars in, standard-form copy out
         TimedLaunch tl("msm_digits", st);
         k_digits_count<<<blocks_for(n, 256), 256, 0, st>>>((const uint4*)d_scalars, montgomery ? 1 : 0, (uint32_t)n,
-                                                          c, s.W, kw, (uint4*)s.d_scalars_std, s.d_counts);
+                                                          c, s.W, kw, sink, (uint4*)s.d_scalars_std, s.d_counts);
     }
     G16_CUDA(cudaGetLastError());
-    G16_CUDA(scan(s.d_counts, s.d_offsets, s.K, s.d_scan_tmp, s.d_total, st));
+    G16_CUDA(scan(s.d_counts, s.d_offsets, s.Ks, s.d_scan_tmp, s.d_total, st));
     {
         TimedLaunch tl("msm_copy", st);
-        k_copy_u32<<<blocks_for(s.K, 256), 256, 0, st>>>(s.d_cursor, s.d_offsets, s.K);
+        k_copy_u32<<<blocks_for(s.Ks, 256), 256, 0, st>>>(s.d_cursor, s.d_offsets, s.Ks);
     }
     if (n) {
         TimedLaunch tl("msm_scatter", st);
         k_scatter<<<blocks_for(n, 256), 256, 0, st>>>((const uint4*)s.d_scalars_std, (uint32_t)n, c, s.W, kw, ew,
-                                                     s.d_cursor, s.d_entries);
+                                                     sink, s.d_cursor, s.d_entries);
     }
     G16_CUDA(cudaGetLastError());
     // per-bucket segment counts -> segment base (into counts, then scanned)
     {
         TimedLaunch tl("msm_nseg", st);
-        k_nseg<<<blocks_for(s.K, 256), 256, 0, st>>>(s.d_offsets, s.K, s.chunk, s.d_counts, s.d_fat_list,
-                                                      s.d_total + 2);
+        k_nseg<<<blocks_for(s.Ks, 256), 256, 0, st>>>(s.d_offsets, s.Ks, s.K, s.chunk, s.d_counts, s.d_fat_list,
+                                                       s.d_total + 2, s.d_total);
     }
-    G16_CUDA(scan(s.d_counts, s.d_seg_base, s.K, s.d_scan_tmp, s.d_total + 1, st));
+    G16_CUDA(scan(s.d_counts, s.d_seg_base, s.Ks, s.d_scan_tmp, s.d_total + 1, st));
     return cudaSuccess;
 }
 
@@ -615,7 +698,7 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
                               uint32_t n_bases, cudaStream_t st, size_t xyzz_bytes, const char* tag) {
     size_t max_entries = (s.n ? s.n : 1) * (size_t)s.W;
     size_t chunks = (max_entries + s.chunk - 1) / s.chunk;
-    size_t max_partials = (size_t)s.K + chunks + 1;
+    size_t max_partials = (size_t)s.Ks + chunks + 1;
     G16_CUDA(grow_bytes(acc.d_partials, acc.cap_partials, max_partials * xyzz_bytes));
     const uint32_t Wr = s.shared ? 1u : (uint32_t)s.W;   // bucket sets to reduce
     const uint32_t seg = msm_segment_len(Wr, s.B);
@@ -631,25 +714,25 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     uint4* groups = (uint4*)((uint8_t*)acc.d_segments + (size_t)Wr * P * xyzz_bytes);
     {
         TimedLaunch tl(tag, st);
-        k_accumulate<F><<<blocks_for(chunks, 128), 128, 0, st>>>(s.d_entries, s.d_offsets, s.d_seg_base, s.K,
-                                                                  s.d_total, s.chunk, (const uint4*)d_bases,
+        k_accumulate<F><<<blocks_for(chunks, 128), 128, 0, st>>>(s.d_entries, s.d_offsets, s.d_seg_base, s.Ks,
+                                                                  s.d_total, s.d_total + 3, (const uint4*)d_bases,
                                                                   base_offset, n_bases, partials, acc.d_work);
     }
     G16_CUDA(cudaGetLastError());
     {
         TimedLaunch tl("msm_fat_merge", st);
         k_fat_merge_jobs<F><<<296, 128, 128 * xyzz_bytes, st>>>(partials, s.d_offsets, s.d_seg_base, s.d_fat_list,
-                                                                s.d_total + 2, s.chunk);
+                                                                s.d_total + 2, s.d_total + 3);
     }
     {
         TimedLaunch tl("msm_fat_merge", st);
         k_fat_merge_final<F><<<148, 64, 64 * xyzz_bytes, st>>>(partials, s.d_offsets, s.d_seg_base, s.d_fat_list,
-                                                               s.d_total + 2, s.chunk);
+                                                               s.d_total + 2, s.d_total + 3);
     }
     G16_CUDA(cudaGetLastError());
     {
         TimedLaunch tl("msm_bucket_sums", st);
-        k_bucket_sums<F><<<blocks_for(s.K, 128), 128, 0, st>>>(partials, s.d_offsets, s.d_seg_base, s.K, s.chunk,
+        k_bucket_sums<F><<<blocks_for(s.K, 128), 128, 0, st>>>(partials, s.d_offsets, s.d_seg_base, s.K, s.d_total + 3,
                                                                 (uint4*)acc.d_buckets);
     }
     {

@@ -39,9 +39,11 @@ struct MsmSort {
     int c = 0, W = 0;
     uint32_t B = 0;        // buckets per window, 2^(c-1)
     uint32_t K = 0;        // W * B, or B when the windows share one bucket set
+    uint32_t Ks = 0;       // buckets sorted into: K, or K + 1 with the constant-work sink bucket
     bool shared = false;   // entries index window-shifted bases (w * n + i), one bucket set
+    bool constant_work = false;   // zero digits are sorted into the sink bucket K
     size_t n = 0;          // scalars sorted
-    uint32_t chunk = 16;   // accumulate chunk length
+    uint32_t chunk = 16;   // smallest accumulate chunk (buffers are sized for it)
     // device buffers (capacities in elements)
     uint32_t* d_scalars_std = nullptr;  size_t cap_scalars = 0;   // 8 u32 per scalar
     uint32_t* d_counts = nullptr;       size_t cap_k = 0;         // K + 1
@@ -51,7 +53,7 @@ struct MsmSort {
     uint32_t* d_fat_list = nullptr;                               // buckets with many partials
     uint32_t* d_scan_tmp = nullptr;     size_t cap_tmp = 0;
     uint32_t* d_entries = nullptr;      size_t cap_entries = 0;
-    uint32_t* d_total = nullptr;                                  // [0] = M, [1] = S, [2] = fat buckets
+    uint32_t* d_total = nullptr;                                  // [0] = M, [1] = S, [2] = fat buckets, [3] = L
     void release();
 };
 
@@ -74,8 +76,12 @@ int msm_window_bits(size_t m);
 // shared_windows: the bases are the window-shifted table 2^(c w) P_i laid out
 // at w * n + i (msm_window_table); all windows then fall into one bucket set
 // and the result needs no Horner step.
+// constant_work (the reference's Work::Constant, crates/msm/src/lib.rs:206-220):
+// every window of every scalar becomes an entry, zero digits included, which
+// go to a sink bucket K that no reduction reads; the entry count, the
+// accumulate launch and its additions then follow the key, not the witness.
 cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomery, int c, cudaStream_t st,
-                     bool shared_windows = false);
+                     bool shared_windows = false, bool constant_work = false);
 
 // Window count for c-bit signed digits over 255 bits.
 inline int msm_windows(int c) { return (255 + c - 1) / c; }

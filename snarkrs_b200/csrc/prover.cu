@@ -141,6 +141,7 @@ struct g16_backend {
     int ordinal = 0;
     uint64_t vram_limit = 0;
     std::atomic<uint64_t> vram_used{0};
+    std::atomic<bool> constant_work{false};   // Work::Constant for every MSM of this backend
     cudaStream_t stream = nullptr;
     std::mutex mu;   // primitives share the scratch below
     MsmSort sort;
@@ -175,6 +176,7 @@ struct Workspace {
     cudaEvent_t ev_side[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaGraphExec_t graph = nullptr;   // stages 0-9 captured once, replayed per proof
     uint64_t graph_kernels = 0;
+    bool graph_constant_work = false;  // the mode the graph was captured in
     uint64_t proofs = 0;
     uint64_t bytes = 0;                // fixed device buffers
 
@@ -548,7 +550,7 @@ int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
     for (int i = 0; i < 4; i++) st[i] = c->serial ? ws->stream : ws->side[i];
     CK(cudaEventRecord(ws->ev_fork, ws->stream), "event");
     CK(cudaStreamWaitEvent(st[0], ws->ev_fork, 0), "stream wait");
-    CK(msm_sort(ws->sort_w, d_w, c->n_vars, true, c->c_w, st[0], true), "witness sort");
+    CK(msm_sort(ws->sort_w, d_w, c->n_vars, true, c->c_w, st[0], true, c->be->constant_work), "witness sort");
     CK(cudaEventRecord(ws->ev_sort, st[0]), "event");
     for (int i = 1; i < 4; i++) CK(cudaStreamWaitEvent(st[i], ws->ev_sort, 0), "stream wait");
     // acc slots: 0 A, 1 B2, 2 B1, 3 L (4 is H); one stream per MSM so that
@@ -573,7 +575,7 @@ int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
 int enqueue_h_msm(g16_circuit* c, Workspace* ws, const void* d_h) {
     cudaStream_t st = ws->stream;
     const uint32_t nh = c->n * (uint32_t)msm_windows(c->c_h);
-    CK(msm_sort(ws->sort_h, d_h, c->n, true, c->c_h, st, true), "H sort");
+    CK(msm_sort(ws->sort_h, d_h, c->n, true, c->c_h, st, true, c->be->constant_work), "H sort");
     CK(msm_accumulate_g1(ws->sort_h, ws->acc[4], c->t_h, 0, nh, st), "H accumulate");
     CK(cudaMemcpyAsync(ws->h_win + 4 * WIN_SLOT, ws->acc[4].d_windows, XYZZ_G1_BYTES, cudaMemcpyDeviceToHost, st),
        "window readback");
@@ -625,7 +627,12 @@ int run_proof(g16_circuit* c, Workspace* ws, const void* d_w, MsmJac& out) {
     if (use_graph) {
         if (d_w != ws->d_w)
             CK(cudaMemcpyAsync(ws->d_w, d_w, 32ull * c->n_vars, cudaMemcpyDeviceToDevice, ws->stream), "witness copy");
+        if (ws->graph && ws->graph_constant_work != c->be->constant_work) {   // captured in the other mode
+            cudaGraphExecDestroy(ws->graph);
+            ws->graph = nullptr;
+        }
         if (!ws->graph) {
+            ws->graph_constant_work = c->be->constant_work;
             uint64_t k0 = timer().launches.load();
             CK(cudaStreamBeginCapture(ws->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
             int rc = enqueue_proof(c, ws, ws->d_w);
@@ -946,6 +953,12 @@ size_t g16_last_error(char* buf, size_t len) {
         buf[k] = 0;
     }
     return e.size();
+}
+
+int g16_backend_set_constant_work(g16_backend* b, int on) {
+    if (!b) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    b->constant_work = on != 0;
+    return G16_OK;
 }
 
 int g16_backend_open(int ordinal, uint64_t vram_limit, g16_backend** out) {
@@ -1452,7 +1465,7 @@ static int msm_device_impl(g16_backend* b, const void* d_bases, const void* d_sc
         return G16_OK;
     }
     cudaStream_t st = b->stream;
-    CK(msm_sort(b->sort, d_scalars, n, form == G16_SCALARS_MONTGOMERY, 0, st), "MSM sort");
+    CK(msm_sort(b->sort, d_scalars, n, form == G16_SCALARS_MONTGOMERY, 0, st, false, b->constant_work), "MSM sort");
     if (g2) CK(msm_accumulate_g2(b->sort, b->acc, d_bases, 0, (uint32_t)n, st), "MSM accumulate");
     else CK(msm_accumulate_g1(b->sort, b->acc, d_bases, 0, (uint32_t)n, st), "MSM accumulate");
     size_t bytes = (size_t)b->sort.W * (g2 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES);
