@@ -214,57 +214,96 @@ __global__ void k_copy_u32(uint32_t* dst, const uint32_t* src, uint32_t n) {
 }
 
 // ---- accumulate: one thread per chunk of L sorted entries ----
-template <class F>
-__global__ void __launch_bounds__(128) k_accumulate(const uint32_t* __restrict__ entries,
-                                                    const uint32_t* __restrict__ offsets,
-                                                    const uint32_t* __restrict__ seg_base, uint32_t K,
-                                                    const uint32_t* __restrict__ d_M, const uint32_t* __restrict__ d_L,
-                                                    const uint4* __restrict__ bases, uint32_t base_offset,
-                                                    uint32_t n_bases, uint4* __restrict__ partials,
-                                                    unsigned long long* __restrict__ work) {
+// LOCKSTEP: a block-wide barrier after every entry keeps the block's warps on
+// the same instructions.  A fully inlined G1 madd is too long for the
+// instruction cache, and warps that drift apart stall on instruction fetch
+// (ncu: no_instruction was the top stall); in lockstep, one fetch serves the
+// whole block.  G2 calls out-of-line Fq2 products and runs without it.
+template <class F, bool LOCKSTEP>
+__device__ __forceinline__ void accumulate_chunks(const uint32_t* __restrict__ entries,
+                                                  const uint32_t* __restrict__ offsets,
+                                                  const uint32_t* __restrict__ seg_base, uint32_t K, uint32_t M,
+                                                  uint32_t L, const uint4* __restrict__ bases, uint32_t base_offset,
+                                                  uint32_t n_bases, uint4* __restrict__ partials,
+                                                  unsigned long long* __restrict__ work) {
     size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t M = *d_M, L = *d_L;
     size_t start = t * L;
-    if (start >= M) return;
-    size_t end = start + L < M ? start + L : M;
+    const bool active = start < M;
+    if (!LOCKSTEP && !active) return;
+    size_t end = active ? (start + L < M ? start + L : M) : start;
     // last bucket g with offsets[g] <= start; then offsets[g+1] > start
-    uint32_t lo = 0, hi = K;
-    while (hi - lo > 1) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (offsets[mid] <= start) lo = mid; else hi = mid;
+    uint32_t g = 0, next = 0;
+    if (active) {
+        uint32_t lo = 0, hi = K;
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (offsets[mid] <= start) lo = mid; else hi = mid;
+        }
+        g = lo;
+        next = offsets[g + 1];
     }
-    uint32_t g = lo;
-    uint32_t next = offsets[g + 1];
     Xyzz<F> acc = Xyzz<F>::identity();
     unsigned adds = 0;
-    for (size_t k = start; k < end; k++) {
-        if (k == next) {
-            st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), acc);
-            acc = Xyzz<F>::identity();
-            do {
-                g++;
-                next = offsets[g + 1];
-            } while (next <= k);
-        }
-        uint32_t e = entries[k];
-        uint32_t idx = e & 0x7fffffffu;
-        if (idx >= base_offset && idx - base_offset < n_bases) {
-            Affine<F> p = ld_affine<F>(bases, idx - base_offset);
-            if (!p.is_inf()) {
-                if (e >> 31) p.y = neg(p.y);
-                // G1 keeps its products inlined; the Fq2 body is large enough
-                // that one out-of-line Fq2 product (three Fq chains) runs
-                // faster than inlined code that misses the instruction cache
-                acc = xyzz_add_affine<F, !std::is_same<F, Fq2>::value>(acc, p.x, p.y);
-                adds++;
+    const size_t stop = LOCKSTEP ? start + L : end;   // lockstep: every thread runs L steps
+    for (size_t k = start; k < stop; k++) {
+        if (!LOCKSTEP || k < end) {
+            if (k == next) {
+                st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), acc);
+                acc = Xyzz<F>::identity();
+                do {
+                    g++;
+                    next = offsets[g + 1];
+                } while (next <= k);
+            }
+            uint32_t e = entries[k];
+            uint32_t idx = e & 0x7fffffffu;
+            if (idx >= base_offset && idx - base_offset < n_bases) {
+                Affine<F> p = ld_affine<F>(bases, idx - base_offset);
+                if (!p.is_inf()) {
+                    if (e >> 31) p.y = neg(p.y);
+                    // G1 keeps its products inlined; the Fq2 body is large enough
+                    // that one out-of-line Fq2 product (three Fq chains) runs
+                    // faster than inlined code that misses the instruction cache
+                    acc = xyzz_add_affine<F, !std::is_same<F, Fq2>::value>(acc, p.x, p.y);
+                    adds++;
+                }
             }
         }
+        if (LOCKSTEP) __syncthreads();
     }
-    st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), acc);
-    // mixed additions performed, one atomic per converged group of lanes
+    if (active) st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), acc);
+    // mixed additions performed, one atomic per warp (every lane reaches here in lockstep mode)
     unsigned mask = __activemask();
     unsigned total = __reduce_add_sync(mask, adds);
-    if ((threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1)) atomicAdd(work, (unsigned long long)total);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1) && total) atomicAdd(work, (unsigned long long)total);
+}
+
+constexpr int ACC_BLOCK_G1 = 512;   // lockstep block: 16 warps, one block per SM (<= 128 registers)
+constexpr int ACC_BLOCK_G2 = 128;
+
+__global__ void __launch_bounds__(ACC_BLOCK_G1, 1) k_accumulate_g1(const uint32_t* __restrict__ entries,
+                                                                   const uint32_t* __restrict__ offsets,
+                                                                   const uint32_t* __restrict__ seg_base, uint32_t K,
+                                                                   const uint32_t* __restrict__ d_M,
+                                                                   const uint32_t* __restrict__ d_L,
+                                                                   const uint4* __restrict__ bases, uint32_t base_offset,
+                                                                   uint32_t n_bases, uint4* __restrict__ partials,
+                                                                   unsigned long long* __restrict__ work) {
+    const uint32_t M = *d_M, L = *d_L;
+    if ((size_t)blockIdx.x * blockDim.x * L >= M) return;   // the whole block has no entries
+    accumulate_chunks<Fq, true>(entries, offsets, seg_base, K, M, L, bases, base_offset, n_bases, partials, work);
+}
+
+__global__ void __launch_bounds__(ACC_BLOCK_G2) k_accumulate_g2(const uint32_t* __restrict__ entries,
+                                                               const uint32_t* __restrict__ offsets,
+                                                               const uint32_t* __restrict__ seg_base, uint32_t K,
+                                                               const uint32_t* __restrict__ d_M,
+                                                               const uint32_t* __restrict__ d_L,
+                                                               const uint4* __restrict__ bases, uint32_t base_offset,
+                                                               uint32_t n_bases, uint4* __restrict__ partials,
+                                                               unsigned long long* __restrict__ work) {
+    accumulate_chunks<Fq2, false>(entries, offsets, seg_base, K, *d_M, *d_L, bases, base_offset, n_bases, partials,
+                                  work);
 }
 
 __device__ __forceinline__ uint32_t n_partials(const uint32_t* offsets, uint32_t g, uint32_t L) {
@@ -714,9 +753,14 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     uint4* groups = (uint4*)((uint8_t*)acc.d_segments + (size_t)Wr * P * xyzz_bytes);
     {
         TimedLaunch tl(tag, st);
-        k_accumulate<F><<<blocks_for(chunks, 128), 128, 0, st>>>(s.d_entries, s.d_offsets, s.d_seg_base, s.Ks,
-                                                                  s.d_total, s.d_total + 3, (const uint4*)d_bases,
-                                                                  base_offset, n_bases, partials, acc.d_work);
+        if (std::is_same<F, g16d::Fq>::value)
+            k_accumulate_g1<<<blocks_for(chunks, ACC_BLOCK_G1), ACC_BLOCK_G1, 0, st>>>(
+                s.d_entries, s.d_offsets, s.d_seg_base, s.Ks, s.d_total, s.d_total + 3, (const uint4*)d_bases,
+                base_offset, n_bases, partials, acc.d_work);
+        else
+            k_accumulate_g2<<<blocks_for(chunks, ACC_BLOCK_G2), ACC_BLOCK_G2, 0, st>>>(
+                s.d_entries, s.d_offsets, s.d_seg_base, s.Ks, s.d_total, s.d_total + 3, (const uint4*)d_bases,
+                base_offset, n_bases, partials, acc.d_work);
     }
     G16_CUDA(cudaGetLastError());
     {
