@@ -182,13 +182,17 @@ __device__ __forceinline__ uint32_t fat_job_len(uint32_t ns) {
 }
 
 // Entries per accumulate thread, chosen on the device from the sorted count
-// M: at least L_min, and no more threads than ACC_THREADS, so that sparse
-// scalars (witnesses of zeros and ones) still spread over the whole GPU and
-// dense ones keep per-bucket partial counts low.
+// M and the K real buckets: at least L_min, no more than ACC_THREADS threads,
+// and about M / (4 K) or more, so that an average bucket gets at most ~4
+// partial sums and only skewed buckets (a repeated scalar such as 1) take the
+// fat-bucket path.  Sparse scalars (witnesses of zeros and ones) still spread
+// over the whole GPU.
 constexpr uint32_t ACC_THREADS = 1u << 19;
 
-__device__ __forceinline__ uint32_t chunk_len(uint32_t M, uint32_t L_min) {
+__device__ __forceinline__ uint32_t chunk_len(uint32_t M, uint32_t K, uint32_t L_min) {
     uint32_t L = (uint32_t)(((uint64_t)M + ACC_THREADS - 1) / ACC_THREADS);
+    uint32_t per_bucket = (uint32_t)(((uint64_t)M + 4ull * K - 1) / (4ull * K));
+    if (per_bucket > L) L = per_bucket;
     return L > L_min ? L : L_min;
 }
 
@@ -199,7 +203,7 @@ __global__ void k_nseg(const uint32_t* __restrict__ offsets, uint32_t Ks, uint32
                        uint32_t* __restrict__ nseg, uint32_t* __restrict__ fat_list, uint32_t* __restrict__ fat_count,
                        uint32_t* __restrict__ total) {
     uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t L = chunk_len(total[0], L_min);
+    const uint32_t L = chunk_len(total[0], K, L_min);
     if (g == 0) total[3] = L;
     if (g >= Ks) return;
     uint32_t lo = offsets[g], hi = offsets[g + 1];

@@ -87,6 +87,22 @@ def test_msm_g1_config_sizes_match_oracle(backend, n, dist):
     assert got == want
 
 
+def test_msm_g1_2_22_matches_oracle_and_splits(backend):
+    """The largest configured G1 MSM (2^22 points): equal to the oracle for both scalar
+    distributions, and to the sum of the MSMs of its two halves."""
+    n = 1 << 22
+    bases = S.synth_points(1, 4242, n)
+    msm = S.CudaMsm(backend)
+    for dist in (0, 1):
+        scal = S.synth_scalars(4243 + dist, n, dist)
+        got = msm.msm_g1(bases, scal)
+        assert got == O.msm_g1(bases, scal)
+        h = n // 2
+        lo = msm.msm_g1(bases[:64 * h], scal[:32 * h])
+        hi = msm.msm_g1(bases[64 * h:], scal[32 * h:])
+        assert O.g1_add(lo, hi) == got
+
+
 @pytest.mark.parametrize("n,dist", [(1, 0), (77, 0), (4096, 1), (1 << 16, 0)])
 def test_msm_g2_matches_oracle(backend, n, dist):
     got, want = msm_pair(backend, n, dist, 31 + n, g2=True)
