@@ -65,6 +65,54 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
 
+class Ranks:
+    """One process per GPU, as torchrun launches them: a barrier and the max over
+    ranks through torch.distributed (NCCL between GPUs; gloo where no GPU is
+    used).  Proofs are independent, so nothing else crosses ranks: each rank
+    proves its own witnesses (witness_seed) on its own replica of the key."""
+
+    def __init__(self, backend="nccl", timeout_s=600):
+        import datetime
+        import torch
+        self.rank, self.local_rank, self.world = dist_env()
+        self.dist = None
+        self.device = "cuda" if backend == "nccl" else "cpu"
+        if self.world > 1:
+            import torch.distributed as dist
+            if backend == "nccl":
+                torch.cuda.set_device(self.local_rank)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, x):
+        if not self.dist:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def witness_seed(rank, step):
+    """Distinct witnesses per rank and step."""
+    return rank * 1_000_000 + step
+
+
+def whole_job_rate(world, steps, max_ms):
+    """Units all ranks processed over the slowest rank's time (weak scaling)."""
+    return world * steps / (max_ms / 1e3)
+
+
 def workload_name(nc, domain, n_vars):
     return "groth16 prove, synthetic R1CS %d constraints (domain 2^%d, %d wires), BN254" % (
         nc, domain.bit_length() - 1, n_vars)
@@ -194,25 +242,9 @@ def run_reference(args):
 def run_ours(args):
     import torch
     import snarkrs_b200 as S
-    rank, local_rank, world = dist_env()
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    def barrier():
-        if dist:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
+    ranks = Ranks("nccl")
+    rank, local_rank, world = ranks.rank, ranks.local_rank, ranks.world
+    barrier, max_over_ranks = ranks.barrier, ranks.max
     torch.cuda.set_device(local_rank)
     backend = S.CudaBackend(local_rank)
     sc = S.SynthCircuit(CIRCUIT_SEED, args.constraints, N_INPUTS, N_PUBLIC)
@@ -230,9 +262,9 @@ def run_ours(args):
     wits = []
     for i in range(W + K):
         t = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
-        t.numpy()[:] = memoryview(sc.witness(rank * 1_000_000 + i))
+        t.numpy()[:] = memoryview(sc.witness(witness_seed(rank, i)))
         wits.append(t)
-    bl = [blinders(rank * 1_000_000 + i) for i in range(W + K)]
+    bl = [blinders(witness_seed(rank, i)) for i in range(W + K)]
     # device-resident copies for the kernel-side number
     dwit = [torch.empty(nbytes, dtype=torch.uint8, device="cuda") for _ in range(W + K)]
     for d, h in zip(dwit, wits):
@@ -257,7 +289,7 @@ def run_ours(args):
     barrier()
     launches = int(S.launch_count() - launches0)
     ms = max_over_ranks(e0.elapsed_time(e1))
-    value = world * K / (ms / 1e3)
+    value = whole_job_rate(world, K, ms)
 
     # ---- e2e: host buffers through the C ABI, pinned witness copied every step ----
     lat = []
@@ -270,7 +302,7 @@ def run_ours(args):
         lat.append(time.perf_counter() - t0)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t_all)
-    e2e_value = world * K / e2e_s
+    e2e_value = whole_job_rate(world, K, 1e3 * e2e_s)
     readback = int(circ.readback_bytes())
 
     # ---- per-kernel times: the same proofs replayed with every stage on one stream ----
@@ -287,7 +319,7 @@ def run_ours(args):
     circ.set_serial(False)
 
     if rank != 0:
-        barrier()
+        ranks.close()
         return
 
     # ---- roofline of the dominant kernel ----
@@ -375,8 +407,7 @@ def run_ours(args):
         except Exception as e:
             line["served"] = {"error": repr(e)[:300]}
     print(json.dumps(line), flush=True)
-    if dist:
-        barrier()
+    ranks.close()
 
 
 def traffic_for(workload, name):
