@@ -175,7 +175,20 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def synth_key(sc, nc, seed=CIRCUIT_SEED, toxic=TOXIC_SEED):
+def make_key(sc, toxic, device_ok=True):
+    """The synthetic .zkey, its point sections on this rank's GPU when there is one
+    (the same bytes as the host generator)."""
+    if device_ok:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return sc.zkey(toxic, device=dist_env()[1])
+        except ImportError:
+            pass
+    return sc.zkey(toxic)
+
+
+def synth_key(sc, nc, seed=CIRCUIT_SEED, toxic=TOXIC_SEED, device_ok=True):
     """The workload's .zkey; cached under /tmp so repeated runs on one host skip the key generation."""
     path = os.path.join(os.environ.get("G16_BENCH_CACHE", "/tmp"), "g16b200_bench_%d_%d_%d.zkey" % (
         seed, nc, toxic))
@@ -184,7 +197,7 @@ def synth_key(sc, nc, seed=CIRCUIT_SEED, toxic=TOXIC_SEED):
             return f.read()
     except OSError:
         pass
-    zk = sc.zkey(toxic)
+    zk = make_key(sc, toxic, device_ok)
     try:
         with open(path + ".tmp", "wb") as f:
             f.write(zk)
@@ -218,7 +231,7 @@ def run_reference(args):
         return
     import snarkrs_b200 as S
     sc = S.SynthCircuit(CIRCUIT_SEED, args.constraints, N_INPUTS, N_PUBLIC)
-    zk = synth_key(sc, args.constraints)
+    zk = synth_key(sc, args.constraints, device_ok=False)   # this arm uses no GPU code at all
     times, threads = cpu_prove_rate(zk, sc, args.warmup + args.steps)
     timed = times[args.warmup:]
     value = len(timed) / sum(timed)
@@ -563,7 +576,7 @@ def run_batch(args, backend=None, emit=True, steps=None):
     t_tune = 0.0
     for i, nc in enumerate(sizes):
         sc = S.SynthCircuit(500 + i, nc, N_INPUTS, N_PUBLIC)
-        circs.append(backend.prepare(S.ProvingKey.from_bytes(sc.zkey(TOXIC_SEED + i), check_points=False)))
+        circs.append(backend.prepare(S.ProvingKey.from_bytes(make_key(sc, TOXIC_SEED + i), check_points=False)))
         wits.append([sc.witness(1000 * i + j) for j in range(8)])
         if not args.no_autotune:
             # the batched objective: as many proofs in flight as prove_batch has lanes

@@ -330,6 +330,11 @@ uint32_t g16_synth_domain_size(const g16_synth *s);
 int g16_synth_witness(const g16_synth *s, uint64_t witness_seed, uint8_t *out_mont);
 /* .zkey bytes; out = NULL to size. threads = 0 uses all cores. */
 int g16_synth_zkey(const g16_synth *s, uint64_t toxic_seed, int threads, uint8_t *out, size_t cap, size_t *len_out);
+/* The same .zkey bytes with the point sections (fixed-base multiplications of
+ * the generators, ~4.4M G1 and 1.1M G2 points at 2^21) computed on the GPU
+ * `device`; G16_ERR_DEVICE if a CUDA call fails. */
+int g16_synth_zkey_device(const g16_synth *s, uint64_t toxic_seed, int device, uint8_t *out, size_t cap,
+                          size_t *len_out);
 /* circom .r1cs bytes; out = NULL to size. */
 int g16_synth_r1cs(const g16_synth *s, uint8_t *out, size_t cap, size_t *len_out);
 /* n affine points k_i G with k_i uniform in [1, r) (group 1 = G1, 64 B each;

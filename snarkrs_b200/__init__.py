@@ -679,12 +679,19 @@ class SynthCircuit:
         check(lib().g16_synth_witness(self._h, ctypes.c_uint64(witness_seed), out))
         return out.raw
 
-    def zkey(self, toxic_seed, threads=0):
+    def zkey(self, toxic_seed, threads=0, device=None):
+        """The .zkey bytes from seeded toxic waste; device=ordinal computes the point
+        sections on that GPU (the same bytes), otherwise host threads do."""
         n = ctypes.c_size_t()
-        check(lib().g16_synth_zkey(self._h, ctypes.c_uint64(toxic_seed), int(threads), None, ctypes.c_size_t(0),
-                                   ctypes.byref(n)))
+        if device is None:
+            fn = lambda buf, cap: lib().g16_synth_zkey(self._h, ctypes.c_uint64(toxic_seed), int(threads), buf, cap,
+                                                       ctypes.byref(n))
+        else:
+            fn = lambda buf, cap: lib().g16_synth_zkey_device(self._h, ctypes.c_uint64(toxic_seed), int(device), buf,
+                                                              cap, ctypes.byref(n))
+        check(fn(None, ctypes.c_size_t(0)))
         out = ctypes.create_string_buffer(n.value)
-        check(lib().g16_synth_zkey(self._h, ctypes.c_uint64(toxic_seed), int(threads), out, n, ctypes.byref(n)))
+        check(fn(out, n))
         return out.raw
 
     def r1cs(self):

@@ -520,6 +520,30 @@ __global__ void __launch_bounds__(128) k_window_normalize(const uint4* __restric
     }
 }
 
+// Fixed-base multiplication for key generation: P_i = k_i G with 8-bit windows,
+// table[w * 256 + d] = d 2^(8 w) G (affine; d = 0 unused), k_i Montgomery Fr.
+// The XYZZ result goes to tmp for k_window_normalize.
+template <class F>
+__global__ void __launch_bounds__(128) k_fixed_base(const uint4* __restrict__ table, const uint4* __restrict__ scalars,
+                                                    size_t n, uint4* __restrict__ tmp) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fr k;
+    uint4 a = __ldg(scalars + 2 * i), b = __ldg(scalars + 2 * i + 1);
+    k.v[0] = a.x; k.v[1] = a.y; k.v[2] = a.z; k.v[3] = a.w;
+    k.v[4] = b.x; k.v[5] = b.y; k.v[6] = b.z; k.v[7] = b.w;
+    k = from_mont(k);
+    Xyzz<F> acc = Xyzz<F>::identity();
+    for (int w = 0; w < 32; w++) {
+        uint32_t d = (k.v[w >> 2] >> (8 * (w & 3))) & 255u;
+        if (d) {
+            Affine<F> p = ld_affine<F>(table, (size_t)w * 256 + d);
+            acc = xyzz_add_affine<F, !std::is_same<F, Fq2>::value>(acc, p.x, p.y);
+        }
+    }
+    st_xyzz<F>(tmp, i, acc);
+}
+
 }  // namespace g16d
 
 namespace g16 {
@@ -585,6 +609,38 @@ static cudaError_t window_table(const void* d_in, size_t n, uint32_t skip, int c
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(tmp);
     return e;
+}
+
+template <class F>
+static cudaError_t fixed_base(const void* d_table, const void* d_scalars, size_t n, void* d_out, cudaStream_t st,
+                              size_t xyzz_bytes) {
+    if (!n) return cudaSuccess;
+    void* tmp = nullptr;
+    G16_CUDA(cudaMalloc(&tmp, n * xyzz_bytes));
+    cudaError_t e;
+    {
+        TimedLaunch tl("fixed_base", st);
+        k_fixed_base<F><<<blocks_for(n, 128), 128, 0, st>>>((const uint4*)d_table, (const uint4*)d_scalars, n,
+                                                            (uint4*)tmp);
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        TimedLaunch tl("fixed_base", st);
+        k_window_normalize<F><<<blocks_for((n + NORM_RUN - 1) / NORM_RUN, 128), 128, 0, st>>>((const uint4*)tmp, n,
+                                                                                            (uint4*)d_out);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(tmp);
+    return e;
+}
+
+cudaError_t fixed_base_g1(const void* d_table, const void* d_scalars, size_t n, void* d_out, cudaStream_t st) {
+    return fixed_base<g16d::Fq>(d_table, d_scalars, n, d_out, st, XYZZ_G1_BYTES);
+}
+
+cudaError_t fixed_base_g2(const void* d_table, const void* d_scalars, size_t n, void* d_out, cudaStream_t st) {
+    return fixed_base<g16d::Fq2>(d_table, d_scalars, n, d_out, st, XYZZ_G2_BYTES);
 }
 
 cudaError_t msm_window_table_g1(const void* d_in, size_t n, uint32_t skip, int c, void* d_out, cudaStream_t st) {

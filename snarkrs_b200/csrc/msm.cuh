@@ -105,6 +105,12 @@ int msm_shared_window_bits(size_t m);
 
 // Build the window-shifted base table: out[w * n + i] = 2^(c w) P_i, affine,
 // for i < n, where P_i = in[i - skip] for i >= skip and infinity below skip.
+// Fixed-base multiplication (key generation): out[i] = k_i G (affine, packed;
+// the point at infinity for k_i = 0), k_i Montgomery Fr on the device, with
+// table[w * 256 + d] = d 2^(8 w) G packed affine (32 x 256 entries).
+cudaError_t fixed_base_g1(const void* d_table, const void* d_scalars, size_t n, void* d_out, cudaStream_t st);
+cudaError_t fixed_base_g2(const void* d_table, const void* d_scalars, size_t n, void* d_out, cudaStream_t st);
+
 cudaError_t msm_window_table_g1(const void* d_in, size_t n, uint32_t skip, int c, void* d_out, cudaStream_t st);
 cudaError_t msm_window_table_g2(const void* d_in, size_t n, uint32_t skip, int c, void* d_out, cudaStream_t st);
 

@@ -31,7 +31,9 @@
 #include "formats.hpp"
 #include "g16b200.h"
 #include "host_bn254.hpp"
+#include "msm.cuh"
 #include <algorithm>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -224,7 +226,65 @@ static void points_into(const FixedBase<F>& fb, const Fr* scalars, size_t n, uin
     for (auto& th : pool) th.join();
 }
 
-static std::vector<uint8_t> write_zkey(const g16_synth& s, uint64_t toxic_seed, int threads) {
+// Where the key's point sections are computed: out[i * stride] = k_i G for the
+// group's generator (1 = G1, 2 = G2), packed affine.  Returns false on failure
+// (error set).
+typedef std::function<bool(int group, const Fr* scalars, size_t n, uint8_t* out)> PointsFn;
+
+// The device path: the same fixed-base 8-bit-window sums on the GPU
+// (fixed_base_g1/g2), normalised with batched inversions, bit-identical.
+struct DevicePoints {
+    int device;
+    cudaStream_t st = nullptr;
+    void *d_t1 = nullptr, *d_t2 = nullptr, *d_k = nullptr, *d_out = nullptr;
+    size_t cap_k = 0, cap_out = 0;
+    bool ok = true;
+    explicit DevicePoints(int dev) : device(dev) {}
+    ~DevicePoints() {
+        for (void* p : {d_t1, d_t2, d_k, d_out})
+            if (p) cudaFree(p);
+        if (st) cudaStreamDestroy(st);
+    }
+    bool check(cudaError_t e, const char* what) {
+        if (e == cudaSuccess) return true;
+        set_error("device key generation: %s: %s", what, cudaGetErrorString(e));
+        ok = false;
+        return false;
+    }
+    template <class F>
+    bool upload_table(const std::vector<Affine<F>>& t, void*& d, size_t point_bytes) {
+        std::vector<uint8_t> packed(t.size() * point_bytes);
+        for (size_t i = 0; i < t.size(); i++) pack(packed.data() + i * point_bytes, t[i]);
+        return check(cudaMalloc(&d, packed.size()), "table") &&
+               check(cudaMemcpy(d, packed.data(), packed.size(), cudaMemcpyHostToDevice), "table upload");
+    }
+    bool points(int group, const Fr* k, size_t n, uint8_t* out) {
+        const size_t pb = group == 1 ? 64 : 128;
+        if (!n) return true;
+        if (n * 32 > cap_k) {
+            if (d_k) cudaFree(d_k);
+            d_k = nullptr;
+            cap_k = 0;
+            if (!check(cudaMalloc(&d_k, n * 32), "scalars")) return false;
+            cap_k = n * 32;
+        }
+        if (n * pb > cap_out) {
+            if (d_out) cudaFree(d_out);
+            d_out = nullptr;
+            cap_out = 0;
+            if (!check(cudaMalloc(&d_out, n * pb), "points")) return false;
+            cap_out = n * pb;
+        }
+        return check(cudaMemcpyAsync(d_k, k, n * 32, cudaMemcpyHostToDevice, st), "scalar upload") &&
+               check(group == 1 ? fixed_base_g1(d_t1, d_k, n, d_out, st) : fixed_base_g2(d_t2, d_k, n, d_out, st),
+                     "fixed-base kernels") &&
+               check(cudaMemcpyAsync(out, d_out, n * pb, cudaMemcpyDeviceToHost, st), "point readback") &&
+               check(cudaStreamSynchronize(st), "synchronize");
+    }
+};
+
+static std::vector<uint8_t> write_zkey(const g16_synth& s, uint64_t toxic_seed, int threads, int device = -1,
+                                       bool* failed = nullptr) {
     host_init();
     SplitMix rng{toxic_seed ^ 0x243F6A8885A308D3ULL};
     const uint32_t n = s.domain, nv = s.n_vars, npub = s.n_public, nc = s.n_constraints;
@@ -301,6 +361,24 @@ static std::vector<uint8_t> write_zkey(const g16_synth& s, uint64_t toxic_seed, 
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     FixedBase<Fq> fb1(G1_GENERATOR);
     FixedBase<Fq2> fb2(G2_GENERATOR);
+    std::unique_ptr<DevicePoints> dev;
+    PointsFn points_of;
+    if (device >= 0) {
+        dev = std::make_unique<DevicePoints>(device);
+        if (!dev->check(cudaSetDevice(device), "cudaSetDevice") ||
+            !dev->check(cudaStreamCreateWithFlags(&dev->st, cudaStreamNonBlocking), "stream") ||
+            !dev->upload_table(fb1.t, dev->d_t1, 64) || !dev->upload_table(fb2.t, dev->d_t2, 128)) {
+            if (failed) *failed = true;
+            return {};
+        }
+        points_of = [&](int group, const Fr* k, size_t n, uint8_t* out) { return dev->points(group, k, n, out); };
+    } else {
+        points_of = [&](int group, const Fr* k, size_t n, uint8_t* out) {
+            if (group == 1) points_into(fb1, k, n, out, 64, threads);
+            else points_into(fb2, k, n, out, 128, threads);
+            return true;
+        };
+    }
 
     BinWriter w;
     w.begin("zkey", 1, 10);
@@ -351,25 +429,24 @@ static std::vector<uint8_t> write_zkey(const g16_synth& s, uint64_t toxic_seed, 
             for (uint32_t t = s.ptr[m][k]; t < s.ptr[m][k + 1]; t++) rec(m, k, s.terms[m][t].sig, s.terms[m][t].coef);
     for (uint32_t j = 0; j <= npub; j++) rec(0, nc + j, j, Fr::one());
     w.end_section();
-    auto g1_section = [&](uint32_t id, const std::vector<Fr>& sc) {
+    bool good = true;
+    auto point_section = [&](uint32_t id, int group, const std::vector<Fr>& sc) {
         w.section(id);
         size_t at = w.buf.size();
-        w.buf.resize(at + sc.size() * 64);
-        points_into(fb1, sc.data(), sc.size(), w.buf.data() + at, 64, threads);
+        w.buf.resize(at + sc.size() * (group == 1 ? 64 : 128));
+        if (good) good = points_of(group, sc.data(), sc.size(), w.buf.data() + at);
         w.end_section();
     };
-    g1_section(3, ic_s);
-    g1_section(9, h_s);
-    g1_section(8, l_s);
-    g1_section(5, u);
-    g1_section(6, v);
-    w.section(7);
-    {
-        size_t at = w.buf.size();
-        w.buf.resize(at + (size_t)nv * 128);
-        points_into(fb2, v.data(), nv, w.buf.data() + at, 128, threads);
+    point_section(3, 1, ic_s);
+    point_section(9, 1, h_s);
+    point_section(8, 1, l_s);
+    point_section(5, 1, u);
+    point_section(6, 1, v);
+    point_section(7, 2, v);
+    if (!good) {
+        if (failed) *failed = true;
+        return {};
     }
-    w.end_section();
     // 10: contributions (empty transcript)
     w.section(10);
     uint8_t zero64[64] = {0};
@@ -441,6 +518,34 @@ int g16_synth_new(uint64_t seed, uint32_t n_constraints, uint32_t n_inputs, uint
     s->domain = 1u << (p + 1);
     build_structure(*s, seed);
     *out = s.release();
+    return G16_OK;
+}
+
+int g16_synth_zkey_device(const g16_synth* cs, uint64_t toxic_seed, int device, uint8_t* out, size_t cap,
+                          size_t* len_out) {
+    if (!cs || !len_out || device < 0) {
+        set_error("g16_synth_zkey_device: null argument or negative device");
+        return G16_ERR_INVALID_ARGUMENT;
+    }
+    g16_synth* s = const_cast<g16_synth*>(cs);
+    std::lock_guard<std::mutex> g(s->mu);
+    if (!s->cached || s->cached_seed != toxic_seed) {
+        bool failed = false;
+        std::vector<uint8_t> z = write_zkey(*s, toxic_seed, 0, device, &failed);
+        if (failed) return G16_ERR_DEVICE;
+        s->zkey = std::move(z);
+        s->cached = true;
+        s->cached_seed = toxic_seed;
+    }
+    *len_out = s->zkey.size();
+    if (!out) return G16_OK;
+    if (cap < s->zkey.size()) {
+        set_error("g16_synth_zkey_device: buffer of %zu bytes, need %zu", cap, s->zkey.size());
+        return G16_ERR_INVALID_ARGUMENT;
+    }
+    std::memcpy(out, s->zkey.data(), s->zkey.size());
+    std::vector<uint8_t>().swap(s->zkey);
+    s->cached = false;
     return G16_OK;
 }
 

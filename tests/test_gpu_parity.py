@@ -246,3 +246,12 @@ def test_batch_equals_singles(backend, circuits):
     batch = backend.prove_batch(jobs)
     for (c, w, r, s), p in zip(jobs, batch):
         assert p == c.prove_with_blinders(w, r, s)
+
+
+def test_device_key_generation_is_the_host_one(backend):
+    """g16_synth_zkey_device: the point sections computed on the GPU give the same
+    .zkey bytes as the host generator (and so the same proofs)."""
+    for nc, npub in ((300, 4), (20000, 16)):
+        host = S.SynthCircuit(seed=808 + nc, n_constraints=nc, n_inputs=40, n_public=npub).zkey(99)
+        dev = S.SynthCircuit(seed=808 + nc, n_constraints=nc, n_inputs=40, n_public=npub).zkey(99, device=0)
+        assert dev == host
