@@ -13,16 +13,17 @@
 //      histogram with warp-aggregated atomics;
 //   2. exclusive scan -> bucket offsets; scatter of (point index | sign) into
 //      bucket order: a counting sort of (window, bucket, point) keys;
-//   3. accumulate: the sorted list is cut into fixed-length chunks, one
-//      thread per chunk adds its points into XYZZ partial bucket sums, so a
-//      fat bucket (a repeated witness value) is spread over many threads;
+//   3. accumulate: the sorted list is cut into chunks whose length the
+//      device picks from the entry count, one thread per chunk adds its
+//      points into XYZZ partial bucket sums, so a fat bucket (a repeated
+//      witness value) is spread over many threads;
 //   4. fat buckets (more than a few partials, e.g. every scalar equal to 1)
 //      are folded by blocks in two tree stages; then one thread per bucket
 //      sums its partials into S_b;
-//   5. the running-sum reduction sum_b (b+1) S_b in segments of 8 buckets
-//      (two short dependent chains per thread), each segment weighted by its
-//      offset, then block tree sums per window: depth stays short because a
-//      dependent XYZZ addition costs microseconds of latency;
+//   5. the running-sum reduction sum_b (b+1) S_b in segments of 1-8 buckets
+//      (two short dependent chains per thread; msm_segment_len), each segment
+//      weighted by its offset, then block tree sums per window: depth stays
+//      short because a dependent XYZZ addition costs microseconds of latency;
 //   6. host: Horner over the W window sums (c doublings between windows).
 // One sort serves every base vector that shares the scalars: the prover
 // sorts the witness once and accumulates A, B1, L (G1) and B2 (G2) from it.
