@@ -137,12 +137,20 @@ class Clocks:
         self.proc = None
 
     def start(self):
+        """Start sampling every 50 ms and return once the first sample is in, so the
+        samples cover the region timed next."""
+        self.first = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return
+        import select
+        ready, _, _ = select.select([self.proc.stdout], [], [], 10.0)
+        if ready:
+            self.first = self.proc.stdout.readline()   # taken before the timed region: not counted
 
     def stop(self):
         if not self.proc:
