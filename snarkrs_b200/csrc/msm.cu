@@ -401,50 +401,100 @@ __global__ void __launch_bounds__(128) k_bucket_sums(const uint4* __restrict__ p
     st_xyzz<F>(buckets, g, acc);
 }
 
-// Segment (w, p) of seg buckets: running sums give run = sum S_b and
-// tot = sum (b - p seg + 1) S_b over the segment; the segment's share of
-// sum_b (b + 1) S_b is then tot + (p seg) run.  seg is 1..8: short segments
-// when there are few buckets (more threads, a shorter dependent chain), up to
-// 8 when there are enough segments to fill the GPU anyway (msm_segment_len).
-
-template <class F>
-__global__ void __launch_bounds__(128) k_segments(const uint4* __restrict__ buckets, uint32_t B, uint32_t W,
-                                                  uint32_t P, uint32_t seg, uint4* __restrict__ seg_out) {
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= W * P) return;
-    uint32_t w = t / P, p = t % P;
+// Bucket reduction, step 1.  A set's buckets S_0 .. S_{B-1} (S_b holds the
+// points whose digit is b + 1) are cut into pieces of seg buckets; thread t of
+// block j owns piece p = j 2^LB + t and folds it by running sums into
+//   run_p = sum_i S_{p seg + i},   tot_p = sum_i (i + 1) S_{p seg + i},
+// so that the set's sum_b (b + 1) S_b = sum_p tot_p + seg sum_p p run_p.
+// The weights p are split over their bits instead of being multiplied out (a
+// double-and-add per piece costs more than the piece's running sums): the
+// block halves its 2^LB run values LB times in shared memory, v_t += v_(t+h)
+// for h = 2^(LB-1) .. 1, and the upper half [h, 2h) that a halving reads holds
+// exactly the folded values whose piece index has bit log2(h) set.  Once
+// frozen, each upper half is summed by a tree that runs alongside the later
+// halvings, so G_j = sum over the pieces with bit j set of run_p ends in slot
+// 2^j after LB steps.  The tot values halve into T on the threads [h, 2h),
+// which the run halving leaves idle (with seg = 1, tot = run and T = R).  Each
+// step costs a thread at most one addition: a dependent XYZZ addition takes
+// microseconds on an otherwise idle SM, so the depth is what counts here.
+// The block writes T, G_0 .. G_(LB-1) and its run total R (LB + 2 points).
+template <class F, int LB>
+__global__ void __launch_bounds__(1 << LB) k_reduce_pieces(const uint4* __restrict__ buckets, uint32_t B,
+                                                           uint32_t seg, uint4* __restrict__ out) {
+    constexpr uint32_t N = 1u << LB;
+    extern __shared__ uint4 smem[];
+    uint4* s_run = smem;
+    uint4* s_tot = smem + N * 4 * Codec<F>::U4;
+    const uint32_t t = threadIdx.x, set = blockIdx.y;
+    const uint32_t p = blockIdx.x * N + t;
+    const bool weighted = seg > 1;   // uniform: tot differs from run
     Xyzz<F> run = Xyzz<F>::identity(), tot = Xyzz<F>::identity();
-    size_t g0 = (size_t)w * B + (size_t)p * seg;
+    if ((size_t)p * seg < B) {
+        const size_t g0 = (size_t)set * B + (size_t)p * seg;
 #pragma unroll 1
-    for (int j = (int)seg - 1; j >= 0; j--) {
-        run = xyzz_add<F, false>(run, ld_xyzz<F>(buckets, g0 + j));
-        tot = xyzz_add<F, false>(tot, run);
-    }
-    uint32_t k = p * seg;
-    Xyzz<F> acc = Xyzz<F>::identity();
-    if (k) {
-        for (int bit = 31 - __clz(k); bit >= 0; bit--) {
-            acc = xyzz_dbl<F, false>(acc);
-            if ((k >> bit) & 1u) acc = xyzz_add<F, false>(acc, run);
+        for (int i = (int)seg - 1; i >= 0; i--) {
+            run = xyzz_add<F, false>(run, ld_xyzz<F>(buckets, g0 + i));
+            if (weighted) tot = xyzz_add<F, false>(tot, run);
         }
     }
-    st_xyzz<F>(seg_out, t, xyzz_add<F, false>(tot, acc));
+    // run stays equal to slot t of s_run: thread t is the only writer of slot t
+    st_xyzz<F>(s_run, t, run);
+    if (weighted) st_xyzz<F>(s_tot, t, tot);
+    const uint32_t lg = t ? 31 - __clz(t) : 0;   // slot t lies in the upper half [2^lg, 2^(lg+1))
+#pragma unroll 1
+    for (uint32_t k = 1; k <= (uint32_t)LB; k++) {
+        __syncthreads();
+        const uint32_t h = N >> k;
+        // a step reads no slot that another thread writes in the same step:
+        // run halving reads [h, 2h) and writes [0, h); the tot halving on
+        // thread t in [h, 2h) reads t - h and t and writes t - h; the trees
+        // stay at 2h and above
+        if (t < h) {
+            run = xyzz_add<F, false>(run, ld_xyzz<F>(s_run, t + h));
+            st_xyzz<F>(s_run, t, run);
+        } else if (t < 2 * h) {
+            if (weighted) {
+                tot = xyzz_add<F, false>(ld_xyzz<F>(s_tot, t - h), ld_xyzz<F>(s_tot, t));
+                st_xyzz<F>(s_tot, t - h, tot);   // at the last step (t = 1) this is T
+            }
+        } else {
+            // the half [2^lg, 2^(lg+1)) froze at step LB - lg; tree level k - (LB - lg) - 1 now
+            const uint32_t hs = 1u << lg, s = 1u << (k - (LB - lg) - 1), o = t - hs;
+            if ((o & (2 * s - 1)) == 0 && o + s < hs) {
+                run = xyzz_add<F, false>(run, ld_xyzz<F>(s_run, t + s));
+                st_xyzz<F>(s_run, t, run);
+            }
+        }
+    }
+    const size_t o0 = ((size_t)set * gridDim.x + blockIdx.x) * (LB + 2);
+    if (t == 0) {
+        if (!weighted) st_xyzz<F>(out, o0, run);
+        st_xyzz<F>(out, o0 + LB + 1, run);
+    } else if ((t & (t - 1)) == 0) {
+        st_xyzz<F>(out, o0 + 1 + lg, run);   // G_lg
+        if (t == 1 && weighted) st_xyzz<F>(out, o0, tot);
+    }
 }
 
-// Group sums: grid (blocks per group, groups); each block folds `per` items per
-// thread and writes one partial per block.
-template <class F>
-__global__ void __launch_bounds__(128) k_group_sum(const uint4* __restrict__ in, uint32_t items_per_group,
-                                                   uint4* __restrict__ out) {
+// Bucket reduction, step 2 (when a set has more than a couple of blocks):
+// block (o, set) sums one term over the set's nb blocks: o = 0 gives T,
+// o = 1 .. LB gives G_(o-1), o = LB + 1 + i gives Gb_i, the sum of the run
+// totals R of the blocks whose index has bit i set.  The host then forms
+// T + seg (sum_j 2^j G_j + 2^LB sum_i 2^i Gb_i) by doublings and additions.
+template <class F, int LB>
+__global__ void __launch_bounds__(128) k_reduce_sets(const uint4* __restrict__ in, uint32_t nb,
+                                                     uint4* __restrict__ out) {
     extern __shared__ uint4 smem[];
-    uint32_t grp = blockIdx.y;
-    uint32_t chunk = (items_per_group + gridDim.x - 1) / gridDim.x;
-    uint32_t lo = blockIdx.x * chunk, hi = min(lo + chunk, items_per_group);
+    const uint32_t o = blockIdx.x, set = blockIdx.y;
+    const size_t base = (size_t)set * nb * (LB + 2);
     Xyzz<F> acc = Xyzz<F>::identity();
-    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
-        acc = xyzz_add<F, false>(acc, ld_xyzz<F>(in, (size_t)grp * items_per_group + i));
+    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
+        if (o <= (uint32_t)LB) acc = xyzz_add<F, false>(acc, ld_xyzz<F>(in, base + (size_t)j * (LB + 2) + o));
+        else if ((j >> (o - LB - 1)) & 1u)
+            acc = xyzz_add<F, false>(acc, ld_xyzz<F>(in, base + (size_t)j * (LB + 2) + LB + 1));
+    }
     acc = block_sum(acc, smem);
-    if (threadIdx.x == 0) st_xyzz<F>(out, (size_t)grp * gridDim.x + blockIdx.x, acc);
+    if (threadIdx.x == 0) st_xyzz<F>(out, (size_t)set * gridDim.x + o, acc);
 }
 
 // Window-shifted base table: out[w n + i] = 2^(c w) P_i (affine).  Built once
@@ -800,17 +850,16 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     size_t max_partials = (size_t)s.Ks + chunks + 1;
     G16_CUDA(grow_bytes(acc.d_partials, acc.cap_partials, max_partials * xyzz_bytes));
     const uint32_t Wr = s.shared ? 1u : (uint32_t)s.W;   // bucket sets to reduce
-    const uint32_t seg = msm_segment_len(Wr, s.B);
-    const uint32_t P = s.B / seg;                  // segments per window
-    const uint32_t G = (uint32_t)msm_group_blocks(P);   // group-sum blocks per window
-    acc.segs_per_window = P;
+    constexpr int LB = std::is_same<F, g16d::Fq>::value ? 7 : 6;   // pieces per reduction block: 2^LB
+    const MsmReducePlan plan = msm_reduce_plan(Wr, s.B, LB == 6);
+    acc.plan = plan;
     G16_CUDA(grow_bytes(acc.d_buckets, acc.cap_buckets, (size_t)s.K * xyzz_bytes));
-    G16_CUDA(grow_bytes(acc.d_segments, acc.cap_segments, ((size_t)Wr * P + (size_t)Wr * G) * xyzz_bytes));
-    G16_CUDA(grow_bytes(acc.d_windows, acc.cap_windows, (size_t)Wr * xyzz_bytes));
+    if (!plan.direct)
+        G16_CUDA(grow_bytes(acc.d_segments, acc.cap_segments, plan.block_points() * xyzz_bytes));
+    G16_CUDA(grow_bytes(acc.d_windows, acc.cap_windows, plan.result_points() * xyzz_bytes));
     if (!acc.d_work) G16_CUDA(cudaMalloc((void**)&acc.d_work, sizeof(unsigned long long)));
     G16_CUDA(cudaMemsetAsync(acc.d_work, 0, sizeof(unsigned long long), st));
     uint4* partials = (uint4*)acc.d_partials;
-    uint4* groups = (uint4*)((uint8_t*)acc.d_segments + (size_t)Wr * P * xyzz_bytes);
     {
         TimedLaunch tl(tag, st);
         if (std::is_same<F, g16d::Fq>::value)
@@ -840,17 +889,16 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
                                                                 (uint4*)acc.d_buckets);
     }
     {
-        TimedLaunch tl("msm_segments", st);
-        k_segments<F><<<blocks_for((size_t)Wr * P, 128), 128, 0, st>>>((const uint4*)acc.d_buckets, s.B, Wr, P, seg,
-                                                                        (uint4*)acc.d_segments);
+        TimedLaunch tl("msm_reduce", st);
+        uint4* blocks = (uint4*)(plan.direct ? acc.d_windows : acc.d_segments);
+        k_reduce_pieces<F, LB><<<dim3(plan.nb, Wr), 1u << LB, 2 * ((size_t)1 << LB) * xyzz_bytes, st>>>(
+            (const uint4*)acc.d_buckets, s.B, plan.seg, blocks);
     }
-    {
-        TimedLaunch tl("msm_window_sum", st);
-        k_group_sum<F><<<dim3(G, Wr), 128, 128 * xyzz_bytes, st>>>((const uint4*)acc.d_segments, P, groups);
-    }
-    {
-        TimedLaunch tl("msm_window_sum", st);
-        k_group_sum<F><<<dim3(1, Wr), 128, 128 * xyzz_bytes, st>>>(groups, G, (uint4*)acc.d_windows);
+    if (!plan.direct) {
+        TimedLaunch tl("msm_reduce", st);
+        const unsigned threads = plan.nb < 128 ? plan.nb : 128;
+        k_reduce_sets<F, LB><<<dim3(LB + 1 + plan.hb, Wr), threads, threads * xyzz_bytes, st>>>(
+            (const uint4*)acc.d_segments, plan.nb, (uint4*)acc.d_windows);
     }
     G16_CUDA(cudaGetLastError());
     return cudaSuccess;
@@ -880,64 +928,69 @@ Fq read_coord<Fq>(const uint8_t* p) { return fq_at(p); }
 template <>
 Fq2 read_coord<Fq2>(const uint8_t* p) { return {fq_at(p), fq_at(p + 32)}; }
 
+// XYZZ (x = X / ZZ, y = Y / ZZZ) -> Jacobian (x = X' / Z^2, y = Y' / Z^3)
+// without an inversion: Z = ZZ ZZZ, X' = X ZZ ZZZ^2, Y' = Y ZZ^3 ZZZ^2.
 template <class F>
-static Jac<F> combine(const uint8_t* w, int W, int c) {
+static Jac<F> xyzz_to_jac(const uint8_t* p) {
     const size_t cs = sizeof(F) == sizeof(Fq) ? 32 : 64;   // coordinate bytes
-    std::vector<F> zz(W), zzz(W);
-    std::vector<F> X(W), Y(W);
-    std::vector<char> inf(W);
-    for (int i = 0; i < W; i++) {
-        const uint8_t* p = w + (size_t)i * 4 * cs;
-        X[i] = read_coord<F>(p);
-        Y[i] = read_coord<F>(p + cs);
-        zz[i] = read_coord<F>(p + 2 * cs);
-        zzz[i] = read_coord<F>(p + 3 * cs);
-        inf[i] = zz[i].is_zero();
+    F X = read_coord<F>(p), Y = read_coord<F>(p + cs), zz = read_coord<F>(p + 2 * cs), zzz = read_coord<F>(p + 3 * cs);
+    if (zz.is_zero()) return Jac<F>::identity();
+    F zzz2 = zzz.sqr();
+    Jac<F> r;
+    r.z = zz * zzz;
+    r.x = X * zz * zzz2;
+    r.y = Y * zz.sqr() * zz * zzz2;
+    return r;
+}
+
+// One set's sum_b (b + 1) S_b from the reduction's points (msm_reduce_plan).
+template <class F>
+static Jac<F> set_sum(const uint8_t* p, const MsmReducePlan& pl) {
+    const size_t pb = 4 * (sizeof(F) == sizeof(Fq) ? 32 : 64);
+    auto at = [&](size_t i) { return xyzz_to_jac<F>(p + i * pb); };
+    Jac<F> T = Jac<F>::identity();
+    std::vector<Jac<F>> G(pl.lb, Jac<F>::identity()), Gb(pl.hb, Jac<F>::identity());
+    if (pl.direct) {
+        for (uint32_t j = 0; j < pl.nb; j++) {
+            const size_t o = (size_t)j * pl.block_terms();
+            T = T + at(o);
+            for (uint32_t i = 0; i < pl.lb; i++) G[i] = G[i] + at(o + 1 + i);
+            if (pl.hb) {
+                Jac<F> R = at(o + pl.lb + 1);
+                for (uint32_t i = 0; i < pl.hb; i++)
+                    if ((j >> i) & 1u) Gb[i] = Gb[i] + R;
+            }
+        }
+    } else {
+        T = at(0);
+        for (uint32_t i = 0; i < pl.lb; i++) G[i] = at(1 + i);
+        for (uint32_t i = 0; i < pl.hb; i++) Gb[i] = at(pl.lb + 1 + i);
     }
-    // batch inversion of every nonzero zz and zzz
-    std::vector<F> vals, pref;
-    for (int i = 0; i < W; i++)
-        if (!inf[i]) {
-            vals.push_back(zz[i]);
-            vals.push_back(zzz[i]);
-        }
-    std::vector<F> invs(vals.size());
-    if (!vals.empty()) {
-        pref.resize(vals.size());
-        F run = F::one();
-        for (size_t k = 0; k < vals.size(); k++) {
-            pref[k] = run;
-            run = run * vals[k];
-        }
-        F iv = run.inv();
-        for (size_t k = vals.size(); k-- > 0;) {
-            invs[k] = iv * pref[k];
-            iv = iv * vals[k];
-        }
-    }
-    std::vector<Affine<F>> aff(W);
-    size_t k = 0;
-    for (int i = 0; i < W; i++) {
-        if (inf[i]) {
-            aff[i].x = F::zero();
-            aff[i].y = F::zero();
-            aff[i].inf = true;
-            continue;
-        }
-        aff[i].x = X[i] * invs[k];
-        aff[i].y = Y[i] * invs[k + 1];
-        aff[i].inf = false;
-        k += 2;
-    }
-    Jac<F> acc = Jac<F>::from_affine(aff[W - 1]);
+    Jac<F> acc = Jac<F>::identity();
+    for (int i = (int)pl.hb - 1; i >= 0; i--) acc = acc.dbl() + Gb[i];
+    for (int j = (int)pl.lb - 1; j >= 0; j--) acc = acc.dbl() + G[j];
+    for (uint32_t s = pl.seg; s > 1; s >>= 1) acc = acc.dbl();
+    return acc + T;
+}
+
+template <class F>
+static Jac<F> combine(const uint8_t* result, const MsmReducePlan& pl, int c) {
+    const size_t set_bytes = (size_t)pl.set_terms() * 4 * (sizeof(F) == sizeof(Fq) ? 32 : 64);
+    const int W = (int)pl.sets;
+    if (W == 0) return Jac<F>::identity();
+    Jac<F> acc = set_sum<F>(result + (size_t)(W - 1) * set_bytes, pl);
     for (int i = W - 2; i >= 0; i--) {
         for (int j = 0; j < c; j++) acc = acc.dbl();
-        acc = acc.add_affine(aff[i]);
+        acc = acc + set_sum<F>(result + (size_t)i * set_bytes, pl);
     }
     return acc;
 }
 
-G1J msm_combine_g1(const uint8_t* windows_xyzz, int W, int c) { return combine<Fq>(windows_xyzz, W, c); }
-G2J msm_combine_g2(const uint8_t* windows_xyzz, int W, int c) { return combine<Fq2>(windows_xyzz, W, c); }
+G1J msm_combine_g1(const uint8_t* result_xyzz, const MsmReducePlan& plan, int c) {
+    return combine<Fq>(result_xyzz, plan, c);
+}
+G2J msm_combine_g2(const uint8_t* result_xyzz, const MsmReducePlan& plan, int c) {
+    return combine<Fq2>(result_xyzz, plan, c);
+}
 
 }  // namespace g16

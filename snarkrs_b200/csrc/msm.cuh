@@ -20,11 +20,13 @@
 //   4. fat buckets (more than a few partials, e.g. every scalar equal to 1)
 //      are folded by blocks in two tree stages; then one thread per bucket
 //      sums its partials into S_b;
-//   5. the running-sum reduction sum_b (b+1) S_b in segments of 1-8 buckets
-//      (two short dependent chains per thread; msm_segment_len), each segment
-//      weighted by its offset, then block tree sums per window: depth stays
-//      short because a dependent XYZZ addition costs microseconds of latency;
-//   6. host: Horner over the W window sums (c doublings between windows).
+//   5. the reduction sum_b (b+1) S_b: threads fold pieces of seg buckets by
+//      running sums, blocks split the pieces' weights over their bits in
+//      shared memory (msm_reduce_plan), a second kernel sums the blocks' bit
+//      terms per set; no step has a long dependent chain, since a dependent
+//      XYZZ addition costs microseconds of latency;
+//   6. host: each set's sum from its bit terms, then Horner over the W
+//      window sums (c doublings between windows).
 // One sort serves every base vector that shares the scalars: the prover
 // sorts the witness once and accumulates A, B1, L (G1) and B2 (G2) from it.
 #pragma once
@@ -34,6 +36,47 @@
 #include "host_bn254.hpp"
 
 namespace g16 {
+
+// Bucket reduction plan for `sets` bucket sets of B buckets each (B a power of
+// two).  A set's sum is sum_b (b + 1) S_b.  Its buckets are cut into pieces of
+// seg buckets (one thread's running sums), 2^lb pieces per block (lb = 7 for
+// G1, 6 for G2, so that a block's two shared-memory point arrays fit in 32 KiB),
+// nb = 2^hb blocks per set.  Each block leaves lb + 2 points, T, G_0 .. G_(lb-1)
+// and its run total R; with more than two blocks in all, a second kernel sums
+// them per set into lb + 1 + hb points, T, G_0 .. G_(lb-1), Gb_0 .. Gb_(hb-1),
+// and the host forms
+//   set sum = T + seg (sum_j 2^j G_j + 2^lb sum_i 2^i Gb_i).
+// seg grows (up to 32) until the pieces over all sets number at most
+// MSM_REDUCE_PIECES.  Fewer, longer pieces keep the reduction's footprint
+// small (it runs beside the other MSMs' accumulations, whose 512-thread blocks
+// need a whole SM); 8192 measured best for the 2^21-constraint prove (45.7
+// proofs/s against 44.1 with 32768) and equal at 2^17.
+constexpr uint64_t MSM_REDUCE_PIECES = 8192;
+constexpr uint32_t MSM_REDUCE_MAX_SEG = 32;
+
+struct MsmReducePlan {
+    uint32_t sets = 0, B = 0, seg = 1, lb = 7, nb = 1, hb = 0;
+    bool direct = true;   // the host reads the blocks' own points
+    constexpr uint32_t block_terms() const { return lb + 2; }
+    constexpr uint32_t set_terms() const { return direct ? nb * (lb + 2) : lb + 1 + hb; }
+    constexpr size_t block_points() const { return (size_t)sets * nb * (lb + 2); }
+    constexpr size_t result_points() const { return (size_t)sets * set_terms(); }
+};
+
+constexpr MsmReducePlan msm_reduce_plan(uint32_t sets, uint32_t B, bool g2) {
+    MsmReducePlan r;
+    r.sets = sets;
+    r.B = B;
+    r.lb = g2 ? 6 : 7;
+    r.seg = 1;
+    while (r.seg < MSM_REDUCE_MAX_SEG && r.seg < B && (uint64_t)sets * B / r.seg > MSM_REDUCE_PIECES) r.seg *= 2;
+    const uint32_t pieces = B / r.seg;
+    r.nb = (pieces >> r.lb) ? (pieces >> r.lb) : 1;
+    r.hb = 0;
+    while ((1u << r.hb) < r.nb) r.hb++;
+    r.direct = (uint64_t)sets * r.nb <= 2;
+    return r;
+}
 
 struct MsmSort {
     // parameters
@@ -64,7 +107,8 @@ struct MsmAccum {
     void* d_segments = nullptr;    size_t cap_segments = 0;   // bytes
     void* d_windows = nullptr;     size_t cap_windows = 0;    // bytes
     unsigned long long* d_work = nullptr;                      // mixed additions performed
-    uint32_t segs_per_window = 0;
+    MsmReducePlan plan;                                        // shape of d_windows
+    size_t result_bytes(size_t xyzz_bytes) const { return plan.result_points() * xyzz_bytes; }
     void release();
 };
 
@@ -86,20 +130,6 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
 
 // Window count for c-bit signed digits over 255 bits.
 inline int msm_windows(int c) { return (255 + c - 1) / c; }
-// Buckets per running-sum segment (1..8) when bucket_sets sets of
-// buckets_per_set buckets are reduced.  A segment thread runs 2 seg additions
-// and a double-and-add of ~1.5 log2(buckets) operations, so short segments
-// shorten the dependent chain but multiply the total work.  Reductions of up
-// to 2048 buckets (small proofs, latency-bound) get one segment thread per
-// bucket; from 16384 buckets on, segments of 8 keep the work near 5 additions
-// per bucket.
-constexpr uint32_t msm_segment_len(uint64_t bucket_sets, uint64_t buckets_per_set) {
-    uint32_t seg = 1;
-    while (seg < 8 && bucket_sets * buckets_per_set / seg > 2048) seg *= 2;
-    return seg;
-}
-// Group-sum blocks per bucket set for P segments per set.
-constexpr uint64_t msm_group_blocks(uint64_t segs_per_set) { return (segs_per_set + 511) / 512; }
 // Window width for window-shifted bases: the cost is ~m * ceil(255/c) mixed
 // additions plus a single bucket reduction over 2^(c-1) buckets.
 int msm_shared_window_bits(size_t m);
@@ -123,9 +153,11 @@ cudaError_t msm_accumulate_g1(const MsmSort& s, MsmAccum& acc, const void* d_bas
 cudaError_t msm_accumulate_g2(const MsmSort& s, MsmAccum& acc, const void* d_bases, uint32_t base_offset,
                               uint32_t n_bases, cudaStream_t st);
 
-// Host side: W XYZZ window sums (as copied back) -> Horner -> Jacobian.
-G1J msm_combine_g1(const uint8_t* windows_xyzz, int W, int c);
-G2J msm_combine_g2(const uint8_t* windows_xyzz, int W, int c);
+// Host side: the reduction's points (acc.d_windows as copied back, laid out by
+// plan) -> each set's sum -> Horner over the sets with c doublings between
+// them -> Jacobian.
+G1J msm_combine_g1(const uint8_t* result_xyzz, const MsmReducePlan& plan, int c);
+G2J msm_combine_g2(const uint8_t* result_xyzz, const MsmReducePlan& plan, int c);
 
 constexpr size_t XYZZ_G1_BYTES = 128;
 constexpr size_t XYZZ_G2_BYTES = 256;

@@ -43,8 +43,7 @@ constexpr int NOALLOC_W = (255 + NOALLOC_C - 1) / NOALLOC_C;      // 24 windows
 constexpr size_t NOALLOC_B = (size_t)1 << (NOALLOC_C - 1);        // 1024 buckets per window
 constexpr size_t NOALLOC_K = NOALLOC_W * NOALLOC_B;               // 24576 buckets in all
 constexpr size_t NOALLOC_CHUNK = 16;                              // entries per accumulate thread
-constexpr size_t NOALLOC_SEGS = NOALLOC_B / g16::msm_segment_len(NOALLOC_W, NOALLOC_B);   // segments per window
-constexpr size_t NOALLOC_GROUPS = g16::msm_group_blocks(NOALLOC_SEGS);                      // per window
+constexpr g16::MsmReducePlan NOALLOC_PLAN = g16::msm_reduce_plan(NOALLOC_W, NOALLOC_B, false);
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -67,9 +66,9 @@ constexpr size_t PARTIALS_BYTES =
 constexpr size_t OFF_BUCKETS = align256(OFF_PARTIALS + PARTIALS_BYTES);
 constexpr size_t BUCKETS_BYTES = g16::XYZZ_G1_BYTES * NOALLOC_K;
 constexpr size_t OFF_SEGMENTS = align256(OFF_BUCKETS + BUCKETS_BYTES);
-constexpr size_t SEGMENTS_BYTES = g16::XYZZ_G1_BYTES * (NOALLOC_W * NOALLOC_SEGS + NOALLOC_W * NOALLOC_GROUPS);
+constexpr size_t SEGMENTS_BYTES = g16::XYZZ_G1_BYTES * NOALLOC_PLAN.block_points();
 constexpr size_t OFF_WINDOWS = align256(OFF_SEGMENTS + SEGMENTS_BYTES);
-constexpr size_t WINDOWS_BYTES = g16::XYZZ_G1_BYTES * NOALLOC_W;
+constexpr size_t WINDOWS_BYTES = g16::XYZZ_G1_BYTES * NOALLOC_PLAN.result_points();
 constexpr size_t OFF_WORK = align256(OFF_WINDOWS + WINDOWS_BYTES);
 constexpr size_t NOALLOC_SCRATCH_BYTES = align256(OFF_WORK + 8);
 
@@ -157,7 +156,10 @@ extern "C" int g16_msm_g1_device_noalloc(int device, const void* d_bases, const 
     cudaStream_t st = 0;   // the legacy default stream: no stream is created
     e = g16::msm_sort(s, d_scalars, n, scalars_form == G16_SCALARS_MONTGOMERY, NOALLOC_C, st);
     if (e == cudaSuccess) e = g16::msm_accumulate_g1(s, acc, d_bases, 0, (uint32_t)n, st);
-    uint8_t windows[g16::XYZZ_G1_BYTES * NOALLOC_W];
+    static_assert(WINDOWS_BYTES <= 64 * 1024, "the reduction's result is read into a stack buffer");
+    uint8_t windows[WINDOWS_BYTES];
+    const g16::MsmReducePlan plan = acc.plan;
+    if (e == cudaSuccess && acc.result_bytes(g16::XYZZ_G1_BYTES) != WINDOWS_BYTES) e = cudaErrorInvalidValue;
     if (e == cudaSuccess) e = cudaMemcpy(windows, acc.d_windows, sizeof windows, cudaMemcpyDeviceToHost);
     // the views must not free the library's array
     s = g16::MsmSort();
@@ -166,6 +168,6 @@ extern "C" int g16_msm_g1_device_noalloc(int device, const void* d_bases, const 
         g16::set_error("g16_msm_g1_device_noalloc: %s", cudaGetErrorString(e));
         return e == cudaErrorMemoryAllocation ? G16_ERR_DEVICE_MEMORY : G16_ERR_DEVICE;
     }
-    g16::pack(out64, g16::msm_combine_g1(windows, NOALLOC_W, NOALLOC_C).to_affine());
+    g16::pack(out64, g16::msm_combine_g1(windows, plan, NOALLOC_C).to_affine());
     return G16_OK;
 }

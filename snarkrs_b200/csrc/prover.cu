@@ -562,7 +562,8 @@ int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
     const int stream_of[4] = {0, 3, 1, 2};   // acc slot -> stream
     for (int i = 0; i < 4; i++) {
         cudaStream_t s_i = st[stream_of[i]];
-        size_t bytes = i == 1 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES;   // one shared window per MSM
+        const size_t bytes = ws->acc[i].result_bytes(i == 1 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES);
+        if (bytes > WIN_SLOT) return fail(G16_ERR_BACKEND, "MSM result of %zu bytes exceeds its slot", bytes);
         CK(cudaMemcpyAsync(ws->h_win + i * WIN_SLOT, ws->acc[i].d_windows, bytes, cudaMemcpyDeviceToHost, s_i),
            "window readback");
         if (timer().enabled)
@@ -577,7 +578,9 @@ int enqueue_h_msm(g16_circuit* c, Workspace* ws, const void* d_h) {
     const uint32_t nh = c->n * (uint32_t)msm_windows(c->c_h);
     CK(msm_sort(ws->sort_h, d_h, c->n, true, c->c_h, st, true, c->be->constant_work), "H sort");
     CK(msm_accumulate_g1(ws->sort_h, ws->acc[4], c->t_h, 0, nh, st), "H accumulate");
-    CK(cudaMemcpyAsync(ws->h_win + 4 * WIN_SLOT, ws->acc[4].d_windows, XYZZ_G1_BYTES, cudaMemcpyDeviceToHost, st),
+    const size_t bytes = ws->acc[4].result_bytes(XYZZ_G1_BYTES);
+    if (bytes > WIN_SLOT) return fail(G16_ERR_BACKEND, "MSM result of %zu bytes exceeds its slot", bytes);
+    CK(cudaMemcpyAsync(ws->h_win + 4 * WIN_SLOT, ws->acc[4].d_windows, bytes, cudaMemcpyDeviceToHost, st),
        "window readback");
     if (timer().enabled)
         CK(cudaMemcpyAsync(ws->h_work + 4, ws->acc[4].d_work, 8, cudaMemcpyDeviceToHost, st), "work readback");
@@ -595,18 +598,19 @@ int collect_msms(g16_circuit* c, Workspace* ws, MsmJac& out) {
     timer().collect();
     {
         std::lock_guard<std::mutex> g(c->mu);
-        c->readback_bytes = 3 * XYZZ_G1_BYTES + XYZZ_G2_BYTES + XYZZ_G1_BYTES;
+        c->readback_bytes = 0;
+        for (int i = 0; i < 5; i++) c->readback_bytes += ws->acc[i].result_bytes(i == 1 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES);
     }
     if (timer().enabled) {
         timer().add_units("msm_accumulate_g1",
                           (double)(ws->h_work[0] + ws->h_work[2] + ws->h_work[3] + ws->h_work[4]));
         timer().add_units("msm_accumulate_g2", (double)ws->h_work[1]);
     }
-    out.a = msm_combine_g1(ws->h_win + 0 * WIN_SLOT, 1, c->c_w);
-    out.b2 = msm_combine_g2(ws->h_win + 1 * WIN_SLOT, 1, c->c_w);
-    out.b1 = msm_combine_g1(ws->h_win + 2 * WIN_SLOT, 1, c->c_w);
-    out.l = msm_combine_g1(ws->h_win + 3 * WIN_SLOT, 1, c->c_w);
-    out.h = msm_combine_g1(ws->h_win + 4 * WIN_SLOT, 1, c->c_h);
+    out.a = msm_combine_g1(ws->h_win + 0 * WIN_SLOT, ws->acc[0].plan, c->c_w);
+    out.b2 = msm_combine_g2(ws->h_win + 1 * WIN_SLOT, ws->acc[1].plan, c->c_w);
+    out.b1 = msm_combine_g1(ws->h_win + 2 * WIN_SLOT, ws->acc[2].plan, c->c_w);
+    out.l = msm_combine_g1(ws->h_win + 3 * WIN_SLOT, ws->acc[3].plan, c->c_w);
+    out.h = msm_combine_g1(ws->h_win + 4 * WIN_SLOT, ws->acc[4].plan, c->c_h);
     return G16_OK;
 }
 
@@ -1468,12 +1472,13 @@ static int msm_device_impl(g16_backend* b, const void* d_bases, const void* d_sc
     CK(msm_sort(b->sort, d_scalars, n, form == G16_SCALARS_MONTGOMERY, 0, st, false, b->constant_work), "MSM sort");
     if (g2) CK(msm_accumulate_g2(b->sort, b->acc, d_bases, 0, (uint32_t)n, st), "MSM accumulate");
     else CK(msm_accumulate_g1(b->sort, b->acc, d_bases, 0, (uint32_t)n, st), "MSM accumulate");
-    size_t bytes = (size_t)b->sort.W * (g2 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES);
+    const size_t bytes = b->acc.result_bytes(g2 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES);
     if (bytes > b->cap_pinned) {
         cudaFreeHost(b->h_pinned);
         b->h_pinned = nullptr;
-        CK(cudaMallocHost((void**)&b->h_pinned, 32 * 256), "pinned buffer");
-        b->cap_pinned = 32 * 256;
+        b->cap_pinned = 0;
+        CK(cudaMallocHost((void**)&b->h_pinned, bytes), "pinned buffer");
+        b->cap_pinned = bytes;
     }
     CK(cudaMemcpyAsync(b->h_pinned, b->acc.d_windows, bytes, cudaMemcpyDeviceToHost, st), "window readback");
     if (timer().enabled) {
@@ -1489,8 +1494,8 @@ static int msm_device_impl(g16_backend* b, const void* d_bases, const void* d_sc
         timer().add_units(g2 ? "msm_accumulate_g2" : "msm_accumulate_g1", (double)b->h_work[0]);
         timer().add_bytes("msm_scatter", 32.0 * n + 4.0 * (double)b->h_work[1]);   // scalars in, entries out
     }
-    if (g2) pack(out, msm_combine_g2(b->h_pinned, b->sort.W, b->sort.c).to_affine());
-    else pack(out, msm_combine_g1(b->h_pinned, b->sort.W, b->sort.c).to_affine());
+    if (g2) pack(out, msm_combine_g2(b->h_pinned, b->acc.plan, b->sort.c).to_affine());
+    else pack(out, msm_combine_g1(b->h_pinned, b->acc.plan, b->sort.c).to_affine());
     return G16_OK;
 }
 
