@@ -39,7 +39,13 @@ N_CONSTRAINTS = 1_100_000
 N_INPUTS, N_PUBLIC = 256, 16
 CIRCUIT_SEED, TOXIC_SEED = 21, 0x5EED
 FQ_MUL_IMAD = 264            # 8x32-bit CIOS Montgomery product: 32-bit multiply-adds
-MADD_FQ_MULS = {"msm_accumulate_g1": 10, "msm_accumulate_g2": 30}   # madd-2008-s: 8M + 2S (Fq2 = 3 Fq)
+FQ_SQR_IMAD = 208            # separated squaring: 36 limb products + 8 x 17 for the reduction
+# 32-bit multiply-adds per mixed addition (madd-2008-s, 8M + 2S): G1 squares with
+# the separated squaring; an Fq2 product is 3 Fq products and an Fq2 square 2
+MADD_IMAD = {"msm_accumulate_g1": 8 * FQ_MUL_IMAD + 2 * FQ_SQR_IMAD,
+             "msm_accumulate_g2": (8 * 3 + 2 * 2) * FQ_MUL_IMAD}
+MADD_WORK = {"msm_accumulate_g1": "8 Fq products x 264 + 2 Fq squares x 208 IMAD",
+             "msm_accumulate_g2": "28 Fq products x 264 IMAD"}
 
 
 def parse():
@@ -350,20 +356,20 @@ def run_ours(args):
     name, (tot_ms, n_launch, units) = dom[0], dom[1]
     roof = {"kernel": name, "launches": n_launch, "avg_ms": tot_ms / max(n_launch, 1),
             "measured_over": "serialized replay of the %d timed proofs (CUDA events per launch)" % K}
-    if name in MADD_FQ_MULS:
-        imad_per_launch = units / max(n_launch, 1) * MADD_FQ_MULS[name] * FQ_MUL_IMAD
+    if name in MADD_IMAD:
+        imad_per_launch = units / max(n_launch, 1) * MADD_IMAD[name]
         achieved = imad_per_launch / (roof["avg_ms"] / 1e3)
         roof.update({"bound": "imad", "achieved": achieved / 1e12, "peak": imad_peak / 1e12, "unit": "TIMAD/s",
                      "frac": achieved / imad_peak, "peak_source": "measured in this run by the mad.lo/mad.hi "
                                                                     "issue-rate probe (g16_imad_peak)",
-                     "work_per_launch": "%.0f mixed additions x %d Fq products x %d IMAD" % (
-                         units / max(n_launch, 1), MADD_FQ_MULS[name], FQ_MUL_IMAD)})
+                     "work_per_launch": "%.0f mixed additions x (%s)" % (
+                         units / max(n_launch, 1), MADD_WORK[name])})
     roof["traffic"] = traffic_for("prove-%d" % args.constraints, name)
     # whole-proof integer work: MSM mixed additions (measured counters) + the NTT chain
     n_dom = sc.domain_size
     log_n = n_dom.bit_length() - 1
     ntt_muls = 6 * (n_dom // 2) * log_n + 3 * n_dom + 2 * n_dom
-    msm_imad = sum(kern.get(k, (0, 0, 0))[2] * MADD_FQ_MULS[k] * FQ_MUL_IMAD for k in MADD_FQ_MULS) / K
+    msm_imad = sum(kern.get(k, (0, 0, 0))[2] * MADD_IMAD[k] for k in MADD_IMAD) / K
     proof_imad = msm_imad + ntt_muls * FQ_MUL_IMAD
     whole = {"imad_per_proof": proof_imad, "achieved_timad_s": proof_imad / (ms / K / 1e3) / 1e12,
              "frac_of_peak": proof_imad / (ms / K / 1e3) / imad_peak,
@@ -455,8 +461,8 @@ def kernel_rooflines(kern, kbytes, imad_peak, hbm_peak):
             continue
         row = {}
         imad = None
-        if name in MADD_FQ_MULS:
-            imad = units * MADD_FQ_MULS[name] * FQ_MUL_IMAD
+        if name in MADD_IMAD:
+            imad = units * MADD_IMAD[name]
         elif name in NTT_KERNELS:
             imad = units * FQ_MUL_IMAD
         if imad:

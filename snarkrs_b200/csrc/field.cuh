@@ -282,9 +282,75 @@ __device__ __forceinline__ Fp<Params> mul(const Fp<Params>& a, const Fp<Params>&
     return r;
 }
 
+// a^2 R^-1 mod p, left in [0, 2p) in r[0..7] (separated operand scanning):
+// the 28 cross products a_i a_j (i < j) once, doubled by a one-bit shift, plus
+// the 8 squares a_i^2, then a Montgomery reduction of the 16-limb square.  36
+// limb products and 64 for the reduction against CIOS's 128: the same REDC
+// value (a^2 + M p) / R, M being the unique multiple in [0, R), so the result
+// is identical to mul(a, a).  Host-callable for the unit check of the limbs.
+template <class Params>
+__host__ __device__ __forceinline__ void sqr_redc(const uint32_t* a, uint32_t* r) {
+    uint32_t t[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) t[k] = 0;
+    // cross products: row i adds a_i a_j (j > i) at limb i + j; t[i + 8] is untouched before row i
+#pragma unroll
+    for (int i = 0; i < 7; i++) {
+        uint64_t c = 0;
+#pragma unroll
+        for (int j = i + 1; j < 8; j++) {
+            uint64_t p = (uint64_t)a[i] * a[j] + t[i + j] + c;
+            t[i + j] = (uint32_t)p;
+            c = p >> 32;
+        }
+        t[i + 8] = (uint32_t)c;
+    }
+    // double (the cross sum is below 2^511, so the shift loses nothing)
+    t[15] = t[14] >> 31;
+#pragma unroll
+    for (int k = 14; k >= 1; k--) t[k] = (t[k] << 1) | (t[k - 1] >> 31);
+    // t[0] is zero: no cross product lands on limb 0
+    // add the squares a_i^2 at limbs 2i, 2i + 1
+    {
+        uint64_t c = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            uint64_t q = (uint64_t)a[i] * a[i];
+            uint64_t s0 = (uint64_t)t[2 * i] + (uint32_t)q + c;
+            t[2 * i] = (uint32_t)s0;
+            uint64_t s1 = (uint64_t)t[2 * i + 1] + (q >> 32) + (s0 >> 32);
+            t[2 * i + 1] = (uint32_t)s1;
+            c = s1 >> 32;
+        }
+    }
+    // reduction: row i adds m p 2^(32 i), m = t[i] (-p^-1) mod 2^32, which
+    // zeroes limb i; the carry out of limb i + 8 rides into the next row
+    uint32_t extra = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        uint32_t m = t[i] * Params::N0;
+        uint64_t c = ((uint64_t)m * Params::P(0) + t[i]) >> 32;
+#pragma unroll
+        for (int j = 1; j < 8; j++) {
+            uint64_t p = (uint64_t)m * Params::P(j) + t[i + j] + c;
+            t[i + j] = (uint32_t)p;
+            c = p >> 32;
+        }
+        uint64_t s = (uint64_t)t[i + 8] + c + extra;
+        t[i + 8] = (uint32_t)s;
+        extra = (uint32_t)(s >> 32);
+    }
+    // (a^2 + M p) / R < 2p < 2^255: extra is zero here
+#pragma unroll
+    for (int k = 0; k < 8; k++) r[k] = t[k + 8];
+}
+
 template <class Params>
 __device__ __forceinline__ Fp<Params> sqr(const Fp<Params>& a) {
-    return mul(a, a);
+    Fp<Params> r;
+    sqr_redc<Params>(a.v, r.v);
+    reduce_once<Params>(r.v);
+    return r;
 }
 
 // Montgomery -> standard form: a * 1 * R^-1
@@ -342,7 +408,8 @@ __device__ __forceinline__ Fp<Params> fmul(const Fp<Params>& a, const Fp<Params>
 }
 template <bool INL, class Params>
 __device__ __forceinline__ Fp<Params> fsqr(const Fp<Params>& a) {
-    return fmul<INL>(a, a);
+    if constexpr (INL) return sqr(a);
+    else return mul_ool(a, a);
 }
 
 // Out-of-line copies that hold several independent products.  A warp issues

@@ -428,18 +428,25 @@ __global__ void __launch_bounds__(1 << LB) k_reduce_pieces(const uint4* __restri
     const uint32_t t = threadIdx.x, set = blockIdx.y;
     const uint32_t p = blockIdx.x * N + t;
     const bool weighted = seg > 1;   // uniform: tot differs from run
+    // G2: tot waits in shared memory while run is added, so that the two
+    // 64-register points and the addition's operands fit without spilling
+    constexpr bool TOT_SHARED = sizeof(F) > sizeof(g16d::Fq);
     Xyzz<F> run = Xyzz<F>::identity(), tot = Xyzz<F>::identity();
+    if (TOT_SHARED && weighted) st_xyzz<F>(s_tot, t, tot);
     if ((size_t)p * seg < B) {
         const size_t g0 = (size_t)set * B + (size_t)p * seg;
 #pragma unroll 1
         for (int i = (int)seg - 1; i >= 0; i--) {
             run = xyzz_add<F, false>(run, ld_xyzz<F>(buckets, g0 + i));
-            if (weighted) tot = xyzz_add<F, false>(tot, run);
+            if (weighted) {
+                if constexpr (TOT_SHARED) st_xyzz<F>(s_tot, t, xyzz_add<F, false>(ld_xyzz<F>(s_tot, t), run));
+                else tot = xyzz_add<F, false>(tot, run);
+            }
         }
     }
     // run stays equal to slot t of s_run: thread t is the only writer of slot t
     st_xyzz<F>(s_run, t, run);
-    if (weighted) st_xyzz<F>(s_tot, t, tot);
+    if (!TOT_SHARED && weighted) st_xyzz<F>(s_tot, t, tot);
     const uint32_t lg = t ? 31 - __clz(t) : 0;   // slot t lies in the upper half [2^lg, 2^(lg+1))
 #pragma unroll 1
     for (uint32_t k = 1; k <= (uint32_t)LB; k++) {
