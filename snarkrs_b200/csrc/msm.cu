@@ -4,6 +4,7 @@
 #include "common.cuh"
 #include "curve.cuh"
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 namespace g16d {
@@ -186,24 +187,37 @@ __device__ __forceinline__ uint32_t fat_job_len(uint32_t ns) {
 // and about M / (4 K) or more, so that an average bucket gets at most ~4
 // partial sums and only skewed buckets (a repeated scalar such as 1) take the
 // fat-bucket path.  Sparse scalars (witnesses of zeros and ones) still spread
-// over the whole GPU.
+// over the whole GPU.  Last, the chunks are fitted to whole waves of `wave`
+// threads (one 512-thread G1 block per SM) when that saves 5% or more: a
+// launch takes about (waves x L) additions per thread, so 2.4 waves of 16
+// entries lose to 2 waves of 20 (a sparse witness MSM of the 2^21 prove).
 constexpr uint32_t ACC_THREADS = 1u << 19;
 
-__device__ __forceinline__ uint32_t chunk_len(uint32_t M, uint32_t K, uint32_t L_min) {
+__device__ __forceinline__ uint32_t chunk_len(uint32_t M, uint32_t K, uint32_t L_min, uint32_t wave) {
     uint32_t L = (uint32_t)(((uint64_t)M + ACC_THREADS - 1) / ACC_THREADS);
     uint32_t per_bucket = (uint32_t)(((uint64_t)M + 4ull * K - 1) / (4ull * K));
     if (per_bucket > L) L = per_bucket;
-    return L > L_min ? L : L_min;
+    if (L < L_min) L = L_min;
+    if (wave && M) {
+        const uint64_t chunks = ((uint64_t)M + L - 1) / L;
+        const uint64_t waves = (chunks + wave - 1) / wave;
+        if (waves > 1) {
+            const uint64_t L2 = ((uint64_t)M + (waves - 1) * wave - 1) / ((waves - 1) * wave);
+            // only for a clear gain: block times vary, and more, shorter waves balance better
+            if (20 * (waves - 1) * L2 < 19 * waves * L) L = (uint32_t)L2;
+        }
+    }
+    return L;
 }
 
 // partials per bucket for the Ks sorted buckets; only the K real ones can be
 // fat (the constant-work sink bucket K is accumulated but never reduced).
 // Also stores the chunk length L in total[3] for the kernels that follow.
-__global__ void k_nseg(const uint32_t* __restrict__ offsets, uint32_t Ks, uint32_t K, uint32_t L_min,
+__global__ void k_nseg(const uint32_t* __restrict__ offsets, uint32_t Ks, uint32_t K, uint32_t L_min, uint32_t wave,
                        uint32_t* __restrict__ nseg, uint32_t* __restrict__ fat_list, uint32_t* __restrict__ fat_count,
                        uint32_t* __restrict__ total) {
     uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t L = chunk_len(total[0], K, L_min);
+    const uint32_t L = chunk_len(total[0], K, L_min, wave);
     if (g == 0) total[3] = L;
     if (g >= Ks) return;
     uint32_t lo = offsets[g], hi = offsets[g + 1];
@@ -216,6 +230,10 @@ __global__ void k_copy_u32(uint32_t* dst, const uint32_t* src, uint32_t n) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = src[i];
 }
+
+// a partial sum as stored: G1 accumulators run below 2p, stored below p
+__device__ __forceinline__ Xyzz<Fq> stored(const Xyzz<Fq>& a) { return canonical_point(a); }
+__device__ __forceinline__ Xyzz<Fq2> stored(const Xyzz<Fq2>& a) { return a; }
 
 // ---- accumulate: one thread per chunk of L sorted entries ----
 // LOCKSTEP: a block-wide barrier after every entry keeps the block's warps on
@@ -252,7 +270,7 @@ __device__ __forceinline__ void accumulate_chunks(const uint32_t* __restrict__ e
     for (size_t k = start; k < stop; k++) {
         if (!LOCKSTEP || k < end) {
             if (k == next) {
-                st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), acc);
+                st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), stored(acc));
                 acc = Xyzz<F>::identity();
                 do {
                     g++;
@@ -265,17 +283,19 @@ __device__ __forceinline__ void accumulate_chunks(const uint32_t* __restrict__ e
                 Affine<F> p = ld_affine<F>(bases, idx - base_offset);
                 if (!p.is_inf()) {
                     if (e >> 31) p.y = neg(p.y);
-                    // G1 keeps its products inlined; the Fq2 body is large enough
-                    // that one out-of-line Fq2 product (three Fq chains) runs
-                    // faster than inlined code that misses the instruction cache
-                    acc = xyzz_add_affine<F, !std::is_same<F, Fq2>::value>(acc, p.x, p.y);
+                    // G1 keeps its products inlined, with coordinates below 2p
+                    // between entries; the Fq2 body is large enough that one
+                    // out-of-line Fq2 product (three Fq chains) runs faster
+                    // than inlined code that misses the instruction cache
+                    if constexpr (std::is_same<F, Fq2>::value) acc = xyzz_add_affine<F, false>(acc, p.x, p.y);
+                    else acc = xyzz_add_affine_nr<F>(acc, p.x, p.y);
                     adds++;
                 }
             }
         }
         if (LOCKSTEP) __syncthreads();
     }
-    if (active) st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), acc);
+    if (active) st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), stored(acc));
     // mixed additions performed, one atomic per warp (every lane reaches here in lockstep mode)
     unsigned mask = __activemask();
     unsigned total = __reduce_add_sync(mask, adds);
@@ -284,6 +304,22 @@ __device__ __forceinline__ void accumulate_chunks(const uint32_t* __restrict__ e
 
 constexpr int ACC_BLOCK_G1 = 512;   // lockstep block: 16 warps, one block per SM (<= 128 registers)
 constexpr int ACC_BLOCK_G2 = 128;
+
+// Threads in one wave of G1 accumulate blocks on the current device (one
+// block per SM), for chunk_len; 0 (no fitting) if the device cannot be read.
+static uint32_t accumulate_wave() {
+    static std::atomic<uint32_t> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    uint32_t w = cache[dev].load(std::memory_order_relaxed);
+    if (!w) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) return 0;
+        w = (uint32_t)sms * ACC_BLOCK_G1;
+        cache[dev].store(w, std::memory_order_relaxed);
+    }
+    return w;
+}
 
 __global__ void __launch_bounds__(ACC_BLOCK_G1, 1) k_accumulate_g1(const uint32_t* __restrict__ entries,
                                                                    const uint32_t* __restrict__ offsets,
@@ -842,8 +878,8 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
     // per-bucket segment counts -> segment base (into counts, then scanned)
     {
         TimedLaunch tl("msm_nseg", st);
-        k_nseg<<<blocks_for(s.Ks, 256), 256, 0, st>>>(s.d_offsets, s.Ks, s.K, s.chunk, s.d_counts, s.d_fat_list,
-                                                       s.d_total + 2, s.d_total);
+        k_nseg<<<blocks_for(s.Ks, 256), 256, 0, st>>>(s.d_offsets, s.Ks, s.K, s.chunk, accumulate_wave(),
+                                                       s.d_counts, s.d_fat_list, s.d_total + 2, s.d_total);
     }
     G16_CUDA(scan(s.d_counts, s.d_seg_base, s.Ks, s.d_scan_tmp, s.d_total + 1, st));
     return cudaSuccess;
