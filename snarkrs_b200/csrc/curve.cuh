@@ -134,45 +134,6 @@ __device__ __forceinline__ Xyzz<F> xyzz_add_affine(const Xyzz<F>& p, const F& x2
     return r;
 }
 
-// The same mixed addition with p's coordinates kept below 2p (the *_nr field
-// operations: no final subtraction after a product), the affine point below
-// p.  Every value stays congruent to the one xyzz_add_affine computes and the
-// exceptional cases test zero mod p, so the point is the same once its
-// coordinates are brought below p (canonical_point).  The G1 accumulate's
-// inner loop, which saves the final subtraction of ten products per entry.
-template <class F>
-__device__ __forceinline__ Xyzz<F> xyzz_add_affine_nr(const Xyzz<F>& p, const F& x2, const F& y2) {
-    if (p.is_inf()) {   // zz is literally 0 only for the identity: a nonzero product is never p
-        Xyzz<F> r;
-        r.x = x2;
-        r.y = y2;
-        r.zz = F::one();
-        r.zzz = F::one();
-        return r;
-    }
-    F u2 = mul_nr(x2, p.zz), s2 = mul_nr(y2, p.zzz);
-    F pp_ = sub_nr(u2, p.x);
-    F rr = sub_nr(s2, p.y);
-    if (is_zero_nr(pp_)) {
-        if (is_zero_nr(rr)) return xyzz_dbl_affine_ool<F>(x2, y2);
-        return Xyzz<F>::identity();
-    }
-    Xyzz<F> r;
-    F pp = sqr_nr(pp_);
-    F ppp = mul_nr(pp_, pp);
-    F q = mul_nr(p.x, pp);
-    r.x = sub_nr(sub_nr(sqr_nr(rr), ppp), add_nr(q, q));
-    r.y = sub_nr(mul_nr(rr, sub_nr(q, r.x)), mul_nr(p.y, ppp));
-    r.zz = mul_nr(p.zz, pp);
-    r.zzz = mul_nr(p.zzz, ppp);
-    return r;
-}
-
-template <class F>
-__device__ __forceinline__ Xyzz<F> canonical_point(const Xyzz<F>& a) {
-    return {canonical(a.x), canonical(a.y), canonical(a.zz), canonical(a.zzz)};
-}
-
 // p + q (add-2008-s)
 template <class F, bool INL = true>
 __device__ __forceinline__ Xyzz<F> xyzz_add(const Xyzz<F>& p, const Xyzz<F>& q) {

@@ -244,11 +244,9 @@ __device__ __forceinline__ Fp<Params> mul_cc(const Fp<Params>& a, const Fp<Param
     return r;
 }
 
-// CIOS with 64-bit sums: t[j] + a[j] b[i] + carry < 2^64 always holds.
-// mul_nr leaves a b R^-1 in [0, 2p) without the final conditional
-// subtraction; inputs below 2p are allowed (a b < 4p^2 < R p since 4p < R).
+// CIOS with 64-bit sums: t[j] + a[j] b[i] + carry < 2^64 always holds
 template <class Params>
-__device__ __forceinline__ Fp<Params> mul_nr(const Fp<Params>& a, const Fp<Params>& b) {
+__device__ __forceinline__ Fp<Params> mul(const Fp<Params>& a, const Fp<Params>& b) {
     uint32_t t[10];
 #pragma unroll
     for (int i = 0; i < 10; i++) t[i] = 0;
@@ -277,16 +275,10 @@ __device__ __forceinline__ Fp<Params> mul_nr(const Fp<Params>& a, const Fp<Param
         t[7] = (uint32_t)s;
         t[8] = t[9] + (uint32_t)(s >> 32);
     }
+    reduce_once<Params>(t);
     Fp<Params> r;
 #pragma unroll
     for (int i = 0; i < 8; i++) r.v[i] = t[i];
-    return r;
-}
-
-template <class Params>
-__device__ __forceinline__ Fp<Params> mul(const Fp<Params>& a, const Fp<Params>& b) {
-    Fp<Params> r = mul_nr(a, b);
-    reduce_once<Params>(r.v);
     return r;
 }
 
@@ -358,111 +350,6 @@ __device__ __forceinline__ Fp<Params> sqr(const Fp<Params>& a) {
     Fp<Params> r;
     sqr_redc<Params>(a.v, r.v);
     reduce_once<Params>(r.v);
-    return r;
-}
-
-// ---- values kept in [0, 2p) ("lazy"): the G1 accumulate's register chain ----
-// Products take and give values below 2p (no final subtraction); sums and
-// differences are kept below 2p by subtracting or adding 2p.  A value is
-// zero mod p when it is 0 or p.  canonical() brings it back below p.
-template <class Params>
-__host__ __device__ constexpr uint32_t two_p(int i) {
-    return (Params::P(i) << 1) | (i ? Params::P(i - 1) >> 31 : 0u);
-}
-
-template <class Params>
-__device__ __forceinline__ Fp<Params> sqr_nr(const Fp<Params>& a) {
-    Fp<Params> r;
-    sqr_redc<Params>(a.v, r.v);
-    return r;
-}
-
-template <class Params>
-__device__ __forceinline__ Fp<Params> canonical(const Fp<Params>& a) {
-    Fp<Params> r = a;
-    reduce_once<Params>(r.v);
-    return r;
-}
-
-template <class Params>
-__device__ __forceinline__ bool is_zero_nr(const Fp<Params>& a) {
-    bool z = true, e = true;
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-        z &= a.v[i] == 0;
-        e &= a.v[i] == Params::P(i);
-    }
-    return z || e;
-}
-
-// a - b, both below 2p: adds 2p when the subtraction borrows
-template <class Params>
-__device__ __forceinline__ Fp<Params> sub_nr(const Fp<Params>& a, const Fp<Params>& b) {
-    Fp<Params> r;
-    uint32_t borrow;
-    asm("sub.cc.u32  %0, %9, %17;\n\t"
-        "subc.cc.u32 %1, %10, %18;\n\t"
-        "subc.cc.u32 %2, %11, %19;\n\t"
-        "subc.cc.u32 %3, %12, %20;\n\t"
-        "subc.cc.u32 %4, %13, %21;\n\t"
-        "subc.cc.u32 %5, %14, %22;\n\t"
-        "subc.cc.u32 %6, %15, %23;\n\t"
-        "subc.cc.u32 %7, %16, %24;\n\t"
-        "subc.u32    %8, 0, 0;"
-        : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
-          "=r"(r.v[7]), "=r"(borrow)
-        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
-          "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
-    uint32_t m = borrow;
-    asm("add.cc.u32  %0, %0, %8;\n\t"
-        "addc.cc.u32 %1, %1, %9;\n\t"
-        "addc.cc.u32 %2, %2, %10;\n\t"
-        "addc.cc.u32 %3, %3, %11;\n\t"
-        "addc.cc.u32 %4, %4, %12;\n\t"
-        "addc.cc.u32 %5, %5, %13;\n\t"
-        "addc.cc.u32 %6, %6, %14;\n\t"
-        "addc.u32    %7, %7, %15;"
-        : "+r"(r.v[0]), "+r"(r.v[1]), "+r"(r.v[2]), "+r"(r.v[3]), "+r"(r.v[4]), "+r"(r.v[5]), "+r"(r.v[6]),
-          "+r"(r.v[7])
-        : "r"(two_p<Params>(0) & m), "r"(two_p<Params>(1) & m), "r"(two_p<Params>(2) & m),
-          "r"(two_p<Params>(3) & m), "r"(two_p<Params>(4) & m), "r"(two_p<Params>(5) & m),
-          "r"(two_p<Params>(6) & m), "r"(two_p<Params>(7) & m));
-    return r;
-}
-
-// a + b, both below 2p (the sum is below 4p < 2^256): subtracts 2p when the sum reaches it
-template <class Params>
-__device__ __forceinline__ Fp<Params> add_nr(const Fp<Params>& a, const Fp<Params>& b) {
-    Fp<Params> r;
-    asm("add.cc.u32  %0, %8, %16;\n\t"
-        "addc.cc.u32 %1, %9, %17;\n\t"
-        "addc.cc.u32 %2, %10, %18;\n\t"
-        "addc.cc.u32 %3, %11, %19;\n\t"
-        "addc.cc.u32 %4, %12, %20;\n\t"
-        "addc.cc.u32 %5, %13, %21;\n\t"
-        "addc.cc.u32 %6, %14, %22;\n\t"
-        "addc.u32    %7, %15, %23;"
-        : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
-          "=r"(r.v[7])
-        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
-          "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
-    uint32_t d[8], borrow;
-    asm("sub.cc.u32  %0, %9, %17;\n\t"
-        "subc.cc.u32 %1, %10, %18;\n\t"
-        "subc.cc.u32 %2, %11, %19;\n\t"
-        "subc.cc.u32 %3, %12, %20;\n\t"
-        "subc.cc.u32 %4, %13, %21;\n\t"
-        "subc.cc.u32 %5, %14, %22;\n\t"
-        "subc.cc.u32 %6, %15, %23;\n\t"
-        "subc.cc.u32 %7, %16, %24;\n\t"
-        "subc.u32    %8, 0, 0;"
-        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
-          "=r"(borrow)
-        : "r"(r.v[0]), "r"(r.v[1]), "r"(r.v[2]), "r"(r.v[3]), "r"(r.v[4]), "r"(r.v[5]), "r"(r.v[6]), "r"(r.v[7]),
-          "n"(two_p<Params>(0)), "n"(two_p<Params>(1)), "n"(two_p<Params>(2)), "n"(two_p<Params>(3)),
-          "n"(two_p<Params>(4)), "n"(two_p<Params>(5)), "n"(two_p<Params>(6)), "n"(two_p<Params>(7)));
-#pragma unroll
-    for (int i = 0; i < 8; i++) r.v[i] = borrow ? r.v[i] : d[i];
     return r;
 }
 

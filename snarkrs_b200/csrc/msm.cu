@@ -231,10 +231,6 @@ __global__ void k_copy_u32(uint32_t* dst, const uint32_t* src, uint32_t n) {
     if (i < n) dst[i] = src[i];
 }
 
-// a partial sum as stored: G1 accumulators run below 2p, stored below p
-__device__ __forceinline__ Xyzz<Fq> stored(const Xyzz<Fq>& a) { return canonical_point(a); }
-__device__ __forceinline__ Xyzz<Fq2> stored(const Xyzz<Fq2>& a) { return a; }
-
 // ---- accumulate: one thread per chunk of L sorted entries ----
 // LOCKSTEP: a block-wide barrier after every entry keeps the block's warps on
 // the same instructions.  A fully inlined G1 madd is too long for the
@@ -270,7 +266,7 @@ __device__ __forceinline__ void accumulate_chunks(const uint32_t* __restrict__ e
     for (size_t k = start; k < stop; k++) {
         if (!LOCKSTEP || k < end) {
             if (k == next) {
-                st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), stored(acc));
+                st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), acc);
                 acc = Xyzz<F>::identity();
                 do {
                     g++;
@@ -283,19 +279,17 @@ __device__ __forceinline__ void accumulate_chunks(const uint32_t* __restrict__ e
                 Affine<F> p = ld_affine<F>(bases, idx - base_offset);
                 if (!p.is_inf()) {
                     if (e >> 31) p.y = neg(p.y);
-                    // G1 keeps its products inlined, with coordinates below 2p
-                    // between entries; the Fq2 body is large enough that one
-                    // out-of-line Fq2 product (three Fq chains) runs faster
-                    // than inlined code that misses the instruction cache
-                    if constexpr (std::is_same<F, Fq2>::value) acc = xyzz_add_affine<F, false>(acc, p.x, p.y);
-                    else acc = xyzz_add_affine_nr<F>(acc, p.x, p.y);
+                    // G1 keeps its products inlined; the Fq2 body is large enough
+                    // that one out-of-line Fq2 product (three Fq chains) runs
+                    // faster than inlined code that misses the instruction cache
+                    acc = xyzz_add_affine<F, !std::is_same<F, Fq2>::value>(acc, p.x, p.y);
                     adds++;
                 }
             }
         }
         if (LOCKSTEP) __syncthreads();
     }
-    if (active) st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), stored(acc));
+    if (active) st_xyzz<F>(partials, seg_base[g] + (uint32_t)(t - offsets[g] / L), acc);
     // mixed additions performed, one atomic per warp (every lane reaches here in lockstep mode)
     unsigned mask = __activemask();
     unsigned total = __reduce_add_sync(mask, adds);
