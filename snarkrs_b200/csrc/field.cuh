@@ -55,6 +55,13 @@ struct FqParams {
                                    0x7879462cu, 0x666ea36fu, 0x9a07df2fu, 0x0e0a77c1u};
         return v[i];
     }
+    // q^2 as 16 limbs (the Fq2 product's offset that keeps a0 b0 - a1 b1 positive)
+    __host__ __device__ static constexpr uint32_t P2W(int i) {
+        constexpr uint32_t v[16] = {0x275d69b1u, 0x3b5458a2u, 0x09eac101u, 0xa602072du, 0x6d96cadcu, 0x4a50189cu,
+                                    0x7a1242c8u, 0x04689e95u, 0x34c6b38du, 0x26edfa5cu, 0x16375606u, 0xb00b8551u,
+                                    0x0348d21cu, 0x599a6f7cu, 0x763cbf9cu, 0x0925c4b8u};
+        return v[i];
+    }
 };
 
 template <class Params>
@@ -282,6 +289,49 @@ __device__ __forceinline__ Fp<Params> mul(const Fp<Params>& a, const Fp<Params>&
     return r;
 }
 
+// Montgomery reduction of a 16-limb t < p R: t R^-1 mod p, left in [0, 2p)
+// in r[0..7] (t is clobbered).  Row i adds m p 2^(32 i), m = t[i] (-p^-1) mod
+// 2^32, which zeroes limb i; the carry out of limb i + 8 rides into the next
+// row.  (t + M p) / R < 2p < 2^255, so no carry is left at the end.
+template <class Params>
+__host__ __device__ __forceinline__ void redc_wide(uint32_t* t, uint32_t* r) {
+    uint32_t extra = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        uint32_t m = t[i] * Params::N0;
+        uint64_t c = ((uint64_t)m * Params::P(0) + t[i]) >> 32;
+#pragma unroll
+        for (int j = 1; j < 8; j++) {
+            uint64_t p = (uint64_t)m * Params::P(j) + t[i + j] + c;
+            t[i + j] = (uint32_t)p;
+            c = p >> 32;
+        }
+        uint64_t s = (uint64_t)t[i + 8] + c + extra;
+        t[i + 8] = (uint32_t)s;
+        extra = (uint32_t)(s >> 32);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) r[k] = t[k + 8];
+}
+
+// a b as a 16-limb integer (schoolbook rows with 64-bit sums; row i writes
+// limb i + 8 fresh, since the rows before it reach limb i + 7 at most)
+__host__ __device__ __forceinline__ void mul_wide(const uint32_t* a, const uint32_t* b, uint32_t* t) {
+#pragma unroll
+    for (int k = 0; k < 16; k++) t[k] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        uint64_t c = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            uint64_t p = (uint64_t)a[j] * b[i] + t[i + j] + c;
+            t[i + j] = (uint32_t)p;
+            c = p >> 32;
+        }
+        t[i + 8] = (uint32_t)c;
+    }
+}
+
 // a^2 R^-1 mod p, left in [0, 2p) in r[0..7] (separated operand scanning):
 // the 28 cross products a_i a_j (i < j) once, doubled by a one-bit shift, plus
 // the 8 squares a_i^2, then a Montgomery reduction of the 16-limb square.  36
@@ -323,26 +373,7 @@ __host__ __device__ __forceinline__ void sqr_redc(const uint32_t* a, uint32_t* r
             c = s1 >> 32;
         }
     }
-    // reduction: row i adds m p 2^(32 i), m = t[i] (-p^-1) mod 2^32, which
-    // zeroes limb i; the carry out of limb i + 8 rides into the next row
-    uint32_t extra = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-        uint32_t m = t[i] * Params::N0;
-        uint64_t c = ((uint64_t)m * Params::P(0) + t[i]) >> 32;
-#pragma unroll
-        for (int j = 1; j < 8; j++) {
-            uint64_t p = (uint64_t)m * Params::P(j) + t[i + j] + c;
-            t[i + j] = (uint32_t)p;
-            c = p >> 32;
-        }
-        uint64_t s = (uint64_t)t[i + 8] + c + extra;
-        t[i + 8] = (uint32_t)s;
-        extra = (uint32_t)(s >> 32);
-    }
-    // (a^2 + M p) / R < 2p < 2^255: extra is zero here
-#pragma unroll
-    for (int k = 0; k < 8; k++) r[k] = t[k + 8];
+    redc_wide<Params>(t, r);
 }
 
 template <class Params>
@@ -376,12 +407,57 @@ __device__ __forceinline__ Fq2 add(const Fq2& a, const Fq2& b) { return {add(a.c
 __device__ __forceinline__ Fq2 sub(const Fq2& a, const Fq2& b) { return {sub(a.c0, b.c0), sub(a.c1, b.c1)}; }
 __device__ __forceinline__ Fq2 neg(const Fq2& a) { return {neg(a.c0), neg(a.c1)}; }
 __device__ __forceinline__ Fq2 dbl(const Fq2& a) { return {dbl(a.c0), dbl(a.c1)}; }
-// Karatsuba: three Fq products
+// (a0 + a1 u)(b0 + b1 u) with two Montgomery reductions instead of three
+// (Karatsuba with the reduction deferred, as in Aranha et al., "Faster explicit
+// formulas for computing pairings over ordinary curves", 2011): the three
+// 512-bit products t0 = a0 b0, t1 = a1 b1, m = (a0 + a1)(b0 + b1) with the
+// sums taken as integers (below 2q), then
+//   c1 = m - t0 - t1 = a0 b1 + a1 b0          (exact, below 2 q^2)
+//   c0 = t0 + q^2 - t1 = a0 b0 - a1 b1 mod q  (positive, below 2 q^2),
+// and one reduction each (inputs below q R give results below 2q).  The
+// coordinates equal those of three reduced products once brought below q.
+// Inputs below q.  Host-callable for the unit check of the limbs.
+__host__ __device__ __forceinline__ void fq2_mul_redc(const uint32_t* a0, const uint32_t* a1, const uint32_t* b0,
+                                                      const uint32_t* b1, uint32_t* r0, uint32_t* r1) {
+    uint32_t t0[16], t1[16], m[16], sa[8], sb[8];
+    {
+        uint64_t ca = 0, cb = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            ca += (uint64_t)a0[i] + a1[i];
+            sa[i] = (uint32_t)ca;
+            ca >>= 32;
+            cb += (uint64_t)b0[i] + b1[i];
+            sb[i] = (uint32_t)cb;
+            cb >>= 32;
+        }
+    }
+    mul_wide(a0, b0, t0);
+    mul_wide(a1, b1, t1);
+    mul_wide(sa, sb, m);
+    // m -= t0 + t1;  t0 += q^2 - t1
+    {
+        int64_t bm = 0, b0w = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            int64_t dm = (int64_t)m[i] - t0[i] - t1[i] + bm;
+            m[i] = (uint32_t)dm;
+            bm = dm >> 32;   // arithmetic shift: 0, -1 or -2
+            int64_t d0 = (int64_t)t0[i] + FqParams::P2W(i) - t1[i] + b0w;
+            t0[i] = (uint32_t)d0;
+            b0w = d0 >> 32;  // -1, 0 or 1
+        }
+    }
+    redc_wide<FqParams>(t0, r0);
+    redc_wide<FqParams>(m, r1);
+}
+
 __device__ __forceinline__ Fq2 mul(const Fq2& a, const Fq2& b) {
-    Fq t0 = mul(a.c0, b.c0);
-    Fq t1 = mul(a.c1, b.c1);
-    Fq m = mul(add(a.c0, a.c1), add(b.c0, b.c1));
-    return {sub(t0, t1), sub(sub(m, t0), t1)};
+    Fq2 r;
+    fq2_mul_redc(a.c0.v, a.c1.v, b.c0.v, b.c1.v, r.c0.v, r.c1.v);
+    reduce_once<FqParams>(r.c0.v);
+    reduce_once<FqParams>(r.c1.v);
+    return r;
 }
 // (a0 + a1 u)^2 = (a0 + a1)(a0 - a1) + 2 a0 a1 u
 __device__ __forceinline__ Fq2 sqr(const Fq2& a) {
