@@ -41,12 +41,13 @@ CIRCUIT_SEED, TOXIC_SEED = 21, 0x5EED
 FQ_MUL_IMAD = 264            # 8x32-bit CIOS Montgomery product: 32-bit multiply-adds
 FQ_SQR_IMAD = 208            # separated squaring: 36 limb products + 8 x 17 for the reduction
 FQ2_MUL_IMAD = 3 * 128 + 2 * 136   # three 8x8-limb products, two Montgomery reductions
+FQ_MUL_SUB_IMAD = 2 * 128 + 136    # a b - c d: two 8x8-limb products, one reduction
 # 32-bit multiply-adds per mixed addition (madd-2008-s, 8M + 2S): G1 squares with
-# the separated squaring; an Fq2 product defers its reductions (656 IMAD), an
-# Fq2 square is 2 Fq products
-MADD_IMAD = {"msm_accumulate_g1": 8 * FQ_MUL_IMAD + 2 * FQ_SQR_IMAD,
+# the separated squaring and forms Y3 = R (Q - X3) - Y1 PPP with one reduction;
+# an Fq2 product defers its reductions (656 IMAD), an Fq2 square is 2 Fq products
+MADD_IMAD = {"msm_accumulate_g1": 6 * FQ_MUL_IMAD + 2 * FQ_SQR_IMAD + FQ_MUL_SUB_IMAD,
              "msm_accumulate_g2": 8 * FQ2_MUL_IMAD + 2 * 2 * FQ_MUL_IMAD}
-MADD_WORK = {"msm_accumulate_g1": "8 Fq products x 264 + 2 Fq squares x 208 IMAD",
+MADD_WORK = {"msm_accumulate_g1": "6 Fq products x 264 + 2 Fq squares x 208 + 1 product difference x 392 IMAD",
              "msm_accumulate_g2": "8 Fq2 products x 656 + 2 Fq2 squares x 528 IMAD"}
 
 

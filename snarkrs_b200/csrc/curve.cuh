@@ -119,7 +119,7 @@ __device__ __forceinline__ Xyzz<F> xyzz_add_affine(const Xyzz<F>& p, const F& x2
         F ppp = mul(pp_, pp);
         F q = mul(p.x, pp);
         r.x = sub(sub(sqr(rr), ppp), dbl(q));
-        r.y = sub(mul(rr, sub(q, r.x)), mul(p.y, ppp));
+        r.y = mul_sub(rr, sub(q, r.x), p.y, ppp);   // G1: one reduction for both products
         r.zz = mul(p.zz, pp);
         r.zzz = mul(p.zzz, ppp);
     } else {

@@ -407,6 +407,54 @@ __device__ __forceinline__ Fq2 add(const Fq2& a, const Fq2& b) { return {add(a.c
 __device__ __forceinline__ Fq2 sub(const Fq2& a, const Fq2& b) { return {sub(a.c0, b.c0), sub(a.c1, b.c1)}; }
 __device__ __forceinline__ Fq2 neg(const Fq2& a) { return {neg(a.c0), neg(a.c1)}; }
 __device__ __forceinline__ Fq2 dbl(const Fq2& a) { return {dbl(a.c0), dbl(a.c1)}; }
+// (a b - c d) R^-1 mod p, left in [0, 2p), with one Montgomery reduction
+// instead of two: the 512-bit a b + p^2 - c d is positive and below 2 p^2 < p R
+// for inputs below p, and its reduction equals (a b R^-1 - c d R^-1) mod p.
+// c d is subtracted row by row; the borrow out of limb i + 8 rides into the
+// next row, as the carry does in redc_wide (the running value never drops
+// below a b + p^2 - c d > 0).  Params must carry p^2 (P2W).  Host-callable.
+template <class Params>
+__host__ __device__ __forceinline__ void mul_sub_redc(const uint32_t* a, const uint32_t* b, const uint32_t* c,
+                                                      const uint32_t* d, uint32_t* r) {
+    uint32_t t[16];
+    mul_wide(a, b, t);
+    {
+        uint64_t k = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            k += (uint64_t)t[i] + Params::P2W(i);
+            t[i] = (uint32_t)k;
+            k >>= 32;
+        }
+    }
+    int64_t pend = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        uint64_t cy = 0;
+        int64_t br = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            uint64_t pr = (uint64_t)c[j] * d[i] + cy;
+            cy = pr >> 32;
+            int64_t x = (int64_t)t[i + j] - (int64_t)(uint32_t)pr + br;
+            t[i + j] = (uint32_t)x;
+            br = x >> 32;
+        }
+        int64_t x = (int64_t)t[i + 8] - (int64_t)cy + br + pend;
+        t[i + 8] = (uint32_t)x;
+        pend = x >> 32;
+    }
+    redc_wide<Params>(t, r);
+}
+
+// a b - c d in Fq with one reduction (mul_sub_redc)
+__device__ __forceinline__ Fq mul_sub(const Fq& a, const Fq& b, const Fq& c, const Fq& d) {
+    Fq r;
+    mul_sub_redc<FqParams>(a.v, b.v, c.v, d.v, r.v);
+    reduce_once<FqParams>(r.v);
+    return r;
+}
+
 // (a0 + a1 u)(b0 + b1 u) with two Montgomery reductions instead of three
 // (Karatsuba with the reduction deferred, as in Aranha et al., "Faster explicit
 // formulas for computing pairings over ordinary curves", 2011): the three
@@ -458,6 +506,10 @@ __device__ __forceinline__ Fq2 mul(const Fq2& a, const Fq2& b) {
     reduce_once<FqParams>(r.c0.v);
     reduce_once<FqParams>(r.c1.v);
     return r;
+}
+// a b - c d in Fq2: two products and a difference
+__device__ __forceinline__ Fq2 mul_sub(const Fq2& a, const Fq2& b, const Fq2& c, const Fq2& d) {
+    return sub(mul(a, b), mul(c, d));
 }
 // (a0 + a1 u)^2 = (a0 + a1)(a0 - a1) + 2 a0 a1 u
 __device__ __forceinline__ Fq2 sqr(const Fq2& a) {
