@@ -104,7 +104,7 @@ struct MsmSort {
 struct MsmAccum {
     void* d_partials = nullptr;    size_t cap_partials = 0;   // bytes
     void* d_buckets = nullptr;     size_t cap_buckets = 0;    // bytes, one XYZZ sum per bucket
-    void* d_segments = nullptr;    size_t cap_segments = 0;   // bytes
+    void* d_segments = nullptr;    size_t cap_segments = 0;   // bytes, the reduction blocks' points
     void* d_windows = nullptr;     size_t cap_windows = 0;    // bytes
     unsigned long long* d_work = nullptr;                      // mixed additions performed
     MsmReducePlan plan;                                        // shape of d_windows
