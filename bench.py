@@ -51,6 +51,13 @@ MADD_WORK = {"msm_accumulate_g1": "6 Fq products x 264 + 2 Fq squares x 208 + 1 
              "msm_accumulate_g2": "8 Fq2 products x 656 + 2 Fq2 squares x 528 IMAD"}
 
 
+# g16_ntt modes (CpuNtt, crates/ntt/src/lib.rs:415-584) by bench name
+NTT_MODES = {"forward": 0, "inverse": 1, "intt-coset-ntt": 2, "coset": 3}
+NTT_WHAT = {"forward": "Fr NTT forward", "inverse": "Fr NTT inverse (with 1/n)",
+            "intt-coset-ntt": "Fr iNTT -> coset -> NTT (intt_coset_ntt)",
+            "coset": "Fr coset NTT (distribute_powers(shift) then forward)"}
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -63,6 +70,8 @@ def parse():
                    help="prove (default): full proofs; msm-g1/msm-g2/ntt: the standalone primitives")
     p.add_argument("--log-n", type=int, default=20, help="primitive size 2^log_n")
     p.add_argument("--dist", type=int, default=0, help="MSM scalars: 0 uniform, 1 = 70%% in {0,1}")
+    p.add_argument("--ntt-mode", default="intt-coset-ntt", choices=list(NTT_MODES),
+                   help="ntt workload: the transform (CpuNtt::ntt forward/inverse, coset, intt_coset_ntt)")
     p.add_argument("--lanes", type=int, default=4, help="served proving: concurrent proofs")
     p.add_argument("--no-autotune", action="store_true", help="batched proving: keep the cost model's tuning")
     p.add_argument("--no-mix", action="store_true",
@@ -480,6 +489,34 @@ def kernel_rooflines(kern, kbytes, imad_peak, hbm_peak):
     return out
 
 
+def reference_window_size(m):
+    """c of the reference CPU MSM for m general scalars (crates/msm/src/lib.rs:160-172): the c in
+    3..16 minimising ceil(255/c) * (m + 3 * 2^(c-1))."""
+    best, best_cost = 3, None
+    for c in range(3, 17):
+        cost = -(-255 // c) * (m + 3 * (1 << (c - 1)))
+        if best_cost is None or cost < best_cost:
+            best, best_cost = c, cost
+    return best
+
+
+def msm_work_model(scalars, g2):
+    """Algorithmic work of one MSM by the reference's model: m general (not 0 or 1) scalars,
+    c = window_size(m), W = ceil(255/c), B = 2^(c-1); Fq products = 10 m W + 28 B W plus 10 per
+    scalar equal to 1, three times that in G2; 264 IMAD per Fq product."""
+    import numpy as np
+    v = np.frombuffer(scalars, dtype=np.uint64).reshape(-1, 4)
+    high_zero = (v[:, 1] | v[:, 2] | v[:, 3]) == 0
+    zeros = int(np.count_nonzero(high_zero & (v[:, 0] == 0)))
+    ones = int(np.count_nonzero(high_zero & (v[:, 0] == 1)))
+    m = len(v) - zeros - ones
+    c = reference_window_size(m) if m else 3
+    w, b = -(-255 // c), 1 << (c - 1)
+    muls = (10 * m * w + 28 * b * w + 10 * ones) * (3 if g2 else 1)
+    return {"general_scalars": m, "ones": ones, "zeros": zeros, "c": c, "fq_products": muls,
+            "imad": muls * FQ_MUL_IMAD}
+
+
 def run_primitive(args):
     """Standalone MSM (points/s) or NTT (elements/s) on device-resident inputs."""
     import torch
@@ -506,9 +543,11 @@ def run_primitive(args):
         data = S.synth_scalars(79 + rank, n, 0)
         d = torch.frombuffer(bytearray(data), dtype=torch.uint8).cuda()
         ntt = S.CudaNtt(backend)
-        step = lambda: ntt.ntt_device(S.NTT_INTT_COSET_NTT, args.log_n, d.data_ptr())
-        unit, what = "elements/s", "Fr iNTT -> coset -> NTT (intt_coset_ntt), n = 2^%d" % args.log_n
-        host = lambda: ntt.intt_coset_ntt(data)
+        mode = NTT_MODES[args.ntt_mode]
+        step = lambda: ntt.ntt_device(mode, args.log_n, d.data_ptr())
+        unit, what = "elements/s", "%s, n = 2^%d" % (NTT_WHAT[args.ntt_mode], args.log_n)
+        host = {"forward": lambda: ntt.ntt(data), "inverse": lambda: ntt.ntt(data, inverse=True),
+                "coset": lambda: ntt.coset_ntt(data), "intt-coset-ntt": lambda: ntt.intt_coset_ntt(data)}[args.ntt_mode]
         h2d = len(data)
     for _ in range(W):
         step()
@@ -556,6 +595,14 @@ def run_primitive(args):
     roof["traffic"] = traffic_for("%s-2^%d" % (args.workload, args.log_n), name)
     line["roofline"] = roof
     line["kernel_rooflines"] = per_kernel
+    if args.workload.startswith("msm"):
+        # the whole MSM against the reference's work model (its window size, 10 products per
+        # bucket addition, 28 B W for the bucket reduction), per timed step
+        wm = msm_work_model(scal, g2)
+        rate = wm["imad"] / (ms / K / 1e3)
+        wm.update({"achieved": rate / 1e12, "peak": imad_pk / 1e12, "unit": "TIMAD/s", "frac": rate / imad_pk,
+                   "note": "reference work model (crates/msm/src/lib.rs:160-172) / timed ms per MSM"})
+        line["work_model_roofline"] = wm
     if not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
@@ -564,7 +611,7 @@ def run_primitive(args):
         if args.workload.startswith("msm"):
             (O.msm_g2 if g2 else O.msm_g1)(bases, scal)
         else:
-            O.ntt(args.log_n, O.NTT_INTT_COSET_NTT, data)
+            O.ntt(args.log_n, NTT_MODES[args.ntt_mode], data)
         dt = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": n / dt, "unit": unit, "cores": O.max_threads(), "kind": "port",
                                 "sample": "1 run of the same input on the C restatement, %.2f s" % dt}

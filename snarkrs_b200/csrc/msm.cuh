@@ -46,13 +46,19 @@ namespace g16 {
 // them per set into lb + 1 + hb points, T, G_0 .. G_(lb-1), Gb_0 .. Gb_(hb-1),
 // and the host forms
 //   set sum = T + seg (sum_j 2^j G_j + 2^lb sum_i 2^i Gb_i).
-// seg grows (up to 32) until the pieces over all sets number at most
-// MSM_REDUCE_PIECES.  Fewer, longer pieces keep the reduction's footprint
-// small (it runs beside the other MSMs' accumulations, whose 512-thread blocks
-// need a whole SM); 8192 measured best for the 2^21-constraint prove (45.7
-// proofs/s against 44.1 with 32768) and equal at 2^17.
+// seg grows (up to 32) until the pieces over all sets number at most the
+// target.  Fewer, longer pieces keep the reduction's footprint small where it
+// runs beside other MSMs' accumulations, whose 512-thread blocks need a whole
+// SM: the prover's window-shifted MSMs (one bucket set) aim at 8192 pieces,
+// measured best for the 2^21-constraint prove (45.7 proofs/s against 44.1
+// with 32768) and equal at 2^17.  A standalone MSM (one set per window) has
+// the GPU to itself and aims at 32768, shortening the chains.
 constexpr uint64_t MSM_REDUCE_PIECES = 8192;
+constexpr uint64_t MSM_REDUCE_PIECES_ALONE = 32768;
 constexpr uint32_t MSM_REDUCE_MAX_SEG = 32;
+constexpr uint64_t msm_reduce_pieces(bool shared_windows) {
+    return shared_windows ? MSM_REDUCE_PIECES : MSM_REDUCE_PIECES_ALONE;
+}
 
 struct MsmReducePlan {
     uint32_t sets = 0, B = 0, seg = 1, lb = 7, nb = 1, hb = 0;
@@ -63,13 +69,13 @@ struct MsmReducePlan {
     constexpr size_t result_points() const { return (size_t)sets * set_terms(); }
 };
 
-constexpr MsmReducePlan msm_reduce_plan(uint32_t sets, uint32_t B, bool g2) {
+constexpr MsmReducePlan msm_reduce_plan(uint32_t sets, uint32_t B, bool g2, uint64_t pieces_target) {
     MsmReducePlan r;
     r.sets = sets;
     r.B = B;
     r.lb = g2 ? 6 : 7;
     r.seg = 1;
-    while (r.seg < MSM_REDUCE_MAX_SEG && r.seg < B && (uint64_t)sets * B / r.seg > MSM_REDUCE_PIECES) r.seg *= 2;
+    while (r.seg < MSM_REDUCE_MAX_SEG && r.seg < B && (uint64_t)sets * B / r.seg > pieces_target) r.seg *= 2;
     const uint32_t pieces = B / r.seg;
     r.nb = (pieces >> r.lb) ? (pieces >> r.lb) : 1;
     r.hb = 0;

@@ -43,7 +43,8 @@ constexpr int NOALLOC_W = (255 + NOALLOC_C - 1) / NOALLOC_C;      // 24 windows
 constexpr size_t NOALLOC_B = (size_t)1 << (NOALLOC_C - 1);        // 1024 buckets per window
 constexpr size_t NOALLOC_K = NOALLOC_W * NOALLOC_B;               // 24576 buckets in all
 constexpr size_t NOALLOC_CHUNK = 16;                              // entries per accumulate thread
-constexpr g16::MsmReducePlan NOALLOC_PLAN = g16::msm_reduce_plan(NOALLOC_W, NOALLOC_B, false);
+constexpr g16::MsmReducePlan NOALLOC_PLAN =
+    g16::msm_reduce_plan(NOALLOC_W, NOALLOC_B, false, g16::msm_reduce_pieces(false));
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
