@@ -274,6 +274,11 @@ __device__ __forceinline__ void accumulate_chunks(const uint32_t* __restrict__ e
                 } while (next <= k);
             }
             uint32_t e = entries[k];
+            if (k + 1 < end) {   // bring the next entry's base towards L1 while this one is added
+                uint32_t nx = (entries[k + 1] & 0x7fffffffu) - base_offset;
+                if (nx < n_bases)
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(bases + (size_t)nx * (2 * Codec<F>::U4)));
+            }
             uint32_t idx = e & 0x7fffffffu;
             if (idx >= base_offset && idx - base_offset < n_bases) {
                 Affine<F> p = ld_affine<F>(bases, idx - base_offset);
