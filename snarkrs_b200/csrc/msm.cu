@@ -893,7 +893,8 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     G16_CUDA(grow_bytes(acc.d_partials, acc.cap_partials, max_partials * xyzz_bytes));
     const uint32_t Wr = s.shared ? 1u : (uint32_t)s.W;   // bucket sets to reduce
     constexpr int LB = std::is_same<F, g16d::Fq>::value ? 7 : 6;   // pieces per reduction block: 2^LB
-    const MsmReducePlan plan = msm_reduce_plan(Wr, s.B, LB == 6, msm_reduce_pieces(s.shared));
+    const MsmReducePlan plan =
+        msm_reduce_plan(Wr, s.B, LB == 6, s.reduce_pieces ? s.reduce_pieces : msm_reduce_pieces(s.shared));
     acc.plan = plan;
     G16_CUDA(grow_bytes(acc.d_buckets, acc.cap_buckets, (size_t)s.K * xyzz_bytes));
     if (!plan.direct)

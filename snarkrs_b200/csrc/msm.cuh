@@ -52,7 +52,9 @@ namespace g16 {
 // SM: the prover's window-shifted MSMs (one bucket set) aim at 8192 pieces,
 // measured best for the 2^21-constraint prove (45.7 proofs/s against 44.1
 // with 32768) and equal at 2^17.  A standalone MSM (one set per window) has
-// the GPU to itself and aims at 32768, shortening the chains.
+// the GPU to itself and aims at 32768, shortening the chains; so does the
+// prover's H MSM (MsmSort::reduce_pieces), whose reduction runs last, when the
+// witness MSMs' accumulations are mostly done.
 constexpr uint64_t MSM_REDUCE_PIECES = 8192;
 constexpr uint64_t MSM_REDUCE_PIECES_ALONE = 32768;
 constexpr uint32_t MSM_REDUCE_MAX_SEG = 32;
@@ -92,6 +94,7 @@ struct MsmSort {
     uint32_t Ks = 0;       // buckets sorted into: K, or K + 1 with the constant-work sink bucket
     bool shared = false;   // entries index window-shifted bases (w * n + i), one bucket set
     bool constant_work = false;   // zero digits are sorted into the sink bucket K
+    uint64_t reduce_pieces = 0;   // bucket-reduction piece target; 0: msm_reduce_pieces(shared)
     size_t n = 0;          // scalars sorted
     uint32_t chunk = 16;   // smallest accumulate chunk (buffers are sized for it)
     // device buffers (capacities in elements)

@@ -576,6 +576,9 @@ int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
 int enqueue_h_msm(g16_circuit* c, Workspace* ws, const void* d_h) {
     cudaStream_t st = ws->stream;
     const uint32_t nh = c->n * (uint32_t)msm_windows(c->c_h);
+    // the H reduction runs last on the main stream, mostly alone: shorter chains pay
+    // (2^21 prove +0.5%, 2^18 +1.5%, 2^20 +1.3% against the 8192-piece default)
+    ws->sort_h.reduce_pieces = MSM_REDUCE_PIECES_ALONE;
     CK(msm_sort(ws->sort_h, d_h, c->n, true, c->c_h, st, true, c->be->constant_work), "H sort");
     CK(msm_accumulate_g1(ws->sort_h, ws->acc[4], c->t_h, 0, nh, st), "H accumulate");
     const size_t bytes = ws->acc[4].result_bytes(XYZZ_G1_BYTES);
