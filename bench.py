@@ -67,6 +67,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--constraints", type=int, default=N_CONSTRAINTS)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-oracle-check", action="store_true",
+                   help="skip comparing a timed proof (and the batched proofs) with the oracle's")
     p.add_argument("--workload", default="prove", choices=["prove", "msm-g1", "msm-g2", "ntt", "batch", "serve"],
                    help="prove (default): full proofs; msm-g1/msm-g2/ntt: the standalone primitives")
     p.add_argument("--log-n", type=int, default=20, help="primitive size 2^log_n")
@@ -234,11 +236,16 @@ def synth_key(sc, nc, seed=CIRCUIT_SEED, toxic=TOXIC_SEED, device_ok=True):
     return zk
 
 
-def cpu_prove_rate(zk, sc, n_proofs):
-    """The oracle proving n_proofs different witnesses of the same circuit, all host threads."""
+def oracle_module():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.build()
+    return O
+
+
+def cpu_prove_rate(zk, sc, n_proofs):
+    """The oracle proving n_proofs different witnesses of the same circuit, all host threads."""
+    O = oracle_module()
     ok = O.Zkey(zk)
     threads = O.max_threads()
     times = []
@@ -250,6 +257,20 @@ def cpu_prove_rate(zk, sc, n_proofs):
         times.append(time.perf_counter() - t0)
     ok.close()
     return times, threads
+
+
+def oracle_proofs(zk, jobs):
+    """The oracle's proofs of [(witness_mont, r_mont, s_mont), ...] on one key, with the
+    time each took (all host threads)."""
+    O = oracle_module()
+    ok = O.Zkey(zk)
+    out = []
+    for w, r, s in jobs:
+        t0 = time.perf_counter()
+        p = ok.prove(w, O.from_bytes(r), O.from_bytes(s))
+        out.append((p, time.perf_counter() - t0))
+    ok.close()
+    return out, O.max_threads()
 
 
 def run_reference(args):
@@ -320,9 +341,10 @@ def run_ours(args):
     launches0 = S.launch_count()
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    proofs = []
     e0.record()
     for i in range(W, W + K):
-        circ.prove_with_blinders_device(dwit[i].data_ptr(), sc.n_vars, *bl[i])
+        proofs.append(circ.prove_with_blinders_device(dwit[i].data_ptr(), sc.n_vars, *bl[i]))
     e1.record()
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -333,17 +355,26 @@ def run_ours(args):
 
     # ---- e2e: host buffers through the C ABI, pinned witness copied every step ----
     lat = []
+    e2e_proofs = []
     barrier()
     torch.cuda.synchronize()
     t_all = time.perf_counter()
     for i in range(W, W + K):
         t0 = time.perf_counter()
-        circ.prove_with_blinders(wits[i].numpy(), *bl[i])
+        e2e_proofs.append(circ.prove_with_blinders(wits[i].numpy(), *bl[i]))
         lat.append(time.perf_counter() - t0)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t_all)
     e2e_value = whole_job_rate(world, K, 1e3 * e2e_s)
     readback = int(circ.readback_bytes())
+
+    # ---- parity of the timed proofs (after timing): each passes the product's pairing
+    # check, the e2e proofs equal the device-resident ones, and (rank 0, below) the first
+    # timed proof equals the oracle's proof of the same witness with the same r and s ----
+    pub_bytes = 32 * N_PUBLIC
+    for i, p in zip(range(W, W + K), proofs):
+        circ.verify(bytes(wits[i].numpy()[32:32 + pub_bytes]), p)      # raises VerifyError
+    same_e2e = all(a == b for a, b in zip(proofs, e2e_proofs))
 
     # ---- per-kernel times: the same proofs replayed with every stage on one stream ----
     # (the timed region overlaps three streams, so event spans there would include
@@ -392,11 +423,16 @@ def run_ours(args):
     t = circ.stage_timings()
 
     cpu = None
-    if not args.no_cpu_baseline and world == 1:
-        times, threads = cpu_prove_rate(zk, sc, 1)
-        cpu = {"value": 1 / times[0], "unit": "proofs/s", "cores": threads, "kind": "port",
-               "sample": "1 full proof of the same workload by the C restatement of the reference CPU prover "
-                         "(OpenMP, all host threads), %.1f s" % times[0]}
+    parity = {"pairing_checked": K, "e2e_equals_device_resident": same_e2e}
+    if not args.no_oracle_check:
+        # the oracle proves the first timed witness; its time is the CPU baseline's sample
+        (want, dt), = oracle_proofs(zk, [(bytes(wits[W].numpy()), bl[W][0], bl[W][1])])[0]
+        parity["bit_exact_vs_oracle"] = proofs[0].to_bytes() == want
+        parity["oracle_checked"] = "step %d of %d (witness seed %d)" % (W, W + K, witness_seed(rank, W))
+        if not args.no_cpu_baseline and world == 1:
+            cpu = {"value": 1 / dt, "unit": "proofs/s", "cores": oracle_module().max_threads(), "kind": "port",
+                   "sample": "1 full proof of the same workload (the first timed witness) by the C restatement "
+                             "of the reference CPU prover (OpenMP, all host threads), %.1f s" % dt}
     line = {
         "metric": "proofs/s", "value": value, "unit": "proofs/s", "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -418,6 +454,8 @@ def run_ours(args):
         "kernel_rooflines": per_kernel,
         "stage_us_total": t,
         "gpu_launches": launches,
+        "parity": parity,
+        "bit_exact_vs_oracle": parity.get("bit_exact_vs_oracle"),
         "clocks": clk,
         "hbm_peak_gbs": peaks.get("hbm_gbs"), "hbm_peak_source": peak_kind,
         "reference_published": "T4 warm CUDA prove at domain 2^21: 1263 ms (bench/results/cuda-size-sweep-2026-11-10.md:26)",
@@ -433,6 +471,10 @@ def run_ours(args):
                                "plain_value": b["plain"]["value"], "plain_p50_ms": b["plain"]["p50_ms"],
                                "plain_p99_ms": b["plain"]["p99_ms"], "speedup_vs_plain": b["speedup_vs_plain"],
                                "bit_exact_vs_plain": b["bit_exact_vs_plain"],
+                               "bit_exact_vs_oracle": b["bit_exact_vs_oracle"],
+                               "p50_ms": b["p50_ms"], "p99_ms": b["p99_ms"],
+                               "plain_queued_p50_ms": b["plain"]["queued_p50_ms"],
+                               "plain_queued_p99_ms": b["plain"]["queued_p99_ms"],
                                "per_instance_tuning": b["config"]["per_instance_tuning"]}
         except Exception as e:   # the plain-prove line above stands on its own
             line["batched"] = {"error": repr(e)[:300]}
@@ -637,11 +679,12 @@ def run_batch(args, backend=None, emit=True, steps=None):
     torch.cuda.set_device(local_rank)
     backend = backend or S.CudaBackend(local_rank)
     sizes = batch_circuits()
-    circs, wits, tunes = [], [], []
+    circs, wits, tunes, zks = [], [], [], []
     t_tune = 0.0
     for i, nc in enumerate(sizes):
         sc = S.SynthCircuit(500 + i, nc, N_INPUTS, N_PUBLIC)
-        circs.append(backend.prepare(S.ProvingKey.from_bytes(make_key(sc, TOXIC_SEED + i), check_points=False)))
+        zks.append(make_key(sc, TOXIC_SEED + i))
+        circs.append(backend.prepare(S.ProvingKey.from_bytes(zks[-1], check_points=False)))
         wits.append([sc.witness(1000 * i + j) for j in range(8)])
         if not args.no_autotune:
             # the batched objective: as many proofs in flight as prove_batch has lanes
@@ -650,11 +693,12 @@ def run_batch(args, backend=None, emit=True, steps=None):
             t_tune += time.perf_counter() - t0
         else:
             tunes.append(dict(circs[-1].tuning(), constraints=nc))
-    jobs = []
+    jobs, job_circuit = [], []
     for j in range(8):
         for i in range(len(sizes)):
             r, s_ = blinders(100 * i + j)
             jobs.append((circs[i], wits[i][j], r, s_))
+            job_circuit.append(i)
     # warm-up: every circuit once on its own, then one batch (workspaces, graphs)
     for c, w, r, s_ in jobs[:len(sizes)]:
         c.prove_with_blinders(w, r, s_)
@@ -666,14 +710,31 @@ def run_batch(args, backend=None, emit=True, steps=None):
         plain.append(c.prove_with_blinders(w, r, s_))
         lat.append(time.perf_counter() - t1)
     t_plain = time.perf_counter() - t0
-    best, out = None, None
+    best, out, done = None, None, None
     steps = steps or args.steps
     for _ in range(max(1, steps)):
+        d = []
         t0 = time.perf_counter()
-        out = backend.prove_batch(jobs)
+        out = backend.prove_batch(jobs, done_ms=d)
         dt = time.perf_counter() - t0
-        best = dt if best is None else min(best, dt)
+        if best is None or dt < best:
+            best, done = dt, d
     assert all(a == b for a, b in zip(out, plain)), "batched proofs differ from single proofs"
+    # latency of a batch submitted at once: each proof's completion time from the
+    # submission, batched, against the same 64 jobs queued FIFO one at a time
+    fifo, acc = [], 0.0
+    for x in lat:
+        acc += x
+        fifo.append(1e3 * acc)
+    done, fifo = sorted(done), sorted(fifo)
+    pct = lambda v, q: v[min(len(v) - 1, int(q * len(v)))]
+    exact = None
+    if not args.no_oracle_check:
+        exact = True
+        for i in range(len(sizes)):
+            mine = [(k, jobs[k]) for k in range(len(jobs)) if job_circuit[k] == i]
+            want, _ = oracle_proofs(zks[i], [(w, r, s_) for _, (_, w, r, s_) in mine])
+            exact &= all(out[k].to_bytes() == p for (k, _), (p, _) in zip(mine, want))
     lat.sort()
     line = {"metric": "proofs/s", "value": len(jobs) / best, "unit": "proofs/s", "n_gpus": 1, "steps": steps,
             "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -685,9 +746,13 @@ def run_batch(args, backend=None, emit=True, steps=None):
                                               "circuits)" % (BATCH_LANES, t_tune)
                        if not args.no_autotune else "cost model", "tuning": tunes},
             "plain": {"value": len(jobs) / t_plain, "unit": "proofs/s", "p50_ms": 1e3 * lat[len(lat) // 2],
-                      "p99_ms": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+                      "p99_ms": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                      "queued_p50_ms": pct(fifo, 0.5), "queued_p99_ms": pct(fifo, 0.99)},
+            "p50_ms": pct(done, 0.5), "p99_ms": pct(done, 0.99),
+            "latency_note": "p50/p99: completion time of each proof from the submission of all 64 at once; "
+                            "plain.queued_*: the same 64 queued FIFO one at a time; plain.p50/p99: one proof alone",
             "batch_ms": 1e3 * best, "speedup_vs_plain": t_plain / best,
-            "bit_exact_vs_plain": True}
+            "bit_exact_vs_plain": True, "bit_exact_vs_oracle": exact}
     for c in circs:
         c.close()
     if emit:

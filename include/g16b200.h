@@ -39,7 +39,8 @@ enum {
     G16_ERR_DEVICE = 4,           /* ProveError::Device: a CUDA call failed */
     G16_ERR_DEVICE_MEMORY = 5,    /* ProveError::DeviceMemory: refused before allocating */
     G16_ERR_SELF_VERIFY = 6,      /* ProveError::SelfVerify: g16_prove's proof failed its check */
-    G16_ERR_TIMEOUT = 7,          /* a bounded device wait gave up */
+    G16_ERR_TIMEOUT = 7,          /* reserved for a bounded device wait that gives up; no
+                                     entry point waits on the device that way, so none returns it */
     G16_ERR_INVALID_ARGUMENT = 8, /* null pointer, bad size, bad enum */
     G16_ERR_FORMAT = 9,           /* ZkeyError: malformed .zkey / .wtns bytes */
     G16_ERR_VERIFY = 10           /* verify::VerifyError: the proof does not verify */
@@ -229,6 +230,12 @@ int g16_autotune(g16_circuit *c, const uint8_t *witness_mont, size_t n, int conc
  * witnesses[i] has lens[i] Montgomery Fr; r, s: count x 32 bytes. */
 int g16_prove_batch(g16_backend *b, size_t count, g16_circuit *const *circuits, const uint8_t *const *witnesses,
                     const size_t *lens, const uint8_t *r_mont, const uint8_t *s_mont, g16_proof *out);
+/* The same, and done_ms[i] (count doubles, NULL to skip) receives the
+ * milliseconds from the call's start until job i's proof was complete: the
+ * per-proof latency of a batch submitted at once. */
+int g16_prove_batch_timed(g16_backend *b, size_t count, g16_circuit *const *circuits,
+                          const uint8_t *const *witnesses, const size_t *lens, const uint8_t *r_mont,
+                          const uint8_t *s_mont, g16_proof *out, double *done_ms);
 
 /* Served proving (no reference counterpart; the reference proves one request
  * per call).  A request loop with continuous batching: `lanes` workers take
@@ -277,9 +284,12 @@ int g16_msm_g2_device(g16_backend *b, const void *d_bases, const void *d_scalars
  * library holds until the process exits.  At most 16384 points (larger n is
  * refused with G16_ERR_INVALID_ARGUMENT); runs on `device`'s legacy default
  * stream and returns with the result on the host.  The first call on a device
- * looks up the array's address (make it before any stream capture).  All
- * calls share the array: calls whose device work overlaps race and must be
- * serialised by the caller.  Kernel timing must be off. */
+ * looks up the array's address (make it before any stream capture); under
+ * CUDA's lazy module loading it is also when the device commits the array and
+ * loads the MSM kernels, so make it at start-up (a full device fails it with
+ * G16_ERR_DEVICE_MEMORY).  Resetting the device after that first call is not
+ * supported.  All calls share the array: calls whose device work overlaps
+ * race and must be serialised by the caller.  Kernel timing must be off. */
 int g16_msm_g1_device_noalloc(int device, const void *d_bases, const void *d_scalars, size_t n, int scalars_form,
                               uint8_t *out64);
 
@@ -298,6 +308,8 @@ void g16_kernel_timing_reset(void);
 size_t g16_kernel_timing_report(char *buf, size_t len);
 /* Kernels launched by this library since load (every launch site counts). */
 uint64_t g16_launch_count(void);
+/* Device allocations (cudaMalloc calls) this library has made since load. */
+uint64_t g16_device_alloc_count(void);
 /* serial != 0 runs every stage of this circuit's proofs on one stream (no
  * overlap), so per-kernel event times do not include concurrent work: for
  * profiling.  Results are identical either way. */

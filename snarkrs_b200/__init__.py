@@ -496,8 +496,11 @@ class CudaBackend:
         check(lib().g16_prepare(self._h, ctypes.byref(pk._view), ctypes.byref(c)))
         return CudaCircuit(self, c, pk)
 
-    def prove_batch(self, jobs):
-        """Prove [(circuit, witness_mont, r_mont, s_mont), ...] in one submission."""
+    def prove_batch(self, jobs, done_ms=None):
+        """Prove [(circuit, witness_mont, r_mont, s_mont), ...] in one submission.
+
+        done_ms: an optional list that receives, per job, the milliseconds from the
+        submission until that proof was complete."""
         n = len(jobs)
         circ = (ctypes.c_void_p * n)(*[j[0]._h for j in jobs])
         bufs = [bytes(j[1]) for j in jobs]
@@ -506,7 +509,10 @@ class CudaBackend:
         r = b"".join(bytes(j[2]) for j in jobs)
         s = b"".join(bytes(j[3]) for j in jobs)
         out = (_Proof * n)()
-        check(lib().g16_prove_batch(self._h, ctypes.c_size_t(n), circ, wits, lens, r, s, out))
+        done = (ctypes.c_double * max(n, 1))()
+        check(lib().g16_prove_batch_timed(self._h, ctypes.c_size_t(n), circ, wits, lens, r, s, out, done))
+        if done_ms is not None:
+            done_ms[:] = list(done)[:n]
         return [Proof(p.a, p.b, p.c) for p in out]
 
     # device memory helpers
@@ -758,6 +764,12 @@ def launch_count():
     """Kernels this library has launched since it was loaded."""
     lib().g16_launch_count.restype = ctypes.c_uint64
     return lib().g16_launch_count()
+
+
+def device_alloc_count():
+    """Device allocations (cudaMalloc calls) this library has made since it was loaded."""
+    lib().g16_device_alloc_count.restype = ctypes.c_uint64
+    return lib().g16_device_alloc_count()
 
 
 def imad_peak(backend):

@@ -38,6 +38,7 @@ struct KernelTimer {
     std::map<std::string, double> units;                     // algorithmic work, per kernel class
     std::map<std::string, double> bytes;                     // algorithmic HBM bytes, per kernel class
     std::atomic<uint64_t> launches{0};                        // every kernel this library launched
+    std::atomic<uint64_t> device_allocs{0};                   // every cudaMalloc this library made
     std::mutex mu;
 
     void add_units(const char* name, double u) {
@@ -109,6 +110,14 @@ struct TimedLaunch {
     }
     ~TimedLaunch() { timer().end(s); }
 };
+
+// Every device allocation of the library goes through here, so that the number
+// of allocations it has made is observable (g16_device_alloc_count).
+template <class T>
+inline cudaError_t dev_malloc(T** p, size_t bytes) {
+    timer().device_allocs.fetch_add(1, std::memory_order_relaxed);
+    return cudaMalloc((void**)p, bytes);
+}
 
 inline unsigned blocks_for(size_t n, unsigned threads) { return (unsigned)((n + threads - 1) / threads); }
 

@@ -683,7 +683,7 @@ static cudaError_t window_table(const void* d_in, size_t n, uint32_t skip, int c
     const int W = msm_windows(c);
     const size_t count = n * (size_t)(W - 1);
     void* tmp = nullptr;
-    G16_CUDA(cudaMalloc(&tmp, (count ? count : 1) * xyzz_bytes));
+    G16_CUDA(g16::dev_malloc(&tmp, (count ? count : 1) * xyzz_bytes));
     cudaError_t e = cudaSuccess;
     {
         TimedLaunch tl("msm_window_table", st);
@@ -708,7 +708,7 @@ static cudaError_t fixed_base(const void* d_table, const void* d_scalars, size_t
                               size_t xyzz_bytes) {
     if (!n) return cudaSuccess;
     void* tmp = nullptr;
-    G16_CUDA(cudaMalloc(&tmp, n * xyzz_bytes));
+    G16_CUDA(g16::dev_malloc(&tmp, n * xyzz_bytes));
     cudaError_t e;
     {
         TimedLaunch tl("fixed_base", st);
@@ -759,13 +759,20 @@ int msm_window_bits(size_t m) {
     return best;
 }
 
+// Buffers that are views (fixed) are never reallocated: too small is an error.
+static cudaError_t fixed_too_small(size_t need_bytes, size_t cap_bytes) {
+    set_error("fixed MSM scratch holds %zu bytes where %zu are needed", cap_bytes, need_bytes);
+    return cudaErrorInvalidValue;
+}
+
 template <class T>
-static cudaError_t grow(T*& p, size_t& cap, size_t need_elems) {
+static cudaError_t grow(T*& p, size_t& cap, size_t need_elems, bool fixed = false) {
     if (need_elems <= cap && p) return cudaSuccess;
+    if (fixed) return fixed_too_small(need_elems * sizeof(T), cap * sizeof(T));
     cudaFree(p);
     p = nullptr;
     size_t n = need_elems + need_elems / 8 + 64;
-    cudaError_t e = cudaMalloc((void**)&p, n * sizeof(T));
+    cudaError_t e = g16::dev_malloc((void**)&p, n * sizeof(T));
     if (e != cudaSuccess) {
         cap = 0;
         set_error("cudaMalloc of %zu bytes for MSM scratch failed: %s", n * sizeof(T), cudaGetErrorString(e));
@@ -775,12 +782,13 @@ static cudaError_t grow(T*& p, size_t& cap, size_t need_elems) {
     return cudaSuccess;
 }
 
-static cudaError_t grow_bytes(void*& p, size_t& cap, size_t need) {
+static cudaError_t grow_bytes(void*& p, size_t& cap, size_t need, bool fixed = false) {
     if (need <= cap && p) return cudaSuccess;
+    if (fixed) return fixed_too_small(need, cap);
     cudaFree(p);
     p = nullptr;
     size_t n = need + need / 8 + 256;
-    cudaError_t e = cudaMalloc(&p, n);
+    cudaError_t e = g16::dev_malloc(&p, n);
     if (e != cudaSuccess) {
         cap = 0;
         set_error("cudaMalloc of %zu bytes for MSM scratch failed: %s", n, cudaGetErrorString(e));
@@ -835,8 +843,10 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
     const uint32_t kw = shared_windows ? 0u : s.B, ew = shared_windows ? (uint32_t)n : 0u;
     const uint32_t sink = constant_work ? s.K : NO_KEY;
     size_t nn = n ? n : 1;
-    G16_CUDA(grow(s.d_scalars_std, s.cap_scalars, nn * 8));
+    G16_CUDA(grow(s.d_scalars_std, s.cap_scalars, nn * 8, s.fixed));
     size_t kk = (size_t)s.Ks + 1;
+    if (s.fixed && (kk > s.cap_k || !s.d_counts || !s.d_offsets || !s.d_cursor || !s.d_seg_base || !s.d_fat_list))
+        G16_CUDA(fixed_too_small(kk * sizeof(uint32_t), s.cap_k * sizeof(uint32_t)));
     if (kk > s.cap_k || !s.d_counts) {
         size_t cap = 0;
         G16_CUDA(grow(s.d_counts, cap, kk));
@@ -850,9 +860,12 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
         G16_CUDA(grow(s.d_fat_list, cap, kk));
         s.cap_k = cap;
     }
-    G16_CUDA(grow(s.d_scan_tmp, s.cap_tmp, kk / 1024 + 2));
-    G16_CUDA(grow(s.d_entries, s.cap_entries, nn * s.W));
-    if (!s.d_total) G16_CUDA(cudaMalloc((void**)&s.d_total, 4 * sizeof(uint32_t)));
+    G16_CUDA(grow(s.d_scan_tmp, s.cap_tmp, kk / 1024 + 2, s.fixed));
+    G16_CUDA(grow(s.d_entries, s.cap_entries, nn * s.W, s.fixed));
+    if (!s.d_total) {
+        if (s.fixed) G16_CUDA(fixed_too_small(4 * sizeof(uint32_t), 0));
+        G16_CUDA(g16::dev_malloc((void**)&s.d_total, 4 * sizeof(uint32_t)));
+    }
 
     G16_CUDA(cudaMemsetAsync(s.d_counts, 0, kk * sizeof(uint32_t), st));
     G16_CUDA(cudaMemsetAsync(s.d_total, 0, 4 * sizeof(uint32_t), st));
@@ -890,17 +903,20 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     size_t max_entries = (s.n ? s.n : 1) * (size_t)s.W;
     size_t chunks = (max_entries + s.chunk - 1) / s.chunk;
     size_t max_partials = (size_t)s.Ks + chunks + 1;
-    G16_CUDA(grow_bytes(acc.d_partials, acc.cap_partials, max_partials * xyzz_bytes));
+    G16_CUDA(grow_bytes(acc.d_partials, acc.cap_partials, max_partials * xyzz_bytes, acc.fixed));
     const uint32_t Wr = s.shared ? 1u : (uint32_t)s.W;   // bucket sets to reduce
     constexpr int LB = std::is_same<F, g16d::Fq>::value ? 7 : 6;   // pieces per reduction block: 2^LB
     const MsmReducePlan plan =
         msm_reduce_plan(Wr, s.B, LB == 6, s.reduce_pieces ? s.reduce_pieces : msm_reduce_pieces(s.shared));
     acc.plan = plan;
-    G16_CUDA(grow_bytes(acc.d_buckets, acc.cap_buckets, (size_t)s.K * xyzz_bytes));
+    G16_CUDA(grow_bytes(acc.d_buckets, acc.cap_buckets, (size_t)s.K * xyzz_bytes, acc.fixed));
     if (!plan.direct)
-        G16_CUDA(grow_bytes(acc.d_segments, acc.cap_segments, plan.block_points() * xyzz_bytes));
-    G16_CUDA(grow_bytes(acc.d_windows, acc.cap_windows, plan.result_points() * xyzz_bytes));
-    if (!acc.d_work) G16_CUDA(cudaMalloc((void**)&acc.d_work, sizeof(unsigned long long)));
+        G16_CUDA(grow_bytes(acc.d_segments, acc.cap_segments, plan.block_points() * xyzz_bytes, acc.fixed));
+    G16_CUDA(grow_bytes(acc.d_windows, acc.cap_windows, plan.result_points() * xyzz_bytes, acc.fixed));
+    if (!acc.d_work) {
+        if (acc.fixed) G16_CUDA(fixed_too_small(sizeof(unsigned long long), 0));
+        G16_CUDA(g16::dev_malloc((void**)&acc.d_work, sizeof(unsigned long long)));
+    }
     G16_CUDA(cudaMemsetAsync(acc.d_work, 0, sizeof(unsigned long long), st));
     uint4* partials = (uint4*)acc.d_partials;
     {

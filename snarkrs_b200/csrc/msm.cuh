@@ -107,6 +107,10 @@ struct MsmSort {
     uint32_t* d_scan_tmp = nullptr;     size_t cap_tmp = 0;
     uint32_t* d_entries = nullptr;      size_t cap_entries = 0;
     uint32_t* d_total = nullptr;                                  // [0] = M, [1] = S, [2] = fat buckets, [3] = L
+    // the buffers are views into memory the struct does not own (the
+    // allocation-free entry point's fixed scratch): a buffer too small for a
+    // call is an error, never a cudaFree and cudaMalloc
+    bool fixed = false;
     void release();
 };
 
@@ -117,6 +121,7 @@ struct MsmAccum {
     void* d_windows = nullptr;     size_t cap_windows = 0;    // bytes
     unsigned long long* d_work = nullptr;                      // mixed additions performed
     MsmReducePlan plan;                                        // shape of d_windows
+    bool fixed = false;                                        // views, as MsmSort::fixed
     size_t result_bytes(size_t xyzz_bytes) const { return plan.result_points() * xyzz_bytes; }
     void release();
 };
@@ -170,6 +175,10 @@ G2J msm_combine_g2(const uint8_t* result_xyzz, const MsmReducePlan& plan, int c)
 
 constexpr size_t XYZZ_G1_BYTES = 128;
 constexpr size_t XYZZ_G2_BYTES = 256;
+
+// The prover reads each of its five MSM results (the reduction's points) back
+// into a pinned host slot of this many bytes.
+constexpr size_t MSM_RESULT_SLOT_BYTES = 32 * 256;
 
 // kernel-time accounting hook (events around each kernel class), optional
 struct KernelTimer;

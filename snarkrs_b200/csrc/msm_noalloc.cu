@@ -26,7 +26,13 @@
 //     the caller;
 //   * the first call on each device looks up the array's device address with
 //     cudaGetSymbolAddress (with that device current) and caches it; make that
-//     first call before any stream capture begins;
+//     first call before any stream capture begins.  With CUDA's lazy module
+//     loading (the default since CUDA 12.2) that first call is also when the
+//     device commits the array's memory and loads the MSM kernels, so make it
+//     at start-up: on a device whose memory is already full it can fail, with
+//     G16_ERR_DEVICE_MEMORY;
+//   * the cached address belongs to the device's context at the first call:
+//     resetting the device (cudaDeviceReset) after it is not supported;
 //   * kernel timing (g16_kernel_timing_enable) must be off, since timing
 //     creates CUDA events.
 #include <mutex>
@@ -122,7 +128,8 @@ extern "C" int g16_msm_g1_device_noalloc(int device, const void* d_bases, const 
             e = cudaGetSymbolAddress(&p, g_msm_noalloc_scratch);
             if (e != cudaSuccess || !p) {
                 g16::set_error("g16_msm_g1_device_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-                return G16_ERR_DEVICE;
+                // lazy module loading commits the array here: a full device is a memory error
+                return e == cudaErrorMemoryAllocation ? G16_ERR_DEVICE_MEMORY : G16_ERR_DEVICE;
             }
             g_scratch_addr[device] = (unsigned char*)p;
         }
@@ -131,6 +138,7 @@ extern "C" int g16_msm_g1_device_noalloc(int device, const void* d_bases, const 
     g16::host_init();
     // views into the scratch, with capacities that make every grow() a no-op
     g16::MsmSort s;
+    s.fixed = true;
     s.d_scalars_std = (uint32_t*)(base + OFF_SCALARS);
     s.cap_scalars = 8 * NOALLOC_MAX_POINTS;
     s.d_counts = (uint32_t*)(base + OFF_COUNTS);
@@ -145,6 +153,7 @@ extern "C" int g16_msm_g1_device_noalloc(int device, const void* d_bases, const 
     s.cap_entries = ENTRIES_ELEMS;
     s.d_total = (uint32_t*)(base + OFF_TOTAL);
     g16::MsmAccum acc;
+    acc.fixed = true;
     acc.d_partials = base + OFF_PARTIALS;
     acc.cap_partials = PARTIALS_BYTES;
     acc.d_buckets = base + OFF_BUCKETS;

@@ -239,9 +239,9 @@ cudaError_t ntt_tables(NttTables& t, int log_n, cudaStream_t st) {
     host_init();
     t.release();
     size_t n = (size_t)1 << log_n;
-    G16_CUDA(cudaMalloc(&t.d_tw, (n / 2) * 32));
-    G16_CUDA(cudaMalloc(&t.d_tw_inv, (n / 2) * 32));
-    G16_CUDA(cudaMalloc(&t.d_coset, n * 32 + 32));   // + one slot holding 1/n for the scale epilogue
+    G16_CUDA(g16::dev_malloc(&t.d_tw, (n / 2) * 32));
+    G16_CUDA(g16::dev_malloc(&t.d_tw_inv, (n / 2) * 32));
+    G16_CUDA(g16::dev_malloc(&t.d_coset, n * 32 + 32));   // + one slot holding 1/n for the scale epilogue
     g16::Fr w = domain_root(log_n), wi = w.inv();
     g16::Fr ninv = g16::Fr::from_u64(n).inv();
     g16::Fr shift = domain_root(log_n + 1);

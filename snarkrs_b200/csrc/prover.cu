@@ -181,10 +181,10 @@ struct Workspace {
     uint64_t bytes = 0;                // fixed device buffers
 
     cudaError_t init(uint32_t n_vars, uint32_t n) {
-        cudaError_t e = cudaMalloc(&d_w, 32ull * n_vars);
-        if (e == cudaSuccess) e = cudaMalloc(&d_abc, 32ull * n * 3);
-        if (e == cudaSuccess) e = cudaMalloc(&d_hpoly, 32ull * n);
-        if (e == cudaSuccess) e = cudaMallocHost((void**)&h_win, 5 * 32 * 256);
+        cudaError_t e = g16::dev_malloc(&d_w, 32ull * n_vars);
+        if (e == cudaSuccess) e = g16::dev_malloc(&d_abc, 32ull * n * 3);
+        if (e == cudaSuccess) e = g16::dev_malloc(&d_hpoly, 32ull * n);
+        if (e == cudaSuccess) e = cudaMallocHost((void**)&h_win, 5 * MSM_RESULT_SLOT_BYTES);
         if (e == cudaSuccess) e = cudaMallocHost((void**)&h_work, 8 * sizeof(unsigned long long));
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
         for (auto& x : side)
@@ -291,7 +291,7 @@ int cuda_fail(cudaError_t e, const char* what) {
     } while (0)
 
 cudaError_t circuit_alloc(g16_circuit* c, void** p, size_t bytes) {
-    cudaError_t e = cudaMalloc(p, bytes ? bytes : 32);
+    cudaError_t e = g16::dev_malloc(p, bytes ? bytes : 32);
     if (e == cudaSuccess) {
         c->allocs.push_back(*p);
         c->device_bytes += bytes;
@@ -542,7 +542,7 @@ int run_h(g16_circuit* c, Workspace* ws, const void* d_w, void* h_out) {
 // the witness upload; the sort on the first), while the main stream does
 // gather -> NTT -> H sort -> H accumulate; the main stream joins them before
 // the results are read back.
-constexpr size_t WIN_SLOT = 32 * 256;
+constexpr size_t WIN_SLOT = MSM_RESULT_SLOT_BYTES;
 
 int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
     const uint32_t nw = c->n_vars * (uint32_t)msm_windows(c->c_w);
@@ -1182,7 +1182,7 @@ int g16_compute_h(g16_circuit* c, const uint8_t* w, size_t n, g16_hpoly** out) {
     auto h = std::make_unique<g16_hpoly>();
     h->owner = c;
     h->n = c->n;
-    CK(cudaMalloc(&h->d_h, 32ull * c->n), "H allocation");
+    CK(g16::dev_malloc(&h->d_h, 32ull * c->n), "H allocation");
     if ((rc = upload_witness(g.ws, w, n)) || (rc = run_h(c, g.ws, g.ws->d_w, h->d_h))) {
         cudaFree(h->d_h);
         return rc;
@@ -1416,8 +1416,19 @@ int g16_stage_timings_get(const g16_circuit* c, g16_stage_timings* out) {
 // Several proofs in flight at once: `lanes` host threads each take the next job
 // and prove it on a workspace of its circuit, so the jobs' kernels, copies and
 // host-side assembly overlap.  Each result is the same as a single call's.
+int g16_prove_batch_timed(g16_backend* b, size_t count, g16_circuit* const* circuits,
+                          const uint8_t* const* witnesses, const size_t* lens, const uint8_t* r, const uint8_t* s,
+                          g16_proof* out, double* done_ms);
+
 int g16_prove_batch(g16_backend* b, size_t count, g16_circuit* const* circuits, const uint8_t* const* witnesses,
                     const size_t* lens, const uint8_t* r, const uint8_t* s, g16_proof* out) {
+    return g16_prove_batch_timed(b, count, circuits, witnesses, lens, r, s, out, nullptr);
+}
+
+int g16_prove_batch_timed(g16_backend* b, size_t count, g16_circuit* const* circuits,
+                          const uint8_t* const* witnesses, const size_t* lens, const uint8_t* r, const uint8_t* s,
+                          g16_proof* out, double* done_ms) {
+    const auto t_start = std::chrono::steady_clock::now();
     if (!b || (count && (!circuits || !witnesses || !lens || !r || !s || !out)))
         return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     for (size_t i = 0; i < count; i++) {
@@ -1437,6 +1448,9 @@ int g16_prove_batch(g16_backend* b, size_t count, g16_circuit* const* circuits, 
         for (size_t i; (i = next.fetch_add(1)) < count;) {
             rcs[i] = g16_prove_with_blinders(circuits[i], witnesses[i], lens[i], r + 32 * i, s + 32 * i, out + i);
             if (rcs[i]) errs[i] = g_err;
+            if (done_ms)
+                done_ms[i] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start)
+                                 .count();
         }
     };
     std::vector<std::thread> pool;
@@ -1458,7 +1472,7 @@ static int grow_dev(void*& p, size_t& cap, size_t need) {
     cudaFree(p);
     p = nullptr;
     cap = 0;
-    CK(cudaMalloc(&p, need ? need : 32), "scratch allocation");
+    CK(g16::dev_malloc(&p, need ? need : 32), "scratch allocation");
     cap = need;
     return G16_OK;
 }
@@ -1723,6 +1737,7 @@ int g16_autotune(g16_circuit* c, const uint8_t* w, size_t n, int concurrency, g1
 }
 
 uint64_t g16_launch_count(void) { return timer().launches.load(); }
+uint64_t g16_device_alloc_count(void) { return timer().device_allocs.load(); }
 
 uint64_t g16_circuit_readback_bytes(const g16_circuit* c) { return c ? c->readback_bytes : 0; }
 
@@ -1742,7 +1757,7 @@ int g16_imad_peak(g16_backend* b, double* imad_per_s) {
     unsigned blocks = (unsigned)sms * 8, threads = 256;
     uint32_t iters = 4096;
     uint32_t* d = nullptr;
-    CK(cudaMalloc(&d, (size_t)blocks * threads * 4), "probe buffer");
+    CK(g16::dev_malloc(&d, (size_t)blocks * threads * 4), "probe buffer");
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -1776,7 +1791,7 @@ int g16_imad_peak(g16_backend* b, double* imad_per_s) {
 int g16_device_alloc(g16_backend* b, size_t bytes, void** d_out) {
     if (!b || !d_out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
-    CK(cudaMalloc(d_out, bytes ? bytes : 32), "device allocation");
+    CK(g16::dev_malloc(d_out, bytes ? bytes : 32), "device allocation");
     return G16_OK;
 }
 int g16_device_free(g16_backend* b, void* d) {

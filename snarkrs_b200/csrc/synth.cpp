@@ -255,7 +255,7 @@ struct DevicePoints {
     bool upload_table(const std::vector<Affine<F>>& t, void*& d, size_t point_bytes) {
         std::vector<uint8_t> packed(t.size() * point_bytes);
         for (size_t i = 0; i < t.size(); i++) pack(packed.data() + i * point_bytes, t[i]);
-        return check(cudaMalloc(&d, packed.size()), "table") &&
+        return check(g16::dev_malloc(&d, packed.size()), "table") &&
                check(cudaMemcpy(d, packed.data(), packed.size(), cudaMemcpyHostToDevice), "table upload");
     }
     bool points(int group, const Fr* k, size_t n, uint8_t* out) {
@@ -265,14 +265,14 @@ struct DevicePoints {
             if (d_k) cudaFree(d_k);
             d_k = nullptr;
             cap_k = 0;
-            if (!check(cudaMalloc(&d_k, n * 32), "scalars")) return false;
+            if (!check(g16::dev_malloc(&d_k, n * 32), "scalars")) return false;
             cap_k = n * 32;
         }
         if (n * pb > cap_out) {
             if (d_out) cudaFree(d_out);
             d_out = nullptr;
             cap_out = 0;
-            if (!check(cudaMalloc(&d_out, n * pb), "points")) return false;
+            if (!check(g16::dev_malloc(&d_out, n * pb), "points")) return false;
             cap_out = n * pb;
         }
         return check(cudaMemcpyAsync(d_k, k, n * 32, cudaMemcpyHostToDevice, st), "scalar upload") &&

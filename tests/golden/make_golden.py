@@ -1,7 +1,7 @@
 """Regenerate the golden fixtures in this directory from the reference tree.
 
-Reads (never writes) the reference checkout, by default at the path given in
-``G16_REFERENCE`` or ``/root/reference``, and writes:
+Reads (never writes) the reference checkout whose path is given as the first
+argument or in ``G16_REFERENCE`` (there is no default), and writes:
 
 * ``reference_constants.json`` -- the constants the reference's own tests pin:
   the ffjavascript domain roots for 2^28 and 2^4
@@ -14,7 +14,7 @@ Reads (never writes) the reference checkout, by default at the path given in
   (test-support/gnark/toy/{vk.bin,proof.bin,public.bin}) as hex: a real
   gnark-produced Groth16 proof that an independent pairing must accept.
 
-Run: ``python tests/golden/make_golden.py``.
+Run: ``python tests/golden/make_golden.py <reference checkout>``.
 """
 import json
 import os
@@ -22,7 +22,9 @@ import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("G16_REFERENCE", "/root/reference")
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("G16_REFERENCE")
+if __name__ == "__main__" and not REF:
+    sys.exit("usage: make_golden.py <reference checkout> (or set G16_REFERENCE)")
 
 
 def read(rel):

@@ -32,12 +32,19 @@ def test_ntt_all_modes_match_oracle(backend, log_n):
     assert ntt.coset_ntt(data, O.to_bytes(shift), inverse=True) == O.ntt(log_n, O.NTT_COSET_INVERSE, data, shift)
 
 
-@pytest.mark.parametrize("log_n", [20, 22])
-def test_ntt_large_matches_oracle(backend, log_n):
+@pytest.mark.parametrize("log_n", [20, 22, 24])
+def test_ntt_config_sizes_all_modes_match_oracle(backend, log_n):
+    """Every transform of the standalone-kernel configuration (log n = 20, 22, 24):
+    forward, inverse (with 1/n), coset forward with the proving shift, coset inverse
+    with another shift, and intt_coset_ntt, each against the oracle."""
     ntt = S.CudaNtt(backend)
     data = S.synth_scalars(log_n, 1 << log_n, 0)          # standard-form values are valid Montgomery limbs
-    assert ntt.intt_coset_ntt(data) == O.ntt(log_n, O.NTT_INTT_COSET_NTT, data)
     assert ntt.ntt(data) == O.ntt(log_n, O.NTT_FORWARD, data)
+    assert ntt.ntt(data, inverse=True) == O.ntt(log_n, O.NTT_INVERSE, data)
+    assert ntt.coset_ntt(data) == O.ntt(log_n, O.NTT_COSET_FORWARD, data)
+    shift = O.to_mont(5)
+    assert ntt.coset_ntt(data, O.to_bytes(shift), inverse=True) == O.ntt(log_n, O.NTT_COSET_INVERSE, data, shift)
+    assert ntt.intt_coset_ntt(data) == O.ntt(log_n, O.NTT_INTT_COSET_NTT, data)
 
 
 def _limb_sum(data, sign=None):
@@ -109,8 +116,10 @@ def test_msm_g2_matches_oracle(backend, n, dist):
     assert got == want
 
 
-def test_msm_g2_2_20(backend):
-    got, want = msm_pair(backend, 1 << 20, 0, 9, g2=True)
+@pytest.mark.parametrize("dist", [0, 1])
+def test_msm_g2_2_20(backend, dist):
+    """The configured G2 MSM, 2^20 points, uniform scalars and 70% in {0,1}."""
+    got, want = msm_pair(backend, 1 << 20, dist, 9 + dist, g2=True)
     assert got == want
 
 
@@ -244,8 +253,11 @@ def test_batch_equals_singles(backend, circuits):
             r, s = blinders(100 + ws)
             jobs.append((circs[name], sc.witness(ws), r, s))
     batch = backend.prove_batch(jobs)
-    for (c, w, r, s), p in zip(jobs, batch):
+    oks = {name: circuits[name][2] for name in circs}
+    names = [name for name in ("tiny", "small") for _ in range(3)]
+    for (c, w, r, s), p, name in zip(jobs, batch, names):
         assert p == c.prove_with_blinders(w, r, s)
+        assert p.to_bytes() == oks[name].prove(w, O.from_bytes(r), O.from_bytes(s))
 
 
 def test_device_key_generation_is_the_host_one(backend):

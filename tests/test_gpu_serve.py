@@ -1,5 +1,6 @@
 """Served proving (continuous batching, LRU key residency): every proof equals
-the same request proved alone, under overlap and under key eviction."""
+the same request proved alone and the oracle's proof of it, under overlap and
+under key eviction."""
 import random
 
 import pytest
@@ -50,9 +51,11 @@ def test_served_results_equal_proofs_alone(backend, keys, lanes, budget):
     assert st["completed"] == len(jobs)
     if budget:
         assert st["evicted"] > 0
+    oks = [O.Zkey(zk) for _, zk in keys]
     for p, i, w, r, s in got:
         assert p == alone(backend, keys[i][1], w, r, s)
-        ok = O.Zkey(keys[i][1])
+        ok = oks[i]
+        assert p.to_bytes() == ok.prove(w, O.from_bytes(r), O.from_bytes(s))
         assert ok.verify(w[32:32 * (1 + ok.n_public)], p.to_bytes())
 
 

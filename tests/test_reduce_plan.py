@@ -5,7 +5,7 @@ For every window width the prover and the standalone MSM can use, over G1 and
 G2 and both piece targets, the plan must cover every bucket exactly once
 (pieces x seg = B, blocks x 2^lb >= pieces), keep seg a power of two no larger
 than 32, take the direct path only for at most two blocks in all, and give a
-prover MSM result that fits the prover's 8 KiB readback slot per MSM.
+prover MSM result that fits the prover's readback slot per MSM (MSM_RESULT_SLOT_BYTES).
 """
 import os
 import shutil
@@ -19,6 +19,7 @@ PROBE = r"""
 #include <cstdio>
 #include "msm.cuh"
 int main() {
+    printf("%zu\n", g16::MSM_RESULT_SLOT_BYTES);
     unsigned sets, B, g2;
     unsigned long long target;
     while (scanf("%u %u %u %llu", &sets, &B, &g2, &target) == 4) {
@@ -45,8 +46,9 @@ def plan():
     def run(cases):
         text = "\n".join("%d %d %d %d" % c for c in cases) + "\n"
         out = subprocess.run([exe], input=text, capture_output=True, text=True, check=True).stdout.split("\n")
+        run.slot_bytes = int(out[0])
         keys = ("seg", "lb", "nb", "hb", "direct", "set_terms", "block_points", "result_points")
-        return [dict(zip(keys, map(int, l.split()))) for l in out if l.strip()]
+        return [dict(zip(keys, map(int, l.split()))) for l in out[1:] if l.strip()]
     yield run
     shutil.rmtree(d, ignore_errors=True)
 
@@ -78,8 +80,11 @@ def test_plans_cover_every_bucket(plan):
 
 
 def test_prover_results_fit_the_readback_slot(plan):
-    # the prover reads each MSM's result into an 8 KiB pinned slot; its windows share one
-    # bucket set, with c up to 22 and either target (the H MSM uses the larger one)
+    # the prover reads each MSM's result into a pinned slot of MSM_RESULT_SLOT_BYTES; its
+    # windows share one bucket set, with c up to 22 and either target (the H MSM uses the
+    # larger one)
     cases = [(1, 1 << (c - 1), g2, t) for c in range(1, 23) for g2 in (0, 1) for t in (8192, 32768)]
-    for (_, _, g2, _), p in zip(cases, plan(cases)):
-        assert p["result_points"] * (256 if g2 else 128) <= 32 * 256
+    results = plan(cases)
+    assert plan.slot_bytes == 32 * 256
+    for (_, _, g2, _), p in zip(cases, results):
+        assert p["result_points"] * (256 if g2 else 128) <= plan.slot_bytes
