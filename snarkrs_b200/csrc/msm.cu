@@ -9,6 +9,9 @@
 
 namespace g16d {
 
+using g16::MSM_DEAD;
+using g16::MSM_MAX_SETS;
+
 // Bits [off, off + width) of a 256-bit little-endian scalar held in shared
 // memory (8 words, row stride 9 to spread banks); reads past bit 255 are 0.
 __device__ __forceinline__ uint32_t read_bits(const uint32_t* s, int off, int width) {
@@ -92,6 +95,92 @@ __global__ void __launch_bounds__(256) k_scatter(const uint4* __restrict__ scala
         if (key != NO_KEY && (int)lane == leader) base = atomicAdd(&cursor[key], (uint32_t)__popc(mask));
         base = __shfl_sync(0xffffffffu, base, leader);
         if (key != NO_KEY) entries[base + __popc(mask & lt)] = ((uint32_t)w * ew + i) | (d < 0 ? 0x80000000u : 0u);
+    }
+}
+
+// ---- one scalar vector sorted for several live sets (the prover's witness MSMs) ----
+// Set j keeps scalar i when rank[j][i] != MSM_DEAD; its entries name row
+// rank[j][i] of the set's own window-shifted table: w * rows[j] + rank[j][i].
+// The digits are computed once and sorted into every set the scalar is live
+// in, so a base at infinity never becomes an entry (a lockstep step of the
+// accumulate that adds nothing).
+struct LiveSetArgs {
+    const uint32_t* rank[MSM_MAX_SETS];
+    uint32_t* counts[MSM_MAX_SETS];
+    uint32_t* cursor[MSM_MAX_SETS];
+    uint32_t* entries[MSM_MAX_SETS];
+    uint32_t rows[MSM_MAX_SETS];
+};
+
+__global__ void __launch_bounds__(256) k_digits_count_sets(const uint4* __restrict__ scalars, int mont, uint32_t n,
+                                                           int c, int W, uint32_t sink, int nsets, LiveSetArgs a,
+                                                           uint4* __restrict__ scalars_std) {
+    __shared__ uint32_t sh[256 * 9];
+    uint32_t i = blockIdx.x * 256 + threadIdx.x;
+    bool valid = i < n;
+    Fr s = Fr::zero();
+    bool live[MSM_MAX_SETS];
+#pragma unroll
+    for (int j = 0; j < MSM_MAX_SETS; j++) live[j] = valid && j < nsets && __ldg(a.rank[j] + i) != MSM_DEAD;
+    if (valid) {
+        uint4 x = __ldg(scalars + 2 * (size_t)i), y = __ldg(scalars + 2 * (size_t)i + 1);
+        s.v[0] = x.x; s.v[1] = x.y; s.v[2] = x.z; s.v[3] = x.w;
+        s.v[4] = y.x; s.v[5] = y.y; s.v[6] = y.z; s.v[7] = y.w;
+        if (mont) s = from_mont(s);
+        scalars_std[2 * (size_t)i] = make_uint4(s.v[0], s.v[1], s.v[2], s.v[3]);
+        scalars_std[2 * (size_t)i + 1] = make_uint4(s.v[4], s.v[5], s.v[6], s.v[7]);
+    }
+    uint32_t* row = sh + threadIdx.x * 9;
+#pragma unroll
+    for (int j = 0; j < 8; j++) row[j] = s.v[j];
+    unsigned lane = threadIdx.x & 31;
+    for (int w = 0; w < W; w++) {
+        int d = signed_digit(row, w, c);
+        uint32_t key = d != 0 ? (uint32_t)(d < 0 ? -d : d) - 1u : sink;
+#pragma unroll
+        for (int j = 0; j < MSM_MAX_SETS; j++) {
+            if (j >= nsets) break;
+            uint32_t kj = live[j] ? key : NO_KEY;
+            unsigned mask = __match_any_sync(0xffffffffu, kj);
+            if (kj != NO_KEY && lane == (unsigned)(__ffs(mask) - 1)) atomicAdd(&a.counts[j][kj], (uint32_t)__popc(mask));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_scatter_sets(const uint4* __restrict__ scalars_std, uint32_t n, int c, int W,
+                                                      uint32_t sink, int nsets, LiveSetArgs a) {
+    __shared__ uint32_t sh[256 * 9];
+    uint32_t i = blockIdx.x * 256 + threadIdx.x;
+    bool valid = i < n;
+    uint32_t rank[MSM_MAX_SETS];
+#pragma unroll
+    for (int j = 0; j < MSM_MAX_SETS; j++) rank[j] = valid && j < nsets ? __ldg(a.rank[j] + i) : MSM_DEAD;
+    uint32_t* row = sh + threadIdx.x * 9;
+    if (valid) {
+        uint4 x = scalars_std[2 * (size_t)i], y = scalars_std[2 * (size_t)i + 1];
+        row[0] = x.x; row[1] = x.y; row[2] = x.z; row[3] = x.w;
+        row[4] = y.x; row[5] = y.y; row[6] = y.z; row[7] = y.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; j++) row[j] = 0;
+    }
+    unsigned lane = threadIdx.x & 31;
+    unsigned lt = (1u << lane) - 1u;
+    for (int w = 0; w < W; w++) {
+        int d = signed_digit(row, w, c);
+        uint32_t key = d != 0 ? (uint32_t)(d < 0 ? -d : d) - 1u : sink;
+        const uint32_t sign = d < 0 ? 0x80000000u : 0u;
+#pragma unroll
+        for (int j = 0; j < MSM_MAX_SETS; j++) {
+            if (j >= nsets) break;
+            uint32_t kj = rank[j] != MSM_DEAD ? key : NO_KEY;
+            unsigned mask = __match_any_sync(0xffffffffu, kj);
+            int leader = __ffs(mask) - 1;
+            uint32_t base = 0;
+            if (kj != NO_KEY && (int)lane == leader) base = atomicAdd(&a.cursor[j][kj], (uint32_t)__popc(mask));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (kj != NO_KEY) a.entries[j][base + __popc(mask & lt)] = ((uint32_t)w * a.rows[j] + rank[j]) | sign;
+        }
     }
 }
 
@@ -894,6 +983,98 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
                                                        s.d_counts, s.d_fat_list, s.d_total + 2, s.d_total);
     }
     G16_CUDA(scan(s.d_counts, s.d_seg_base, s.Ks, s.d_scan_tmp, s.d_total + 1, st));
+    return cudaSuccess;
+}
+
+cudaError_t msm_sort_sets(MsmSort* sorts, const MsmLiveSets& sets, const void* d_scalars, size_t n, bool montgomery,
+                          int c, cudaStream_t st, bool constant_work) {
+    if (sets.count < 1 || sets.count > MSM_MAX_SETS) {
+        set_error("%d live sets (1 to %d)", sets.count, MSM_MAX_SETS);
+        return cudaErrorInvalidValue;
+    }
+    if (c < 4 || c > 24) {
+        set_error("MSM window of %d bits outside [4, 24]", c);
+        return cudaErrorInvalidValue;
+    }
+    const int W = (255 + c - 1) / c;
+    if (n >= 0x80000000ull) {
+        set_error("MSM of %zu scalars exceeds the 2^31 index limit", n);
+        return cudaErrorInvalidValue;
+    }
+    LiveSetArgs a = {};
+    for (int j = 0; j < sets.count; j++) {
+        MsmSort& s = sorts[j];
+        s.c = c;
+        s.W = W;
+        s.B = 1u << (c - 1);
+        s.shared = true;
+        s.K = s.B;
+        s.constant_work = constant_work;
+        s.Ks = s.K + (constant_work ? 1u : 0u);
+        s.n = sets.rows[j];
+        s.chunk = 16;
+        if ((size_t)sets.rows[j] * (size_t)W >= 0x80000000ull || sets.rows[j] > n) {
+            set_error("live set of %u rows x %d windows exceeds the 2^31 entry-index limit", sets.rows[j], W);
+            return cudaErrorInvalidValue;
+        }
+        const size_t kk = (size_t)s.Ks + 1;
+        if (kk > s.cap_k || !s.d_counts) {
+            size_t cap = 0;
+            G16_CUDA(grow(s.d_counts, cap, kk));
+            cap = 0;
+            G16_CUDA(grow(s.d_offsets, cap, kk));
+            cap = 0;
+            G16_CUDA(grow(s.d_cursor, cap, kk));
+            cap = 0;
+            G16_CUDA(grow(s.d_seg_base, cap, kk));
+            cap = 0;
+            G16_CUDA(grow(s.d_fat_list, cap, kk));
+            s.cap_k = cap;
+        }
+        G16_CUDA(grow(s.d_scan_tmp, s.cap_tmp, kk / 1024 + 2));
+        G16_CUDA(grow(s.d_entries, s.cap_entries, (size_t)(sets.rows[j] ? sets.rows[j] : 1) * W));
+        if (!s.d_total) G16_CUDA(g16::dev_malloc((void**)&s.d_total, 4 * sizeof(uint32_t)));
+        G16_CUDA(cudaMemsetAsync(s.d_counts, 0, kk * sizeof(uint32_t), st));
+        G16_CUDA(cudaMemsetAsync(s.d_total, 0, 4 * sizeof(uint32_t), st));
+        a.rank[j] = sets.d_rank[j];
+        a.counts[j] = s.d_counts;
+        a.cursor[j] = s.d_cursor;
+        a.entries[j] = s.d_entries;
+        a.rows[j] = sets.rows[j];
+    }
+    // the standard-form copy of the scalars, shared by the sets, lives in the first
+    MsmSort& s0 = sorts[0];
+    G16_CUDA(grow(s0.d_scalars_std, s0.cap_scalars, (n ? n : 1) * 8));
+    const uint32_t sink = constant_work ? sorts[0].K : NO_KEY;
+    if (n) {
+        timer().add_bytes("msm_digits", 64.0 * n);   // scalars in, standard-form copy out
+        TimedLaunch tl("msm_digits", st);
+        k_digits_count_sets<<<blocks_for(n, 256), 256, 0, st>>>((const uint4*)d_scalars, montgomery ? 1 : 0,
+                                                               (uint32_t)n, c, W, sink, sets.count, a,
+                                                               (uint4*)s0.d_scalars_std);
+    }
+    G16_CUDA(cudaGetLastError());
+    for (int j = 0; j < sets.count; j++) {
+        MsmSort& s = sorts[j];
+        G16_CUDA(scan(s.d_counts, s.d_offsets, s.Ks, s.d_scan_tmp, s.d_total, st));
+        TimedLaunch tl("msm_copy", st);
+        k_copy_u32<<<blocks_for(s.Ks, 256), 256, 0, st>>>(s.d_cursor, s.d_offsets, s.Ks);
+    }
+    if (n) {
+        TimedLaunch tl("msm_scatter", st);
+        k_scatter_sets<<<blocks_for(n, 256), 256, 0, st>>>((const uint4*)s0.d_scalars_std, (uint32_t)n, c, W, sink,
+                                                          sets.count, a);
+    }
+    G16_CUDA(cudaGetLastError());
+    for (int j = 0; j < sets.count; j++) {
+        MsmSort& s = sorts[j];
+        {
+            TimedLaunch tl("msm_nseg", st);
+            k_nseg<<<blocks_for(s.Ks, 256), 256, 0, st>>>(s.d_offsets, s.Ks, s.K, s.chunk, accumulate_wave(),
+                                                           s.d_counts, s.d_fat_list, s.d_total + 2, s.d_total);
+        }
+        G16_CUDA(scan(s.d_counts, s.d_seg_base, s.Ks, s.d_scan_tmp, s.d_total + 1, st));
+    }
     return cudaSuccess;
 }
 

@@ -142,6 +142,25 @@ int msm_window_bits(size_t m);
 cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomery, int c, cudaStream_t st,
                      bool shared_windows = false, bool constant_work = false);
 
+// One scalar vector sorted for several MSMs over window-shifted tables whose
+// bases differ in which are at infinity (the prover's witness MSMs: A; B1 and
+// B2; L).  Set j keeps scalar i when d_rank[j][i] != MSM_DEAD, and its entries
+// name row d_rank[j][i] of the set's own table of rows[j] bases (infinity
+// bases compacted out): entry w * rows[j] + d_rank[j][i].  The digits are
+// computed once and each lands in every set its scalar is live in, so a base
+// at infinity costs no accumulate step (the reference's prescan and key_live:
+// crates/msm/src/lib.rs:534-563, crates/cuda/src/msm.rs:1308).  sorts[j] gets
+// set j's sort, as msm_sort(shared_windows = true) would give for it.
+constexpr uint32_t MSM_DEAD = 0xffffffffu;
+constexpr int MSM_MAX_SETS = 3;
+struct MsmLiveSets {
+    int count = 0;
+    const uint32_t* d_rank[MSM_MAX_SETS] = {nullptr, nullptr, nullptr};
+    uint32_t rows[MSM_MAX_SETS] = {0, 0, 0};
+};
+cudaError_t msm_sort_sets(MsmSort* sorts, const MsmLiveSets& sets, const void* d_scalars, size_t n, bool montgomery,
+                          int c, cudaStream_t st, bool constant_work = false);
+
 // Window count for c-bit signed digits over 255 bits.
 inline int msm_windows(int c) { return (255 + c - 1) / c; }
 // Window width for window-shifted bases: the cost is ~m * ceil(255/c) mixed

@@ -165,7 +165,7 @@ struct Workspace {
     void* d_w = nullptr;       // witness, n_vars Fr
     void* d_abc = nullptr;     // A | B | C, n Fr each
     void* d_hpoly = nullptr;   // H, n Fr
-    MsmSort sort_w, sort_h;
+    MsmSort sort_w[3], sort_h;  // witness sorts: the A, B (B1 and B2) and L live sets
     MsmAccum acc[5];           // A, B2, B1, L, H
     uint8_t* h_win = nullptr;  // pinned readback of the MSM results
     unsigned long long* h_work = nullptr;
@@ -203,7 +203,7 @@ struct Workspace {
         cudaFree(d_w);
         cudaFree(d_abc);
         cudaFree(d_hpoly);
-        sort_w.release();
+        for (auto& x : sort_w) x.release();
         sort_h.release();
         for (auto& a : acc) a.release();
         if (h_win) cudaFreeHost(h_win);
@@ -227,8 +227,12 @@ struct g16_circuit {
     // resident key
     uint32_t *d_rp[2] = {nullptr, nullptr}, *d_sig[2] = {nullptr, nullptr}, *d_vid[2] = {nullptr, nullptr};
     void* d_values = nullptr;
+    // the witness MSMs' bases with the points at infinity compacted out: A over
+    // the A live set, B1 and B2 over the B set, L over the L set (live_sets)
     void *d_a = nullptr, *d_b1 = nullptr, *d_b2 = nullptr, *d_l = nullptr, *d_h = nullptr;
-    // window-shifted base tables 2^(c w) P_i at w * N + i (msm_window_table)
+    uint32_t* d_rank[3] = {nullptr, nullptr, nullptr};   // wire -> row in the set's bases, or MSM_DEAD
+    uint32_t rows[3] = {0, 0, 0};                        // live wires of the A, B and L sets
+    // window-shifted base tables 2^(c w) P_i at w * rows + i (msm_window_table)
     void *t_a = nullptr, *t_b1 = nullptr, *t_b2 = nullptr, *t_l = nullptr, *t_h = nullptr;
     int c_w = 0, c_h = 0;   // window bits of the witness and H MSMs
     NttTables ntt;
@@ -301,13 +305,14 @@ cudaError_t circuit_alloc(g16_circuit* c, void** p, size_t bytes) {
 }
 
 // Device bytes of one workspace: witness, A|B|C, H, and the MSM scratch
-// (sorted entries, partial sums, bucket sums) at window bits c_w and c_h.
-uint64_t workspace_estimate(uint64_t nv, uint64_t n, int c_w, int c_h) {
+// (sorted entries, partial sums, bucket sums) at window bits c_w and c_h, for
+// live sets of ra (A), rb (B1, B2) and rl (L) wires.
+uint64_t workspace_estimate(uint64_t nv, uint64_t n, int c_w, int c_h, uint64_t ra, uint64_t rb, uint64_t rl) {
     const uint64_t Ww = (uint64_t)msm_windows(c_w), Wh = (uint64_t)msm_windows(c_h);
     const uint64_t Kw = 1ull << (c_w - 1), Kh = 1ull << (c_h - 1);
     uint64_t b = nv * 32 + n * 32 * 4;
-    b += nv * 32 + nv * Ww * 4 + 24 * (Kw + 1) + n * 32 + n * Wh * 4 + 24 * (Kh + 1);
-    b += 3 * 128 * (Kw * 2 + nv * Ww / 16 + 1) + 256 * (Kw * 2 + nv * Ww / 16 + 1);
+    b += nv * 32 + (ra + rb + rl) * Ww * 4 + 3 * 24 * (Kw + 1) + n * 32 + n * Wh * 4 + 24 * (Kh + 1);
+    b += 128 * (3 * Kw * 2 + (ra + rb + rl) * Ww / 16 + 3) + 256 * (Kw * 2 + rb * Ww / 16 + 1);
     b += 128 * (Kh * 2 + n * Wh / 16 + 1) + (16ull << 20);
     return b;
 }
@@ -325,30 +330,37 @@ void circuit_free_alloc(g16_circuit* c, void* p, uint64_t bytes) {
 }
 
 // (Re)build the window-shifted tables of the witness MSMs (A, B1, L, B2) for
-// window bits cw; the new tables replace the old ones only when all are built.
+// window bits cw, each over its live set's compacted bases; the new tables
+// replace the old ones only when all are built.
 int build_witness_tables(g16_circuit* c, int cw, cudaStream_t st) {
-    const uint64_t nv = c->n_vars, W = (uint64_t)msm_windows(cw);
-    if (nv * W >= 0x80000000ull) return fail(G16_ERR_BACKEND, "circuit too large for 31-bit MSM entry indices");
+    const uint64_t W = (uint64_t)msm_windows(cw);
+    const uint64_t ra = c->rows[0], rb = c->rows[1], rl = c->rows[2];
+    if (std::max(ra, std::max(rb, rl)) * W >= 0x80000000ull)
+        return fail(G16_ERR_BACKEND, "circuit too large for 31-bit MSM entry indices");
     void *ta = nullptr, *tb1 = nullptr, *tl = nullptr, *tb2 = nullptr;
-    cudaError_t e = circuit_alloc(c, &ta, 64 * nv * W);
-    if (e == cudaSuccess) e = circuit_alloc(c, &tb1, 64 * nv * W);
-    if (e == cudaSuccess) e = circuit_alloc(c, &tl, 64 * nv * W);
-    if (e == cudaSuccess) e = circuit_alloc(c, &tb2, 128 * nv * W);
-    if (e == cudaSuccess) e = msm_window_table_g1(c->d_a, nv, 0, cw, ta, st);
-    if (e == cudaSuccess) e = msm_window_table_g1(c->d_b1, nv, 0, cw, tb1, st);
-    if (e == cudaSuccess) e = msm_window_table_g1(c->d_l, nv, c->n_public + 1, cw, tl, st);
-    if (e == cudaSuccess) e = msm_window_table_g2(c->d_b2, nv, 0, cw, tb2, st);
+    cudaError_t e = circuit_alloc(c, &ta, 64 * ra * W);
+    if (e == cudaSuccess) e = circuit_alloc(c, &tb1, 64 * rb * W);
+    if (e == cudaSuccess) e = circuit_alloc(c, &tl, 64 * rl * W);
+    if (e == cudaSuccess) e = circuit_alloc(c, &tb2, 128 * rb * W);
+    if (e == cudaSuccess && ra) e = msm_window_table_g1(c->d_a, ra, 0, cw, ta, st);
+    if (e == cudaSuccess && rb) e = msm_window_table_g1(c->d_b1, rb, 0, cw, tb1, st);
+    if (e == cudaSuccess && rl) e = msm_window_table_g1(c->d_l, rl, 0, cw, tl, st);
+    if (e == cudaSuccess && rb) e = msm_window_table_g2(c->d_b2, rb, 0, cw, tb2, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         int rc = cuda_fail(e, "window tables");
-        for (void* p : {ta, tb1, tl}) circuit_free_alloc(c, p, 64 * nv * W);
-        circuit_free_alloc(c, tb2, 128 * nv * W);
+        circuit_free_alloc(c, ta, 64 * ra * W);
+        circuit_free_alloc(c, tb1, 64 * rb * W);
+        circuit_free_alloc(c, tl, 64 * rl * W);
+        circuit_free_alloc(c, tb2, 128 * rb * W);
         return rc;
     }
     if (c->c_w) {
         const uint64_t Wo = (uint64_t)msm_windows(c->c_w);
-        for (void* p : {c->t_a, c->t_b1, c->t_l}) circuit_free_alloc(c, p, 64 * nv * Wo);
-        circuit_free_alloc(c, c->t_b2, 128 * nv * Wo);
+        circuit_free_alloc(c, c->t_a, 64 * ra * Wo);
+        circuit_free_alloc(c, c->t_b1, 64 * rb * Wo);
+        circuit_free_alloc(c, c->t_l, 64 * rl * Wo);
+        circuit_free_alloc(c, c->t_b2, 128 * rb * Wo);
     }
     c->t_a = ta;
     c->t_b1 = tb1;
@@ -545,20 +557,27 @@ int run_h(g16_circuit* c, Workspace* ws, const void* d_w, void* h_out) {
 constexpr size_t WIN_SLOT = MSM_RESULT_SLOT_BYTES;
 
 int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
-    const uint32_t nw = c->n_vars * (uint32_t)msm_windows(c->c_w);
+    const uint32_t W = (uint32_t)msm_windows(c->c_w);
     cudaStream_t st[4];
     for (int i = 0; i < 4; i++) st[i] = c->serial ? ws->stream : ws->side[i];
     CK(cudaEventRecord(ws->ev_fork, ws->stream), "event");
     CK(cudaStreamWaitEvent(st[0], ws->ev_fork, 0), "stream wait");
-    CK(msm_sort(ws->sort_w, d_w, c->n_vars, true, c->c_w, st[0], true, c->be->constant_work), "witness sort");
+    // one pass over the witness digits sorts the A, B and L live sets
+    MsmLiveSets sets;
+    sets.count = 3;
+    for (int j = 0; j < 3; j++) {
+        sets.d_rank[j] = c->d_rank[j];
+        sets.rows[j] = c->rows[j];
+    }
+    CK(msm_sort_sets(ws->sort_w, sets, d_w, c->n_vars, true, c->c_w, st[0], c->be->constant_work), "witness sort");
     CK(cudaEventRecord(ws->ev_sort, st[0]), "event");
     for (int i = 1; i < 4; i++) CK(cudaStreamWaitEvent(st[i], ws->ev_sort, 0), "stream wait");
     // acc slots: 0 A, 1 B2, 2 B1, 3 L (4 is H); one stream per MSM so that
     // their latency-bound reduction tails run side by side
-    CK(msm_accumulate_g1(ws->sort_w, ws->acc[0], c->t_a, 0, nw, st[0]), "A accumulate");
-    CK(msm_accumulate_g1(ws->sort_w, ws->acc[2], c->t_b1, 0, nw, st[1]), "B1 accumulate");
-    CK(msm_accumulate_g1(ws->sort_w, ws->acc[3], c->t_l, 0, nw, st[2]), "L accumulate");
-    CK(msm_accumulate_g2(ws->sort_w, ws->acc[1], c->t_b2, 0, nw, st[3]), "B2 accumulate");
+    CK(msm_accumulate_g1(ws->sort_w[0], ws->acc[0], c->t_a, 0, c->rows[0] * W, st[0]), "A accumulate");
+    CK(msm_accumulate_g1(ws->sort_w[1], ws->acc[2], c->t_b1, 0, c->rows[1] * W, st[1]), "B1 accumulate");
+    CK(msm_accumulate_g1(ws->sort_w[2], ws->acc[3], c->t_l, 0, c->rows[2] * W, st[2]), "L accumulate");
+    CK(msm_accumulate_g2(ws->sort_w[1], ws->acc[1], c->t_b2, 0, c->rows[1] * W, st[3]), "B2 accumulate");
     const int stream_of[4] = {0, 3, 1, 2};   // acc slot -> stream
     for (int i = 0; i < 4; i++) {
         cudaStream_t s_i = st[stream_of[i]];
@@ -828,7 +847,7 @@ struct TuningLock {
                 w->graph = nullptr;
                 w->proofs = 0;
             }
-            c->ws_estimate = workspace_estimate(c->n_vars, c->n, c->c_w, c->c_h);
+            c->ws_estimate = workspace_estimate(c->n_vars, c->n, c->c_w, c->c_h, c->rows[0], c->rows[1], c->rows[2]);
         }
         {
             std::lock_guard<std::mutex> g(c->mu);
@@ -890,6 +909,48 @@ double time_concurrent(g16_circuit* c, const std::vector<Workspace*>& all, int r
     }
     for (auto& x : ev) cudaEventDestroy(x);
     return best == -2.0 ? -1.0 : best;
+}
+
+// The witness MSMs' live sets, computed on the host at prepare: per set the
+// compacted bases and, per wire, its row in them (MSM_DEAD where its base is
+// the point at infinity).  Set 0 is A, 1 is B (B1 and B2), 2 is L.
+struct LiveSetsHost {
+    std::vector<uint8_t> a, b1, b2, l;
+    std::vector<uint32_t> rank[3];
+    uint32_t rows[3] = {0, 0, 0};
+};
+
+bool all_zero(const uint8_t* p, size_t bytes) {
+    for (size_t i = 0; i < bytes; i++)
+        if (p[i]) return false;
+    return true;
+}
+
+LiveSetsHost live_sets(const g16_zkey_view& k) {
+    LiveSetsHost r;
+    const size_t nv = k.n_vars, first = (size_t)k.n_public + 1;
+    for (auto& x : r.rank) x.assign(nv, MSM_DEAD);
+    for (size_t i = 0; i < nv; i++) {
+        const uint8_t* a = k.a_query + 64 * i;
+        if (!all_zero(a, 64)) {
+            r.rank[0][i] = r.rows[0]++;
+            r.a.insert(r.a.end(), a, a + 64);
+        }
+        const uint8_t *b1 = k.b_g1_query + 64 * i, *b2 = k.b_g2_query + 128 * i;
+        if (!all_zero(b1, 64) || !all_zero(b2, 128)) {
+            r.rank[1][i] = r.rows[1]++;
+            r.b1.insert(r.b1.end(), b1, b1 + 64);
+            r.b2.insert(r.b2.end(), b2, b2 + 128);
+        }
+        if (i >= first) {
+            const uint8_t* l = k.l_query + 64 * (i - first);
+            if (!all_zero(l, 64)) {
+                r.rank[2][i] = r.rows[2]++;
+                r.l.insert(r.l.end(), l, l + 64);
+            }
+        }
+    }
+    return r;
 }
 
 bool window_bits_ok(int b) { return b >= 8 && b <= 20; }
@@ -1069,16 +1130,24 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
             if (k->value_id[m][i] >= k->n_values) return fail(G16_ERR_BACKEND, "matrix %d nonzero %u references value %u", m, i, k->value_id[m][i]);
         }
     }
-    uint64_t nv = k->n_vars, nl = nv - k->n_public - 1;
+    uint64_t nv = k->n_vars;
+    // live sets (the reference's key_live, crates/cuda/src/msm.rs:1308, and
+    // prescan's infinity filter, crates/msm/src/lib.rs:554-563): a wire whose
+    // base is the point at infinity adds nothing to that MSM, so its bases are
+    // compacted out and its digits never become entries.  A: a_query finite;
+    // B: b_g1_query or b_g2_query finite (B1 and B2 share one sort); L: a
+    // private wire whose l_query point is finite.
+    LiveSetsHost live = live_sets(*k);
+    const uint64_t ra = live.rows[0], rb = live.rows[1], rl = live.rows[2];
     // memory budget, refused before any allocation (backend.rs:367-381)
-    uint64_t key_bytes = 4ull * (n + 1) * 2 + 8ull * (k->nnz[0] + k->nnz[1]) + 32ull * k->n_values + nv * 64 * 2 +
-                         nv * 128 + nl * 64 + (uint64_t)n * 64 + (uint64_t)n * 32 * 2 + 32;
+    uint64_t key_bytes = 4ull * (n + 1) * 2 + 8ull * (k->nnz[0] + k->nnz[1]) + 32ull * k->n_values + ra * 64 +
+                         rb * (64 + 128) + rl * 64 + 12 * nv + (uint64_t)n * 64 + (uint64_t)n * 32 * 2 + 32;
     const int c_w = msm_shared_window_bits(nv / 2 + 1), c_h = msm_shared_window_bits(n);
     const uint64_t Ww = (uint64_t)msm_windows(c_w), Wh = (uint64_t)msm_windows(c_h);
     if (nv * Ww >= 0x80000000ull || (uint64_t)n * Wh >= 0x80000000ull)
         return fail(G16_ERR_BACKEND, "circuit too large for 31-bit MSM entry indices");
-    key_bytes += nv * Ww * (64 * 3 + 128) + (uint64_t)n * Wh * 64;
-    const uint64_t ws_bytes = workspace_estimate(nv, n, c_w, c_h);
+    key_bytes += (ra + rl) * Ww * 64 + rb * Ww * (64 + 128) + (uint64_t)n * Wh * 64;
+    const uint64_t ws_bytes = workspace_estimate(nv, n, c_w, c_h, ra, rb, rl);
     if (b->vram_used + key_bytes + ws_bytes > b->vram_limit)
         return fail(G16_ERR_DEVICE_MEMORY, "circuit needs about %llu MiB of device memory, %llu MiB of the %llu MiB budget are free",
                     (unsigned long long)((key_bytes + ws_bytes) >> 20),
@@ -1090,6 +1159,7 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
     c->n_public = k->n_public;
     c->n = n;
     c->ws_estimate = ws_bytes;
+    for (int j = 0; j < 3; j++) c->rows[j] = live.rows[j];
     if (const char* g = std::getenv("G16_CUDA_GRAPHS")) c->graphs = std::strcmp(g, "0") != 0;
     while ((1u << c->log_n) < n) c->log_n++;
     if (!unpack(c->alpha1, k->alpha_g1) || !unpack(c->beta1, k->beta_g1) || !unpack(c->delta1, k->delta_g1) ||
@@ -1116,10 +1186,13 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
         {(void**)&c->d_vid[0], k->value_id[0], 4ull * k->nnz[0]},
         {(void**)&c->d_vid[1], k->value_id[1], 4ull * k->nnz[1]},
         {&c->d_values, k->values, 32ull * k->n_values},
-        {&c->d_a, k->a_query, 64ull * nv},
-        {&c->d_b1, k->b_g1_query, 64ull * nv},
-        {&c->d_b2, k->b_g2_query, 128ull * nv},
-        {&c->d_l, k->l_query, 64ull * nl},
+        {&c->d_a, live.a.data(), live.a.size()},
+        {&c->d_b1, live.b1.data(), live.b1.size()},
+        {&c->d_b2, live.b2.data(), live.b2.size()},
+        {&c->d_l, live.l.data(), live.l.size()},
+        {(void**)&c->d_rank[0], live.rank[0].data(), 4ull * nv},
+        {(void**)&c->d_rank[1], live.rank[1].data(), 4ull * nv},
+        {(void**)&c->d_rank[2], live.rank[2].data(), 4ull * nv},
         {&c->d_h, k->h_query, 64ull * n},
     };
     g16_circuit* cp = c.get();

@@ -267,3 +267,30 @@ def test_device_key_generation_is_the_host_one(backend):
         host = S.SynthCircuit(seed=808 + nc, n_constraints=nc, n_inputs=40, n_public=npub).zkey(99)
         dev = S.SynthCircuit(seed=808 + nc, n_constraints=nc, n_inputs=40, n_public=npub).zkey(99, device=0)
         assert dev == host
+
+
+def test_live_sets_with_every_base_at_infinity(backend, circuits):
+    """The witness MSMs skip wires whose base is the point at infinity (the reference's
+    prescan and key_live).  With every B query base at infinity the B live set is empty:
+    B1 and B2 come out at infinity and the A, L and H outputs are those of the intact key;
+    with every A base at infinity as well, A is at infinity too."""
+    import ctypes
+    sc, zk, ok = circuits["small"]
+    w = sc.witness(4)
+    intact = backend.prepare(S.ProvingKey.from_bytes(zk)).h_and_msms(w).as_dict()
+    assert intact == ok.msms(w, ok.compute_h(w))
+    pk = S.ProvingKey.from_bytes(zk)
+    nv = pk.n_vars
+    ctypes.memset(ctypes.addressof(pk._view.b_g1_query.contents), 0, 64 * nv)
+    ctypes.memset(ctypes.addressof(pk._view.b_g2_query.contents), 0, 128 * nv)
+    circ = backend.prepare(pk)
+    got = circ.h_and_msms(w).as_dict()
+    assert got["b_g1"] == bytes(64) and got["b_g2"] == bytes(128)
+    assert all(got[k] == intact[k] for k in ("a_g1", "l_g1", "h_g1"))
+    circ.close()
+    ctypes.memset(ctypes.addressof(pk._view.a_query.contents), 0, 64 * nv)
+    circ = backend.prepare(pk)
+    got = circ.h_and_msms(w).as_dict()
+    assert got["a_g1"] == bytes(64) and got["b_g1"] == bytes(64)
+    assert got["l_g1"] == intact["l_g1"] and got["h_g1"] == intact["h_g1"]
+    circ.close()
