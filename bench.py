@@ -20,8 +20,10 @@ MSMs, blinding and assembly).  Every step proves a different witness.
   cpu_baseline  the CPU oracle (a C restatement of the reference's CPU
           prover) proving the same circuit on this host's cores.
 
-`--impl reference` times that CPU restatement alone (the reference is Rust
-and cannot be built on this image), rank 0 only.
+`--impl reference` times the reference's CPU prover restated in C (the
+reference is Rust and cannot be built on this image): the faithful port of its
+fast algorithms (oracle/port_*.c), on inputs from the oracle's own generator,
+rank 0 only; that arm loads no product code.
 """
 import argparse
 import json
@@ -35,6 +37,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+R_MOD = 21888242871839275222246405745257275088548364400416034343698204186575808495617
 N_CONSTRAINTS = 1_100_000
 N_INPUTS, N_PUBLIC = 256, 16
 CIRCUIT_SEED, TOXIC_SEED = 21, 0x5EED
@@ -139,11 +142,37 @@ def workload_name(nc, domain, n_vars):
         nc, domain.bit_length() - 1, n_vars)
 
 
+def fr_mont_bytes(x):
+    """A field element of Fr as 32 Montgomery-form bytes."""
+    return ((int(x) << 256) % R_MOD).to_bytes(32, "little")
+
+
 def blinders(i):
     import random
-    import snarkrs_b200 as S
     rng = random.Random(1000 + i)
-    return S.fr_to_mont_bytes(rng.randrange(1, S.R_MOD)), S.fr_to_mont_bytes(rng.randrange(1, S.R_MOD))
+    return fr_mont_bytes(rng.randrange(1, R_MOD)), fr_mont_bytes(rng.randrange(1, R_MOD))
+
+
+# The reference's own published CPU prove of this workload's shape, for context
+# beside the CPU baseline timed here.
+PUBLISHED_CPU = {"ms": 625.7, "proofs_per_s": 1e3 / 625.7,
+                 "what": "reference CPU prover (Rust, AVX-512 IFMA field code), warm anon-aadhaar prove: "
+                         "1,115,080 constraints, domain 2^21, 16-vCPU c7i.4xlarge",
+                 "source": "bench/results/x86-ntt-2026-10-13.md:39"}
+
+
+def host_cpu():
+    """This host's CPU model and logical core count."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count()}
 
 
 class Clocks:
@@ -217,16 +246,21 @@ def make_key(sc, toxic, device_ok=True):
     return sc.zkey(toxic)
 
 
-def synth_key(sc, nc, seed=CIRCUIT_SEED, toxic=TOXIC_SEED, device_ok=True):
-    """The workload's .zkey; cached under /tmp so repeated runs on one host skip the key generation."""
-    path = os.path.join(os.environ.get("G16_BENCH_CACHE", "/tmp"), "g16b200_bench_%d_%d_%d.zkey" % (
-        seed, nc, toxic))
+def key_cache_path(seed, nc, toxic):
+    return os.path.join(os.environ.get("G16_BENCH_CACHE", "/tmp"), "g16b200_bench_%d_%d_%d.zkey" % (seed, nc, toxic))
+
+
+def cached_key(seed, nc, toxic, make):
+    """The workload's .zkey, cached under /tmp so repeated runs on one host skip the key
+    generation.  The product's generator and the oracle's give the same bytes for the same
+    seeds (tests/test_port.py), so either arm may fill the cache for the other."""
+    path = key_cache_path(seed, nc, toxic)
     try:
         with open(path, "rb") as f:
             return f.read()
     except OSError:
         pass
-    zk = make_key(sc, toxic, device_ok)
+    zk = make()
     try:
         with open(path + ".tmp", "wb") as f:
             f.write(zk)
@@ -234,6 +268,11 @@ def synth_key(sc, nc, seed=CIRCUIT_SEED, toxic=TOXIC_SEED, device_ok=True):
     except OSError:
         pass
     return zk
+
+
+def synth_key(sc, nc, seed=CIRCUIT_SEED, toxic=TOXIC_SEED, device_ok=True):
+    """The workload's .zkey from the product's generator (point sections on this rank's GPU)."""
+    return cached_key(seed, nc, toxic, lambda: make_key(sc, toxic, device_ok))
 
 
 def oracle_module():
@@ -274,15 +313,46 @@ def oracle_proofs(zk, jobs):
 
 
 def run_reference(args):
+    """The reference's CPU prover (its fast algorithms restated in C: oracle/port_*.c) on the
+    same workload, on all host threads, with inputs from the oracle's own generator: this arm
+    loads no product code.  Every proof passes the oracle's pairing check, the first equals the
+    oracle's plain prover's proof, and one proof is also timed on one core."""
     rank, _, world = dist_env()
     if rank != 0:
         return
-    import snarkrs_b200 as S
-    sc = S.SynthCircuit(CIRCUIT_SEED, args.constraints, N_INPUTS, N_PUBLIC)
-    zk = synth_key(sc, args.constraints, device_ok=False)   # this arm uses no GPU code at all
-    times, threads = cpu_prove_rate(zk, sc, args.warmup + args.steps)
+    O = oracle_module()
+    sc = O.Synth(CIRCUIT_SEED, args.constraints, N_INPUTS, N_PUBLIC)
+    zk = cached_key(CIRCUIT_SEED, args.constraints, TOXIC_SEED, lambda: sc.zkey(TOXIC_SEED))
+    ok = O.Zkey(zk)
+    port = O.PortProver(ok)
+    threads = O.max_threads()
+    pub = 32 * N_PUBLIC
+    times, verified, first = [], 0, None
+    for i in range(args.warmup + args.steps):
+        seed = witness_seed(0, i)
+        w = sc.witness(seed)
+        r, s = blinders(seed)
+        t0 = time.perf_counter()
+        p = port.prove(w, r, s)
+        times.append(time.perf_counter() - t0)
+        verified += ok.verify(w[32:32 + pub], p)
+        if i == args.warmup:
+            first = (w, r, s, p)
+    w, r, s, p = first
+    exact = p == ok.prove(w, O.from_bytes(r), O.from_bytes(s))
+    O.set_threads(1)
+    t0 = time.perf_counter()
+    port.prove(w, r, s)
+    one_core = time.perf_counter() - t0
+    O.set_threads(threads)
     timed = times[args.warmup:]
     value = len(timed) / sum(timed)
+    cpu = dict(host_cpu(), value=value, unit="proofs/s", cores=threads, kind="port",
+               sample="%d full proofs of the workload (after %d warm-up) by the reference CPU prover's algorithms "
+                      "restated in C (batch-affine MSM fill, five MSMs concurrently, 2^11-blocked intt_coset_ntt), "
+                      "OpenMP over all host threads" % (len(timed), args.warmup),
+               one_core={"value": 1 / one_core, "unit": "proofs/s", "ms": 1e3 * one_core,
+                         "sample": "1 full proof on one thread"})
     line = {
         "impl": "reference", "metric": "proofs/s", "value": value, "unit": "proofs/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(timed) / len(timed),
@@ -290,13 +360,16 @@ def run_reference(args):
         "data": "synthetic",
         "config": {"workload": workload_name(args.constraints, sc.domain_size, sc.n_vars),
                    "n_constraints": args.constraints, "domain": sc.domain_size, "n_vars": sc.n_vars},
-        "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "port",
-                         "sample": "%d full proofs of the workload (after %d warm-up), C restatement of the "
-                                   "reference CPU prover, OpenMP over all host threads" % (len(timed), args.warmup)},
+        "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "p50_ms": 1e3 * statistics.median(timed),
-        "note": "the reference is Rust (ark-* 0.5 not vendored, no cargo here); this arm times the C restatement",
+        "parity": {"pairing_checked": verified, "of": len(times), "bit_exact_vs_oracle": exact},
+        "reference_published_cpu": PUBLISHED_CPU,
+        "note": "the reference is Rust (ark-* 0.5 not vendored, no cargo here); this arm times its CPU prover's "
+                "algorithms restated in C, the portable path without AVX-512 IFMA",
     }
+    port.close()
+    ok.close()
     print(json.dumps(line), flush=True)
 
 
@@ -425,14 +498,27 @@ def run_ours(args):
     cpu = None
     parity = {"pairing_checked": K, "e2e_equals_device_resident": same_e2e}
     if not args.no_oracle_check:
-        # the oracle proves the first timed witness; its time is the CPU baseline's sample
+        # the oracle proves the first timed witness with its r and s
         (want, dt), = oracle_proofs(zk, [(bytes(wits[W].numpy()), bl[W][0], bl[W][1])])[0]
         parity["bit_exact_vs_oracle"] = proofs[0].to_bytes() == want
         parity["oracle_checked"] = "step %d of %d (witness seed %d)" % (W, W + K, witness_seed(rank, W))
-        if not args.no_cpu_baseline and world == 1:
-            cpu = {"value": 1 / dt, "unit": "proofs/s", "cores": oracle_module().max_threads(), "kind": "port",
-                   "sample": "1 full proof of the same workload (the first timed witness) by the C restatement "
-                             "of the reference CPU prover (OpenMP, all host threads), %.1f s" % dt}
+    if not args.no_cpu_baseline and world == 1:
+        # the reference CPU prover's algorithms (oracle/port_*.c) prove the same witness
+        O = oracle_module()
+        ok = O.Zkey(zk)
+        port = O.PortProver(ok)
+        w0 = bytes(wits[W].numpy())
+        t0 = time.perf_counter()
+        got = port.prove(w0, *bl[W])
+        dt = time.perf_counter() - t0
+        parity["cpu_baseline_proof_equal"] = got == proofs[0].to_bytes()
+        cpu = dict(host_cpu(), value=1 / dt, unit="proofs/s", cores=O.max_threads(), kind="port",
+                   sample="1 full proof of the same workload (the first timed witness) by the reference CPU "
+                          "prover's algorithms restated in C (batch-affine MSM fill, five MSMs concurrently, "
+                          "2^11-blocked intt_coset_ntt; OpenMP, all host threads), %.2f s" % dt,
+                   reference_published=PUBLISHED_CPU)
+        port.close()
+        ok.close()
     line = {
         "metric": "proofs/s", "value": value, "unit": "proofs/s", "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

@@ -282,3 +282,120 @@ def verify_vk(alpha, beta, gamma, delta, ic, public_mont, proof):
     if rc < 0:
         raise ValueError("bad verifying key")
     return bool(rc)
+
+
+# ---- the timed CPU baseline (port_*.c) ----
+def _port_lib():
+    L = lib()
+    if not getattr(L, "_port_bound", False):
+        L.oracle_port_prepare.restype = ctypes.c_void_p
+        L.oracle_port_prepare.argtypes = [ctypes.c_void_p]
+        L.oracle_port_free.argtypes = [ctypes.c_void_p]
+        L.oracle_port_prove.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p,
+                                        ctypes.c_char_p, ctypes.c_char_p]
+        L.oracle_port_msm_g1.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p]
+        L.oracle_port_msm_g2.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p]
+        L.oracle_port_intt_coset_ntt.argtypes = [ctypes.c_int, ctypes.c_char_p]
+        L.oracle_synth_new.restype = ctypes.c_void_p
+        L.oracle_synth_new.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
+        L.oracle_synth_free.argtypes = [ctypes.c_void_p]
+        L.oracle_synth_info.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_synth_witness.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p]
+        L.oracle_synth_zkey.restype = ctypes.POINTER(ctypes.c_uint8)
+        L.oracle_synth_zkey.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_size_t)]
+        L.oracle_synth_buffer_free.argtypes = [ctypes.POINTER(ctypes.c_uint8)]
+        L._port_bound = True
+    return L
+
+
+class PortProver:
+    """The reference CPU prover's algorithms restated for speed (batch-affine MSM fill,
+    the five MSMs concurrently, 2^11-blocked intt_coset_ntt): the timed CPU baseline.
+    Its proofs equal the oracle's."""
+
+    def __init__(self, zkey):
+        self.zkey = zkey
+        self._h = _port_lib().oracle_port_prepare(ctypes.c_void_p(zkey._h))
+        if not self._h:
+            raise ValueError("port prepare failed")
+
+    def prove(self, witness_mont, r_mont, s_mont):
+        """r_mont, s_mont: 32-byte Montgomery Fr."""
+        out = ctypes.create_string_buffer(256)
+        rc = _port_lib().oracle_port_prove(ctypes.c_void_p(self._h), bytes(witness_mont),
+                                           ctypes.c_size_t(len(witness_mont) // 32), bytes(r_mont), bytes(s_mont),
+                                           out)
+        if rc != 0:
+            raise ValueError("port prove failed")
+        return out.raw
+
+    def close(self):
+        if self._h:
+            _port_lib().oracle_port_free(ctypes.c_void_p(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def port_msm_g1(bases, scalars_std):
+    out = ctypes.create_string_buffer(64)
+    if _port_lib().oracle_port_msm_g1(bytes(bases), bytes(scalars_std), len(bases) // 64, out) != 0:
+        raise ValueError("bad base")
+    return out.raw
+
+
+def port_msm_g2(bases, scalars_std):
+    out = ctypes.create_string_buffer(128)
+    if _port_lib().oracle_port_msm_g2(bytes(bases), bytes(scalars_std), len(bases) // 128, out) != 0:
+        raise ValueError("bad base")
+    return out.raw
+
+
+def port_intt_coset_ntt(log_n, data):
+    buf = ctypes.create_string_buffer(bytes(data), len(data))
+    if _port_lib().oracle_port_intt_coset_ntt(log_n, buf) != 0:
+        raise ValueError("bad size")
+    return buf.raw
+
+
+class Synth:
+    """The synthetic workload generator restated on the oracle's side (synth.c): the
+    same seeds give the same circuit, witnesses and .zkey bytes as the product's."""
+
+    def __init__(self, seed, n_constraints, n_inputs=256, n_public=16):
+        L = _port_lib()
+        self._h = L.oracle_synth_new(seed, n_constraints, n_inputs, n_public)
+        if not self._h:
+            raise ValueError("bad synthetic circuit shape")
+        info = (ctypes.c_uint32 * 2)()
+        L.oracle_synth_info(ctypes.c_void_p(self._h), info)
+        self.n_vars, self.domain_size, self.n_public = info[0], info[1], n_public
+
+    def witness(self, witness_seed):
+        out = ctypes.create_string_buffer(32 * self.n_vars)
+        _port_lib().oracle_synth_witness(ctypes.c_void_p(self._h), witness_seed, out)
+        return out.raw
+
+    def zkey(self, toxic_seed):
+        L = _port_lib()
+        n = ctypes.c_size_t()
+        p = L.oracle_synth_zkey(ctypes.c_void_p(self._h), toxic_seed, ctypes.byref(n))
+        try:
+            return ctypes.string_at(p, n.value)
+        finally:
+            L.oracle_synth_buffer_free(p)
+
+    def close(self):
+        if self._h:
+            _port_lib().oracle_synth_free(ctypes.c_void_p(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

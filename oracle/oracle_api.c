@@ -278,3 +278,86 @@ int oracle_pairing_check(const uint8_t *g1s, const uint8_t *g2s, int n) {
     free(q);
     return r;
 }
+
+/* ---- the timed CPU baseline (port_*.c): same results, the reference's fast algorithms ---- */
+#include "port.h"
+
+int oracle_port_msm_g1(const uint8_t *bases, const uint8_t *scalars_std, size_t n, uint8_t *out) {
+    g1a_t *b = malloc((n ? n : 1) * sizeof(g1a_t));
+    for (size_t i = 0; i < n; i++) if (!unpack_g1(&b[i], bases + 64 * i)) { free(b); return -1; }
+    g1j_t r;
+    port_msm_g1(&r, b, (const fp_t *)scalars_std, n);
+    g1a_t a;
+    g1j_to_affine(&a, &r);
+    pack_g1(out, &a);
+    free(b);
+    return 0;
+}
+
+int oracle_port_msm_g2(const uint8_t *bases, const uint8_t *scalars_std, size_t n, uint8_t *out) {
+    g2a_t *b = malloc((n ? n : 1) * sizeof(g2a_t));
+    for (size_t i = 0; i < n; i++) if (!unpack_g2(&b[i], bases + 128 * i)) { free(b); return -1; }
+    g2j_t r;
+    port_msm_g2(&r, b, (const fp_t *)scalars_std, n);
+    g2a_t a;
+    g2j_to_affine(&a, &r);
+    pack_g2(out, &a);
+    free(b);
+    return 0;
+}
+
+int oracle_port_intt_coset_ntt(int log_n, uint8_t *data) {
+    port_ntt *t = port_ntt_new(log_n);
+    if (!t) return -1;
+    port_intt_coset_ntt(t, (fp_t *)data);
+    port_ntt_free(t);
+    return 0;
+}
+
+/* A prepared port prover: the parsed key and the domain tables, built once
+ * (the reference's warm mode: key parsed and tables cached before timing). */
+typedef struct { const zkey_t *k; port_ntt *t; } port_prover;
+
+void *oracle_port_prepare(const void *kv) {
+    const zkey_t *k = kv;
+    int log_n = 0;
+    while (((size_t)1 << log_n) < k->domain_size) log_n++;
+    port_prover *p = malloc(sizeof *p);
+    p->k = k;
+    p->t = port_ntt_new(log_n);
+    if (!p->t) { free(p); return NULL; }
+    return p;
+}
+
+void oracle_port_free(void *pv) {
+    port_prover *p = pv;
+    if (!p) return;
+    port_ntt_free(p->t);
+    free(p);
+}
+
+int oracle_port_prove(const void *pv, const uint8_t *w_mont, size_t n, const uint8_t *r_mont, const uint8_t *s_mont,
+                      uint8_t *proof_out) {
+    const port_prover *pp = pv;
+    if (n != pp->k->n_vars) return -1;
+    fp_t r, s;
+    ld(&r, r_mont); ld(&s, s_mont);
+    proof_t p;
+    if (port_prove(pp->k, pp->t, (const fp_t *)w_mont, &r, &s, &p) != 0) return -1;
+    pack_proof(proof_out, &p);
+    return 0;
+}
+
+/* the fast product against the oracle's, for the CPU tests: which 0 = Fr, 1 = Fq */
+void oracle_port_fp_mul(int which, const uint8_t *a, const uint8_t *b, uint8_t *out) {
+    fp_t x, y, z;
+    ld(&x, a); ld(&y, b);
+    if (which) pq_mul(&z, &x, &y); else pr_mul(&z, &x, &y);
+    st(out, &z);
+}
+void oracle_port_fq_inv(const uint8_t *a, uint8_t *out) {
+    fp_t x, z;
+    ld(&x, a);
+    pq_inv(&z, &x);
+    st(out, &z);
+}
