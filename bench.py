@@ -561,6 +561,7 @@ def run_ours(args):
                                "p50_ms": b["p50_ms"], "p99_ms": b["p99_ms"],
                                "plain_queued_p50_ms": b["plain"]["queued_p50_ms"],
                                "plain_queued_p99_ms": b["plain"]["queued_p99_ms"],
+                               "kernel_launches_per_batch": b["kernel_launches_per_batch"],
                                "per_instance_tuning": b["config"]["per_instance_tuning"]}
         except Exception as e:   # the plain-prove line above stands on its own
             line["batched"] = {"error": repr(e)[:300]}
@@ -814,6 +815,13 @@ def run_batch(args, backend=None, emit=True, steps=None):
         fifo.append(1e3 * acc)
     done, fifo = sorted(done), sorted(fifo)
     pct = lambda v, q: v[min(len(v) - 1, int(q * len(v)))]
+    # one more submission with kernel timing on (stage by stage, no graph): each kernel
+    # class's launches and device time for the whole batch
+    S.kernel_timing_reset()
+    S.kernel_timing(True)
+    backend.prove_batch(jobs)
+    S.kernel_timing(False)
+    kern = S.kernel_timing_report()
     exact = None
     if not args.no_oracle_check:
         exact = True
@@ -837,6 +845,8 @@ def run_batch(args, backend=None, emit=True, steps=None):
             "p50_ms": pct(done, 0.5), "p99_ms": pct(done, 0.99),
             "latency_note": "p50/p99: completion time of each proof from the submission of all 64 at once; "
                             "plain.queued_*: the same 64 queued FIFO one at a time; plain.p50/p99: one proof alone",
+            "kernel_launches_per_batch": {k: v[1] for k, v in kern.items()},
+            "kernel_ms_per_batch": {k: round(v[0], 4) for k, v in kern.items()},
             "batch_ms": 1e3 * best, "speedup_vs_plain": t_plain / best,
             "bit_exact_vs_plain": True, "bit_exact_vs_oracle": exact}
     for c in circs:

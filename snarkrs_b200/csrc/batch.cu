@@ -1,0 +1,434 @@
+// Batched proving: many proofs of any mix of prepared circuits, each stage of
+// every proof in one launch.
+//
+// The reference proves one request per call (crates/groth16/src/prove.rs).
+// Here a submission of jobs becomes one pass over the device: one gather
+// launch for every job's rows, one launch per step of every job's
+// iNTT -> coset -> NTT chain (ntt_batch_*), one sort of every witness into the
+// G1 and G2 MSM spaces, one accumulate launch per space covering the A, B1 and
+// L MSMs of every job (and one for every B2), one sort and one accumulate for
+// every H MSM, and one bucket-reduction pass per space (msm_batch_*).  Each job
+// keeps its circuit's own window sizes (tuning) and NTT tiling.  From the
+// second submission of the same jobs' circuits on, the whole sequence over its
+// three streams is captured once as a CUDA graph and replayed.  The host
+// computes the key-only blinder products while the device runs, then
+// assembles the proofs on a thread pool.  Results are bit-identical to single
+// proofs.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <thread>
+#include "common.cuh"
+#include "gather.cuh"
+#include "prover.hpp"
+
+namespace g16d {
+
+// One job's stage 0: rows of its circuit's CSR, witness and A | B | C.
+struct GatherJob {
+    const uint32_t* rp[2];
+    const uint32_t* sig[2];
+    const uint32_t* vid[2];
+    const uint4* values;
+    const uint4* w;
+    uint4* abc;
+    uint32_t n, block_start;
+};
+
+__global__ void __launch_bounds__(256) k_gather_multi(const GatherJob* __restrict__ jobs, uint32_t njobs) {
+    uint32_t lo = 0, hi = njobs;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (jobs[mid].block_start <= blockIdx.x) lo = mid; else hi = mid;
+    }
+    const GatherJob& j = jobs[lo];
+    const uint32_t row = (blockIdx.x - j.block_start) * 256 + threadIdx.x;
+    if (row >= j.n) return;
+    gather_row(row, j.rp[0], j.sig[0], j.vid[0], j.rp[1], j.sig[1], j.vid[1], j.values, j.w, j.abc,
+               j.abc + 2 * (size_t)j.n, j.abc + 4 * (size_t)j.n);
+}
+
+}  // namespace g16d
+
+namespace g16 {
+
+#define CK_BATCH(call)                                               \
+    do {                                                             \
+        cudaError_t e__ = (call);                                    \
+        if (e__ != cudaSuccess) return cuda_fail(e__, #call);        \
+    } while (0)
+
+// The state a job's plan depends on: its circuit, window sizes, tiling and tables.
+struct BatchKey {
+    const g16_circuit* c;
+    int cw, ch;
+    uint32_t tile, outer;
+    const void *ta, *tb1, *tb2, *tl, *th;
+    bool operator==(const BatchKey& o) const {
+        return c == o.c && cw == o.cw && ch == o.ch && tile == o.tile && outer == o.outer && ta == o.ta &&
+               tb1 == o.tb1 && tb2 == o.tb2 && tl == o.tl && th == o.th;
+    }
+};
+
+static BatchKey key_of(const g16_circuit* c) {
+    return {c, c->c_w, c->c_h, c->ntt.tiling.tile_log, c->ntt.tiling.outer_log_l, c->t_a, c->t_b1, c->t_b2, c->t_l,
+            c->t_h};
+}
+
+struct BatchEngine {
+    std::vector<BatchKey> key;
+    void* d_arena = nullptr;
+    uint64_t accounted = 0;                 // device bytes counted against the backend's budget
+    std::vector<size_t> off_w, off_abc, off_h;
+    MsmSpace g1, g2, hs;
+    MsmSources src_w, src_h;
+    NttBatch ntt;
+    void* d_gather = nullptr;
+    uint32_t gather_blocks = 0, gather_jobs = 0;
+    uint8_t* h_res = nullptr;               // pinned: G1, G2 and H results, back to back
+    size_t res_g1 = 0, res_g2 = 0, res_h = 0;
+    cudaStream_t st[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_sorted = nullptr, ev_g1 = nullptr, ev_g2 = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_kernels = 0;
+    int runs = 0;
+
+    void release() {
+        for (cudaStream_t s : st)
+            if (s) cudaStreamSynchronize(s);
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        g1.release();
+        g2.release();
+        hs.release();
+        src_w.release();
+        src_h.release();
+        ntt.release();
+        cudaFree(d_gather);
+        cudaFree(d_arena);
+        if (h_res) cudaFreeHost(h_res);
+        for (cudaEvent_t e : {ev_fork, ev_sorted, ev_g1, ev_g2})
+            if (e) cudaEventDestroy(e);
+        for (cudaStream_t s : st)
+            if (s) cudaStreamDestroy(s);
+        *this = BatchEngine();
+    }
+};
+
+namespace {
+
+constexpr uint64_t BATCH_REDUCE_PIECES = 4096;   // reduction pieces per MSM of a batch
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Device bytes a plan for these jobs takes, for the budget check before any allocation.
+uint64_t plan_estimate(g16_circuit* const* cs, size_t count) {
+    uint64_t b = 0;
+    for (size_t j = 0; j < count; j++) {
+        const g16_circuit* c = cs[j];
+        const uint64_t Ww = (uint64_t)msm_windows(c->c_w), Wh = (uint64_t)msm_windows(c->c_h);
+        const uint64_t Kw = 1ull << (c->c_w - 1), Kh = 1ull << (c->c_h - 1);
+        const uint64_t ew = (uint64_t)(c->rows[0] + 2 * c->rows[1] + c->rows[2]) * Ww, eh = (uint64_t)c->n * Wh;
+        b += 32ull * c->n_vars + 128ull * c->n + 32ull * (c->n_vars + c->n) + 2048;
+        b += (ew + eh) * 4 + (4 * Kw + Kh) * 24;                                 // entries, sort buffers
+        b += (3 * Kw * 2 + (ew - c->rows[1] * Ww) / 16) * XYZZ_G1_BYTES;          // G1 partials, buckets
+        b += (Kw * 2 + c->rows[1] * Ww / 16) * XYZZ_G2_BYTES;
+        b += (Kh * 2 + eh / 16) * XYZZ_G1_BYTES;
+    }
+    return b + (8ull << 20);
+}
+
+int build(g16_backend* be, BatchEngine& E, g16_circuit* const* cs, size_t count) {
+    E.release();
+    for (cudaStream_t* s : {&E.st[0], &E.st[1], &E.st[2]})
+        CK_BATCH(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&E.ev_fork, &E.ev_sorted, &E.ev_g1, &E.ev_g2})
+        CK_BATCH(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    // arena: per job its witness, A | B | C and H
+    size_t off = 0;
+    for (size_t j = 0; j < count; j++) {
+        const g16_circuit* c = cs[j];
+        E.off_w.push_back(off);
+        off = align256(off + 32ull * c->n_vars);
+        E.off_abc.push_back(off);
+        off = align256(off + 96ull * c->n);
+        E.off_h.push_back(off);
+        off = align256(off + 32ull * c->n);
+    }
+    CK_BATCH(g16::dev_malloc(&E.d_arena, off ? off : 256));
+    uint8_t* arena = (uint8_t*)E.d_arena;
+    // MSM spaces: G1 (A, B1, L of every job), G2 (B2), H
+    E.g1.g2 = false;
+    E.g2.g2 = true;
+    E.hs.g2 = false;
+    E.g1.pieces_target = E.g2.pieces_target = E.hs.pieces_target = BATCH_REDUCE_PIECES;
+    for (size_t j = 0; j < count; j++) {
+        const g16_circuit* c = cs[j];
+        const uint32_t Bw = 1u << (c->c_w - 1), Bh = 1u << (c->c_h - 1);
+        const uint32_t Ww = (uint32_t)msm_windows(c->c_w), Wh = (uint32_t)msm_windows(c->c_h);
+        MsmSpaceSeg s;
+        s.B = Bw;
+        s.table = c->t_a;
+        s.n_bases = c->rows[0] * Ww;
+        E.g1.segs.push_back(s);
+        s.table = c->t_b1;
+        s.n_bases = c->rows[1] * Ww;
+        E.g1.segs.push_back(s);
+        s.table = c->t_l;
+        s.n_bases = c->rows[2] * Ww;
+        E.g1.segs.push_back(s);
+        s.table = c->t_b2;
+        s.n_bases = c->rows[1] * Ww;
+        E.g2.segs.push_back(s);
+        s.B = Bh;
+        s.table = c->t_h;
+        s.n_bases = c->n * Wh;
+        E.hs.segs.push_back(s);
+        MsmSourceSpec w;
+        w.d_scalars = arena + E.off_w[j];
+        w.n = c->n_vars;
+        w.c = c->c_w;
+        w.ntargets = 4;
+        w.t[0] = {0, (int)(3 * j), c->d_rank[0], c->rows[0]};
+        w.t[1] = {0, (int)(3 * j + 1), c->d_rank[1], c->rows[1]};
+        w.t[2] = {0, (int)(3 * j + 2), c->d_rank[2], c->rows[2]};
+        w.t[3] = {1, (int)j, c->d_rank[1], c->rows[1]};
+        E.src_w.srcs.push_back(w);
+        MsmSourceSpec h;
+        h.d_scalars = arena + E.off_h[j];
+        h.n = c->n;
+        h.c = c->c_h;
+        h.ntargets = 1;
+        h.t[0] = {0, (int)j, nullptr, c->n};
+        E.src_h.srcs.push_back(h);
+    }
+    MsmSpace* wsp[2] = {&E.g1, &E.g2};
+    MsmSpace* hsp[1] = {&E.hs};
+    CK_BATCH(msm_batch_setup(E.src_w, wsp, 2, E.st[0]));
+    CK_BATCH(msm_batch_setup(E.src_h, hsp, 1, E.st[0]));
+    // the NTT chains and the gather
+    std::vector<NttBatchItem> items;
+    std::vector<g16d::GatherJob> gj;
+    uint32_t blocks = 0;
+    for (size_t j = 0; j < count; j++) {
+        const g16_circuit* c = cs[j];
+        uint8_t* abc = arena + E.off_abc[j];
+        const size_t vb = 32ull * c->n;
+        items.push_back({&c->ntt, abc, abc + vb, abc + 2 * vb, arena + E.off_h[j]});
+        g16d::GatherJob g = {};
+        for (int m = 0; m < 2; m++) {
+            g.rp[m] = c->d_rp[m];
+            g.sig[m] = c->d_sig[m];
+            g.vid[m] = c->d_vid[m];
+        }
+        g.values = (const uint4*)c->d_values;
+        g.w = (const uint4*)(arena + E.off_w[j]);
+        g.abc = (uint4*)abc;
+        g.n = c->n;
+        g.block_start = blocks;
+        blocks += (c->n + 255) / 256;
+        gj.push_back(g);
+    }
+    CK_BATCH(ntt_batch_setup(E.ntt, items, E.st[0]));
+    CK_BATCH(g16::dev_malloc(&E.d_gather, gj.size() * sizeof(g16d::GatherJob)));
+    CK_BATCH(cudaMemcpy(E.d_gather, gj.data(), gj.size() * sizeof(g16d::GatherJob), cudaMemcpyHostToDevice));
+    E.gather_blocks = blocks;
+    E.gather_jobs = (uint32_t)gj.size();
+    E.res_g1 = (size_t)E.g1.result_points * XYZZ_G1_BYTES;
+    E.res_g2 = (size_t)E.g2.result_points * XYZZ_G2_BYTES;
+    E.res_h = (size_t)E.hs.result_points * XYZZ_G1_BYTES;
+    CK_BATCH(cudaMallocHost((void**)&E.h_res, E.res_g1 + E.res_g2 + E.res_h + 64));
+    for (size_t j = 0; j < count; j++) E.key.push_back(key_of(cs[j]));
+    (void)be;
+    return G16_OK;
+}
+
+// Every stage of every job, over the engine's three streams, joined on st[0].
+int enqueue(BatchEngine& E) {
+    cudaStream_t s0 = E.st[0], s1 = E.st[1], s2 = E.st[2];
+    MsmSpace* wsp[2] = {&E.g1, &E.g2};
+    MsmSpace* hsp[1] = {&E.hs};
+    CK_BATCH(cudaEventRecord(E.ev_fork, s0));
+    CK_BATCH(cudaStreamWaitEvent(s1, E.ev_fork, 0));
+    // the witnesses' MSMs: one sort, then the G1 space on s1 and the G2 space on s2
+    CK_BATCH(msm_batch_sort(E.src_w, wsp, 2, s1));
+    CK_BATCH(cudaEventRecord(E.ev_sorted, s1));
+    CK_BATCH(cudaStreamWaitEvent(s2, E.ev_sorted, 0));
+    CK_BATCH(msm_space_accumulate(E.g2, s2));
+    CK_BATCH(cudaMemcpyAsync(E.h_res + E.res_g1, E.g2.acc.d_windows, E.res_g2, cudaMemcpyDeviceToHost, s2));
+    CK_BATCH(cudaEventRecord(E.ev_g2, s2));
+    CK_BATCH(msm_space_accumulate(E.g1, s1));
+    CK_BATCH(cudaMemcpyAsync(E.h_res, E.g1.acc.d_windows, E.res_g1, cudaMemcpyDeviceToHost, s1));
+    CK_BATCH(cudaEventRecord(E.ev_g1, s1));
+    // stage 0, the NTT chains and the H MSMs on s0
+    if (E.gather_blocks) {
+        TimedLaunch tl("gather", s0);
+        g16d::k_gather_multi<<<E.gather_blocks, 256, 0, s0>>>((const g16d::GatherJob*)E.d_gather, E.gather_jobs);
+    }
+    CK_BATCH(cudaGetLastError());
+    CK_BATCH(ntt_batch_run(E.ntt, s0));
+    CK_BATCH(msm_batch_sort(E.src_h, hsp, 1, s0));
+    CK_BATCH(msm_space_accumulate(E.hs, s0));
+    CK_BATCH(cudaMemcpyAsync(E.h_res + E.res_g1 + E.res_g2, E.hs.acc.d_windows, E.res_h, cudaMemcpyDeviceToHost, s0));
+    CK_BATCH(cudaStreamWaitEvent(s0, E.ev_g1, 0));
+    CK_BATCH(cudaStreamWaitEvent(s0, E.ev_g2, 0));
+    return G16_OK;
+}
+
+// Runs fn(i) for i < n on up to `threads` host threads.
+template <class Fn>
+void parallel_for(size_t n, size_t threads, Fn&& fn) {
+    threads = std::max<size_t>(1, std::min(threads, n));
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        for (size_t i; (i = next.fetch_add(1)) < n;) fn(i);
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < threads; t++) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+}
+
+size_t host_threads() {
+    size_t h = std::thread::hardware_concurrency();
+    return std::max<size_t>(1, std::min<size_t>(h ? h : 4, 32));
+}
+
+}  // namespace
+
+void batch_forget(g16_backend* b, const g16_circuit* c) {
+    std::lock_guard<std::mutex> g(b->batch_mu);
+    if (!b->batch) return;
+    for (auto& k : b->batch->key)
+        if (k.c == c) {
+            b->vram_used -= std::min<uint64_t>(b->vram_used, b->batch->accounted);
+            b->batch->release();
+            return;
+        }
+}
+
+void batch_free(g16_backend* b) {
+    std::lock_guard<std::mutex> g(b->batch_mu);
+    if (!b->batch) return;
+    b->vram_used -= std::min<uint64_t>(b->vram_used, b->batch->accounted);
+    b->batch->release();
+    delete b->batch;
+    b->batch = nullptr;
+}
+
+int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, const uint8_t* const* witnesses,
+                       const size_t* lens, const uint8_t* r, const uint8_t* s, g16_proof* out, double* done_ms) {
+    const auto t_start = std::chrono::steady_clock::now();
+    if (!count) return G16_OK;
+    std::lock_guard<std::mutex> bg(b->batch_mu);
+    // no circuit may be retuned while the batch reads its tables
+    std::vector<g16_circuit*> distinct(cs, cs + count);
+    std::sort(distinct.begin(), distinct.end());
+    distinct.erase(std::unique(distinct.begin(), distinct.end()), distinct.end());
+    for (g16_circuit* c : distinct) {
+        std::unique_lock<std::mutex> lk(c->mu);
+        c->cv.wait(lk, [&] { return !c->tuning; });
+        c->batch_users++;
+    }
+    struct Release {
+        std::vector<g16_circuit*>& cs;
+        ~Release() {
+            for (g16_circuit* c : cs) {
+                {
+                    std::lock_guard<std::mutex> g(c->mu);
+                    c->batch_users--;
+                }
+                c->cv.notify_all();
+            }
+        }
+    } release_guard{distinct};
+    if (!b->batch) b->batch = new BatchEngine();
+    BatchEngine& E = *b->batch;
+    bool same = E.key.size() == count;
+    for (size_t j = 0; same && j < count; j++) same = E.key[j] == key_of(cs[j]);
+    if (!same) {
+        b->vram_used -= std::min<uint64_t>(b->vram_used, E.accounted);
+        E.release();
+        const uint64_t need = plan_estimate(cs, count);
+        if (b->vram_used + need > b->vram_limit)
+            return fail(G16_ERR_DEVICE_MEMORY, "batch of %zu proofs needs about %llu MiB of device memory", count,
+                        (unsigned long long)(need >> 20));
+        int rc = build(b, E, cs, count);
+        if (rc != G16_OK) {
+            E.release();
+            return rc;
+        }
+        E.accounted = need;
+        b->vram_used += need;
+    }
+    // witnesses in, and the key-only blinder products on the host meanwhile
+    for (size_t j = 0; j < count; j++)
+        CK_BATCH(cudaMemcpyAsync((uint8_t*)E.d_arena + E.off_w[j], witnesses[j], 32 * lens[j], cudaMemcpyHostToDevice,
+                                 E.st[0]));
+    std::vector<BlinderTerms> terms(count);
+    std::vector<Fr> rr(count), ss(count);
+    for (size_t j = 0; j < count; j++) {
+        uint64_t a[4], c[4];
+        std::memcpy(a, r + 32 * j, 32);
+        std::memcpy(c, s + 32 * j, 32);
+        if (!Fr::canonical(a) || !Fr::canonical(c)) return fail(G16_ERR_INVALID_ARGUMENT, "job %zu: r or s not below r", j);
+        rr[j] = Fr::raw(a);
+        ss[j] = Fr::raw(c);
+    }
+    const size_t threads = host_threads();
+    std::thread blinders([&] { parallel_for(count, threads, [&](size_t j) { terms[j] = blinder_terms(cs[j], rr[j], ss[j]); }); });
+    int rc = G16_OK;
+    const bool use_graph = !timer().enabled && E.runs > 0;
+    if (use_graph && !E.graph) {
+        uint64_t k0 = timer().launches.load();
+        cudaError_t e = cudaStreamBeginCapture(E.st[0], cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            rc = enqueue(E);
+            cudaGraph_t g = nullptr;
+            cudaError_t e2 = cudaStreamEndCapture(E.st[0], &g);
+            if (rc == G16_OK && e2 != cudaSuccess) rc = cuda_fail(e2, "batch graph capture");
+            if (rc == G16_OK) {
+                e2 = cudaGraphInstantiate(&E.graph, g, 0);
+                if (e2 != cudaSuccess) rc = cuda_fail(e2, "batch graph instantiate");
+            }
+            if (g) cudaGraphDestroy(g);
+            E.graph_kernels = timer().launches.load() - k0;
+            timer().launches.fetch_sub(E.graph_kernels);   // counted when replayed
+        } else {
+            rc = cuda_fail(e, "batch graph capture");
+        }
+    }
+    if (rc == G16_OK) {
+        if (use_graph) {
+            cudaError_t e = cudaGraphLaunch(E.graph, E.st[0]);
+            if (e != cudaSuccess) rc = cuda_fail(e, "batch graph launch");
+            else timer().launches.fetch_add(E.graph_kernels);
+        } else {
+            rc = enqueue(E);
+        }
+    }
+    if (rc == G16_OK) {
+        cudaError_t e = cudaStreamSynchronize(E.st[0]);
+        if (e != cudaSuccess) rc = cuda_fail(e, "batched proving");
+    }
+    blinders.join();
+    if (rc != G16_OK) return rc;
+    timer().collect();
+    E.runs++;
+    // stage 11 for every job
+    const uint8_t *rg1 = E.h_res, *rg2 = E.h_res + E.res_g1, *rh = E.h_res + E.res_g1 + E.res_g2;
+    parallel_for(count, threads, [&](size_t j) {
+        MsmJac m;
+        m.a = msm_space_combine_g1(rg1, E.g1, 3 * j);
+        m.b1 = msm_space_combine_g1(rg1, E.g1, 3 * j + 1);
+        m.l = msm_space_combine_g1(rg1, E.g1, 3 * j + 2);
+        m.b2 = msm_space_combine_g2(rg2, E.g2, j);
+        m.h = msm_space_combine_g1(rh, E.hs, j);
+        assemble(cs[j], m, terms[j], rr[j], ss[j], out + j);
+        if (done_ms)
+            done_ms[j] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    });
+    return G16_OK;
+}
+
+}  // namespace g16

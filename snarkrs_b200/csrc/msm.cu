@@ -11,6 +11,7 @@ namespace g16d {
 
 using g16::MSM_DEAD;
 using g16::MSM_MAX_SETS;
+using g16::MSM_MAX_TARGETS;
 
 // Bits [off, off + width) of a 256-bit little-endian scalar held in shared
 // memory (8 words, row stride 9 to spread banks); reads past bit 255 are 0.
@@ -320,19 +321,30 @@ __global__ void k_copy_u32(uint32_t* dst, const uint32_t* src, uint32_t n) {
     if (i < n) dst[i] = src[i];
 }
 
+// One MSM of a multi-segment space, as the accumulate kernel reads it.
+struct MsmSegDev {
+    const uint4* bases;   // window-shifted base table
+    uint32_t key_start;   // first bucket of the segment in the space
+    uint32_t n_bases;     // table entries
+};
+
 // ---- accumulate: one thread per chunk of L sorted entries ----
 // LOCKSTEP: a block-wide barrier after every entry keeps the block's warps on
 // the same instructions.  A fully inlined G1 madd is too long for the
 // instruction cache, and warps that drift apart stall on instruction fetch
 // (ncu: no_instruction was the top stall); in lockstep, one fetch serves the
 // whole block.  G2 calls out-of-line Fq2 products and runs without it.
-template <class F, bool LOCKSTEP>
+// MULTI: the buckets belong to several MSMs (segments, msm_space_*), each
+// with its own base table; the segment of bucket g is the last one whose
+// key_start is <= g, followed forward as g grows.
+template <class F, bool LOCKSTEP, bool MULTI = false>
 __device__ __forceinline__ void accumulate_chunks(const uint32_t* __restrict__ entries,
                                                   const uint32_t* __restrict__ offsets,
                                                   const uint32_t* __restrict__ seg_base, uint32_t K, uint32_t M,
                                                   uint32_t L, const uint4* __restrict__ bases, uint32_t base_offset,
                                                   uint32_t n_bases, uint4* __restrict__ partials,
-                                                  unsigned long long* __restrict__ work) {
+                                                  unsigned long long* __restrict__ work,
+                                                  const MsmSegDev* __restrict__ segs = nullptr, uint32_t nsegs = 0) {
     size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     size_t start = t * L;
     const bool active = start < M;
@@ -349,6 +361,19 @@ __device__ __forceinline__ void accumulate_chunks(const uint32_t* __restrict__ e
         g = lo;
         next = offsets[g + 1];
     }
+    uint32_t si = 0, seg_end = 0xffffffffu;
+    if (MULTI && active) {
+        uint32_t lo = 0, hi = nsegs;
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (segs[mid].key_start <= g) lo = mid; else hi = mid;
+        }
+        si = lo;
+        bases = segs[si].bases;
+        n_bases = segs[si].n_bases;
+        base_offset = 0;
+        seg_end = si + 1 < nsegs ? segs[si + 1].key_start : 0xffffffffu;
+    }
     Xyzz<F> acc = Xyzz<F>::identity();
     unsigned adds = 0;
     const size_t stop = LOCKSTEP ? start + L : end;   // lockstep: every thread runs L steps
@@ -361,6 +386,14 @@ __device__ __forceinline__ void accumulate_chunks(const uint32_t* __restrict__ e
                     g++;
                     next = offsets[g + 1];
                 } while (next <= k);
+                if (MULTI) {
+                    while (g >= seg_end) {
+                        si++;
+                        bases = segs[si].bases;
+                        n_bases = segs[si].n_bases;
+                        seg_end = si + 1 < nsegs ? segs[si + 1].key_start : 0xffffffffu;
+                    }
+                }
             }
             uint32_t e = entries[k];
             if (k + 1 < end) {   // bring the next entry's base towards L1 while this one is added
@@ -626,6 +659,239 @@ __global__ void __launch_bounds__(128) k_reduce_sets(const uint4* __restrict__ i
     }
     acc = block_sum(acc, smem);
     if (threadIdx.x == 0) st_xyzz<F>(out, (size_t)set * gridDim.x + o, acc);
+}
+
+// ---- batched MSMs: several scalar vectors, many MSMs, one launch per step ----
+// A space holds the buckets of many MSMs (segments) back to back; sources are
+// scalar vectors, each feeding up to MSM_MAX_TARGETS segments (the witness
+// feeds A, B1 and L in the G1 space and B2 in the G2 space; an H vector feeds
+// its H segment).  One digits pass and one scatter pass sort every source into
+// every space; one accumulate launch per space adds every entry.
+
+struct MsmTargetDev {
+    uint32_t* counts;        // the space's sort buffers
+    uint32_t* cursor;
+    uint32_t* entries;
+    const uint32_t* rank;    // scalar -> table row, MSM_DEAD where the base is infinity; nullptr: the scalar's index
+    uint32_t key_start;      // the segment's first bucket in its space
+    uint32_t rows;           // the segment's table rows
+};
+
+struct MsmSourceDev {
+    const uint4* scalars;    // Montgomery Fr
+    uint4* std_out;          // standard-form copy, for the scatter pass
+    uint32_t n, c, W, ntargets;
+    MsmTargetDev t[MSM_MAX_TARGETS];
+};
+
+// the source of block b: the last s with blk_start[s] <= b
+__device__ __forceinline__ uint32_t source_of(const uint32_t* __restrict__ blk_start, uint32_t nsrc, uint32_t b) {
+    uint32_t lo = 0, hi = nsrc;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (blk_start[mid] <= b) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) k_digits_multi(const MsmSourceDev* __restrict__ srcs,
+                                                      const uint32_t* __restrict__ blk_start, uint32_t nsrc) {
+    __shared__ uint32_t sh[256 * 9];
+    const uint32_t si = source_of(blk_start, nsrc, blockIdx.x);
+    const MsmSourceDev& S = srcs[si];
+    const uint32_t i = (blockIdx.x - blk_start[si]) * 256 + threadIdx.x;
+    const bool valid = i < S.n;
+    const uint32_t nt = S.ntargets, c = S.c, W = S.W;
+    Fr x = Fr::zero();
+    bool live[MSM_MAX_TARGETS];
+#pragma unroll
+    for (int j = 0; j < MSM_MAX_TARGETS; j++)
+        live[j] = valid && (uint32_t)j < nt && (!S.t[j].rank || __ldg(S.t[j].rank + i) != MSM_DEAD);
+    if (valid) {
+        uint4 a = __ldg(S.scalars + 2 * (size_t)i), b = __ldg(S.scalars + 2 * (size_t)i + 1);
+        x.v[0] = a.x; x.v[1] = a.y; x.v[2] = a.z; x.v[3] = a.w;
+        x.v[4] = b.x; x.v[5] = b.y; x.v[6] = b.z; x.v[7] = b.w;
+        x = from_mont(x);
+        S.std_out[2 * (size_t)i] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
+        S.std_out[2 * (size_t)i + 1] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
+    }
+    uint32_t* row = sh + threadIdx.x * 9;
+#pragma unroll
+    for (int j = 0; j < 8; j++) row[j] = x.v[j];
+    const unsigned lane = threadIdx.x & 31;
+    for (uint32_t w = 0; w < W; w++) {
+        const int d = signed_digit(row, (int)w, (int)c);
+        const uint32_t key = d != 0 ? (uint32_t)(d < 0 ? -d : d) - 1u : NO_KEY;
+#pragma unroll
+        for (int j = 0; j < MSM_MAX_TARGETS; j++) {
+            if ((uint32_t)j >= nt) break;
+            const uint32_t kj = live[j] && key != NO_KEY ? S.t[j].key_start + key : NO_KEY;
+            const unsigned mask = __match_any_sync(0xffffffffu, kj);
+            if (kj != NO_KEY && lane == (unsigned)(__ffs(mask) - 1)) atomicAdd(&S.t[j].counts[kj], (uint32_t)__popc(mask));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_scatter_multi(const MsmSourceDev* __restrict__ srcs,
+                                                       const uint32_t* __restrict__ blk_start, uint32_t nsrc) {
+    __shared__ uint32_t sh[256 * 9];
+    const uint32_t si = source_of(blk_start, nsrc, blockIdx.x);
+    const MsmSourceDev& S = srcs[si];
+    const uint32_t i = (blockIdx.x - blk_start[si]) * 256 + threadIdx.x;
+    const bool valid = i < S.n;
+    const uint32_t nt = S.ntargets, c = S.c, W = S.W;
+    uint32_t rowi[MSM_MAX_TARGETS];
+#pragma unroll
+    for (int j = 0; j < MSM_MAX_TARGETS; j++)
+        rowi[j] = valid && (uint32_t)j < nt ? (S.t[j].rank ? __ldg(S.t[j].rank + i) : i) : MSM_DEAD;
+    uint32_t* row = sh + threadIdx.x * 9;
+    if (valid) {
+        uint4 a = S.std_out[2 * (size_t)i], b = S.std_out[2 * (size_t)i + 1];
+        row[0] = a.x; row[1] = a.y; row[2] = a.z; row[3] = a.w;
+        row[4] = b.x; row[5] = b.y; row[6] = b.z; row[7] = b.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; j++) row[j] = 0;
+    }
+    const unsigned lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
+    for (uint32_t w = 0; w < W; w++) {
+        const int d = signed_digit(row, (int)w, (int)c);
+        const uint32_t key = d != 0 ? (uint32_t)(d < 0 ? -d : d) - 1u : NO_KEY;
+        const uint32_t sign = d < 0 ? 0x80000000u : 0u;
+#pragma unroll
+        for (int j = 0; j < MSM_MAX_TARGETS; j++) {
+            if ((uint32_t)j >= nt) break;
+            const uint32_t kj = rowi[j] != MSM_DEAD && key != NO_KEY ? S.t[j].key_start + key : NO_KEY;
+            const unsigned mask = __match_any_sync(0xffffffffu, kj);
+            const int leader = __ffs(mask) - 1;
+            uint32_t base = 0;
+            if (kj != NO_KEY && (int)lane == leader) base = atomicAdd(&S.t[j].cursor[kj], (uint32_t)__popc(mask));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (kj != NO_KEY) S.t[j].entries[base + __popc(mask & lt)] = (w * S.t[j].rows + rowi[j]) | sign;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(ACC_BLOCK_G1, 1) k_accumulate_multi_g1(const uint32_t* __restrict__ entries,
+                                                                         const uint32_t* __restrict__ offsets,
+                                                                         const uint32_t* __restrict__ seg_base,
+                                                                         uint32_t K, const uint32_t* __restrict__ d_M,
+                                                                         const uint32_t* __restrict__ d_L,
+                                                                         const MsmSegDev* __restrict__ segs,
+                                                                         uint32_t nsegs, uint4* __restrict__ partials,
+                                                                         unsigned long long* __restrict__ work) {
+    const uint32_t M = *d_M, L = *d_L;
+    if ((size_t)blockIdx.x * blockDim.x * L >= M) return;   // the whole block has no entries
+    accumulate_chunks<Fq, true, true>(entries, offsets, seg_base, K, M, L, nullptr, 0, 0, partials, work, segs,
+                                      nsegs);
+}
+
+__global__ void __launch_bounds__(ACC_BLOCK_G2) k_accumulate_multi_g2(const uint32_t* __restrict__ entries,
+                                                                     const uint32_t* __restrict__ offsets,
+                                                                     const uint32_t* __restrict__ seg_base,
+                                                                     uint32_t K, const uint32_t* __restrict__ d_M,
+                                                                     const uint32_t* __restrict__ d_L,
+                                                                     const MsmSegDev* __restrict__ segs,
+                                                                     uint32_t nsegs, uint4* __restrict__ partials,
+                                                                     unsigned long long* __restrict__ work) {
+    accumulate_chunks<Fq2, false, true>(entries, offsets, seg_base, K, *d_M, *d_L, nullptr, 0, 0, partials, work,
+                                        segs, nsegs);
+}
+
+// The bucket reduction of one segment of a space (msm_reduce_plan with one set).
+struct MsmReduceDev {
+    uint32_t key_start, B, seg, nb, hb;
+    uint32_t block_start;   // its first k_reduce_pieces_multi block
+    uint32_t out_block;     // its first point in the blocks' output
+    uint32_t out_set;       // its first point in the sets' output
+};
+
+// k_reduce_pieces for many segments: block b works on block b - block_start
+// of the segment that owns it, with that segment's B and seg.
+template <class F, int LB>
+__global__ void __launch_bounds__(1 << LB) k_reduce_pieces_multi(const uint4* __restrict__ buckets,
+                                                                 const MsmReduceDev* __restrict__ segs,
+                                                                 uint32_t nsegs, uint4* __restrict__ out) {
+    constexpr uint32_t N = 1u << LB;
+    extern __shared__ uint4 smem[];
+    uint4* s_run = smem;
+    uint4* s_tot = smem + N * 4 * Codec<F>::U4;
+    uint32_t lo = 0, hi = nsegs;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (segs[mid].block_start <= blockIdx.x) lo = mid; else hi = mid;
+    }
+    const MsmReduceDev sd = segs[lo];
+    const uint32_t t = threadIdx.x, jb = blockIdx.x - sd.block_start;
+    const uint32_t p = jb * N + t, seg = sd.seg, B = sd.B;
+    const bool weighted = seg > 1;
+    constexpr bool TOT_SHARED = sizeof(F) > sizeof(g16d::Fq);
+    Xyzz<F> run = Xyzz<F>::identity(), tot = Xyzz<F>::identity();
+    if (TOT_SHARED && weighted) st_xyzz<F>(s_tot, t, tot);
+    if ((size_t)p * seg < B) {
+        const size_t g0 = (size_t)sd.key_start + (size_t)p * seg;
+#pragma unroll 1
+        for (int i = (int)seg - 1; i >= 0; i--) {
+            run = xyzz_add<F, false>(run, ld_xyzz<F>(buckets, g0 + i));
+            if (weighted) {
+                if constexpr (TOT_SHARED) st_xyzz<F>(s_tot, t, xyzz_add<F, false>(ld_xyzz<F>(s_tot, t), run));
+                else tot = xyzz_add<F, false>(tot, run);
+            }
+        }
+    }
+    st_xyzz<F>(s_run, t, run);
+    if (!TOT_SHARED && weighted) st_xyzz<F>(s_tot, t, tot);
+    const uint32_t lg = t ? 31 - __clz(t) : 0;
+#pragma unroll 1
+    for (uint32_t k = 1; k <= (uint32_t)LB; k++) {
+        __syncthreads();
+        const uint32_t h = N >> k;
+        if (t < h) {
+            run = xyzz_add<F, false>(run, ld_xyzz<F>(s_run, t + h));
+            st_xyzz<F>(s_run, t, run);
+        } else if (t < 2 * h) {
+            if (weighted) {
+                tot = xyzz_add<F, false>(ld_xyzz<F>(s_tot, t - h), ld_xyzz<F>(s_tot, t));
+                st_xyzz<F>(s_tot, t - h, tot);
+            }
+        } else {
+            const uint32_t hs = 1u << lg, s2 = 1u << (k - (LB - lg) - 1), o = t - hs;
+            if ((o & (2 * s2 - 1)) == 0 && o + s2 < hs) {
+                run = xyzz_add<F, false>(run, ld_xyzz<F>(s_run, t + s2));
+                st_xyzz<F>(s_run, t, run);
+            }
+        }
+    }
+    const size_t o0 = (size_t)sd.out_block + (size_t)jb * (LB + 2);
+    if (t == 0) {
+        if (!weighted) st_xyzz<F>(out, o0, run);
+        st_xyzz<F>(out, o0 + LB + 1, run);
+    } else if ((t & (t - 1)) == 0) {
+        st_xyzz<F>(out, o0 + 1 + lg, run);
+        if (t == 1 && weighted) st_xyzz<F>(out, o0, tot);
+    }
+}
+
+// k_reduce_sets for many segments: blockIdx.y picks the segment, blockIdx.x
+// the term (T, G_0 .. G_(LB-1), Gb_0 .. Gb_(hb-1)); terms past the segment's
+// own hb leave at once.
+template <class F, int LB>
+__global__ void __launch_bounds__(128) k_reduce_sets_multi(const uint4* __restrict__ in,
+                                                           const MsmReduceDev* __restrict__ segs,
+                                                           uint4* __restrict__ out) {
+    extern __shared__ uint4 smem[];
+    const MsmReduceDev sd = segs[blockIdx.y];
+    const uint32_t o = blockIdx.x;
+    if (o >= (uint32_t)LB + 1 + sd.hb) return;   // uniform across the block
+    const size_t base = sd.out_block;
+    Xyzz<F> acc = Xyzz<F>::identity();
+    for (uint32_t j = threadIdx.x; j < sd.nb; j += blockDim.x) {
+        if (o <= (uint32_t)LB) acc = xyzz_add<F, false>(acc, ld_xyzz<F>(in, base + (size_t)j * (LB + 2) + o));
+        else if ((j >> (o - LB - 1)) & 1u)
+            acc = xyzz_add<F, false>(acc, ld_xyzz<F>(in, base + (size_t)j * (LB + 2) + LB + 1));
+    }
+    acc = block_sum(acc, smem);
+    if (threadIdx.x == 0) st_xyzz<F>(out, (size_t)sd.out_set + o, acc);
 }
 
 // Window-shifted base table: out[w n + i] = 2^(c w) P_i (affine).  Built once
@@ -1154,6 +1420,254 @@ cudaError_t msm_accumulate_g2(const MsmSort& s, MsmAccum& acc, const void* d_bas
     return accumulate<g16d::Fq2>(s, acc, d_bases, base_offset, n_bases, st, XYZZ_G2_BYTES, "msm_accumulate_g2");
 }
 
+// ---- batched MSMs ----
+void MsmSpace::release() {
+    sort.release();
+    acc.release();
+    cudaFree(d_segdev);
+    cudaFree(d_reduce);
+    d_segdev = d_reduce = nullptr;
+}
+
+void MsmSources::release() {
+    cudaFree(d_desc);
+    cudaFree(d_blk);
+    cudaFree(d_std);
+    d_desc = nullptr;
+    d_blk = nullptr;
+    d_std = nullptr;
+}
+
+template <class T>
+static cudaError_t upload_vec(void*& d, const std::vector<T>& v, cudaStream_t st) {
+    cudaFree(d);
+    d = nullptr;
+    G16_CUDA(g16::dev_malloc(&d, (v.empty() ? 1 : v.size()) * sizeof(T)));
+    if (!v.empty()) G16_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return cudaSuccess;
+}
+
+cudaError_t msm_batch_setup(MsmSources& so, MsmSpace* const* spaces, int nspaces, cudaStream_t st) {
+    // entries each space can receive: every live row of every target, once per window
+    for (int i = 0; i < nspaces; i++) spaces[i]->max_entries = 0;
+    for (auto& src : so.srcs) {
+        if (src.c < 4 || src.c > 24 || src.ntargets < 0 || src.ntargets > MSM_MAX_TARGETS) {
+            set_error("batched MSM source with window %d bits and %d targets", src.c, src.ntargets);
+            return cudaErrorInvalidValue;
+        }
+        const uint32_t W = (uint32_t)msm_windows(src.c);
+        for (int j = 0; j < src.ntargets; j++) {
+            const MsmSourceTgt& t = src.t[j];
+            if (t.space < 0 || t.space >= nspaces || t.seg < 0 || (size_t)t.seg >= spaces[t.space]->segs.size() ||
+                spaces[t.space]->segs[t.seg].B != (1u << (src.c - 1)) || (uint64_t)t.rows * W >= 0x80000000ull) {
+                set_error("batched MSM target does not match its segment");
+                return cudaErrorInvalidValue;
+            }
+            spaces[t.space]->max_entries += (size_t)(t.d_rank ? t.rows : src.n) * W;
+        }
+    }
+    for (int i = 0; i < nspaces; i++) {
+        MsmSpace& sp = *spaces[i];
+        const uint32_t LB = sp.g2 ? 6 : 7;
+        const size_t pb = sp.g2 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES;
+        uint64_t K = 0, blocks = 0, out_block = 0, out_set = 0;
+        sp.max_hb = 0;
+        std::vector<MsmSegDev> segdev;
+        std::vector<MsmReduceDev> red;
+        for (auto& g : sp.segs) {
+            g.key_start = (uint32_t)K;
+            g.plan = msm_reduce_plan(1, g.B, sp.g2, sp.pieces_target);
+            g.plan.direct = false;   // every segment's block terms are summed on the device
+            g.block_start = (uint32_t)blocks;
+            g.out_block = (uint32_t)out_block;
+            g.out_set = (uint32_t)out_set;
+            segdev.push_back({(const uint4*)g.table, g.key_start, g.n_bases});
+            red.push_back({g.key_start, g.B, g.plan.seg, g.plan.nb, g.plan.hb, g.block_start, g.out_block, g.out_set});
+            K += g.B;
+            blocks += g.plan.nb;
+            out_block += (uint64_t)g.plan.nb * (LB + 2);
+            out_set += g.plan.set_terms();
+            sp.max_hb = std::max(sp.max_hb, g.plan.hb);
+        }
+        if (K >= 0x80000000ull || sp.max_entries >= 0x80000000ull) {
+            set_error("batched MSM space of %llu buckets and %zu entries exceeds 32-bit indices",
+                      (unsigned long long)K, sp.max_entries);
+            return cudaErrorInvalidValue;
+        }
+        sp.K = (uint32_t)K;
+        sp.blocks = (uint32_t)blocks;
+        sp.result_points = (uint32_t)out_set;
+        MsmSort& s = sp.sort;
+        s.K = s.Ks = sp.K;
+        s.B = 0;
+        s.shared = true;
+        s.chunk = 16;
+        s.n = sp.max_entries;   // accumulate sizes its partials by entries, W = 1 below
+        s.W = 1;
+        const size_t kk = (size_t)sp.K + 1;
+        if (kk > s.cap_k || !s.d_counts) {
+            size_t cap = 0;
+            G16_CUDA(grow(s.d_counts, cap, kk));
+            cap = 0;
+            G16_CUDA(grow(s.d_offsets, cap, kk));
+            cap = 0;
+            G16_CUDA(grow(s.d_cursor, cap, kk));
+            cap = 0;
+            G16_CUDA(grow(s.d_seg_base, cap, kk));
+            cap = 0;
+            G16_CUDA(grow(s.d_fat_list, cap, kk));
+            s.cap_k = cap;
+        }
+        G16_CUDA(grow(s.d_scan_tmp, s.cap_tmp, kk / 1024 + 2));
+        G16_CUDA(grow(s.d_entries, s.cap_entries, sp.max_entries ? sp.max_entries : 1));
+        if (!s.d_total) G16_CUDA(g16::dev_malloc((void**)&s.d_total, 4 * sizeof(uint32_t)));
+        MsmAccum& a = sp.acc;
+        const size_t chunks = (sp.max_entries + s.chunk - 1) / s.chunk;
+        G16_CUDA(grow_bytes(a.d_partials, a.cap_partials, ((size_t)sp.K + chunks + 1) * pb));
+        G16_CUDA(grow_bytes(a.d_buckets, a.cap_buckets, ((size_t)sp.K + 1) * pb));
+        G16_CUDA(grow_bytes(a.d_segments, a.cap_segments, (out_block + 1) * pb));
+        G16_CUDA(grow_bytes(a.d_windows, a.cap_windows, (out_set + 1) * pb));
+        if (!a.d_work) G16_CUDA(g16::dev_malloc((void**)&a.d_work, sizeof(unsigned long long)));
+        G16_CUDA(upload_vec(sp.d_segdev, segdev, st));
+        G16_CUDA(upload_vec(sp.d_reduce, red, st));
+    }
+    // sources: one block of 256 scalars never straddles two sources
+    std::vector<MsmSourceDev> desc;
+    std::vector<uint32_t> blk;
+    size_t std_elems = 0;
+    for (auto& src : so.srcs) std_elems += src.n;
+    cudaFree(so.d_std);
+    so.d_std = nullptr;
+    G16_CUDA(g16::dev_malloc(&so.d_std, (std_elems ? std_elems : 1) * 32));
+    uint64_t blocks = 0, off = 0;
+    for (auto& src : so.srcs) {
+        MsmSourceDev d = {};
+        d.scalars = (const uint4*)src.d_scalars;
+        d.std_out = (uint4*)((uint8_t*)so.d_std + off * 32);
+        d.n = src.n;
+        d.c = (uint32_t)src.c;
+        d.W = (uint32_t)msm_windows(src.c);
+        d.ntargets = (uint32_t)src.ntargets;
+        for (int j = 0; j < src.ntargets; j++) {
+            MsmSpace& sp = *spaces[src.t[j].space];
+            d.t[j] = {sp.sort.d_counts, sp.sort.d_cursor, sp.sort.d_entries, src.t[j].d_rank,
+                      sp.segs[src.t[j].seg].key_start, src.t[j].d_rank ? src.t[j].rows : src.n};
+        }
+        desc.push_back(d);
+        blk.push_back((uint32_t)blocks);
+        blocks += (src.n + 255) / 256;
+        off += src.n;
+    }
+    if (blocks >= 0x80000000ull) {
+        set_error("batched MSM sources of %llu blocks", (unsigned long long)blocks);
+        return cudaErrorInvalidValue;
+    }
+    so.total_blocks = (uint32_t)blocks;
+    G16_CUDA(upload_vec(so.d_desc, desc, st));
+    void* dblk = so.d_blk;
+    G16_CUDA(upload_vec(dblk, blk, st));
+    so.d_blk = (uint32_t*)dblk;
+    G16_CUDA(cudaStreamSynchronize(st));
+    return cudaSuccess;
+}
+
+cudaError_t msm_batch_sort(MsmSources& so, MsmSpace* const* spaces, int nspaces, cudaStream_t st) {
+    for (int i = 0; i < nspaces; i++) {
+        MsmSort& s = spaces[i]->sort;
+        G16_CUDA(cudaMemsetAsync(s.d_counts, 0, ((size_t)s.K + 1) * sizeof(uint32_t), st));
+        G16_CUDA(cudaMemsetAsync(s.d_total, 0, 4 * sizeof(uint32_t), st));
+    }
+    const uint32_t nsrc = (uint32_t)so.srcs.size();
+    if (so.total_blocks) {
+        TimedLaunch tl("msm_digits", st);
+        k_digits_multi<<<so.total_blocks, 256, 0, st>>>((const MsmSourceDev*)so.d_desc, so.d_blk, nsrc);
+    }
+    G16_CUDA(cudaGetLastError());
+    for (int i = 0; i < nspaces; i++) {
+        MsmSort& s = spaces[i]->sort;
+        G16_CUDA(scan(s.d_counts, s.d_offsets, s.K, s.d_scan_tmp, s.d_total, st));
+        TimedLaunch tl("msm_copy", st);
+        k_copy_u32<<<blocks_for(s.K ? s.K : 1, 256), 256, 0, st>>>(s.d_cursor, s.d_offsets, s.K);
+    }
+    if (so.total_blocks) {
+        TimedLaunch tl("msm_scatter", st);
+        k_scatter_multi<<<so.total_blocks, 256, 0, st>>>((const MsmSourceDev*)so.d_desc, so.d_blk, nsrc);
+    }
+    G16_CUDA(cudaGetLastError());
+    for (int i = 0; i < nspaces; i++) {
+        MsmSort& s = spaces[i]->sort;
+        {
+            TimedLaunch tl("msm_nseg", st);
+            k_nseg<<<blocks_for(s.K ? s.K : 1, 256), 256, 0, st>>>(s.d_offsets, s.K, s.K, s.chunk, accumulate_wave(),
+                                                                   s.d_counts, s.d_fat_list, s.d_total + 2,
+                                                                   s.d_total);
+        }
+        G16_CUDA(scan(s.d_counts, s.d_seg_base, s.K, s.d_scan_tmp, s.d_total + 1, st));
+    }
+    return cudaSuccess;
+}
+
+template <class F, int LB>
+static cudaError_t space_accumulate(MsmSpace& sp, cudaStream_t st, size_t xyzz_bytes, const char* tag) {
+    MsmSort& s = sp.sort;
+    MsmAccum& a = sp.acc;
+    const size_t chunks = (sp.max_entries + s.chunk - 1) / s.chunk;
+    G16_CUDA(cudaMemsetAsync(a.d_work, 0, sizeof(unsigned long long), st));
+    uint4* partials = (uint4*)a.d_partials;
+    const uint32_t nsegs = (uint32_t)sp.segs.size();
+    if (chunks) {
+        TimedLaunch tl(tag, st);
+        if (std::is_same<F, g16d::Fq>::value)
+            k_accumulate_multi_g1<<<blocks_for(chunks, ACC_BLOCK_G1), ACC_BLOCK_G1, 0, st>>>(
+                s.d_entries, s.d_offsets, s.d_seg_base, s.K, s.d_total, s.d_total + 3, (const MsmSegDev*)sp.d_segdev,
+                nsegs, partials, a.d_work);
+        else
+            k_accumulate_multi_g2<<<blocks_for(chunks, ACC_BLOCK_G2), ACC_BLOCK_G2, 0, st>>>(
+                s.d_entries, s.d_offsets, s.d_seg_base, s.K, s.d_total, s.d_total + 3, (const MsmSegDev*)sp.d_segdev,
+                nsegs, partials, a.d_work);
+    }
+    G16_CUDA(cudaGetLastError());
+    int sms = 148;
+    {
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    {
+        TimedLaunch tl("msm_fat_merge", st);
+        k_fat_merge_jobs<F><<<2 * sms, 128, 128 * xyzz_bytes, st>>>(partials, s.d_offsets, s.d_seg_base, s.d_fat_list,
+                                                                    s.d_total + 2, s.d_total + 3);
+    }
+    {
+        TimedLaunch tl("msm_fat_merge", st);
+        k_fat_merge_final<F><<<sms, 64, 64 * xyzz_bytes, st>>>(partials, s.d_offsets, s.d_seg_base, s.d_fat_list,
+                                                              s.d_total + 2, s.d_total + 3);
+    }
+    G16_CUDA(cudaGetLastError());
+    if (s.K) {
+        TimedLaunch tl("msm_bucket_sums", st);
+        k_bucket_sums<F><<<blocks_for(s.K, 128), 128, 0, st>>>(partials, s.d_offsets, s.d_seg_base, s.K, s.d_total + 3,
+                                                                (uint4*)a.d_buckets);
+    }
+    if (sp.blocks) {
+        TimedLaunch tl("msm_reduce", st);
+        k_reduce_pieces_multi<F, LB><<<sp.blocks, 1u << LB, 2 * ((size_t)1 << LB) * xyzz_bytes, st>>>(
+            (const uint4*)a.d_buckets, (const MsmReduceDev*)sp.d_reduce, nsegs, (uint4*)a.d_segments);
+    }
+    if (nsegs) {
+        TimedLaunch tl("msm_reduce", st);
+        k_reduce_sets_multi<F, LB><<<dim3(LB + 1 + sp.max_hb, nsegs), 128, 128 * xyzz_bytes, st>>>(
+            (const uint4*)a.d_segments, (const MsmReduceDev*)sp.d_reduce, (uint4*)a.d_windows);
+    }
+    G16_CUDA(cudaGetLastError());
+    return cudaSuccess;
+}
+
+cudaError_t msm_space_accumulate(MsmSpace& sp, cudaStream_t st) {
+    if (sp.g2) return space_accumulate<g16d::Fq2, 6>(sp, st, XYZZ_G2_BYTES, "msm_accumulate_g2");
+    return space_accumulate<g16d::Fq, 7>(sp, st, XYZZ_G1_BYTES, "msm_accumulate_g1");
+}
+
 // ---- host: window sums -> Horner ----
 static Fq fq_at(const uint8_t* p) {
     uint64_t v[4];
@@ -1231,6 +1745,20 @@ G1J msm_combine_g1(const uint8_t* result_xyzz, const MsmReducePlan& plan, int c)
 }
 G2J msm_combine_g2(const uint8_t* result_xyzz, const MsmReducePlan& plan, int c) {
     return combine<Fq2>(result_xyzz, plan, c);
+}
+
+}  // namespace g16
+
+namespace g16 {
+
+G1J msm_space_combine_g1(const uint8_t* results, const MsmSpace& sp, size_t s) {
+    const MsmSpaceSeg& g = sp.segs[s];
+    return msm_combine_g1(results + (size_t)g.out_set * XYZZ_G1_BYTES, g.plan, 1);
+}
+
+G2J msm_space_combine_g2(const uint8_t* results, const MsmSpace& sp, size_t s) {
+    const MsmSpaceSeg& g = sp.segs[s];
+    return msm_combine_g2(results + (size_t)g.out_set * XYZZ_G2_BYTES, g.plan, 1);
 }
 
 }  // namespace g16

@@ -32,6 +32,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 #include "host_bn254.hpp"
 
@@ -198,6 +199,80 @@ constexpr size_t XYZZ_G2_BYTES = 256;
 // The prover reads each of its five MSM results (the reduction's points) back
 // into a pinned host slot of this many bytes.
 constexpr size_t MSM_RESULT_SLOT_BYTES = 32 * 256;
+
+// ---- batched MSMs (many MSMs in one launch per step) ----
+// A space holds the buckets of many MSMs of one group (segments) back to back;
+// sources are device scalar vectors (Montgomery Fr), each sorted into up to
+// MSM_MAX_TARGETS segments of any spaces in one digits pass and one scatter
+// pass.  One accumulate launch per space then adds every entry of every
+// segment, each against its own window-shifted table, and one reduction pass
+// reduces every segment's bucket set.  Batched proving uses three spaces: the
+// witnesses' G1 MSMs (A, B1, L of every proof), their G2 MSMs (B2) and the H
+// MSMs.
+constexpr int MSM_MAX_TARGETS = 4;
+
+struct MsmSpaceSeg {
+    uint32_t B = 0;                  // buckets, 2^(c-1) for the source's window bits c
+    const void* table = nullptr;     // window-shifted bases (msm_window_table), rows x W entries
+    uint32_t n_bases = 0;            // entries of the table
+    // laid out by msm_batch_setup
+    uint32_t key_start = 0;          // first bucket in the space
+    MsmReducePlan plan;              // one set of B buckets; the sets kernel always runs
+    uint32_t block_start = 0, out_block = 0, out_set = 0;
+};
+
+struct MsmSpace {
+    bool g2 = false;
+    uint64_t pieces_target = 4096;   // reduction pieces per segment
+    std::vector<MsmSpaceSeg> segs;
+    // laid out by msm_batch_setup
+    uint32_t K = 0;                  // buckets over all segments
+    uint32_t blocks = 0;             // reduction blocks over all segments
+    uint32_t max_hb = 0;
+    uint32_t result_points = 0;      // points of acc.d_windows the host reads
+    size_t max_entries = 0;
+    MsmSort sort;                    // sort buffers over the whole space
+    MsmAccum acc;                    // partials, bucket sums, blocks' points (d_segments), results (d_windows)
+    void* d_segdev = nullptr;        // accumulate descriptors
+    void* d_reduce = nullptr;        // reduction descriptors
+    void release();
+};
+
+struct MsmSourceTgt {
+    int space = 0, seg = 0;          // index into the spaces passed to msm_batch_setup, and segment
+    const uint32_t* d_rank = nullptr;   // scalar -> table row, MSM_DEAD for a base at infinity; nullptr: identity
+    uint32_t rows = 0;               // table rows of the segment
+};
+
+struct MsmSourceSpec {
+    const void* d_scalars = nullptr; // Montgomery Fr on the device
+    uint32_t n = 0;
+    int c = 0;                       // window bits (its segments have B = 2^(c-1))
+    int ntargets = 0;
+    MsmSourceTgt t[MSM_MAX_TARGETS];
+};
+
+struct MsmSources {
+    std::vector<MsmSourceSpec> srcs;
+    uint32_t total_blocks = 0;
+    void* d_desc = nullptr;
+    uint32_t* d_blk = nullptr;
+    void* d_std = nullptr;           // standard-form copies of the scalars
+    void release();
+};
+
+// Lays out every space's segments (keys, reduction plans), allocates the
+// spaces' buffers for the entries the sources can produce, and uploads the
+// descriptors.  Synchronises st.
+cudaError_t msm_batch_setup(MsmSources& so, MsmSpace* const* spaces, int nspaces, cudaStream_t st);
+// Sorts every source into its segments (no host synchronisation).
+cudaError_t msm_batch_sort(MsmSources& so, MsmSpace* const* spaces, int nspaces, cudaStream_t st);
+// Accumulates and reduces every segment of one space: results in
+// sp.acc.d_windows, sp.result_points points (no host synchronisation).
+cudaError_t msm_space_accumulate(MsmSpace& sp, cudaStream_t st);
+// Host: segment s's sum from the space's results as read back.
+G1J msm_space_combine_g1(const uint8_t* results, const MsmSpace& sp, size_t s);
+G2J msm_space_combine_g2(const uint8_t* results, const MsmSpace& sp, size_t s);
 
 // kernel-time accounting hook (events around each kernel class), optional
 struct KernelTimer;

@@ -74,21 +74,19 @@ __device__ __forceinline__ void run_stage(uint4* sm, uint32_t j, uint32_t s_lo, 
     }
 }
 
-// Stages [s_lo, s_lo + k) of 2^log_n, one tile of (2^k)*L elements per block;
-// blockIdx.y selects the vector.  Optional epilogues: multiply by *scale,
-// or write h = join_a * join_b - x to join_out instead of storing x.
+// Stages [s_lo, s_lo + k) of 2^log_n, one tile of (2^k)*L elements per block
+// (block bx of the pass).  Optional epilogues: multiply by *scale, or write
+// h = join_a * join_b - x to join_out instead of storing x.
 template <bool DIF>
-__global__ void __launch_bounds__(256) k_ntt_pass(Vec3 vecs, uint32_t log_n, uint32_t s_lo, uint32_t k,
-                                                  uint32_t log_L, const uint4* __restrict__ tw,
-                                                  const uint4* __restrict__ scale, const uint4* __restrict__ join_a,
-                                                  const uint4* __restrict__ join_b, uint4* __restrict__ join_out) {
-    extern __shared__ uint4 sm[];
-    uint4* data = vecs.p[blockIdx.y];
+__device__ __forceinline__ void ntt_pass_tile(uint4* sm, uint4* data, uint32_t bx, uint32_t log_n, uint32_t s_lo,
+                                              uint32_t k, uint32_t log_L, const uint4* __restrict__ tw,
+                                              const uint4* __restrict__ scale, const uint4* __restrict__ join_a,
+                                              const uint4* __restrict__ join_b, uint4* __restrict__ join_out) {
     const uint32_t L = 1u << log_L;
     const uint32_t tile = (1u << k) << log_L;
     const uint32_t bph = s_lo - log_L;
-    const size_t hi = blockIdx.x >> bph;
-    const uint32_t lo0 = (blockIdx.x & ((1u << bph) - 1u)) << log_L;
+    const size_t hi = bx >> bph;
+    const uint32_t lo0 = (bx & ((1u << bph) - 1u)) << log_L;
     for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
         uint32_t mid = e >> log_L, l = e & (L - 1u);
         size_t gi = (hi << (s_lo + k)) | ((size_t)mid << s_lo) | (lo0 + l);
@@ -117,18 +115,27 @@ __global__ void __launch_bounds__(256) k_ntt_pass(Vec3 vecs, uint32_t log_n, uin
     }
 }
 
+// blockIdx.y selects the vector
+template <bool DIF>
+__global__ void __launch_bounds__(256) k_ntt_pass(Vec3 vecs, uint32_t log_n, uint32_t s_lo, uint32_t k,
+                                                  uint32_t log_L, const uint4* __restrict__ tw,
+                                                  const uint4* __restrict__ scale, const uint4* __restrict__ join_a,
+                                                  const uint4* __restrict__ join_b, uint4* __restrict__ join_out) {
+    extern __shared__ uint4 sm[];
+    ntt_pass_tile<DIF>(sm, vecs.p[blockIdx.y], blockIdx.x, log_n, s_lo, k, log_L, tw, scale, join_a, join_b,
+                       join_out);
+}
+
 // The fused middle of iNTT -> coset -> NTT: DIF stages [0, k) with inverse
 // twiddles, a[p] *= coset[p], DIT stages [0, k) with forward twiddles, on
 // contiguous tiles of 2^k.  Optional h = join_a * join_b - x epilogue for a
 // transform that has no outer passes.
-__global__ void __launch_bounds__(256) k_ntt_mid(Vec3 vecs, uint32_t log_n, uint32_t k, const uint4* __restrict__ tw,
-                                                 const uint4* __restrict__ tw_inv, const uint4* __restrict__ coset,
-                                                 const uint4* __restrict__ join_a, const uint4* __restrict__ join_b,
-                                                 uint4* __restrict__ join_out) {
-    extern __shared__ uint4 sm[];
-    uint4* data = vecs.p[blockIdx.y];
+__device__ __forceinline__ void ntt_mid_tile(uint4* sm, uint4* data, uint32_t bx, uint32_t log_n, uint32_t k,
+                                             const uint4* __restrict__ tw, const uint4* __restrict__ tw_inv,
+                                             const uint4* __restrict__ coset, const uint4* __restrict__ join_a,
+                                             const uint4* __restrict__ join_b, uint4* __restrict__ join_out) {
     const uint32_t tile = 1u << k;
-    const size_t base = (size_t)blockIdx.x << k;
+    const size_t base = (size_t)bx << k;
     for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
         sm[2 * e] = data[2 * (base + e)];
         sm[2 * e + 1] = data[2 * (base + e) + 1];
@@ -152,6 +159,53 @@ __global__ void __launch_bounds__(256) k_ntt_mid(Vec3 vecs, uint32_t log_n, uint
             st_g(data, base + e, x);
         }
     }
+}
+
+__global__ void __launch_bounds__(256) k_ntt_mid(Vec3 vecs, uint32_t log_n, uint32_t k, const uint4* __restrict__ tw,
+                                                 const uint4* __restrict__ tw_inv, const uint4* __restrict__ coset,
+                                                 const uint4* __restrict__ join_a, const uint4* __restrict__ join_b,
+                                                 uint4* __restrict__ join_out) {
+    extern __shared__ uint4 sm[];
+    ntt_mid_tile(sm, vecs.p[blockIdx.y], blockIdx.x, log_n, k, tw, tw_inv, coset, join_a, join_b, join_out);
+}
+
+// ---- many transforms per launch (batched proving) ----
+// A job is one vector's pass (or fused middle) of one transform; the blocks
+// of a launch are the jobs' tiles back to back, block_start being a job's
+// first block.
+struct NttJob {
+    uint4* data;
+    const uint4* tw;        // pass: the pass's twiddles; middle: forward twiddles
+    const uint4* tw_inv;    // middle: inverse twiddles
+    const uint4* coset;     // middle: shift^bitrev(p) / n
+    const uint4* join_a;    // join epilogue h = a * b - x, or null
+    const uint4* join_b;
+    uint4* join_out;
+    uint32_t log_n, s_lo, k, log_L, block_start, pad;
+};
+
+__device__ __forceinline__ uint32_t job_of(const NttJob* __restrict__ jobs, uint32_t njobs, uint32_t b) {
+    uint32_t lo = 0, hi = njobs;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (jobs[mid].block_start <= b) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+template <bool DIF>
+__global__ void __launch_bounds__(256) k_ntt_pass_multi(const NttJob* __restrict__ jobs, uint32_t njobs) {
+    extern __shared__ uint4 sm[];
+    const NttJob& j = jobs[job_of(jobs, njobs, blockIdx.x)];
+    ntt_pass_tile<DIF>(sm, j.data, blockIdx.x - j.block_start, j.log_n, j.s_lo, j.k, j.log_L, j.tw, nullptr, j.join_a,
+                       j.join_b, j.join_out);
+}
+
+__global__ void __launch_bounds__(256) k_ntt_mid_multi(const NttJob* __restrict__ jobs, uint32_t njobs) {
+    extern __shared__ uint4 sm[];
+    const NttJob& j = jobs[job_of(jobs, njobs, blockIdx.x)];
+    ntt_mid_tile(sm, j.data, blockIdx.x - j.block_start, j.log_n, j.k, j.tw, j.tw_inv, j.coset, j.join_a, j.join_b,
+                 j.join_out);
 }
 
 __device__ __forceinline__ Fr fr_pow_u64(Fr b, uint64_t e) {
@@ -301,6 +355,9 @@ static void set_attrs() {
     cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k_ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k_ntt_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_ntt_pass_multi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_ntt_pass_multi<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_ntt_mid_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attrs_done = true;
 }
 
@@ -415,6 +472,153 @@ cudaError_t ntt_distribute_powers(void* a, size_t n, const uint64_t* shift_mont,
     TimedLaunch tl("ntt_distribute", st);
     k_distribute<<<blocks_for((n + 15) / 16, 128), 128, 0, st>>>((uint4*)a, s, n);
     return cudaGetLastError();
+}
+
+}  // namespace g16
+
+namespace g16 {
+
+using g16d::NttJob;
+
+void NttBatch::release() {
+    cudaFree(d_jobs);
+    d_jobs = nullptr;
+    phases.clear();
+}
+
+// The batch's launches.  Every transform runs iNTT -> coset -> NTT on its A,
+// B and C and writes H = A B - C: its inverse outer passes (top stages first),
+// the fused middle, its forward outer passes.  The transforms are aligned so
+// that their middles share one launch: inverse phase m runs outer pass
+// Dmax - 1 - m of every transform that has that many, forward phase m runs
+// outer pass m.  C's last pass, which reads the finished A and B for the join,
+// runs after every other phase, in one launch per kind of pass.
+cudaError_t ntt_batch_setup(NttBatch& nb, const std::vector<NttBatchItem>& items, cudaStream_t st) {
+    set_attrs();
+    nb.release();
+    struct ItemPlan {
+        uint32_t log_n, k0;
+        std::vector<Pass> outer;
+    };
+    std::vector<ItemPlan> plans;
+    uint32_t dmax = 0;
+    for (auto& it : items) {
+        if (!it.t || it.t->log_n < 1) {
+            set_error("batched NTT item without tables");
+            return cudaErrorInvalidValue;
+        }
+        ItemPlan p;
+        p.log_n = (uint32_t)it.t->log_n;
+        p.k0 = inner_k(it.t->tiling, p.log_n);
+        p.outer = outer_passes(it.t->tiling, p.log_n, p.k0);
+        dmax = std::max(dmax, (uint32_t)p.outer.size());
+        plans.push_back(p);
+    }
+    std::vector<NttJob> all;
+    auto add_phase = [&](int kind, std::vector<NttJob>& jobs) {
+        if (jobs.empty()) return;
+        NttPhase ph;
+        ph.kind = kind;
+        ph.first = (uint32_t)all.size();
+        ph.njobs = (uint32_t)jobs.size();
+        uint32_t blocks = 0;
+        size_t smem = 0;
+        for (auto& j : jobs) {
+            j.block_start = blocks;
+            const uint32_t tile = kind == 2 ? (1u << j.k) : ((1u << j.k) << j.log_L);
+            blocks += (uint32_t)(((size_t)1 << j.log_n) / tile);
+            smem = std::max(smem, (size_t)tile * 32);
+            ph.products += kind == 2 ? ((double)((size_t)1 << j.log_n) * (j.k + 1)) : ((double)((size_t)1 << j.log_n) / 2 * j.k);
+            ph.bytes += 64.0 * (double)((size_t)1 << j.log_n) * (j.join_out ? 2 : 1);
+        }
+        ph.blocks = blocks;
+        ph.smem = smem;
+        all.insert(all.end(), jobs.begin(), jobs.end());
+        nb.phases.push_back(ph);
+    };
+    auto pass_job = [&](size_t i, int v, const Pass& p, bool dif, bool join) {
+        const NttBatchItem& it = items[i];
+        NttJob j = {};
+        j.data = (uint4*)(v == 0 ? it.a : v == 1 ? it.b : it.c);
+        j.tw = (const uint4*)(dif ? it.t->d_tw_inv : it.t->d_tw);
+        if (join) {
+            j.join_a = (const uint4*)it.a;
+            j.join_b = (const uint4*)it.b;
+            j.join_out = (uint4*)it.h;
+        }
+        j.log_n = plans[i].log_n;
+        j.s_lo = p.s_lo;
+        j.k = p.k;
+        j.log_L = p.log_L;
+        return j;
+    };
+    auto mid_job = [&](size_t i, int v, bool join) {
+        const NttBatchItem& it = items[i];
+        NttJob j = {};
+        j.data = (uint4*)(v == 0 ? it.a : v == 1 ? it.b : it.c);
+        j.tw = (const uint4*)it.t->d_tw;
+        j.tw_inv = (const uint4*)it.t->d_tw_inv;
+        j.coset = (const uint4*)it.t->d_coset;
+        if (join) {
+            j.join_a = (const uint4*)it.a;
+            j.join_b = (const uint4*)it.b;
+            j.join_out = (uint4*)it.h;
+        }
+        j.log_n = plans[i].log_n;
+        j.k = plans[i].k0;
+        return j;
+    };
+    for (uint32_t m = 0; m < dmax; m++) {   // inverse outer passes, right-aligned
+        std::vector<NttJob> jobs;
+        const uint32_t q = dmax - 1 - m;
+        for (size_t i = 0; i < items.size(); i++)
+            if (plans[i].outer.size() > q)
+                for (int v = 0; v < 3; v++) jobs.push_back(pass_job(i, v, plans[i].outer[q], true, false));
+        add_phase(0, jobs);
+    }
+    {
+        std::vector<NttJob> jobs;
+        for (size_t i = 0; i < items.size(); i++)
+            for (int v = 0; v < (plans[i].outer.empty() ? 2 : 3); v++) jobs.push_back(mid_job(i, v, false));
+        add_phase(2, jobs);
+    }
+    for (uint32_t m = 0; m < dmax; m++) {   // forward outer passes, left-aligned
+        std::vector<NttJob> jobs;
+        for (size_t i = 0; i < items.size(); i++) {
+            const size_t np = plans[i].outer.size();
+            if (m >= np) continue;
+            for (int v = 0; v < (m + 1 == np ? 2 : 3); v++) jobs.push_back(pass_job(i, v, plans[i].outer[m], false, false));
+        }
+        add_phase(1, jobs);
+    }
+    {   // C's last pass with the join: middles (no outer passes), then last forward passes
+        std::vector<NttJob> mids, passes;
+        for (size_t i = 0; i < items.size(); i++) {
+            if (plans[i].outer.empty()) mids.push_back(mid_job(i, 2, true));
+            else passes.push_back(pass_job(i, 2, plans[i].outer.back(), false, true));
+        }
+        add_phase(2, mids);
+        add_phase(1, passes);
+    }
+    G16_CUDA(g16::dev_malloc(&nb.d_jobs, (all.empty() ? 1 : all.size()) * sizeof(NttJob)));
+    if (!all.empty()) G16_CUDA(cudaMemcpyAsync(nb.d_jobs, all.data(), all.size() * sizeof(NttJob), cudaMemcpyHostToDevice, st));
+    G16_CUDA(cudaStreamSynchronize(st));
+    return cudaSuccess;
+}
+
+cudaError_t ntt_batch_run(const NttBatch& nb, cudaStream_t st) {
+    for (const NttPhase& ph : nb.phases) {
+        const NttJob* jobs = (const NttJob*)nb.d_jobs + ph.first;
+        const char* name = ph.kind == 0 ? "ntt_pass_dif" : ph.kind == 1 ? "ntt_pass_dit" : "ntt_mid_fused";
+        timer().add_units(name, ph.products);
+        timer().add_bytes(name, ph.bytes);
+        TimedLaunch tl(name, st);
+        if (ph.kind == 0) k_ntt_pass_multi<true><<<ph.blocks, 256, ph.smem, st>>>(jobs, ph.njobs);
+        else if (ph.kind == 1) k_ntt_pass_multi<false><<<ph.blocks, 256, ph.smem, st>>>(jobs, ph.njobs);
+        else k_ntt_mid_multi<<<ph.blocks, 256, ph.smem, st>>>(jobs, ph.njobs);
+        G16_CUDA(cudaGetLastError());
+    }
+    return cudaSuccess;
 }
 
 }  // namespace g16

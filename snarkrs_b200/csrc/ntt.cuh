@@ -17,6 +17,7 @@
 // H = A*B - C (crates/groth16/src/cpu.rs:230-246, no division by Z).
 #pragma once
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace g16 {
@@ -62,5 +63,28 @@ cudaError_t ntt_forward(const NttTables& t, void* a, cudaStream_t st);
 cudaError_t ntt_inverse(const NttTables& t, void* a, cudaStream_t st);   // includes the 1/n scale
 // a[i] *= shift^i (crates/ntt/src/lib.rs:582), shift Montgomery
 cudaError_t ntt_distribute_powers(void* a, size_t n, const uint64_t* shift_mont, cudaStream_t st);
+
+// ---- many prover chains per launch (batched proving) ----
+// ntt_h_pipeline for many proofs of any sizes and tilings: every launch
+// covers one step of every chain (ntt_batch_setup lays the steps out).
+struct NttBatchItem {
+    const NttTables* t;     // the proof's domain tables and tiling
+    void *a, *b, *c, *h;    // device vectors of 2^t->log_n Fr; h = A B - C out
+};
+struct NttPhase {
+    int kind = 0;           // 0 inverse outer pass, 1 forward outer pass, 2 fused middle
+    uint32_t first = 0, njobs = 0, blocks = 0;
+    size_t smem = 0;
+    double products = 0, bytes = 0;   // algorithmic work, for the kernel timer
+};
+struct NttBatch {
+    std::vector<NttPhase> phases;
+    void* d_jobs = nullptr;
+    void release();
+};
+// Lays out and uploads the launches for the items (synchronises st).
+cudaError_t ntt_batch_setup(NttBatch& nb, const std::vector<NttBatchItem>& items, cudaStream_t st);
+// Enqueues them (no host synchronisation).
+cudaError_t ntt_batch_run(const NttBatch& nb, cudaStream_t st);
 
 }  // namespace g16

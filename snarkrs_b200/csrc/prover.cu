@@ -27,6 +27,7 @@
 #include "curve.cuh"
 #include "field.cuh"
 #include "formats.hpp"
+#include "gather.cuh"
 #include "g16b200.h"
 #include "host_bn254.hpp"
 #include "msm.cuh"
@@ -59,9 +60,7 @@ using namespace g16;
 // ---------------------------------------------------------------- kernels
 namespace g16d {
 
-// Stage 0: one thread per constraint row.  Zero witness values are skipped
-// and ones added without a multiply, which is exact either way
-// (crates/groth16/src/cpu.rs:150-170).
+// Stage 0: one thread per constraint row (gather.cuh).
 __global__ void __launch_bounds__(256) k_gather(const uint32_t* __restrict__ rpa, const uint32_t* __restrict__ siga,
                                                 const uint32_t* __restrict__ vida, const uint32_t* __restrict__ rpb,
                                                 const uint32_t* __restrict__ sigb, const uint32_t* __restrict__ vidb,
@@ -70,24 +69,7 @@ __global__ void __launch_bounds__(256) k_gather(const uint32_t* __restrict__ rpa
                                                 uint4* __restrict__ C) {
     uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= n) return;
-    Fr acc[2];
-    const uint32_t* rp[2] = {rpa, rpb};
-    const uint32_t* sg[2] = {siga, sigb};
-    const uint32_t* vd[2] = {vida, vidb};
-#pragma unroll
-    for (int m = 0; m < 2; m++) {
-        Fr a = Fr::zero();
-        for (uint32_t k = rp[m][row]; k < rp[m][row + 1]; k++) {
-            Fr wv = load32(reinterpret_cast<const Fr*>(w) + sg[m][k]);
-            if (wv.is_zero()) continue;
-            Fr v = load32(reinterpret_cast<const Fr*>(values) + vd[m][k]);
-            a = add(a, wv.is_one() ? v : mul(v, wv));
-        }
-        acc[m] = a;
-    }
-    store32(reinterpret_cast<Fr*>(A) + row, acc[0]);
-    store32(reinterpret_cast<Fr*>(B) + row, acc[1]);
-    store32(reinterpret_cast<Fr*>(C) + row, mul(acc[0], acc[1]));
+    gather_row(row, rpa, siga, vida, rpb, sigb, vidb, values, w, A, B, C);
 }
 
 // Stage 0 handed over (h_and_msms_from_rows): C = A * B on the caller's rows,
@@ -136,125 +118,7 @@ __global__ void __launch_bounds__(256) k_imad_peak(uint32_t* out, uint32_t iters
 
 }  // namespace g16d
 
-// ---------------------------------------------------------------- handles
-struct g16_backend {
-    int ordinal = 0;
-    uint64_t vram_limit = 0;
-    std::atomic<uint64_t> vram_used{0};
-    std::atomic<bool> constant_work{false};   // Work::Constant for every MSM of this backend
-    cudaStream_t stream = nullptr;
-    std::mutex mu;   // primitives share the scratch below
-    MsmSort sort;
-    MsmAccum acc;
-    void* d_in = nullptr;
-    size_t cap_in = 0;
-    void* d_in2 = nullptr;
-    size_t cap_in2 = 0;
-    std::vector<std::unique_ptr<NttTables>> ntt;   // by log_n
-    uint8_t* h_pinned = nullptr;                   // window sums readback
-    size_t cap_pinned = 0;
-    unsigned long long* h_work = nullptr;
-};
-
-namespace {
-
-// The device state of one proof in flight.  A prepared circuit keeps a pool of
-// these, so several proofs of the same circuit overlap on the GPU, each on its
-// own five streams (the main one and one per witness MSM) with its own scratch.
-struct Workspace {
-    void* d_w = nullptr;       // witness, n_vars Fr
-    void* d_abc = nullptr;     // A | B | C, n Fr each
-    void* d_hpoly = nullptr;   // H, n Fr
-    MsmSort sort_w[3], sort_h;  // witness sorts: the A, B (B1 and B2) and L live sets
-    MsmAccum acc[5];           // A, B2, B1, L, H
-    uint8_t* h_win = nullptr;  // pinned readback of the MSM results
-    unsigned long long* h_work = nullptr;
-    cudaStream_t stream = nullptr;             // gather -> NTT -> H MSM, and the join
-    cudaStream_t side[4] = {nullptr, nullptr, nullptr, nullptr};   // witness MSMs A, B1, L, B2, one each
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaEvent_t ev_fork = nullptr, ev_sort = nullptr;
-    cudaEvent_t ev_side[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaGraphExec_t graph = nullptr;   // stages 0-9 captured once, replayed per proof
-    uint64_t graph_kernels = 0;
-    bool graph_constant_work = false;  // the mode the graph was captured in
-    uint64_t proofs = 0;
-    uint64_t bytes = 0;                // fixed device buffers
-
-    cudaError_t init(uint32_t n_vars, uint32_t n) {
-        cudaError_t e = g16::dev_malloc(&d_w, 32ull * n_vars);
-        if (e == cudaSuccess) e = g16::dev_malloc(&d_abc, 32ull * n * 3);
-        if (e == cudaSuccess) e = g16::dev_malloc(&d_hpoly, 32ull * n);
-        if (e == cudaSuccess) e = cudaMallocHost((void**)&h_win, 5 * MSM_RESULT_SLOT_BYTES);
-        if (e == cudaSuccess) e = cudaMallocHost((void**)&h_work, 8 * sizeof(unsigned long long));
-        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
-        for (auto& x : side)
-            if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
-        for (auto& x : ev)
-            if (e == cudaSuccess) e = cudaEventCreate(&x);
-        for (cudaEvent_t* x : {&ev_fork, &ev_sort, &ev_side[0], &ev_side[1], &ev_side[2], &ev_side[3]})
-            if (e == cudaSuccess) e = cudaEventCreateWithFlags(x, cudaEventDisableTiming);
-        bytes = 32ull * n_vars + 32ull * n * 4;
-        return e;
-    }
-    void release() {
-        for (cudaStream_t s : {stream, side[0], side[1], side[2], side[3]})
-            if (s) cudaStreamSynchronize(s);
-        if (graph) cudaGraphExecDestroy(graph);
-        cudaFree(d_w);
-        cudaFree(d_abc);
-        cudaFree(d_hpoly);
-        for (auto& x : sort_w) x.release();
-        sort_h.release();
-        for (auto& a : acc) a.release();
-        if (h_win) cudaFreeHost(h_win);
-        if (h_work) cudaFreeHost(h_work);
-        for (auto& x : ev)
-            if (x) cudaEventDestroy(x);
-        for (cudaEvent_t x : {ev_fork, ev_sort, ev_side[0], ev_side[1], ev_side[2], ev_side[3]})
-            if (x) cudaEventDestroy(x);
-        for (cudaStream_t s : {side[0], side[1], side[2], side[3], stream})
-            if (s) cudaStreamDestroy(s);
-        *this = Workspace();
-    }
-};
-
-}  // namespace
-
-struct g16_circuit {
-    g16_backend* be = nullptr;
-    uint32_t n_vars = 0, n_public = 0, n = 0;
-    int log_n = 0;
-    // resident key
-    uint32_t *d_rp[2] = {nullptr, nullptr}, *d_sig[2] = {nullptr, nullptr}, *d_vid[2] = {nullptr, nullptr};
-    void* d_values = nullptr;
-    // the witness MSMs' bases with the points at infinity compacted out: A over
-    // the A live set, B1 and B2 over the B set, L over the L set (live_sets)
-    void *d_a = nullptr, *d_b1 = nullptr, *d_b2 = nullptr, *d_l = nullptr, *d_h = nullptr;
-    uint32_t* d_rank[3] = {nullptr, nullptr, nullptr};   // wire -> row in the set's bases, or MSM_DEAD
-    uint32_t rows[3] = {0, 0, 0};                        // live wires of the A, B and L sets
-    // window-shifted base tables 2^(c w) P_i at w * rows + i (msm_window_table)
-    void *t_a = nullptr, *t_b1 = nullptr, *t_b2 = nullptr, *t_l = nullptr, *t_h = nullptr;
-    int c_w = 0, c_h = 0;   // window bits of the witness and H MSMs
-    NttTables ntt;
-    G1A alpha1, beta1, delta1;
-    G2A beta2, delta2, gamma2;
-    std::vector<G1A> ic;               // verifying key: constant wire, then the public inputs
-    // workspaces: one per proof in flight
-    std::mutex mu;
-    std::condition_variable cv;
-    std::vector<std::unique_ptr<Workspace>> pool;
-    std::vector<Workspace*> idle;
-    uint32_t max_workspaces = 8;
-    uint64_t ws_estimate = 0;          // device bytes of one workspace, scratch included
-    bool serial = false;               // every stage on one stream (profiling)
-    bool graphs = true;                // replay proofs as captured CUDA graphs
-    bool tuning = false;               // g16_autotune / g16_tuning_set running: no new proofs start
-    g16_tuning tuned = {0, 0, 0, 0, 0.0, 0.0};
-    g16_stage_timings t = {0, 0, 0, 0, 0, 0};
-    uint64_t readback_bytes = 0;       // device-to-host bytes of the last proof
-    uint64_t device_bytes = 0;
-    std::vector<void*> allocs;
-};
+#include "prover.hpp"
 
 struct g16_hpoly {
     g16_circuit* owner = nullptr;
@@ -266,7 +130,7 @@ struct g16_zkey {
     ZkeyHost k;
 };
 
-namespace {
+namespace g16 {
 
 int fail(int code, const char* fmt, ...) {
     char buf[1024];
@@ -287,6 +151,10 @@ int cuda_fail(cudaError_t e, const char* what) {
     }();
     return fail(G16_ERR_DEVICE, "%s: %s (%s)", what, cudaGetErrorString(e), prev.c_str());
 }
+
+}  // namespace g16
+
+namespace {
 
 #define CK(call, what)                                  \
     do {                                                \
@@ -457,10 +325,9 @@ G2J g2_mul(const G2J& p, const g16::Fr& k) {
     return p.mul(s);
 }
 
-struct BlinderTerms {
-    G1J d1r, d1s, d1rs;
-    G2J d2s;
-};
+}  // namespace
+
+namespace g16 {
 
 BlinderTerms blinder_terms(const g16_circuit* c, const g16::Fr& r, const g16::Fr& s) {
     BlinderTerms t;
@@ -471,11 +338,6 @@ BlinderTerms blinder_terms(const g16_circuit* c, const g16::Fr& r, const g16::Fr
     t.d2s = g2_mul(G2J::from_affine(c->delta2), s);
     return t;
 }
-
-struct MsmJac {
-    G1J a, b1, l, h;
-    G2J b2;
-};
 
 void assemble(const g16_circuit* c, const MsmJac& m, const BlinderTerms& t, const g16::Fr& r, const g16::Fr& s,
               g16_proof* out) {
@@ -509,6 +371,10 @@ int check_witness(const g16_circuit* c, size_t n, const uint8_t* w_host) {
     if (w_host && !is_one_mont(w_host)) return fail(G16_ERR_CONSTANT_WIRE, "witness[0] is not 1");
     return G16_OK;
 }
+
+}  // namespace g16
+
+namespace {
 
 uint64_t elapsed_us(cudaEvent_t a, cudaEvent_t b) {
     float ms = 0;
@@ -814,11 +680,12 @@ struct TuningLock {
         int rc = acquire(c, &ws);
         if (rc) return rc;
         all.push_back(ws);
-        std::lock_guard<std::mutex> g(c->mu);
+        std::unique_lock<std::mutex> g(c->mu);
         if (c->idle.size() + 1 != c->pool.size())
             return fail(G16_ERR_INVALID_ARGUMENT, "tuning needs a circuit with no proof in flight");
         c->tuning = true;
         held = true;
+        c->cv.wait(g, [&] { return c->batch_users == 0; });   // batched submissions reading the tables finish first
         while ((int)all.size() < want) {
             if (!c->idle.empty()) {
                 all.push_back(c->idle.back());
@@ -1054,6 +921,7 @@ int g16_backend_open(int ordinal, uint64_t vram_limit, g16_backend** out) {
 void g16_backend_free(g16_backend* b) {
     if (!b) return;
     cudaSetDevice(b->ordinal);
+    batch_free(b);
     cudaStreamSynchronize(b->stream);
     b->sort.release();
     b->acc.release();
@@ -1230,6 +1098,7 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
 void g16_circuit_free(g16_circuit* c) {
     if (!c) return;
     cudaSetDevice(c->be->ordinal);
+    batch_forget(c->be, c);
     for (auto& ws : c->pool) ws->release();
     c->pool.clear();
     c->idle.clear();
@@ -1509,6 +1378,14 @@ int g16_prove_batch_timed(g16_backend* b, size_t count, g16_circuit* const* circ
         if (circuits[i]->be != b) return fail(G16_ERR_INVALID_ARGUMENT, "job %zu belongs to another backend", i);
         int rc = check_witness(circuits[i], lens[i], witnesses[i]);
         if (rc) return rc;
+    }
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    // one launch per stage for every job; host lanes only for constant-work MSMs, when
+    // G16_BATCH_ENGINE=0, or when the batch's working set does not fit the device budget
+    const char* eng = std::getenv("G16_BATCH_ENGINE");
+    if (!b->constant_work && !(eng && std::strcmp(eng, "0") == 0)) {
+        int rc = prove_batch_engine(b, count, circuits, witnesses, lens, r, s, out, done_ms);
+        if (rc != G16_ERR_DEVICE_MEMORY) return rc;
     }
     size_t lanes = 8;
     if (const char* e = std::getenv("G16_BATCH_LANES")) lanes = (size_t)std::max(1, std::atoi(e));

@@ -1,0 +1,89 @@
+"""Batched proving in one launch per stage (g16_prove_batch): every proof of a
+submission of mixed circuit sizes, repeated circuits and different tunings
+equals the same job proved alone and the oracle's proof, on the first
+submission (enqueued stage by stage), on the second (captured as a CUDA graph)
+and on the third (the graph replayed); a retuned circuit rebuilds the plan; the
+host-lane path (G16_BATCH_ENGINE=0) gives the same proofs."""
+import os
+import random
+
+import pytest
+
+import oracle as O
+import snarkrs_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+
+def blinders(seed):
+    rng = random.Random(seed)
+    return O.to_bytes(O.to_mont(rng.randrange(1, O.R_MOD))), O.to_bytes(O.to_mont(rng.randrange(1, O.R_MOD)))
+
+
+@pytest.fixture(scope="module")
+def mix(backend):
+    out = []
+    for i, (nc, ni, npub) in enumerate(((90, 8, 2), (700, 20, 4), (4500, 64, 8), (21000, 256, 16))):
+        sc = S.SynthCircuit(300 + i, nc, ni, npub)
+        zk = sc.zkey(77 + i)
+        out.append((sc, zk, O.Zkey(zk), backend.prepare(S.ProvingKey.from_bytes(zk))))
+    yield out
+    for _, _, ok, c in out:
+        c.close()
+        ok.close()
+
+
+def jobs_of(mix, order, seed):
+    jobs, meta = [], []
+    for k, i in enumerate(order):
+        sc, zk, ok, circ = mix[i]
+        w = sc.witness(seed + k)
+        r, s = blinders(seed + k)
+        jobs.append((circ, w, r, s))
+        meta.append((ok, w, r, s))
+    return jobs, meta
+
+
+def check(batch, jobs, meta):
+    for p, (circ, w, r, s), (ok, _, _, _) in zip(batch, jobs, meta):
+        assert p == circ.prove_with_blinders(w, r, s)
+        assert p.to_bytes() == ok.prove(w, O.from_bytes(r), O.from_bytes(s))
+        assert ok.verify(w[32:32 * (1 + ok.n_public)], p.to_bytes())
+
+
+def test_batch_engine_equals_singles_and_oracle(backend, mix):
+    order = [0, 1, 2, 3, 3, 2, 1, 0, 2, 2, 1]
+    jobs, meta = jobs_of(mix, order, 10)
+    launches = S.launch_count()
+    done = []
+    first = backend.prove_batch(jobs, done_ms=done)
+    assert len(done) == len(jobs) and all(d > 0 for d in done)
+    check(first, jobs, meta)
+    # the same shape twice more: captured, then replayed; different witnesses each time
+    for rep in (1, 2):
+        jobs2, meta2 = jobs_of(mix, order, 100 * rep)
+        check(backend.prove_batch(jobs2), jobs2, meta2)
+    assert S.launch_count() > launches
+
+
+def test_batch_engine_after_retuning(backend, mix):
+    sc, zk, ok, circ = mix[2]
+    t = circ.tuning()
+    circ.set_tuning(t["msm_window_bits_witness"] - 1, t["msm_window_bits_h"] + 1, 10, 1)
+    try:
+        jobs, meta = jobs_of(mix, [2, 3, 2], 500)
+        check(backend.prove_batch(jobs), jobs, meta)
+    finally:
+        circ.set_tuning(t["msm_window_bits_witness"], t["msm_window_bits_h"], t["ntt_tile_log"], t["ntt_outer_log_l"])
+
+
+def test_batch_lanes_give_the_same_proofs(backend, mix):
+    jobs, meta = jobs_of(mix, [3, 0, 1], 900)
+    engine = backend.prove_batch(jobs)
+    os.environ["G16_BATCH_ENGINE"] = "0"
+    try:
+        lanes = backend.prove_batch(jobs)
+    finally:
+        del os.environ["G16_BATCH_ENGINE"]
+    assert engine == lanes
+    check(engine, jobs, meta)
