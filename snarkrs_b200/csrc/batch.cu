@@ -86,6 +86,8 @@ struct BatchEngine {
     void* d_gather = nullptr;
     uint32_t gather_blocks = 0, gather_jobs = 0;
     uint8_t* h_res = nullptr;               // pinned: G1, G2 and H results, back to back
+    uint8_t* h_stage = nullptr;             // pinned: the jobs' witnesses, laid out as the arena's first region
+    size_t w_bytes = 0;                     // bytes of that region
     size_t res_g1 = 0, res_g2 = 0, res_h = 0;
     cudaStream_t st[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_sorted = nullptr, ev_g1 = nullptr, ev_g2 = nullptr;
@@ -107,6 +109,7 @@ struct BatchEngine {
         cudaFree(d_gather);
         cudaFree(d_arena);
         if (h_res) cudaFreeHost(h_res);
+        if (h_stage) cudaFreeHost(h_stage);
         for (cudaEvent_t e : {ev_fork, ev_sorted, ev_g1, ev_g2})
             if (e) cudaEventDestroy(e);
         for (cudaStream_t s : st)
@@ -116,8 +119,6 @@ struct BatchEngine {
 };
 
 namespace {
-
-constexpr uint64_t BATCH_REDUCE_PIECES = 4096;   // reduction pieces per MSM of a batch
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -144,24 +145,31 @@ int build(g16_backend* be, BatchEngine& E, g16_circuit* const* cs, size_t count)
         CK_BATCH(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
     for (cudaEvent_t* e : {&E.ev_fork, &E.ev_sorted, &E.ev_g1, &E.ev_g2})
         CK_BATCH(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-    // arena: per job its witness, A | B | C and H
+    // arena: every job's witness (one region, filled by one copy from the pinned
+    // staging buffer), then every job's A | B | C, then every job's H
     size_t off = 0;
     for (size_t j = 0; j < count; j++) {
-        const g16_circuit* c = cs[j];
         E.off_w.push_back(off);
-        off = align256(off + 32ull * c->n_vars);
+        off = align256(off + 32ull * cs[j]->n_vars);
+    }
+    E.w_bytes = off;
+    for (size_t j = 0; j < count; j++) {
         E.off_abc.push_back(off);
-        off = align256(off + 96ull * c->n);
+        off = align256(off + 96ull * cs[j]->n);
+    }
+    for (size_t j = 0; j < count; j++) {
         E.off_h.push_back(off);
-        off = align256(off + 32ull * c->n);
+        off = align256(off + 32ull * cs[j]->n);
     }
     CK_BATCH(g16::dev_malloc(&E.d_arena, off ? off : 256));
+    CK_BATCH(cudaMallocHost((void**)&E.h_stage, E.w_bytes ? E.w_bytes : 256));
     uint8_t* arena = (uint8_t*)E.d_arena;
     // MSM spaces: G1 (A, B1, L of every job), G2 (B2), H
     E.g1.g2 = false;
     E.g2.g2 = true;
     E.hs.g2 = false;
-    E.g1.pieces_target = E.g2.pieces_target = E.hs.pieces_target = BATCH_REDUCE_PIECES;
+    // reduction pieces: one length per space, from its bucket count (msm_batch_setup)
+    E.g1.pieces_target = E.g2.pieces_target = E.hs.pieces_target = 0;
     for (size_t j = 0; j < count; j++) {
         const g16_circuit* c = cs[j];
         const uint32_t Bw = 1u << (c->c_w - 1), Bh = 1u << (c->c_h - 1);
@@ -245,7 +253,10 @@ int build(g16_backend* be, BatchEngine& E, g16_circuit* const* cs, size_t count)
 
 // Every stage of every job, over the engine's three streams, joined on st[0].
 int enqueue(BatchEngine& E) {
-    cudaStream_t s0 = E.st[0], s1 = E.st[1], s2 = E.st[2];
+    // with kernel timing on, every step runs on one stream, so that each
+    // launch's event span is its own duration
+    const bool serial = timer().enabled;
+    cudaStream_t s0 = E.st[0], s1 = serial ? s0 : E.st[1], s2 = serial ? s0 : E.st[2];
     MsmSpace* wsp[2] = {&E.g1, &E.g2};
     MsmSpace* hsp[1] = {&E.hs};
     CK_BATCH(cudaEventRecord(E.ev_fork, s0));
@@ -361,10 +372,11 @@ int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, con
         E.accounted = need;
         b->vram_used += need;
     }
-    // witnesses in, and the key-only blinder products on the host meanwhile
-    for (size_t j = 0; j < count; j++)
-        CK_BATCH(cudaMemcpyAsync((uint8_t*)E.d_arena + E.off_w[j], witnesses[j], 32 * lens[j], cudaMemcpyHostToDevice,
-                                 E.st[0]));
+    // witnesses in: gathered into pinned memory by host threads, then one copy
+    const size_t threads = host_threads();
+    parallel_for(count, threads, [&](size_t j) { std::memcpy(E.h_stage + E.off_w[j], witnesses[j], 32 * lens[j]); });
+    CK_BATCH(cudaMemcpyAsync(E.d_arena, E.h_stage, E.w_bytes, cudaMemcpyHostToDevice, E.st[0]));
+    // the key-only blinder products on the host while the device runs
     std::vector<BlinderTerms> terms(count);
     std::vector<Fr> rr(count), ss(count);
     for (size_t j = 0; j < count; j++) {
@@ -375,7 +387,6 @@ int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, con
         rr[j] = Fr::raw(a);
         ss[j] = Fr::raw(c);
     }
-    const size_t threads = host_threads();
     std::thread blinders([&] { parallel_for(count, threads, [&](size_t j) { terms[j] = blinder_terms(cs[j], rr[j], ss[j]); }); });
     int rc = G16_OK;
     const bool use_graph = !timer().enabled && E.runs > 0;

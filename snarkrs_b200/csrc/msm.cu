@@ -4,6 +4,7 @@
 #include "common.cuh"
 #include "curve.cuh"
 #include <algorithm>
+#include <cstdlib>
 #include <atomic>
 #include <vector>
 
@@ -266,10 +267,12 @@ __global__ void __launch_bounds__(256) k_scan_add(uint32_t* __restrict__ out, ui
 constexpr uint32_t FAT_PARTIALS = 16;
 constexpr uint32_t FAT_JOBS = 64;
 
-// partials per job of a fat bucket: at least FAT_PARTIALS, at most FAT_JOBS jobs
+// partials per job of a fat bucket: at least one per thread of the folding
+// block (FAT_JOB_MIN), at most FAT_JOBS jobs
+constexpr uint32_t FAT_JOB_MIN = 128;
 __device__ __forceinline__ uint32_t fat_job_len(uint32_t ns) {
     uint32_t j = (ns + FAT_JOBS - 1) / FAT_JOBS;
-    return j < FAT_PARTIALS ? FAT_PARTIALS : j;
+    return j < FAT_JOB_MIN ? FAT_JOB_MIN : j;
 }
 
 // Entries per accumulate thread, chosen on the device from the sorted count
@@ -425,6 +428,21 @@ __device__ __forceinline__ void accumulate_chunks(const uint32_t* __restrict__ e
 
 constexpr int ACC_BLOCK_G1 = 512;   // lockstep block: 16 warps, one block per SM (<= 128 registers)
 constexpr int ACC_BLOCK_G2 = 128;
+
+// Multiprocessors of the current device (148 on a B200), cached per device.
+static uint32_t device_sms() {
+    static std::atomic<uint32_t> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    uint32_t v = cache[dev].load(std::memory_order_relaxed);
+    if (!v) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) return 148;
+        v = (uint32_t)sms;
+        cache[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
 
 // Threads in one wave of G1 accumulate blocks on the current device (one
 // block per SM), for chunk_len; 0 (no fitting) if the device cannot be read.
@@ -1380,12 +1398,14 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     G16_CUDA(cudaGetLastError());
     {
         TimedLaunch tl("msm_fat_merge", st);
-        k_fat_merge_jobs<F><<<296, 128, 128 * xyzz_bytes, st>>>(partials, s.d_offsets, s.d_seg_base, s.d_fat_list,
+        k_fat_merge_jobs<F><<<2 * device_sms(), 128, 128 * xyzz_bytes, st>>>(partials, s.d_offsets, s.d_seg_base,
+                                                                          s.d_fat_list,
                                                                 s.d_total + 2, s.d_total + 3);
     }
     {
         TimedLaunch tl("msm_fat_merge", st);
-        k_fat_merge_final<F><<<148, 64, 64 * xyzz_bytes, st>>>(partials, s.d_offsets, s.d_seg_base, s.d_fat_list,
+        k_fat_merge_final<F><<<device_sms(), 64, 64 * xyzz_bytes, st>>>(partials, s.d_offsets, s.d_seg_base,
+                                                                        s.d_fat_list,
                                                                s.d_total + 2, s.d_total + 3);
     }
     G16_CUDA(cudaGetLastError());
@@ -1472,11 +1492,23 @@ cudaError_t msm_batch_setup(MsmSources& so, MsmSpace* const* spaces, int nspaces
         const size_t pb = sp.g2 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES;
         uint64_t K = 0, blocks = 0, out_block = 0, out_set = 0;
         sp.max_hb = 0;
+        for (auto& g : sp.segs) K += g.B;
+        // one piece length for the space: its pieces about fill the device
+        // (two reduction blocks of 2^LB threads per SM), runs of at most 32
+        uint32_t piece_len = 1;
+        const uint64_t fill = (uint64_t)device_sms() * 2 * (1u << LB);
+        while (piece_len < MSM_REDUCE_MAX_SEG && K / piece_len > fill) piece_len *= 2;
+        if (const char* e = std::getenv("G16_BATCH_PIECE_LEN")) {   // tuning knob: 1, 2, 4, ..., 32
+            const int v = std::atoi(e);
+            if (v >= 1 && v <= (int)MSM_REDUCE_MAX_SEG && !(v & (v - 1))) piece_len = (uint32_t)v;
+        }
+        K = 0;
         std::vector<MsmSegDev> segdev;
         std::vector<MsmReduceDev> red;
         for (auto& g : sp.segs) {
             g.key_start = (uint32_t)K;
-            g.plan = msm_reduce_plan(1, g.B, sp.g2, sp.pieces_target);
+            const uint64_t target = sp.pieces_target ? sp.pieces_target : std::max<uint64_t>(1, g.B / piece_len);
+            g.plan = msm_reduce_plan(1, g.B, sp.g2, target);
             g.plan.direct = false;   // every segment's block terms are summed on the device
             g.block_start = (uint32_t)blocks;
             g.out_block = (uint32_t)out_block;
@@ -1627,12 +1659,7 @@ static cudaError_t space_accumulate(MsmSpace& sp, cudaStream_t st, size_t xyzz_b
                 nsegs, partials, a.d_work);
     }
     G16_CUDA(cudaGetLastError());
-    int sms = 148;
-    {
-        int dev = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+    const uint32_t sms = device_sms();
     {
         TimedLaunch tl("msm_fat_merge", st);
         k_fat_merge_jobs<F><<<2 * sms, 128, 128 * xyzz_bytes, st>>>(partials, s.d_offsets, s.d_seg_base, s.d_fat_list,
@@ -1655,7 +1682,7 @@ static cudaError_t space_accumulate(MsmSpace& sp, cudaStream_t st, size_t xyzz_b
             (const uint4*)a.d_buckets, (const MsmReduceDev*)sp.d_reduce, nsegs, (uint4*)a.d_segments);
     }
     if (nsegs) {
-        TimedLaunch tl("msm_reduce", st);
+        TimedLaunch tl("msm_reduce_sets", st);
         k_reduce_sets_multi<F, LB><<<dim3(LB + 1 + sp.max_hb, nsegs), 128, 128 * xyzz_bytes, st>>>(
             (const uint4*)a.d_segments, (const MsmReduceDev*)sp.d_reduce, (uint4*)a.d_windows);
     }

@@ -223,7 +223,10 @@ struct MsmSpaceSeg {
 
 struct MsmSpace {
     bool g2 = false;
-    uint64_t pieces_target = 4096;   // reduction pieces per segment
+    // reduction pieces per segment; 0: every segment's buckets run in pieces of
+    // one length, chosen from the space's bucket count so that the pieces of
+    // all segments about fill the device
+    uint64_t pieces_target = 0;
     std::vector<MsmSpaceSeg> segs;
     // laid out by msm_batch_setup
     uint32_t K = 0;                  // buckets over all segments
