@@ -889,9 +889,9 @@ def run_serve(args, backend=None, emit=True, fracs=(0.5, 0.9, 1.5), n_req=None):
         wits.append([sc.witness(7000 + 10 * len(wits) + j) for j in range(2)])
     budget = 120 << 30
 
-    def run(lanes, rate, n_req, seed):
+    def run(lanes, rate, n_req, seed, max_batch=64):
         rng = random.Random(seed)
-        srv = S.ProofServer(backend, budget, lanes)
+        srv = S.ProofServer(backend, budget, lanes, max_batch)
         for i, k in enumerate(keys):
             srv.register_key(i, k)
         # warm every key outside the measurement: prepare, one workspace per
@@ -930,14 +930,14 @@ def run_serve(args, backend=None, emit=True, fracs=(0.5, 0.9, 1.5), n_req=None):
                 "stats": stats}, proofs
 
     # plain capacity: mean service time over the mix, one request at a time
-    calib, _ = run(1, 1e6, 60, 1)     # back-to-back arrivals = saturated FIFO
+    calib, _ = run(1, 1e6, 60, 1, max_batch=1)     # back-to-back arrivals = saturated FIFO
     cap = calib["throughput"]
     n_req = n_req or max(100, args.steps * 40)
     results = []
     mix_ok = True
     for frac in fracs:
         rate = frac * cap
-        plain, pp = run(1, rate, n_req, 42 + int(frac * 10))
+        plain, pp = run(1, rate, n_req, 42 + int(frac * 10), max_batch=1)
         served, sp = run(args.lanes, rate, n_req, 42 + int(frac * 10))
         mix_ok &= all(pp[j] == sp[j] for j in pp)
         results.append({"offered_fraction_of_plain_capacity": frac, "plain_fifo": plain, "served": served})

@@ -238,19 +238,26 @@ int g16_prove_batch_timed(g16_backend *b, size_t count, g16_circuit *const *circ
                           const uint8_t *s_mont, g16_proof *out, double *done_ms);
 
 /* Served proving (no reference counterpart; the reference proves one request
- * per call).  A request loop with continuous batching: `lanes` workers take
- * queued requests as soon as they are free, so proofs of different circuits
- * and sizes overlap on the device.  Registered keys are prepared on first use
+ * per call).  A request loop with continuous batching: each of `lanes`
+ * workers, as soon as it is free, takes every request queued at that moment
+ * (in arrival order, up to the batch limits) and proves them together as one
+ * g16_prove_batch submission, so requests that arrive while others are on the
+ * GPU are admitted with the next free worker's batch, and the workers'
+ * batches overlap on the device.  Registered keys are prepared on first use
  * and stay resident in HBM while their device bytes fit key_budget_bytes
  * (0 = unlimited); a key that does not fit evicts least recently used idle
- * keys.  A proof starts when its circuit can hand out a workspace within the
- * backend's device-memory budget.  Results equal single g16_prove_with_blinders
- * calls. */
+ * keys.  A batch starts when its working set fits the backend's device-memory
+ * budget.  Results equal single g16_prove_with_blinders calls.  Limits: at
+ * most 64 requests and about 2^21 witness wires per batch (G16_SERVE_BATCH,
+ * G16_SERVE_BATCH_WIRES). */
 typedef struct g16_server g16_server;
 typedef struct {
     uint64_t submitted, completed, prepared, evicted, resident_keys, resident_bytes, queued;
 } g16_server_stats;
 int g16_server_new(g16_backend *b, uint64_t key_budget_bytes, int lanes, g16_server **out);
+/* Requests per batch (at least 1); 1 proves each request alone on a
+ * workspace: plain one-proof-at-a-time serving. */
+int g16_server_set_max_batch(g16_server *s, size_t max_batch);
 /* Keeps a host copy of the .zkey bytes; the key is prepared when first needed. */
 int g16_server_register_key(g16_server *s, uint32_t key_id, const uint8_t *zkey, size_t len);
 /* Copies the witness (n Montgomery Fr) and the blinders; returns a ticket. */

@@ -550,11 +550,13 @@ class _ServerStats(ctypes.Structure):
 class ProofServer:
     """Served proving with continuous batching over a set of registered keys."""
 
-    def __init__(self, backend, key_budget_bytes=0, lanes=4):
+    def __init__(self, backend, key_budget_bytes=0, lanes=4, max_batch=64):
+        """lanes: concurrent batches; max_batch: requests per batch (1 = plain one-at-a-time)."""
         h = ctypes.c_void_p()
         check(lib().g16_server_new(backend._h, ctypes.c_uint64(key_budget_bytes), int(lanes), ctypes.byref(h)))
         self._h = h
         self.backend = backend
+        check(lib().g16_server_set_max_batch(h, ctypes.c_size_t(max_batch)))
 
     def register_key(self, key_id, zkey_bytes):
         check(lib().g16_server_register_key(self._h, ctypes.c_uint32(key_id), bytes(zkey_bytes),

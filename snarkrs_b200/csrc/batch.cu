@@ -75,31 +75,56 @@ static BatchKey key_of(const g16_circuit* c) {
             c->t_h};
 }
 
+// One batched submission's device state.  The buffers are kept across
+// submissions and only grow, so a submission of a new mix of circuits (a new
+// layout) allocates nothing once the engine has seen one as large; the layout
+// itself (offsets, descriptors) is rebuilt when the mix changes, and the CUDA
+// graph is kept for the layout it was captured for.
 struct BatchEngine {
-    std::vector<BatchKey> key;
-    void* d_arena = nullptr;
+    std::vector<BatchKey> key;              // the layout built; empty: none
     uint64_t accounted = 0;                 // device bytes counted against the backend's budget
+    void* d_arena = nullptr;
+    size_t cap_arena = 0;
     std::vector<size_t> off_w, off_abc, off_h;
     MsmSpace g1, g2, hs;
     MsmSources src_w, src_h;
     NttBatch ntt;
     void* d_gather = nullptr;
+    size_t cap_gather = 0;
     uint32_t gather_blocks = 0, gather_jobs = 0;
     uint8_t* h_res = nullptr;               // pinned: G1, G2 and H results, back to back
+    size_t cap_res = 0;
     uint8_t* h_stage = nullptr;             // pinned: the jobs' witnesses, laid out as the arena's first region
+    size_t cap_stage = 0;
     size_t w_bytes = 0;                     // bytes of that region
     size_t res_g1 = 0, res_g2 = 0, res_h = 0;
     cudaStream_t st[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_sorted = nullptr, ev_g1 = nullptr, ev_g2 = nullptr;
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_kernels = 0;
-    int runs = 0;
+    int runs = 0;                           // submissions on the current layout
+
+    // forget the layout (and its graph); the buffers stay
+    void drop_layout() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        graph_kernels = 0;
+        runs = 0;
+        key.clear();
+        off_w.clear();
+        off_abc.clear();
+        off_h.clear();
+        g1.segs.clear();
+        g2.segs.clear();
+        hs.segs.clear();
+        src_w.srcs.clear();
+        src_h.srcs.clear();
+    }
 
     void release() {
         for (cudaStream_t s : st)
             if (s) cudaStreamSynchronize(s);
-        if (graph) cudaGraphExecDestroy(graph);
-        graph = nullptr;
+        drop_layout();
         g1.release();
         g2.release();
         hs.release();
@@ -116,6 +141,15 @@ struct BatchEngine {
             if (s) cudaStreamDestroy(s);
         *this = BatchEngine();
     }
+};
+
+// The backend's engines: several submissions may run at once, each on its own
+// engine and streams, so that one's host work (staging, assembly) overlaps
+// another's device work.
+struct BatchPool {
+    std::vector<std::unique_ptr<BatchEngine>> all;
+    std::vector<BatchEngine*> idle;
+    std::condition_variable cv;
 };
 
 namespace {
@@ -139,12 +173,38 @@ uint64_t plan_estimate(g16_circuit* const* cs, size_t count) {
     return b + (8ull << 20);
 }
 
-int build(g16_backend* be, BatchEngine& E, g16_circuit* const* cs, size_t count) {
-    E.release();
-    for (cudaStream_t* s : {&E.st[0], &E.st[1], &E.st[2]})
-        CK_BATCH(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
-    for (cudaEvent_t* e : {&E.ev_fork, &E.ev_sorted, &E.ev_g1, &E.ev_g2})
-        CK_BATCH(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+// device buffer that only grows
+cudaError_t grow_dev(void*& p, size_t& cap, size_t need) {
+    if (p && need <= cap) return cudaSuccess;
+    cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t n = need + need / 4 + 256;
+    cudaError_t e = g16::dev_malloc(&p, n);
+    if (e == cudaSuccess) cap = n;
+    return e;
+}
+
+// pinned host buffer that only grows
+cudaError_t grow_pinned(uint8_t*& p, size_t& cap, size_t need) {
+    if (p && need <= cap) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    const size_t n = need + need / 4 + 256;
+    cudaError_t e = cudaMallocHost((void**)&p, n);
+    if (e == cudaSuccess) cap = n;
+    return e;
+}
+
+int build(BatchEngine& E, g16_circuit* const* cs, size_t count) {
+    E.drop_layout();
+    if (!E.st[0]) {
+        for (cudaStream_t* s : {&E.st[0], &E.st[1], &E.st[2]})
+            CK_BATCH(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
+        for (cudaEvent_t* e : {&E.ev_fork, &E.ev_sorted, &E.ev_g1, &E.ev_g2})
+            CK_BATCH(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
     // arena: every job's witness (one region, filled by one copy from the pinned
     // staging buffer), then every job's A | B | C, then every job's H
     size_t off = 0;
@@ -161,8 +221,8 @@ int build(g16_backend* be, BatchEngine& E, g16_circuit* const* cs, size_t count)
         E.off_h.push_back(off);
         off = align256(off + 32ull * cs[j]->n);
     }
-    CK_BATCH(g16::dev_malloc(&E.d_arena, off ? off : 256));
-    CK_BATCH(cudaMallocHost((void**)&E.h_stage, E.w_bytes ? E.w_bytes : 256));
+    CK_BATCH(grow_dev(E.d_arena, E.cap_arena, off));
+    CK_BATCH(grow_pinned(E.h_stage, E.cap_stage, E.w_bytes));
     uint8_t* arena = (uint8_t*)E.d_arena;
     // MSM spaces: G1 (A, B1, L of every job), G2 (B2), H
     E.g1.g2 = false;
@@ -238,16 +298,15 @@ int build(g16_backend* be, BatchEngine& E, g16_circuit* const* cs, size_t count)
         gj.push_back(g);
     }
     CK_BATCH(ntt_batch_setup(E.ntt, items, E.st[0]));
-    CK_BATCH(g16::dev_malloc(&E.d_gather, gj.size() * sizeof(g16d::GatherJob)));
+    CK_BATCH(grow_dev(E.d_gather, E.cap_gather, gj.size() * sizeof(g16d::GatherJob)));
     CK_BATCH(cudaMemcpy(E.d_gather, gj.data(), gj.size() * sizeof(g16d::GatherJob), cudaMemcpyHostToDevice));
     E.gather_blocks = blocks;
     E.gather_jobs = (uint32_t)gj.size();
     E.res_g1 = (size_t)E.g1.result_points * XYZZ_G1_BYTES;
     E.res_g2 = (size_t)E.g2.result_points * XYZZ_G2_BYTES;
     E.res_h = (size_t)E.hs.result_points * XYZZ_G1_BYTES;
-    CK_BATCH(cudaMallocHost((void**)&E.h_res, E.res_g1 + E.res_g2 + E.res_h + 64));
+    CK_BATCH(grow_pinned(E.h_res, E.cap_res, E.res_g1 + E.res_g2 + E.res_h + 64));
     for (size_t j = 0; j < count; j++) E.key.push_back(key_of(cs[j]));
-    (void)be;
     return G16_OK;
 }
 
@@ -310,19 +369,23 @@ size_t host_threads() {
 void batch_forget(g16_backend* b, const g16_circuit* c) {
     std::lock_guard<std::mutex> g(b->batch_mu);
     if (!b->batch) return;
-    for (auto& k : b->batch->key)
-        if (k.c == c) {
-            b->vram_used -= std::min<uint64_t>(b->vram_used, b->batch->accounted);
-            b->batch->release();
-            return;
-        }
+    // engines in use belong to submissions whose circuits are alive; idle ones
+    // holding a layout over c forget it
+    for (BatchEngine* E : b->batch->idle)
+        for (auto& k : E->key)
+            if (k.c == c) {
+                E->drop_layout();
+                break;
+            }
 }
 
 void batch_free(g16_backend* b) {
     std::lock_guard<std::mutex> g(b->batch_mu);
     if (!b->batch) return;
-    b->vram_used -= std::min<uint64_t>(b->vram_used, b->batch->accounted);
-    b->batch->release();
+    for (auto& E : b->batch->all) {
+        b->vram_used -= std::min<uint64_t>(b->vram_used, E->accounted);
+        E->release();
+    }
     delete b->batch;
     b->batch = nullptr;
 }
@@ -331,7 +394,42 @@ int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, con
                        const size_t* lens, const uint8_t* r, const uint8_t* s, g16_proof* out, double* done_ms) {
     const auto t_start = std::chrono::steady_clock::now();
     if (!count) return G16_OK;
-    std::lock_guard<std::mutex> bg(b->batch_mu);
+    // an idle engine, preferably one whose layout (and graph) is this mix's
+    std::vector<BatchKey> want;
+    for (size_t j = 0; j < count; j++) want.push_back(key_of(cs[j]));
+    BatchEngine* eng = nullptr;
+    size_t max_engines = 4;
+    if (const char* e = std::getenv("G16_BATCH_ENGINES")) max_engines = (size_t)std::max(1, std::min(8, std::atoi(e)));
+    {
+        std::unique_lock<std::mutex> lk(b->batch_mu);
+        if (!b->batch) b->batch = new BatchPool();
+        BatchPool& P = *b->batch;
+        P.cv.wait(lk, [&] { return !P.idle.empty() || P.all.size() < max_engines; });
+        for (size_t i = 0; i < P.idle.size() && !eng; i++)
+            if (P.idle[i]->key == want) {
+                eng = P.idle[i];
+                P.idle.erase(P.idle.begin() + (long)i);
+            }
+        if (!eng && !P.idle.empty()) {
+            eng = P.idle.back();
+            P.idle.pop_back();
+        }
+        if (!eng) {
+            P.all.push_back(std::make_unique<BatchEngine>());
+            eng = P.all.back().get();
+        }
+    }
+    struct GiveBack {
+        g16_backend* b;
+        BatchEngine* e;
+        ~GiveBack() {
+            {
+                std::lock_guard<std::mutex> g(b->batch_mu);
+                b->batch->idle.push_back(e);
+            }
+            b->batch->cv.notify_all();
+        }
+    } give_back{b, eng};
     // no circuit may be retuned while the batch reads its tables
     std::vector<g16_circuit*> distinct(cs, cs + count);
     std::sort(distinct.begin(), distinct.end());
@@ -353,24 +451,21 @@ int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, con
             }
         }
     } release_guard{distinct};
-    if (!b->batch) b->batch = new BatchEngine();
-    BatchEngine& E = *b->batch;
-    bool same = E.key.size() == count;
-    for (size_t j = 0; same && j < count; j++) same = E.key[j] == key_of(cs[j]);
-    if (!same) {
-        b->vram_used -= std::min<uint64_t>(b->vram_used, E.accounted);
-        E.release();
+    BatchEngine& E = *eng;
+    if (!(E.key == want)) {
         const uint64_t need = plan_estimate(cs, count);
-        if (b->vram_used + need > b->vram_limit)
-            return fail(G16_ERR_DEVICE_MEMORY, "batch of %zu proofs needs about %llu MiB of device memory", count,
-                        (unsigned long long)(need >> 20));
-        int rc = build(b, E, cs, count);
+        if (need > E.accounted) {   // the engine's buffers grow: check and count the difference
+            if (b->vram_used + (need - E.accounted) > b->vram_limit)
+                return fail(G16_ERR_DEVICE_MEMORY, "batch of %zu proofs needs about %llu MiB of device memory", count,
+                            (unsigned long long)(need >> 20));
+            b->vram_used += need - E.accounted;
+            E.accounted = need;
+        }
+        int rc = build(E, cs, count);
         if (rc != G16_OK) {
-            E.release();
+            E.drop_layout();
             return rc;
         }
-        E.accounted = need;
-        b->vram_used += need;
     }
     // witnesses in: gathered into pinned memory by host threads, then one copy
     const size_t threads = host_threads();

@@ -1447,6 +1447,7 @@ void MsmSpace::release() {
     cudaFree(d_segdev);
     cudaFree(d_reduce);
     d_segdev = d_reduce = nullptr;
+    cap_segdev = cap_reduce = 0;
 }
 
 void MsmSources::release() {
@@ -1456,13 +1457,13 @@ void MsmSources::release() {
     d_desc = nullptr;
     d_blk = nullptr;
     d_std = nullptr;
+    cap_desc = cap_blk = cap_std = 0;
 }
 
+// Upload a descriptor table into a device buffer that only grows (cap in bytes).
 template <class T>
-static cudaError_t upload_vec(void*& d, const std::vector<T>& v, cudaStream_t st) {
-    cudaFree(d);
-    d = nullptr;
-    G16_CUDA(g16::dev_malloc(&d, (v.empty() ? 1 : v.size()) * sizeof(T)));
+static cudaError_t upload_vec(void*& d, size_t& cap, const std::vector<T>& v, cudaStream_t st) {
+    G16_CUDA(grow_bytes(d, cap, (v.empty() ? 1 : v.size()) * sizeof(T)));
     if (!v.empty()) G16_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
     return cudaSuccess;
 }
@@ -1560,17 +1561,15 @@ cudaError_t msm_batch_setup(MsmSources& so, MsmSpace* const* spaces, int nspaces
         G16_CUDA(grow_bytes(a.d_segments, a.cap_segments, (out_block + 1) * pb));
         G16_CUDA(grow_bytes(a.d_windows, a.cap_windows, (out_set + 1) * pb));
         if (!a.d_work) G16_CUDA(g16::dev_malloc((void**)&a.d_work, sizeof(unsigned long long)));
-        G16_CUDA(upload_vec(sp.d_segdev, segdev, st));
-        G16_CUDA(upload_vec(sp.d_reduce, red, st));
+        G16_CUDA(upload_vec(sp.d_segdev, sp.cap_segdev, segdev, st));
+        G16_CUDA(upload_vec(sp.d_reduce, sp.cap_reduce, red, st));
     }
     // sources: one block of 256 scalars never straddles two sources
     std::vector<MsmSourceDev> desc;
     std::vector<uint32_t> blk;
     size_t std_elems = 0;
     for (auto& src : so.srcs) std_elems += src.n;
-    cudaFree(so.d_std);
-    so.d_std = nullptr;
-    G16_CUDA(g16::dev_malloc(&so.d_std, (std_elems ? std_elems : 1) * 32));
+    G16_CUDA(grow_bytes(so.d_std, so.cap_std, (std_elems ? std_elems : 1) * 32));
     uint64_t blocks = 0, off = 0;
     for (auto& src : so.srcs) {
         MsmSourceDev d = {};
@@ -1595,9 +1594,9 @@ cudaError_t msm_batch_setup(MsmSources& so, MsmSpace* const* spaces, int nspaces
         return cudaErrorInvalidValue;
     }
     so.total_blocks = (uint32_t)blocks;
-    G16_CUDA(upload_vec(so.d_desc, desc, st));
+    G16_CUDA(upload_vec(so.d_desc, so.cap_desc, desc, st));
     void* dblk = so.d_blk;
-    G16_CUDA(upload_vec(dblk, blk, st));
+    G16_CUDA(upload_vec(dblk, so.cap_blk, blk, st));
     so.d_blk = (uint32_t*)dblk;
     G16_CUDA(cudaStreamSynchronize(st));
     return cudaSuccess;

@@ -238,6 +238,7 @@ struct MsmSpace {
     MsmAccum acc;                    // partials, bucket sums, blocks' points (d_segments), results (d_windows)
     void* d_segdev = nullptr;        // accumulate descriptors
     void* d_reduce = nullptr;        // reduction descriptors
+    size_t cap_segdev = 0, cap_reduce = 0;
     void release();
 };
 
@@ -261,12 +262,14 @@ struct MsmSources {
     void* d_desc = nullptr;
     uint32_t* d_blk = nullptr;
     void* d_std = nullptr;           // standard-form copies of the scalars
+    size_t cap_desc = 0, cap_blk = 0, cap_std = 0;   // bytes; the buffers only grow
     void release();
 };
 
-// Lays out every space's segments (keys, reduction plans), allocates the
-// spaces' buffers for the entries the sources can produce, and uploads the
-// descriptors.  Synchronises st.
+// Lays out every space's segments (keys, reduction plans), grows the spaces'
+// buffers to the entries the sources can produce, and uploads the descriptors;
+// buffers are kept across calls (only grown), so a new layout of a similar
+// batch allocates nothing.  Synchronises st.
 cudaError_t msm_batch_setup(MsmSources& so, MsmSpace* const* spaces, int nspaces, cudaStream_t st);
 // Sorts every source into its segments (no host synchronisation).
 cudaError_t msm_batch_sort(MsmSources& so, MsmSpace* const* spaces, int nspaces, cudaStream_t st);

@@ -41,6 +41,11 @@ __device__ __forceinline__ void st_g(uint4* g, size_t i, const Fr& x) {
     g[2 * i + 1] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
 }
 
+// The butterflies, the coset multiply and the join use mul, the CIOS product
+// on 32x32->64-bit multiply-adds (field.cuh), which measured faster than the
+// PTX carry-chain form mul_cc; the table builders below keep mul_cc, so both
+// forms stay under the parity tests.
+
 // One radix-2 stage on a shared-memory tile.  The tile holds elements
 // i = hi*2^(s_lo+k) + mid*2^s_lo + (lo0 + l) at smem slot mid*L + l; stage
 // s = s_lo + j pairs mid values differing in bit j.  The butterfly's
@@ -63,9 +68,9 @@ __device__ __forceinline__ void run_stage(uint4* sm, uint32_t j, uint32_t s_lo, 
         if (DIF) {
             Fr d = sub(a, b);
             a = add(a, b);
-            b = pos ? mul_cc(d, ld_g(tw, (size_t)pos << (log_n - s - 1))) : d;
+            b = pos ? mul(d, ld_g(tw, (size_t)pos << (log_n - s - 1))) : d;
         } else {
-            Fr t = pos ? mul_cc(b, ld_g(tw, (size_t)pos << (log_n - s - 1))) : b;
+            Fr t = pos ? mul(b, ld_g(tw, (size_t)pos << (log_n - s - 1))) : b;
             b = sub(a, t);
             a = add(a, t);
         }
@@ -105,9 +110,9 @@ __device__ __forceinline__ void ntt_pass_tile(uint4* sm, uint4* data, uint32_t b
         uint32_t mid = e >> log_L, l = e & (L - 1u);
         size_t gi = (hi << (s_lo + k)) | ((size_t)mid << s_lo) | (lo0 + l);
         Fr x = ld_s(sm, e);
-        if (scale) x = mul_cc(x, sc);
+        if (scale) x = mul(x, sc);
         if (join_out) {
-            Fr h = sub(mul_cc(ld_rw(join_a, gi), ld_rw(join_b, gi)), x);
+            Fr h = sub(mul(ld_rw(join_a, gi), ld_rw(join_b, gi)), x);
             st_g(join_out, gi, h);
         } else {
             st_g(data, gi, x);
@@ -145,7 +150,7 @@ __device__ __forceinline__ void ntt_mid_tile(uint4* sm, uint4* data, uint32_t bx
         run_stage<true>(sm, (uint32_t)j, 0, 0, 0, log_n, tile / 2, tw_inv);
         __syncthreads();
     }
-    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) st_s(sm, e, mul_cc(ld_s(sm, e), ld_g(coset, base + e)));
+    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) st_s(sm, e, mul(ld_s(sm, e), ld_g(coset, base + e)));
     __syncthreads();
     for (uint32_t j = 0; j < k; j++) {
         run_stage<false>(sm, j, 0, 0, 0, log_n, tile / 2, tw);
@@ -154,7 +159,7 @@ __device__ __forceinline__ void ntt_mid_tile(uint4* sm, uint4* data, uint32_t bx
     for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
         Fr x = ld_s(sm, e);
         if (join_out) {
-            st_g(join_out, base + e, sub(mul_cc(ld_rw(join_a, base + e), ld_rw(join_b, base + e)), x));
+            st_g(join_out, base + e, sub(mul(ld_rw(join_a, base + e), ld_rw(join_b, base + e)), x));
         } else {
             st_g(data, base + e, x);
         }
@@ -483,6 +488,7 @@ using g16d::NttJob;
 void NttBatch::release() {
     cudaFree(d_jobs);
     d_jobs = nullptr;
+    cap_jobs = 0;
     phases.clear();
 }
 
@@ -495,7 +501,7 @@ void NttBatch::release() {
 // runs after every other phase, in one launch per kind of pass.
 cudaError_t ntt_batch_setup(NttBatch& nb, const std::vector<NttBatchItem>& items, cudaStream_t st) {
     set_attrs();
-    nb.release();
+    nb.phases.clear();
     struct ItemPlan {
         uint32_t log_n, k0;
         std::vector<Pass> outer;
@@ -600,7 +606,14 @@ cudaError_t ntt_batch_setup(NttBatch& nb, const std::vector<NttBatchItem>& items
         add_phase(2, mids);
         add_phase(1, passes);
     }
-    G16_CUDA(g16::dev_malloc(&nb.d_jobs, (all.empty() ? 1 : all.size()) * sizeof(NttJob)));
+    const size_t need = (all.empty() ? 1 : all.size()) * sizeof(NttJob);
+    if (need > nb.cap_jobs) {   // the job table only grows
+        cudaFree(nb.d_jobs);
+        nb.d_jobs = nullptr;
+        nb.cap_jobs = 0;
+        G16_CUDA(g16::dev_malloc(&nb.d_jobs, need + need / 2));
+        nb.cap_jobs = need + need / 2;
+    }
     if (!all.empty()) G16_CUDA(cudaMemcpyAsync(nb.d_jobs, all.data(), all.size() * sizeof(NttJob), cudaMemcpyHostToDevice, st));
     G16_CUDA(cudaStreamSynchronize(st));
     return cudaSuccess;

@@ -80,6 +80,7 @@ struct NttPhase {
 struct NttBatch {
     std::vector<NttPhase> phases;
     void* d_jobs = nullptr;
+    size_t cap_jobs = 0;    // bytes; the job table only grows
     void release();
 };
 // Lays out and uploads the launches for the items (synchronises st).

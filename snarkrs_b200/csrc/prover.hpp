@@ -14,7 +14,7 @@
 #include "ntt.cuh"
 
 namespace g16 {
-struct BatchEngine;   // batched proving (batch.cu)
+struct BatchPool;   // batched proving (batch.cu)
 }
 
 struct g16_backend {
@@ -34,8 +34,8 @@ struct g16_backend {
     uint8_t* h_pinned = nullptr;                   // window sums readback
     size_t cap_pinned = 0;
     unsigned long long* h_work = nullptr;
-    std::mutex batch_mu;                           // one batched submission at a time
-    g16::BatchEngine* batch = nullptr;             // the batched-proving engine, built on first use
+    std::mutex batch_mu;                           // guards batch
+    g16::BatchPool* batch = nullptr;               // the batched-proving engines, built on first use
 };
 
 namespace g16 {

@@ -1,20 +1,25 @@
 // Served proving: a request loop with continuous batching.
 //
 // Requests (a registered key id, a witness, r and s) enter a FIFO queue.
-// `lanes` worker threads each take the next request as soon as they are free,
-// so requests that arrive while others are on the GPU are admitted as lanes
-// free up and their kernels overlap on the device (each proof runs on its own
-// workspace: five streams, its own scratch).  Admission by device memory has
-// two levels:
+// `lanes` worker threads each take, as soon as they are free, every request
+// queued at that moment (in arrival order, up to a work cap) and prove them
+// together in one batched submission (g16_prove_batch: each stage of all of
+// them in one launch, any mix of circuits and sizes).  Requests that arrive
+// while a batch is on the GPU wait for the next free worker, which takes them
+// all, and the workers' batches overlap on the device (each on its own
+// engine: streams and scratch).  Admission by device memory has two levels:
 //   * proving keys are prepared on first use and stay resident in HBM while
 //     the sum of resident keys' device bytes fits the key budget; a key that
 //     does not fit evicts the least recently used idle keys first;
-//   * a proof starts only when its circuit can hand out a workspace, which
-//     waits while the backend's device-memory budget has no room for one.
+//   * a batch starts only when its working set fits the backend's
+//     device-memory budget (otherwise its proofs run one by one on workspaces,
+//     each waiting for room).
 // The result of every request is the same as proving it alone.
 //
 // Built on the public C ABI only (include/g16b200.h).
+#include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -66,6 +71,8 @@ struct g16_server {
     uint64_t submitted = 0, completed = 0, prepared = 0, evicted = 0;
     std::vector<std::thread> workers;
     bool stop = false;
+    size_t max_batch = 64;          // requests per batch
+    uint64_t batch_wires = 1u << 21;   // work cap of a batch: witness wires summed
 };
 
 namespace {
@@ -138,40 +145,106 @@ int ensure_resident(g16_server* sv, uint32_t id, std::unique_lock<std::mutex>& l
     return rc;
 }
 
+std::string last_error_text() {
+    char buf[512];
+    g16_last_error(buf, sizeof buf);
+    return buf;
+}
+
+// Called with the lock held: the request is finished.
+void complete(g16_server* sv, Request* q, int rc, const std::string& err) {
+    q->rc = rc;
+    q->err = err;
+    q->done = true;
+    std::vector<uint8_t>().swap(q->witness);
+    sv->completed++;
+}
+
+// Work of a request for the batch cap: its witness length (wires).
+uint64_t work_of(const Request* q) { return q->witness.size() / 32; }
+
 void worker(g16_server* sv) {
     std::unique_lock<std::mutex> lk(sv->mu);
     for (;;) {
         sv->cv_work.wait(lk, [&] { return sv->stop || !sv->queue.empty(); });
         if (sv->stop && sv->queue.empty()) return;
-        Request* q = sv->queue.front();
-        sv->queue.pop_front();
-        std::string err;
-        int rc = ensure_resident(sv, q->key_id, lk, err);
-        KeyEntry& k = sv->keys[q->key_id];
-        if (rc == G16_OK) {
+        // every queued request, in arrival order, while the batch's work stays
+        // under the cap (the first one always goes)
+        std::vector<Request*> batch;
+        uint64_t work = 0;
+        while (!sv->queue.empty() && batch.size() < sv->max_batch) {
+            Request* q = sv->queue.front();
+            if (!batch.empty() && work + work_of(q) > sv->batch_wires) break;
+            sv->queue.pop_front();
+            work += work_of(q);
+            batch.push_back(q);
+        }
+        if (!sv->queue.empty()) sv->cv_work.notify_one();   // the rest is another worker's
+        // keys resident and pinned for the batch; requests refused up front end here
+        std::vector<Request*> run;
+        std::vector<g16_circuit*> circs;
+        for (Request* q : batch) {
+            std::string err;
+            int rc = ensure_resident(sv, q->key_id, lk, err);
+            KeyEntry& k = sv->keys[q->key_id];
+            if (rc == G16_OK && q->witness.size() / 32 != g16_circuit_n_vars(k.circ)) {
+                rc = G16_ERR_WITNESS_LENGTH;
+                err = "witness has " + std::to_string(q->witness.size() / 32) + " values, the circuit has " +
+                      std::to_string(g16_circuit_n_vars(k.circ)) + " wires";
+            }
+            if (rc != G16_OK) {
+                q->started = q->finished = Clock::now();
+                complete(sv, q, rc, err);
+                continue;
+            }
             k.in_use++;
             k.last_use = ++sv->clock;
-            g16_circuit* c = k.circ;
-            lk.unlock();
-            q->started = Clock::now();
-            rc = g16_prove_with_blinders(c, q->witness.data(), q->witness.size() / 32, q->r, q->s, &q->proof);
-            if (rc != G16_OK) {
-                char buf[512];
-                g16_last_error(buf, sizeof buf);
-                err = buf;
-            }
-            q->finished = Clock::now();
-            lk.lock();
-            k.in_use--;
-            sv->cv_keys.notify_all();
-        } else {
-            q->started = q->finished = Clock::now();
+            run.push_back(q);
+            circs.push_back(k.circ);
         }
-        q->rc = rc;
-        q->err = err;
-        q->done = true;
-        std::vector<uint8_t>().swap(q->witness);
-        sv->completed++;
+        if (!run.empty()) {
+            lk.unlock();
+            const size_t n = run.size();
+            std::vector<const uint8_t*> wits(n);
+            std::vector<size_t> lens(n);
+            std::vector<uint8_t> rs(32 * n), ss(32 * n);
+            std::vector<g16_proof> proofs(n);
+            std::vector<double> done(n, 0.0);
+            for (size_t i = 0; i < n; i++) {
+                wits[i] = run[i]->witness.data();
+                lens[i] = run[i]->witness.size() / 32;
+                std::memcpy(&rs[32 * i], run[i]->r, 32);
+                std::memcpy(&ss[32 * i], run[i]->s, 32);
+            }
+            const Clock::time_point t0 = Clock::now();
+            for (Request* q : run) q->started = t0;
+            // max_batch 1 is plain one-proof-at-a-time proving (a workspace per proof)
+            int rc = sv->max_batch == 1
+                         ? g16_prove_with_blinders(circs[0], wits[0], lens[0], run[0]->r, run[0]->s, &proofs[0])
+                         : g16_prove_batch_timed(sv->b, n, circs.data(), wits.data(), lens.data(), rs.data(),
+                                                 ss.data(), proofs.data(), done.data());
+            if (sv->max_batch == 1 && rc == G16_OK)
+                done[0] = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+            std::vector<int> rcs(n, rc);
+            std::vector<std::string> errs(n, rc == G16_OK ? std::string() : last_error_text());
+            if (rc != G16_OK) {
+                // the batch failed as a whole: each request alone gets its own status
+                for (size_t i = 0; i < n; i++) {
+                    rcs[i] = g16_prove_with_blinders(circs[i], wits[i], lens[i], run[i]->r, run[i]->s, &proofs[i]);
+                    errs[i] = rcs[i] == G16_OK ? std::string() : last_error_text();
+                    done[i] = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+                }
+            }
+            lk.lock();
+            for (size_t i = 0; i < n; i++) {
+                Request* q = run[i];
+                q->finished = t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double, std::milli>(done[i]));
+                q->proof = proofs[i];
+                sv->keys[q->key_id].in_use--;
+                complete(sv, q, rcs[i], errs[i]);
+            }
+            sv->cv_keys.notify_all();
+        }
         sv->cv_done.notify_all();
     }
 }
@@ -188,8 +261,20 @@ int g16_server_new(g16_backend* b, uint64_t key_budget_bytes, int lanes, g16_ser
     auto sv = std::make_unique<g16_server>();
     sv->b = b;
     sv->budget = key_budget_bytes ? key_budget_bytes : ~0ull;
+    if (const char* e = std::getenv("G16_SERVE_BATCH")) sv->max_batch = (size_t)std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("G16_SERVE_BATCH_WIRES")) sv->batch_wires = std::max<uint64_t>(1, std::strtoull(e, nullptr, 10));
     for (int i = 0; i < lanes; i++) sv->workers.emplace_back(worker, sv.get());
     *out = sv.release();
+    return G16_OK;
+}
+
+int g16_server_set_max_batch(g16_server* sv, size_t max_batch) {
+    if (!sv || max_batch < 1) {
+        g16::set_error("g16_server_set_max_batch: need a server and at least 1");
+        return G16_ERR_INVALID_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> g(sv->mu);
+    sv->max_batch = max_batch;
     return G16_OK;
 }
 

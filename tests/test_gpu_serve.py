@@ -32,10 +32,10 @@ def alone(backend, zk, w, r, s):
     return p
 
 
-@pytest.mark.parametrize("lanes,budget", [(4, 0), (3, 1)])
-def test_served_results_equal_proofs_alone(backend, keys, lanes, budget):
-    # budget 1: every new key evicts the idle ones (LRU path)
-    srv = S.ProofServer(backend, budget, lanes)
+@pytest.mark.parametrize("lanes,budget,max_batch", [(4, 0, 64), (3, 1, 64), (2, 0, 1)])
+def test_served_results_equal_proofs_alone(backend, keys, lanes, budget, max_batch):
+    # budget 1: every new key evicts the idle ones (LRU path); max_batch 1: plain serving
+    srv = S.ProofServer(backend, budget, lanes, max_batch)
     for i, (_, zk) in enumerate(keys):
         srv.register_key(i, zk)
     rng = random.Random(lanes)
