@@ -84,12 +84,21 @@ uint64_t live_bytes(g16_server* sv) {
     return t;
 }
 
+// ensure_resident could only go on by waiting, which a worker already holding
+// keys must not do: the request goes back to the queue for a later batch
+constexpr int DEFER = -1;
+
 // Make `id` resident.  Called with the lock held; drops it while preparing.
-int ensure_resident(g16_server* sv, uint32_t id, std::unique_lock<std::mutex>& lk, std::string& err) {
+// may_wait: the caller holds no key, so it may wait for other workers' keys
+// to go idle (a worker that holds keys and waited could wait on a worker that
+// waits on it).
+int ensure_resident(g16_server* sv, uint32_t id, std::unique_lock<std::mutex>& lk, std::string& err,
+                    bool may_wait) {
     KeyEntry& k = sv->keys[id];
     for (;;) {
         if (k.circ) return G16_OK;
         if (!k.preparing) break;
+        if (!may_wait) return DEFER;
         sv->cv_keys.wait(lk);
     }
     k.preparing = true;
@@ -107,6 +116,11 @@ int ensure_resident(g16_server* sv, uint32_t id, std::unique_lock<std::mutex>& l
             bool any_busy = false;
             for (auto& kv : sv->keys) any_busy |= kv.second.circ && kv.second.in_use > 0;
             if (!any_busy) break;   // nothing to evict and nothing will free: try anyway
+            if (!may_wait) {
+                k.preparing = false;
+                sv->cv_keys.notify_all();
+                return DEFER;
+            }
             sv->cv_keys.wait(lk);   // wait for a key to go idle
             continue;
         }
@@ -181,11 +195,15 @@ void worker(g16_server* sv) {
         }
         if (!sv->queue.empty()) sv->cv_work.notify_one();   // the rest is another worker's
         // keys resident and pinned for the batch; requests refused up front end here
-        std::vector<Request*> run;
+        std::vector<Request*> run, deferred;
         std::vector<g16_circuit*> circs;
         for (Request* q : batch) {
             std::string err;
-            int rc = ensure_resident(sv, q->key_id, lk, err);
+            int rc = ensure_resident(sv, q->key_id, lk, err, run.empty());
+            if (rc == DEFER) {
+                deferred.push_back(q);
+                continue;
+            }
             KeyEntry& k = sv->keys[q->key_id];
             if (rc == G16_OK && q->witness.size() / 32 != g16_circuit_n_vars(k.circ)) {
                 rc = G16_ERR_WITNESS_LENGTH;
@@ -202,6 +220,10 @@ void worker(g16_server* sv) {
             run.push_back(q);
             circs.push_back(k.circ);
         }
+        // requests whose keys could not be made resident beside this batch's go
+        // back to the head of the queue, in order
+        for (size_t i = deferred.size(); i-- > 0;) sv->queue.push_front(deferred[i]);
+        if (!deferred.empty()) sv->cv_work.notify_one();
         if (!run.empty()) {
             lk.unlock();
             const size_t n = run.size();
