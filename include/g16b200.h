@@ -114,6 +114,31 @@ size_t g16_last_error(char *buf, size_t len);
  * G16_ERR_DEVICE when no CUDA device is present: there is no CPU fallback. */
 int g16_backend_open(int ordinal, uint64_t vram_limit, g16_backend **out);
 void g16_backend_free(g16_backend *b);
+
+/* ---------------- device faults (crates/cuda/src/context.rs:134-215) ----------------
+ * A CUDA status is a device fault when the device failed rather than the call
+ * being one the driver rejects every time (out of memory, ECC, a kernel
+ * exception, the watchdog, MPS, an unknown internal error), and sticky when
+ * the runtime documents it as leaving the context unusable ("any further CUDA
+ * work will return the same error": the kernel exceptions, the watchdog, a
+ * contained hardware error).  A sticky fault met by any entry point marks the
+ * device for the rest of the process: from then on every entry point that
+ * would use it returns G16_ERR_DEVICE with that reason, without a CUDA call,
+ * and so does g16_backend_open on that device.  Out of memory stays
+ * G16_ERR_DEVICE_MEMORY; every other CUDA failure is G16_ERR_DEVICE. */
+enum { G16_FAULT_DEVICE = 1, G16_FAULT_STICKY = 2 };
+/* The classes of a cudaError_t value: 0, G16_FAULT_DEVICE, or
+ * G16_FAULT_DEVICE | G16_FAULT_STICKY.  Pure; needs no device. */
+int g16_cuda_error_class(int cuda_error);
+/* The sticky cudaError_t value that put this backend out of use (its device's
+ * in this process, or one injected below), or 0. */
+int g16_backend_fault(const g16_backend *b);
+/* Fault injection for tests, on the host: the next entry point on this backend
+ * that would use the device (prepare, prove, batch, MSM, NTT, tuning) fails as
+ * if its first CUDA call had returned cuda_error, and does no device work.  A
+ * sticky value puts this backend alone out of use (a real sticky fault takes
+ * the device for the process).  0 cancels a pending injection. */
+int g16_backend_inject_fault(g16_backend *b, int cuda_error);
 const char *g16_backend_name(const g16_backend *b);   /* "cuda-b200" */
 uint64_t g16_backend_vram_used(const g16_backend *b);
 /* CudaBackend::constant_work (crates/cuda/src/backend.rs:100-118; the CPU
@@ -138,7 +163,31 @@ int g16_wtns_parse(const uint8_t *bytes, size_t len, uint8_t *out_mont, size_t c
 int g16_wtns_write(const uint8_t *w_mont, size_t n, uint8_t *out, size_t cap, size_t *len_out);
 
 /* ---------------- circuits (Backend::prepare, backend.rs:325-457) ---------------- */
+/* How a key is held on the device.  With window tables (the default) each
+ * witness and H MSM reads bases 2^(c w) P_i laid out per window, so all
+ * windows share one bucket set: about ten times the key's bases in memory.  A
+ * compact key holds the plain bases only and runs one bucket set per window
+ * with a Horner step on the host: slower, a tenth of the memory, the same
+ * proofs.  This replaces the reference's runs of MSMs that do not fit VRAM
+ * (resident_schedule / fit_run, crates/cuda/src/msm.rs:966,1117). */
+typedef struct {
+    int window_tables;             /* 1 window tables, 0 compact key */
+    int msm_window_bits_witness;   /* c of the A, B1, L, B2 MSMs */
+    int msm_window_bits_h;         /* c of the H MSM */
+    uint64_t key_bytes;            /* device bytes of the prepared key */
+    uint64_t workspace_bytes;      /* device bytes of one proof in flight */
+} g16_key_plan;
+/* The plan g16_prepare follows with free_bytes of device memory: window tables
+ * when the key, its tables and one workspace fit; else the compact key when it
+ * and one workspace fit (also whenever the environment sets
+ * G16_CUDA_WINDOW_TABLES=0); else G16_ERR_DEVICE_MEMORY.  Host only. */
+int g16_plan_key(const g16_zkey_view *key, uint64_t free_bytes, g16_key_plan *out);
+/* Prepares a key on the device, refused with G16_ERR_DEVICE_MEMORY before any
+ * allocation when g16_plan_key finds no plan within the backend's budget.
+ * Batched submissions that include a compact key run it on host lanes. */
 int g16_prepare(g16_backend *b, const g16_zkey_view *key, g16_circuit **out);
+/* 1 when the circuit holds window tables, 0 for a compact key. */
+int g16_circuit_window_tables(const g16_circuit *c);
 void g16_circuit_free(g16_circuit *c);
 uint32_t g16_circuit_n_vars(const g16_circuit *c);
 uint32_t g16_circuit_n_public(const g16_circuit *c);

@@ -105,6 +105,7 @@ def lib():
         L.g16_circuit_device_bytes.restype = ctypes.c_uint64
         L.g16_circuit_device_bytes.argtypes = [vp]
         L.g16_kernel_timing_report.restype = ctypes.c_size_t
+        L.g16_backend_fault.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -230,6 +231,12 @@ class _ZkeyView(ctypes.Structure):
                 ("a_query", P), ("b_g1_query", P), ("b_g2_query", P), ("l_query", P), ("h_query", P)]
 
 
+class _KeyPlan(ctypes.Structure):
+    _fields_ = [("window_tables", ctypes.c_int), ("msm_window_bits_witness", ctypes.c_int),
+                ("msm_window_bits_h", ctypes.c_int), ("key_bytes", ctypes.c_uint64),
+                ("workspace_bytes", ctypes.c_uint64)]
+
+
 class ProvingKey:
     """A parsed snarkjs .zkey (ProvingKey, crates/formats/src/lib.rs:35-65)."""
 
@@ -253,6 +260,14 @@ class ProvingKey:
     def load(cls, path, check_points=True):
         with open(path, "rb") as f:
             return cls.from_bytes(f.read(), check_points)
+
+    def plan(self, free_bytes):
+        """How prepare would hold this key with free_bytes of device memory:
+        {window_tables, msm_window_bits_witness, msm_window_bits_h, key_bytes,
+        workspace_bytes} (host only; DeviceMemoryError when nothing fits)."""
+        out = _KeyPlan()
+        check(lib().g16_plan_key(ctypes.byref(self._view), ctypes.c_uint64(free_bytes), ctypes.byref(out)))
+        return {n: getattr(out, n) for n, _ in out._fields_}
 
     def _point(self, name, size):
         return ctypes.string_at(getattr(self._view, name), size)
@@ -351,6 +366,10 @@ class CudaCircuit:
 
     def device_bytes(self):
         return lib().g16_circuit_device_bytes(self._h)
+
+    def window_tables(self):
+        """True when the key is held with window tables, False for a compact key."""
+        return bool(lib().g16_circuit_window_tables(self._h))
 
     def compute_h(self, witness_mont):
         h = ctypes.c_void_p()
@@ -487,6 +506,15 @@ class CudaBackend:
 
     def name(self):
         return lib().g16_backend_name(self._h).decode()
+
+    def fault(self):
+        """The sticky cudaError_t value that put this backend out of use, or 0."""
+        return lib().g16_backend_fault(self._h)
+
+    def inject_fault(self, cuda_error):
+        """The next device entry point on this backend fails as if the driver had
+        returned cuda_error; no device work happens (a host-side test hook)."""
+        check(lib().g16_backend_inject_fault(self._h, int(cuda_error)))
 
     def vram_used(self):
         return lib().g16_backend_vram_used(self._h)
@@ -766,6 +794,15 @@ def launch_count():
     """Kernels this library has launched since it was loaded."""
     lib().g16_launch_count.restype = ctypes.c_uint64
     return lib().g16_launch_count()
+
+
+FAULT_DEVICE, FAULT_STICKY = 1, 2
+
+
+def cuda_error_class(cuda_error):
+    """FAULT_DEVICE / FAULT_STICKY classes of a cudaError_t value (is_device_fault and
+    is_sticky, crates/cuda/src/context.rs:134-215).  Needs no device."""
+    return lib().g16_cuda_error_class(int(cuda_error))
 
 
 def device_alloc_count():

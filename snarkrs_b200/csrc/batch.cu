@@ -180,7 +180,7 @@ cudaError_t grow_dev(void*& p, size_t& cap, size_t need) {
     p = nullptr;
     cap = 0;
     const size_t n = need + need / 4 + 256;
-    cudaError_t e = g16::dev_malloc(&p, n);
+    cudaError_t e = g16::dev_malloc_values(&p, n);
     if (e == cudaSuccess) cap = n;
     return e;
 }
@@ -194,6 +194,7 @@ cudaError_t grow_pinned(uint8_t*& p, size_t& cap, size_t need) {
     const size_t n = need + need / 4 + 256;
     cudaError_t e = cudaMallocHost((void**)&p, n);
     if (e == cudaSuccess) cap = n;
+    if (e == cudaSuccess && value_fill_byte() >= 0) std::memset(p, value_fill_byte(), n);
     return e;
 }
 
@@ -299,7 +300,13 @@ int build(BatchEngine& E, g16_circuit* const* cs, size_t count) {
     }
     CK_BATCH(ntt_batch_setup(E.ntt, items, E.st[0]));
     CK_BATCH(grow_dev(E.d_gather, E.cap_gather, gj.size() * sizeof(g16d::GatherJob)));
-    CK_BATCH(cudaMemcpy(E.d_gather, gj.data(), gj.size() * sizeof(g16d::GatherJob), cudaMemcpyHostToDevice));
+    // on st[0] and waited for: a plain cudaMemcpy from pageable memory may return
+    // before its DMA lands, on the legacy stream, which orders nothing against
+    // the engine's non-blocking streams (the gather would read the previous
+    // layout's jobs)
+    CK_BATCH(cudaMemcpyAsync(E.d_gather, gj.data(), gj.size() * sizeof(g16d::GatherJob), cudaMemcpyHostToDevice,
+                             E.st[0]));
+    CK_BATCH(cudaStreamSynchronize(E.st[0]));
     E.gather_blocks = blocks;
     E.gather_jobs = (uint32_t)gj.size();
     E.res_g1 = (size_t)E.g1.result_points * XYZZ_G1_BYTES;

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <atomic>
 #include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <string>
@@ -117,6 +118,34 @@ template <class T>
 inline cudaError_t dev_malloc(T** p, size_t bytes) {
     timer().device_allocs.fetch_add(1, std::memory_order_relaxed);
     return cudaMalloc((void**)p, bytes);
+}
+
+// Byte that new value buffers are filled with, or -1 (the default):
+// G16_FILL_VALUES=<0..255>.  A fresh process gets zeroed pages from the
+// driver, and zeros read as points at infinity and as zero scalars, so a read
+// of a point or a scalar that no kernel wrote goes unnoticed there; a filled
+// buffer exposes it.  Only buffers of values (points, scalars, and tables that
+// are uploaded whole before use) take the fill, never index arrays.
+inline int value_fill_byte() {
+    static const int v = [] {
+        const char* e = std::getenv("G16_FILL_VALUES");
+        if (!e || !*e) return -1;
+        const int b = std::atoi(e);
+        return b >= 0 && b <= 255 ? b : -1;
+    }();
+    return v;
+}
+
+// dev_malloc for a buffer of values (value_fill_byte).
+template <class T>
+inline cudaError_t dev_malloc_values(T** p, size_t bytes) {
+    cudaError_t e = dev_malloc(p, bytes);
+    const int fill = value_fill_byte();
+    // the legacy stream does not order against the library's non-blocking
+    // streams: the fill completes before the buffer is handed out
+    if (e == cudaSuccess && fill >= 0 && bytes) e = cudaMemset((void*)*p, fill, bytes);
+    if (e == cudaSuccess && fill >= 0 && bytes) e = cudaStreamSynchronize(cudaStreamLegacy);
+    return e;
 }
 
 inline unsigned blocks_for(size_t n, unsigned threads) { return (unsigned)((n + threads - 1) / threads); }

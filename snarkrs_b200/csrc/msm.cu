@@ -106,12 +106,16 @@ __global__ void __launch_bounds__(256) k_scatter(const uint4* __restrict__ scala
 // The digits are computed once and sorted into every set the scalar is live
 // in, so a base at infinity never becomes an entry (a lockstep step of the
 // accumulate that adds nothing).
+// With per-window bucket sets instead (plain bases, a compact key) window w's
+// digit d goes to bucket w B + |d| - 1 and its entry is rank[j][i] itself:
+// key_stride = B and rows = 0.
 struct LiveSetArgs {
     const uint32_t* rank[MSM_MAX_SETS];
     uint32_t* counts[MSM_MAX_SETS];
     uint32_t* cursor[MSM_MAX_SETS];
     uint32_t* entries[MSM_MAX_SETS];
-    uint32_t rows[MSM_MAX_SETS];
+    uint32_t rows[MSM_MAX_SETS];   // entry stride per window: the table rows, or 0
+    uint32_t key_stride;           // bucket offset per window: 0 (one shared set), or B
 };
 
 __global__ void __launch_bounds__(256) k_digits_count_sets(const uint4* __restrict__ scalars, int mont, uint32_t n,
@@ -138,7 +142,7 @@ __global__ void __launch_bounds__(256) k_digits_count_sets(const uint4* __restri
     unsigned lane = threadIdx.x & 31;
     for (int w = 0; w < W; w++) {
         int d = signed_digit(row, w, c);
-        uint32_t key = d != 0 ? (uint32_t)(d < 0 ? -d : d) - 1u : sink;
+        uint32_t key = d != 0 ? (uint32_t)w * a.key_stride + (uint32_t)(d < 0 ? -d : d) - 1u : sink;
 #pragma unroll
         for (int j = 0; j < MSM_MAX_SETS; j++) {
             if (j >= nsets) break;
@@ -170,7 +174,7 @@ __global__ void __launch_bounds__(256) k_scatter_sets(const uint4* __restrict__ 
     unsigned lt = (1u << lane) - 1u;
     for (int w = 0; w < W; w++) {
         int d = signed_digit(row, w, c);
-        uint32_t key = d != 0 ? (uint32_t)(d < 0 ? -d : d) - 1u : sink;
+        uint32_t key = d != 0 ? (uint32_t)w * a.key_stride + (uint32_t)(d < 0 ? -d : d) - 1u : sink;
         const uint32_t sign = d < 0 ? 0x80000000u : 0u;
 #pragma unroll
         for (int j = 0; j < MSM_MAX_SETS; j++) {
@@ -1161,7 +1165,7 @@ static cudaError_t grow_bytes(void*& p, size_t& cap, size_t need, bool fixed = f
     cudaFree(p);
     p = nullptr;
     size_t n = need + need / 8 + 256;
-    cudaError_t e = g16::dev_malloc(&p, n);
+    cudaError_t e = g16::dev_malloc_values(&p, n);
     if (e != cudaSuccess) {
         cap = 0;
         set_error("cudaMalloc of %zu bytes for MSM scratch failed: %s", n, cudaGetErrorString(e));
@@ -1271,7 +1275,7 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
 }
 
 cudaError_t msm_sort_sets(MsmSort* sorts, const MsmLiveSets& sets, const void* d_scalars, size_t n, bool montgomery,
-                          int c, cudaStream_t st, bool constant_work) {
+                          int c, cudaStream_t st, bool constant_work, bool shared) {
     if (sets.count < 1 || sets.count > MSM_MAX_SETS) {
         set_error("%d live sets (1 to %d)", sets.count, MSM_MAX_SETS);
         return cudaErrorInvalidValue;
@@ -1291,8 +1295,8 @@ cudaError_t msm_sort_sets(MsmSort* sorts, const MsmLiveSets& sets, const void* d
         s.c = c;
         s.W = W;
         s.B = 1u << (c - 1);
-        s.shared = true;
-        s.K = s.B;
+        s.shared = shared;
+        s.K = shared ? s.B : (uint32_t)W * s.B;
         s.constant_work = constant_work;
         s.Ks = s.K + (constant_work ? 1u : 0u);
         s.n = sets.rows[j];
@@ -1324,8 +1328,9 @@ cudaError_t msm_sort_sets(MsmSort* sorts, const MsmLiveSets& sets, const void* d
         a.counts[j] = s.d_counts;
         a.cursor[j] = s.d_cursor;
         a.entries[j] = s.d_entries;
-        a.rows[j] = sets.rows[j];
+        a.rows[j] = shared ? sets.rows[j] : 0u;
     }
+    a.key_stride = shared ? 0u : (1u << (c - 1));
     // the standard-form copy of the scalars, shared by the sets, lives in the first
     MsmSort& s0 = sorts[0];
     G16_CUDA(grow(s0.d_scalars_std, s0.cap_scalars, (n ? n : 1) * 8));

@@ -151,7 +151,9 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
 // computed once and each lands in every set its scalar is live in, so a base
 // at infinity costs no accumulate step (the reference's prescan and key_live:
 // crates/msm/src/lib.rs:534-563, crates/cuda/src/msm.rs:1308).  sorts[j] gets
-// set j's sort, as msm_sort(shared_windows = true) would give for it.
+// set j's sort, as msm_sort(shared_windows = true) would give for it.  With
+// shared = false the sets read plain (compacted) bases instead: one bucket set
+// per window and entry d_rank[j][i], as msm_sort(shared_windows = false).
 constexpr uint32_t MSM_DEAD = 0xffffffffu;
 constexpr int MSM_MAX_SETS = 3;
 struct MsmLiveSets {
@@ -160,7 +162,7 @@ struct MsmLiveSets {
     uint32_t rows[MSM_MAX_SETS] = {0, 0, 0};
 };
 cudaError_t msm_sort_sets(MsmSort* sorts, const MsmLiveSets& sets, const void* d_scalars, size_t n, bool montgomery,
-                          int c, cudaStream_t st, bool constant_work = false);
+                          int c, cudaStream_t st, bool constant_work = false, bool shared = true);
 
 // Window count for c-bit signed digits over 255 bits.
 inline int msm_windows(int c) { return (255 + c - 1) / c; }

@@ -87,6 +87,15 @@ constexpr int MAX_DEVICES = 64;
 std::mutex g_setup_mu;
 unsigned char* g_scratch_addr[MAX_DEVICES] = {};
 
+}  // namespace
+
+namespace g16 {
+int cuda_fail(cudaError_t e, const char* what);   // prover.cu: status of a failed CUDA call, sticky faults recorded
+int device_fault(int ordinal);                     // prover.cu: the sticky fault that took a device out of use
+}  // namespace g16
+
+namespace {
+
 int fail_noalloc(int code, const char* msg) {
     g16::set_error("%s", msg);
     return code;
@@ -107,6 +116,11 @@ extern "C" int g16_msm_g1_device_noalloc(int device, const void* d_bases, const 
     }
     if (device < 0 || device >= MAX_DEVICES)
         return fail_noalloc(G16_ERR_INVALID_ARGUMENT, "g16_msm_g1_device_noalloc: device ordinal out of range");
+    if (const int f = g16::device_fault(device)) {
+        g16::set_error("g16_msm_g1_device_noalloc: CUDA device %d is out of use after %s: a sticky fault earlier in "
+                       "this process", device, cudaGetErrorString((cudaError_t)f));
+        return G16_ERR_DEVICE;
+    }
     if (g16::timer().enabled)
         return fail_noalloc(G16_ERR_INVALID_ARGUMENT,
                             "g16_msm_g1_device_noalloc: kernel timing creates CUDA events; disable it first");
@@ -175,8 +189,8 @@ extern "C" int g16_msm_g1_device_noalloc(int device, const void* d_bases, const 
     s = g16::MsmSort();
     acc = g16::MsmAccum();
     if (e != cudaSuccess) {
-        g16::set_error("g16_msm_g1_device_noalloc: %s", cudaGetErrorString(e));
-        return e == cudaErrorMemoryAllocation ? G16_ERR_DEVICE_MEMORY : G16_ERR_DEVICE;
+        g16::set_error("%s", "");
+        return g16::cuda_fail(e, "g16_msm_g1_device_noalloc");
     }
     g16::pack(out64, g16::msm_combine_g1(windows, plan, NOALLOC_C).to_affine());
     return G16_OK;

@@ -142,14 +142,100 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
-int cuda_fail(cudaError_t e, const char* what) {
-    if (e == cudaErrorMemoryAllocation) return fail(G16_ERR_DEVICE_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+// Device-fault classes of a CUDA runtime status (the reference's
+// is_device_fault and is_sticky, crates/cuda/src/context.rs:134-215, there over
+// the driver's CUresult; the runtime documents its cudaError_t twins in the
+// same words).
+int error_class(int code) {
+    switch (code) {
+    // kernel exceptions, the watchdog and a contained hardware error: "the
+    // process is left in an inconsistent state and any further CUDA work will
+    // return the same error"
+    case cudaErrorIllegalAddress:
+    case cudaErrorAssert:
+    case cudaErrorHardwareStackError:
+    case cudaErrorIllegalInstruction:
+    case cudaErrorMisalignedAddress:
+    case cudaErrorInvalidAddressSpace:
+    case cudaErrorInvalidPc:
+    case cudaErrorLaunchFailure:
+    case cudaErrorLaunchTimeout:
+    case cudaErrorContained:
+        return G16_FAULT_DEVICE | G16_FAULT_STICKY;
+    // the device or its daemons failed, the context stays usable
+    case cudaErrorMemoryAllocation:
+    case cudaErrorDevicesUnavailable:
+    case cudaErrorECCUncorrectable:
+    case cudaErrorNvlinkUncorrectable:
+    case cudaErrorSystemNotReady:
+    case cudaErrorMpsConnectionFailed:
+    case cudaErrorMpsRpcFailure:
+    case cudaErrorMpsServerNotReady:
+    case cudaErrorMpsMaxClientsReached:
+    case cudaErrorMpsMaxConnectionsReached:
+    case cudaErrorMpsClientTerminated:
+    case cudaErrorTimeout:
+    case cudaErrorExternalDevice:
+    case cudaErrorUnknown:
+        return G16_FAULT_DEVICE;
+    default:
+        return 0;
+    }
+}
+
+// The sticky status that took each device out of use in this process, or 0.
+static std::atomic<int> g_device_fault[64];
+
+static const char* const STICKY_TEXT =
+    "; a sticky fault: the CUDA context is unusable for the rest of this process, and every later call on this "
+    "device is refused; prove on another device or in a new process";
+
+// The status for a failed CUDA call (or an injected one): DEVICE_MEMORY for
+// out of memory, else DEVICE; a sticky code also marks the device (when
+// mark_device) for the rest of the process.
+static int fault_status(int e, const char* what, bool mark_device) {
+    const bool sticky = (error_class(e) & G16_FAULT_STICKY) != 0;
+    if (sticky && mark_device) {
+        int dev = -1;
+        if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) {
+            int none = 0;
+            g_device_fault[dev].compare_exchange_strong(none, e);
+        }
+    }
+    const char* text = cudaGetErrorString((cudaError_t)e);
+    if (e == cudaErrorMemoryAllocation) return fail(G16_ERR_DEVICE_MEMORY, "%s: %s", what, text);
     std::string prev = [] {
         char b[512];
         g16_last_error(b, sizeof b);
         return std::string(b);
     }();
-    return fail(G16_ERR_DEVICE, "%s: %s (%s)", what, cudaGetErrorString(e), prev.c_str());
+    if (prev.empty()) return fail(G16_ERR_DEVICE, "%s: %s%s", what, text, sticky ? STICKY_TEXT : "");
+    return fail(G16_ERR_DEVICE, "%s: %s%s (%s)", what, text, sticky ? STICKY_TEXT : "", prev.c_str());
+}
+
+int cuda_fail(cudaError_t e, const char* what) { return fault_status((int)e, what, true); }
+
+int device_fault(int ordinal) { return ordinal >= 0 && ordinal < 64 ? g_device_fault[ordinal].load() : 0; }
+
+// Called first by every entry point that uses b's device: refuses when a
+// sticky fault took the device (or this backend) out of use, and delivers a
+// pending injected fault.
+int device_usable(g16_backend* b) {
+    int code = b->fault.load();
+    if (!code) code = device_fault(b->ordinal);
+    if (code)
+        return fail(G16_ERR_DEVICE, "CUDA device %d is out of use after %s%s", b->ordinal,
+                    cudaGetErrorString((cudaError_t)code), STICKY_TEXT);
+    const int inj = b->inject.exchange(0);
+    if (inj) {
+        if (error_class(inj) & G16_FAULT_STICKY) {
+            int none = 0;
+            b->fault.compare_exchange_strong(none, inj);
+        }
+        set_error("%s", "");
+        return fault_status(inj, "injected fault", false);
+    }
+    return G16_OK;
 }
 
 }  // namespace g16
@@ -174,10 +260,12 @@ cudaError_t circuit_alloc(g16_circuit* c, void** p, size_t bytes) {
 
 // Device bytes of one workspace: witness, A|B|C, H, and the MSM scratch
 // (sorted entries, partial sums, bucket sums) at window bits c_w and c_h, for
-// live sets of ra (A), rb (B1, B2) and rl (L) wires.
-uint64_t workspace_estimate(uint64_t nv, uint64_t n, int c_w, int c_h, uint64_t ra, uint64_t rb, uint64_t rl) {
+// live sets of ra (A), rb (B1, B2) and rl (L) wires; tables: one bucket set
+// per MSM (window tables), else one per window (compact key).
+uint64_t workspace_estimate(uint64_t nv, uint64_t n, int c_w, int c_h, uint64_t ra, uint64_t rb, uint64_t rl,
+                            bool tables) {
     const uint64_t Ww = (uint64_t)msm_windows(c_w), Wh = (uint64_t)msm_windows(c_h);
-    const uint64_t Kw = 1ull << (c_w - 1), Kh = 1ull << (c_h - 1);
+    const uint64_t Kw = (1ull << (c_w - 1)) * (tables ? 1 : Ww), Kh = (1ull << (c_h - 1)) * (tables ? 1 : Wh);
     uint64_t b = nv * 32 + n * 32 * 4;
     b += nv * 32 + (ra + rb + rl) * Ww * 4 + 3 * 24 * (Kw + 1) + n * 32 + n * Wh * 4 + 24 * (Kh + 1);
     b += 128 * (3 * Kw * 2 + (ra + rb + rl) * Ww / 16 + 3) + 256 * (Kw * 2 + rb * Ww / 16 + 1);
@@ -201,6 +289,10 @@ void circuit_free_alloc(g16_circuit* c, void* p, uint64_t bytes) {
 // window bits cw, each over its live set's compacted bases; the new tables
 // replace the old ones only when all are built.
 int build_witness_tables(g16_circuit* c, int cw, cudaStream_t st) {
+    if (!c->tables) {   // a compact key: the MSMs read the plain bases at any window width
+        c->c_w = cw;
+        return G16_OK;
+    }
     const uint64_t W = (uint64_t)msm_windows(cw);
     const uint64_t ra = c->rows[0], rb = c->rows[1], rl = c->rows[2];
     if (std::max(ra, std::max(rb, rl)) * W >= 0x80000000ull)
@@ -240,6 +332,10 @@ int build_witness_tables(g16_circuit* c, int cw, cudaStream_t st) {
 
 // The same for the H MSM's table at window bits ch.
 int build_h_table(g16_circuit* c, int ch, cudaStream_t st) {
+    if (!c->tables) {
+        c->c_h = ch;
+        return G16_OK;
+    }
     const uint64_t n = c->n, W = (uint64_t)msm_windows(ch);
     if (n * W >= 0x80000000ull) return fail(G16_ERR_BACKEND, "domain too large for 31-bit MSM entry indices");
     void* th = nullptr;
@@ -256,6 +352,12 @@ int build_h_table(g16_circuit* c, int ch, cudaStream_t st) {
     c->c_h = ch;
     return G16_OK;
 }
+
+// Host readback slot of one MSM's reduction terms: one bucket set with window
+// tables; with a compact key one set per window, W (lb + 1 + hb) points, at
+// most 32 x 15 G2 points for window bits in [8, 20].
+constexpr size_t WIN_SLOT_COMPACT = 128 * 1024;
+size_t win_slot(const g16_circuit* c) { return c->tables ? MSM_RESULT_SLOT_BYTES : WIN_SLOT_COMPACT; }
 
 // Take an idle workspace, or build one while the pool is below its cap and the
 // backend's device-memory budget has room; otherwise wait for one to come back.
@@ -274,7 +376,7 @@ int acquire(g16_circuit* c, Workspace** out) {
         bool room = c->be->vram_used + c->ws_estimate <= c->be->vram_limit;
         if (c->pool.size() < c->max_workspaces && (room || c->pool.empty())) {
             auto ws = std::make_unique<Workspace>();
-            cudaError_t e = ws->init(c->n_vars, c->n);
+            cudaError_t e = ws->init(c->n_vars, c->n, win_slot(c));
             if (e == cudaSuccess) {
                 c->device_bytes += c->ws_estimate;
                 c->be->vram_used += c->ws_estimate;
@@ -420,10 +522,11 @@ int run_h(g16_circuit* c, Workspace* ws, const void* d_w, void* h_out) {
 // the witness upload; the sort on the first), while the main stream does
 // gather -> NTT -> H sort -> H accumulate; the main stream joins them before
 // the results are read back.
-constexpr size_t WIN_SLOT = MSM_RESULT_SLOT_BYTES;
-
 int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
-    const uint32_t W = (uint32_t)msm_windows(c->c_w);
+    const size_t WIN_SLOT = ws->win_slot;
+    // window tables: entry w rows + rank of a table of rows W points; compact:
+    // entry rank of the plain bases
+    const uint32_t W = c->tables ? (uint32_t)msm_windows(c->c_w) : 1u;
     cudaStream_t st[4];
     for (int i = 0; i < 4; i++) st[i] = c->serial ? ws->stream : ws->side[i];
     CK(cudaEventRecord(ws->ev_fork, ws->stream), "event");
@@ -435,15 +538,17 @@ int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
         sets.d_rank[j] = c->d_rank[j];
         sets.rows[j] = c->rows[j];
     }
-    CK(msm_sort_sets(ws->sort_w, sets, d_w, c->n_vars, true, c->c_w, st[0], c->be->constant_work), "witness sort");
+    CK(msm_sort_sets(ws->sort_w, sets, d_w, c->n_vars, true, c->c_w, st[0], c->be->constant_work, c->tables),
+       "witness sort");
     CK(cudaEventRecord(ws->ev_sort, st[0]), "event");
     for (int i = 1; i < 4; i++) CK(cudaStreamWaitEvent(st[i], ws->ev_sort, 0), "stream wait");
     // acc slots: 0 A, 1 B2, 2 B1, 3 L (4 is H); one stream per MSM so that
     // their latency-bound reduction tails run side by side
-    CK(msm_accumulate_g1(ws->sort_w[0], ws->acc[0], c->t_a, 0, c->rows[0] * W, st[0]), "A accumulate");
-    CK(msm_accumulate_g1(ws->sort_w[1], ws->acc[2], c->t_b1, 0, c->rows[1] * W, st[1]), "B1 accumulate");
-    CK(msm_accumulate_g1(ws->sort_w[2], ws->acc[3], c->t_l, 0, c->rows[2] * W, st[2]), "L accumulate");
-    CK(msm_accumulate_g2(ws->sort_w[1], ws->acc[1], c->t_b2, 0, c->rows[1] * W, st[3]), "B2 accumulate");
+    const bool t = c->tables;
+    CK(msm_accumulate_g1(ws->sort_w[0], ws->acc[0], t ? c->t_a : c->d_a, 0, c->rows[0] * W, st[0]), "A accumulate");
+    CK(msm_accumulate_g1(ws->sort_w[1], ws->acc[2], t ? c->t_b1 : c->d_b1, 0, c->rows[1] * W, st[1]), "B1 accumulate");
+    CK(msm_accumulate_g1(ws->sort_w[2], ws->acc[3], t ? c->t_l : c->d_l, 0, c->rows[2] * W, st[2]), "L accumulate");
+    CK(msm_accumulate_g2(ws->sort_w[1], ws->acc[1], t ? c->t_b2 : c->d_b2, 0, c->rows[1] * W, st[3]), "B2 accumulate");
     const int stream_of[4] = {0, 3, 1, 2};   // acc slot -> stream
     for (int i = 0; i < 4; i++) {
         cudaStream_t s_i = st[stream_of[i]];
@@ -459,13 +564,14 @@ int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
 }
 
 int enqueue_h_msm(g16_circuit* c, Workspace* ws, const void* d_h) {
+    const size_t WIN_SLOT = ws->win_slot;
     cudaStream_t st = ws->stream;
-    const uint32_t nh = c->n * (uint32_t)msm_windows(c->c_h);
+    const uint32_t nh = c->n * (c->tables ? (uint32_t)msm_windows(c->c_h) : 1u);
     // the H reduction runs last on the main stream, mostly alone: shorter chains pay
     // (2^21 prove +0.5%, 2^18 +1.5%, 2^20 +1.3% against the 8192-piece default)
     ws->sort_h.reduce_pieces = MSM_REDUCE_PIECES_ALONE;
-    CK(msm_sort(ws->sort_h, d_h, c->n, true, c->c_h, st, true, c->be->constant_work), "H sort");
-    CK(msm_accumulate_g1(ws->sort_h, ws->acc[4], c->t_h, 0, nh, st), "H accumulate");
+    CK(msm_sort(ws->sort_h, d_h, c->n, true, c->c_h, st, c->tables, c->be->constant_work), "H sort");
+    CK(msm_accumulate_g1(ws->sort_h, ws->acc[4], c->tables ? c->t_h : c->d_h, 0, nh, st), "H accumulate");
     const size_t bytes = ws->acc[4].result_bytes(XYZZ_G1_BYTES);
     if (bytes > WIN_SLOT) return fail(G16_ERR_BACKEND, "MSM result of %zu bytes exceeds its slot", bytes);
     CK(cudaMemcpyAsync(ws->h_win + 4 * WIN_SLOT, ws->acc[4].d_windows, bytes, cudaMemcpyDeviceToHost, st),
@@ -482,6 +588,7 @@ int enqueue_join(Workspace* ws) {
 }
 
 int collect_msms(g16_circuit* c, Workspace* ws, MsmJac& out) {
+    const size_t WIN_SLOT = ws->win_slot;
     CK(cudaStreamSynchronize(ws->stream), "MSM stages");
     timer().collect();
     {
@@ -694,7 +801,7 @@ struct TuningLock {
             }
             if (c->pool.size() >= c->max_workspaces || c->be->vram_used + c->ws_estimate > c->be->vram_limit) break;
             auto w = std::make_unique<Workspace>();
-            if (w->init(c->n_vars, c->n) != cudaSuccess) {
+            if (w->init(c->n_vars, c->n, win_slot(c)) != cudaSuccess) {
                 w->release();
                 cudaGetLastError();
                 break;
@@ -714,7 +821,7 @@ struct TuningLock {
                 w->graph = nullptr;
                 w->proofs = 0;
             }
-            c->ws_estimate = workspace_estimate(c->n_vars, c->n, c->c_w, c->c_h, c->rows[0], c->rows[1], c->rows[2]);
+            c->ws_estimate = workspace_estimate(c->n_vars, c->n, c->c_w, c->c_h, c->rows[0], c->rows[1], c->rows[2], c->tables);
         }
         {
             std::lock_guard<std::mutex> g(c->mu);
@@ -822,6 +929,54 @@ LiveSetsHost live_sets(const g16_zkey_view& k) {
 
 bool window_bits_ok(int b) { return b >= 8 && b <= 20; }
 
+// How a key is held (g16_plan_key): the window tables when the key, its tables
+// and one workspace fit in free_bytes, else the compact key (plain bases, one
+// bucket set per window) when it and one workspace fit, else DEVICE_MEMORY.
+// G16_CUDA_WINDOW_TABLES=0 takes the compact key whenever it fits.
+int plan_key(const g16_zkey_view& k, const uint32_t rows[3], uint64_t free_bytes, g16_key_plan* out) {
+    const uint64_t nv = k.n_vars, n = k.domain_size;
+    const uint64_t ra = rows[0], rb = rows[1], rl = rows[2];
+    // CSR, interned values, compacted bases, rank arrays, H bases, twiddles and coset table
+    const uint64_t plain = 4ull * (n + 1) * 2 + 8ull * (k.nnz[0] + k.nnz[1]) + 32ull * k.n_values + ra * 64 +
+                           rb * (64 + 128) + rl * 64 + 12 * nv + n * 64 + n * 32 * 2 + 32;
+    const char* env = std::getenv("G16_CUDA_WINDOW_TABLES");
+    const bool allow_tables = !(env && std::strcmp(env, "0") == 0);
+    g16_key_plan t = {};
+    t.window_tables = 1;
+    t.msm_window_bits_witness = msm_shared_window_bits(nv / 2 + 1);
+    t.msm_window_bits_h = msm_shared_window_bits(n);
+    {
+        const uint64_t Ww = (uint64_t)msm_windows(t.msm_window_bits_witness), Wh = (uint64_t)msm_windows(t.msm_window_bits_h);
+        t.key_bytes = plain + (ra + rl) * Ww * 64 + rb * Ww * (64 + 128) + n * Wh * 64;
+        t.workspace_bytes = workspace_estimate(nv, n, t.msm_window_bits_witness, t.msm_window_bits_h, ra, rb, rl, true);
+    }
+    g16_key_plan m = {};
+    m.window_tables = 0;
+    m.msm_window_bits_witness = msm_window_bits(std::max<uint64_t>(1, std::max(ra, std::max(rb, rl))));
+    m.msm_window_bits_h = msm_window_bits(n);
+    m.key_bytes = plain;
+    m.workspace_bytes = workspace_estimate(nv, n, m.msm_window_bits_witness, m.msm_window_bits_h, ra, rb, rl, false);
+    for (const g16_key_plan* p : {&t, &m}) {
+        // sorted entries are 31-bit indices in either form
+        const uint64_t Ww = (uint64_t)msm_windows(p->msm_window_bits_witness), Wh = (uint64_t)msm_windows(p->msm_window_bits_h);
+        if (nv * Ww >= 0x80000000ull || n * Wh >= 0x80000000ull)
+            return fail(G16_ERR_BACKEND, "circuit too large for 31-bit MSM entry indices");
+    }
+    if (allow_tables && t.key_bytes + t.workspace_bytes <= free_bytes) {
+        *out = t;
+        return G16_OK;
+    }
+    if (m.key_bytes + m.workspace_bytes <= free_bytes) {
+        *out = m;
+        return G16_OK;
+    }
+    return fail(G16_ERR_DEVICE_MEMORY,
+                "circuit needs about %llu MiB of device memory with window tables and %llu MiB as a compact key; "
+                "%llu MiB are free",
+                (unsigned long long)((t.key_bytes + t.workspace_bytes) >> 20),
+                (unsigned long long)((m.key_bytes + m.workspace_bytes) >> 20), (unsigned long long)(free_bytes >> 20));
+}
+
 int apply_tuning(g16_circuit* c, Workspace* ws, const g16_tuning& t) {
     NttTiling tl = {(uint32_t)t.ntt_tile_log, (uint32_t)t.ntt_outer_log_l};
     if (!window_bits_ok(t.msm_window_bits_witness) || !window_bits_ok(t.msm_window_bits_h) || t.ntt_tile_log < 2 ||
@@ -890,6 +1045,20 @@ size_t g16_last_error(char* buf, size_t len) {
     return e.size();
 }
 
+int g16_cuda_error_class(int cuda_error) { return error_class(cuda_error); }
+
+int g16_backend_fault(const g16_backend* b) {
+    if (!b) return 0;
+    const int f = b->fault.load();
+    return f ? f : g16::device_fault(b->ordinal);
+}
+
+int g16_backend_inject_fault(g16_backend* b, int cuda_error) {
+    if (!b || cuda_error < 0) return fail(G16_ERR_INVALID_ARGUMENT, "g16_backend_inject_fault: need a backend and a status >= 0");
+    b->inject = cuda_error;
+    return G16_OK;
+}
+
 int g16_backend_set_constant_work(g16_backend* b, int on) {
     if (!b) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     b->constant_work = on != 0;
@@ -904,6 +1073,9 @@ int g16_backend_open(int ordinal, uint64_t vram_limit, g16_backend** out) {
     if (e != cudaSuccess || count == 0)
         return fail(G16_ERR_DEVICE, "no CUDA device: %s", e != cudaSuccess ? cudaGetErrorString(e) : "count is 0");
     if (ordinal < 0 || ordinal >= count) return fail(G16_ERR_DEVICE, "CUDA device %d of %d", ordinal, count);
+    if (const int f = g16::device_fault(ordinal))
+        return fail(G16_ERR_DEVICE, "CUDA device %d is out of use after %s: a sticky fault earlier in this process", ordinal,
+                    cudaGetErrorString((cudaError_t)f));
     CK(cudaSetDevice(ordinal), "cudaSetDevice");
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, ordinal), "cudaGetDeviceProperties");
@@ -982,6 +1154,7 @@ int g16_wtns_write(const uint8_t* w_mont, size_t n, uint8_t* out, size_t cap, si
 // ---- prepare ----
 int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
     if (!b || !k || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    if (int rc_dev = device_usable(b)) return rc_dev;
     CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
     uint32_t n = k->domain_size;
     if (n < 2 || (n & (n - 1)) || n > (1u << 27)) return fail(G16_ERR_BACKEND, "domain size %u is not a power of two in [2, 2^27]", n);
@@ -1006,27 +1179,20 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
     // B: b_g1_query or b_g2_query finite (B1 and B2 share one sort); L: a
     // private wire whose l_query point is finite.
     LiveSetsHost live = live_sets(*k);
-    const uint64_t ra = live.rows[0], rb = live.rows[1], rl = live.rows[2];
-    // memory budget, refused before any allocation (backend.rs:367-381)
-    uint64_t key_bytes = 4ull * (n + 1) * 2 + 8ull * (k->nnz[0] + k->nnz[1]) + 32ull * k->n_values + ra * 64 +
-                         rb * (64 + 128) + rl * 64 + 12 * nv + (uint64_t)n * 64 + (uint64_t)n * 32 * 2 + 32;
-    const int c_w = msm_shared_window_bits(nv / 2 + 1), c_h = msm_shared_window_bits(n);
-    const uint64_t Ww = (uint64_t)msm_windows(c_w), Wh = (uint64_t)msm_windows(c_h);
-    if (nv * Ww >= 0x80000000ull || (uint64_t)n * Wh >= 0x80000000ull)
-        return fail(G16_ERR_BACKEND, "circuit too large for 31-bit MSM entry indices");
-    key_bytes += (ra + rl) * Ww * 64 + rb * Ww * (64 + 128) + (uint64_t)n * Wh * 64;
-    const uint64_t ws_bytes = workspace_estimate(nv, n, c_w, c_h, ra, rb, rl);
-    if (b->vram_used + key_bytes + ws_bytes > b->vram_limit)
-        return fail(G16_ERR_DEVICE_MEMORY, "circuit needs about %llu MiB of device memory, %llu MiB of the %llu MiB budget are free",
-                    (unsigned long long)((key_bytes + ws_bytes) >> 20),
-                    (unsigned long long)((b->vram_limit - std::min<uint64_t>(b->vram_limit, b->vram_used)) >> 20),
-                    (unsigned long long)(b->vram_limit >> 20));
+    // memory budget, refused before any allocation (backend.rs:367-381); the
+    // compact key when the window tables do not fit
+    g16_key_plan plan;
+    const uint64_t free_bytes = b->vram_limit - std::min<uint64_t>(b->vram_limit, b->vram_used);
+    int rc = plan_key(*k, live.rows, free_bytes, &plan);
+    if (rc) return rc;
+    const int c_w = plan.msm_window_bits_witness, c_h = plan.msm_window_bits_h;
     auto c = std::make_unique<g16_circuit>();
     c->be = b;
     c->n_vars = k->n_vars;
     c->n_public = k->n_public;
     c->n = n;
-    c->ws_estimate = ws_bytes;
+    c->tables = plan.window_tables != 0;
+    c->ws_estimate = plan.workspace_bytes;
     for (int j = 0; j < 3; j++) c->rows[j] = live.rows[j];
     if (const char* g = std::getenv("G16_CUDA_GRAPHS")) c->graphs = std::strcmp(g, "0") != 0;
     while ((1u << c->log_n) < n) c->log_n++;
@@ -1084,8 +1250,8 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
         return rc;
     }
     cp->device_bytes += 3ull * 32 * n / 2 * 2;
-    // window-shifted base tables; the plain bases are their window-0 slice
-    int rc = build_witness_tables(cp, c_w, st);
+    // window-shifted base tables (none for a compact key)
+    rc = build_witness_tables(cp, c_w, st);
     if (rc == G16_OK) rc = build_h_table(cp, c_h, st);
     if (rc != G16_OK) {
         cleanup();
@@ -1112,12 +1278,22 @@ uint32_t g16_circuit_n_vars(const g16_circuit* c) { return c ? c->n_vars : 0; }
 uint32_t g16_circuit_n_public(const g16_circuit* c) { return c ? c->n_public : 0; }
 uint32_t g16_circuit_domain_size(const g16_circuit* c) { return c ? c->n : 0; }
 uint64_t g16_circuit_device_bytes(const g16_circuit* c) { return c ? c->device_bytes : 0; }
+int g16_circuit_window_tables(const g16_circuit* c) { return c && c->tables ? 1 : 0; }
+
+int g16_plan_key(const g16_zkey_view* k, uint64_t free_bytes, g16_key_plan* out) {
+    if (!k || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    if (k->domain_size < 2 || (k->domain_size & (k->domain_size - 1)) || (uint64_t)k->n_public + 1 > k->n_vars)
+        return fail(G16_ERR_BACKEND, "malformed key shape");
+    const LiveSetsHost live = live_sets(*k);
+    return plan_key(*k, live.rows, free_bytes, out);
+}
 
 // ---- stages ----
 int g16_compute_h(g16_circuit* c, const uint8_t* w, size_t n, g16_hpoly** out) {
     if (!c || !w || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
+    if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     WsGuard g(c);
     if ((rc = acquire(c, &g.ws))) return rc;
@@ -1155,6 +1331,7 @@ int g16_msms(g16_circuit* c, const uint8_t* w, size_t n, const g16_hpoly* h, g16
     if (h->owner != c) return fail(G16_ERR_BACKEND, "H handle was computed by another circuit");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
+    if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     WsGuard g(c);
     if ((rc = acquire(c, &g.ws))) return rc;
@@ -1173,6 +1350,7 @@ int g16_h_and_msms(g16_circuit* c, const uint8_t* w, size_t n, g16_msm_outputs* 
     if (!c || !w || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
+    if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     WsGuard g(c);
     if ((rc = acquire(c, &g.ws))) return rc;
@@ -1189,6 +1367,7 @@ int g16_h_and_msms_from_rows(g16_circuit* c, const uint8_t* w, size_t n, const u
     if (!c || !w || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, w);
     if (rc || (rc = check_rows(c, a_rows, b_rows, rows))) return rc;
+    if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     WsGuard g(c);
     if ((rc = acquire(c, &g.ws))) return rc;
@@ -1210,6 +1389,7 @@ int g16_prove_with_blinders_from_rows(g16_circuit* c, const uint8_t* w, size_t n
     std::memcpy(rr, r_mont, 32);
     std::memcpy(ss, s_mont, 32);
     if (!g16::Fr::canonical(rr) || !g16::Fr::canonical(ss)) return fail(G16_ERR_INVALID_ARGUMENT, "r or s not below r");
+    if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     WsGuard g(c);
     if ((rc = acquire(c, &g.ws))) return rc;
@@ -1232,6 +1412,7 @@ int g16_prove_with_blinders(g16_circuit* c, const uint8_t* w, size_t n, const ui
     if (!c || !w || !r || !s || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
+    if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     WsGuard g(c);
     if ((rc = acquire(c, &g.ws))) return rc;
@@ -1244,6 +1425,7 @@ int g16_prove_with_blinders_device(g16_circuit* c, const void* d_w, size_t n, co
     if (!c || !d_w || !r || !s || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, nullptr);
     if (rc) return rc;
+    if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     WsGuard g(c);
     if ((rc = acquire(c, &g.ws))) return rc;
@@ -1379,11 +1561,14 @@ int g16_prove_batch_timed(g16_backend* b, size_t count, g16_circuit* const* circ
         int rc = check_witness(circuits[i], lens[i], witnesses[i]);
         if (rc) return rc;
     }
+    if (int rc_dev = device_usable(b)) return rc_dev;
     CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
     // one launch per stage for every job; host lanes only for constant-work MSMs, when
     // G16_BATCH_ENGINE=0, or when the batch's working set does not fit the device budget
     const char* eng = std::getenv("G16_BATCH_ENGINE");
-    if (!b->constant_work && !(eng && std::strcmp(eng, "0") == 0)) {
+    bool all_tables = true;   // the engine reads window tables; compact keys take the lanes
+    for (size_t i = 0; i < count; i++) all_tables &= circuits[i]->tables;
+    if (!b->constant_work && all_tables && !(eng && std::strcmp(eng, "0") == 0)) {
         int rc = prove_batch_engine(b, count, circuits, witnesses, lens, r, s, out, done_ms);
         if (rc != G16_ERR_DEVICE_MEMORY) return rc;
     }
@@ -1470,6 +1655,7 @@ static int msm_host_impl(g16_backend* b, const uint8_t* bases, const uint8_t* sc
                          uint8_t* out) {
     if (!b || (n && (!bases || !scalars)) || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     std::lock_guard<std::mutex> g(b->mu);
+    if (int rc_dev = device_usable(b)) return rc_dev;
     CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
     if (n == 0) {
         std::memset(out, 0, g2 ? 128 : 64);
@@ -1493,12 +1679,14 @@ int g16_msm_g2(g16_backend* b, const uint8_t* bases, const uint8_t* scalars, siz
 int g16_msm_g1_device(g16_backend* b, const void* d_bases, const void* d_scalars, size_t n, int form, uint8_t* out64) {
     if (!b || !out64) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     std::lock_guard<std::mutex> g(b->mu);
+    if (int rc_dev = device_usable(b)) return rc_dev;
     CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
     return msm_device_impl(b, d_bases, d_scalars, n, form, false, out64);
 }
 int g16_msm_g2_device(g16_backend* b, const void* d_bases, const void* d_scalars, size_t n, int form, uint8_t* out128) {
     if (!b || !out128) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     std::lock_guard<std::mutex> g(b->mu);
+    if (int rc_dev = device_usable(b)) return rc_dev;
     CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
     return msm_device_impl(b, d_bases, d_scalars, n, form, true, out128);
 }
@@ -1540,6 +1728,7 @@ static int ntt_device_impl(g16_backend* b, int mode, uint32_t log_n, void* d, co
 int g16_ntt(g16_backend* b, int mode, uint32_t log_n, uint8_t* data, const uint8_t* shift_mont) {
     if (!b || !data) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     std::lock_guard<std::mutex> g(b->mu);
+    if (int rc_dev = device_usable(b)) return rc_dev;
     CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
     if (log_n < 1 || log_n > 27) return fail(G16_ERR_INVALID_ARGUMENT, "log_n %u outside [1, 27]", log_n);
     size_t bytes = ((size_t)1 << log_n) * 32;
@@ -1556,6 +1745,7 @@ int g16_ntt(g16_backend* b, int mode, uint32_t log_n, uint8_t* data, const uint8
 int g16_ntt_device(g16_backend* b, int mode, uint32_t log_n, void* d, const uint8_t* shift_mont) {
     if (!b || !d) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     std::lock_guard<std::mutex> g(b->mu);
+    if (int rc_dev = device_usable(b)) return rc_dev;
     CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
     int rc = ntt_device_impl(b, mode, log_n, d, shift_mont);
     if (rc) return rc;
@@ -1597,6 +1787,7 @@ int g16_tuning_get(const g16_circuit* c, g16_tuning* out) {
 
 int g16_tuning_set(g16_circuit* c, const g16_tuning* t) {
     if (!c || !t) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     TuningLock lock(c);
     int rc = lock.take();
@@ -1609,6 +1800,7 @@ int g16_autotune(g16_circuit* c, const uint8_t* w, size_t n, int concurrency, g1
     if (concurrency < 1 || concurrency > 8) return fail(G16_ERR_INVALID_ARGUMENT, "concurrency must be 1..8");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
+    if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     TuningLock lock(c);
     if ((rc = lock.take(concurrency))) return rc;
@@ -1701,6 +1893,7 @@ int g16_circuit_set_serial(g16_circuit* c, int serial) {
 int g16_imad_peak(g16_backend* b, double* imad_per_s) {
     if (!b || !imad_per_s) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     std::lock_guard<std::mutex> g(b->mu);
+    if (int rc_dev = device_usable(b)) return rc_dev;
     CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->ordinal), "attribute");
@@ -1740,6 +1933,7 @@ int g16_imad_peak(g16_backend* b, double* imad_per_s) {
 // ---- device memory helpers ----
 int g16_device_alloc(g16_backend* b, size_t bytes, void** d_out) {
     if (!b || !d_out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    if (int rc_dev = device_usable(b)) return rc_dev;
     CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
     CK(g16::dev_malloc(d_out, bytes ? bytes : 32), "device allocation");
     return G16_OK;
@@ -1752,12 +1946,17 @@ int g16_device_free(g16_backend* b, void* d) {
 }
 int g16_device_upload(g16_backend* b, void* d_dst, const void* src, size_t bytes) {
     if (!b || !d_dst || !src) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    if (int rc_dev = device_usable(b)) return rc_dev;
     CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
-    CK(cudaMemcpy(d_dst, src, bytes, cudaMemcpyHostToDevice), "upload");
+    // complete on return: a plain cudaMemcpy from pageable memory may return
+    // before its DMA lands, and kernels on non-blocking streams would not wait for it
+    CK(cudaMemcpyAsync(d_dst, src, bytes, cudaMemcpyHostToDevice, b->stream), "upload");
+    CK(cudaStreamSynchronize(b->stream), "upload");
     return G16_OK;
 }
 int g16_device_sync(g16_backend* b) {
     if (!b) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    if (int rc_dev = device_usable(b)) return rc_dev;
     CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
     CK(cudaDeviceSynchronize(), "device synchronize");
     return G16_OK;

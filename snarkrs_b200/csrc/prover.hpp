@@ -36,6 +36,8 @@ struct g16_backend {
     unsigned long long* h_work = nullptr;
     std::mutex batch_mu;                           // guards batch
     g16::BatchPool* batch = nullptr;               // the batched-proving engines, built on first use
+    std::atomic<int> fault{0};                     // sticky status that put this backend out of use (injected)
+    std::atomic<int> inject{0};                    // fault for the next device entry point (g16_backend_inject_fault)
 };
 
 namespace g16 {
@@ -61,12 +63,14 @@ struct Workspace {
     bool graph_constant_work = false;  // the mode the graph was captured in
     uint64_t proofs = 0;
     uint64_t bytes = 0;                // fixed device buffers
+    size_t win_slot = 0;               // bytes of h_win per MSM
 
-    cudaError_t init(uint32_t n_vars, uint32_t n) {
+    cudaError_t init(uint32_t n_vars, uint32_t n, size_t slot) {
+        win_slot = slot;
         cudaError_t e = g16::dev_malloc(&d_w, 32ull * n_vars);
         if (e == cudaSuccess) e = g16::dev_malloc(&d_abc, 32ull * n * 3);
         if (e == cudaSuccess) e = g16::dev_malloc(&d_hpoly, 32ull * n);
-        if (e == cudaSuccess) e = cudaMallocHost((void**)&h_win, 5 * MSM_RESULT_SLOT_BYTES);
+        if (e == cudaSuccess) e = cudaMallocHost((void**)&h_win, 5 * slot);
         if (e == cudaSuccess) e = cudaMallocHost((void**)&h_work, 8 * sizeof(unsigned long long));
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
         for (auto& x : side)
@@ -114,9 +118,14 @@ struct g16_circuit {
     void *d_a = nullptr, *d_b1 = nullptr, *d_b2 = nullptr, *d_l = nullptr, *d_h = nullptr;
     uint32_t* d_rank[3] = {nullptr, nullptr, nullptr};   // wire -> row in the set's bases, or g16::MSM_DEAD
     uint32_t rows[3] = {0, 0, 0};                        // live wires of the A, B and L sets
-    // window-shifted base tables 2^(c w) P_i at w * rows + i (msm_window_table)
+    // window-shifted base tables 2^(c w) P_i at w * rows + i (msm_window_table);
+    // all null when the key is held compact
     void *t_a = nullptr, *t_b1 = nullptr, *t_b2 = nullptr, *t_l = nullptr, *t_h = nullptr;
     int c_w = 0, c_h = 0;   // window bits of the witness and H MSMs
+    // true: the MSMs read the window-shifted tables, all windows in one bucket
+    // set; false (compact key, about a tenth of the memory): they read the plain
+    // bases with one bucket set per window and a Horner step on the host
+    bool tables = true;
     g16::NttTables ntt;
     g16::G1A alpha1, beta1, delta1;
     g16::G2A beta2, delta2, gamma2;
@@ -145,6 +154,13 @@ namespace g16 {
 // Error helpers: set the thread's last error text and return the status.
 int fail(int code, const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what);
+// G16_FAULT_* classes of a cudaError_t value (g16_cuda_error_class).
+int error_class(int code);
+// G16_OK, or the refusal of a device put out of use by a sticky fault; also
+// delivers an injected fault.  First call of every entry point using b's device.
+int device_usable(g16_backend* b);
+// The sticky status that took device `ordinal` out of use in this process, or 0.
+int device_fault(int ordinal);
 
 // The key-only products of stage 11 (BlinderTerms::new, crates/groth16/src/prove.rs:335-346).
 struct BlinderTerms {

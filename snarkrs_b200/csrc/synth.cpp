@@ -255,8 +255,11 @@ struct DevicePoints {
     bool upload_table(const std::vector<Affine<F>>& t, void*& d, size_t point_bytes) {
         std::vector<uint8_t> packed(t.size() * point_bytes);
         for (size_t i = 0; i < t.size(); i++) pack(packed.data() + i * point_bytes, t[i]);
+        // on st and waited for: the kernels run on st, which does not order
+        // against a legacy-stream copy
         return check(g16::dev_malloc(&d, packed.size()), "table") &&
-               check(cudaMemcpy(d, packed.data(), packed.size(), cudaMemcpyHostToDevice), "table upload");
+               check(cudaMemcpyAsync(d, packed.data(), packed.size(), cudaMemcpyHostToDevice, st), "table upload") &&
+               check(cudaStreamSynchronize(st), "table upload");
     }
     bool points(int group, const Fr* k, size_t n, uint8_t* out) {
         const size_t pb = group == 1 ? 64 : 128;

@@ -87,3 +87,36 @@ def test_batch_lanes_give_the_same_proofs(backend, mix):
         del os.environ["G16_BATCH_ENGINE"]
     assert engine == lanes
     check(engine, jobs, meta)
+
+
+def test_concurrent_submissions_each_equal_singles(backend, mix):
+    """Four threads submit batches of random mixes at once, so several engines
+    rebuild layouts and run side by side; every proof equals its single proof."""
+    import threading
+    refs = {}
+    for i in range(len(mix)):
+        sc, zk, ok, circ = mix[i]
+        for k in range(3):
+            w = sc.witness(3000 + 10 * i + k)
+            r, s = blinders(4000 + 10 * i + k)
+            refs[(i, k)] = (w, r, s, circ.prove_with_blinders(w, r, s))
+    bad, errors = [], []
+
+    def worker(tid):
+        rng = random.Random(77 + tid)
+        try:
+            for _ in range(12):
+                picks = [(rng.randrange(len(mix)), rng.randrange(3)) for _ in range(rng.randrange(1, 9))]
+                jobs = [(mix[i][3],) + refs[(i, k)][:3] for i, k in picks]
+                out = backend.prove_batch(jobs)
+                bad.extend(q for q, p in zip(picks, out) if p != refs[q][3])
+        except Exception as e:   # reported below, on the test's thread
+            errors.append(repr(e))
+
+    threads = [threading.Thread(target=worker, args=(t,)) for t in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    assert not bad, bad

@@ -112,3 +112,69 @@ def test_r1cs_writer_layout(small):
     hdr = r.find(O.R_MOD.to_bytes(32, "little"))
     n_wires, n_out, n_pub, n_prv = (int.from_bytes(r[hdr + 32 + 4 * i:hdr + 36 + 4 * i], "little") for i in range(4))
     assert (n_wires, n_out, n_pub, n_prv) == (sc.n_vars, 0, 5, 19)
+
+
+# cudaError_t values from the CUDA runtime's driver_types.h, each with the
+# classes the reference's is_device_fault / is_sticky give its CUresult twin
+# (crates/cuda/src/context.rs:146-215); 0 for calls rejected every time.
+CUDA_STATUS_CLASSES = {
+    0: 0,      # cudaSuccess
+    1: 0,      # cudaErrorInvalidValue
+    2: 1,      # cudaErrorMemoryAllocation
+    46: 1,     # cudaErrorDevicesUnavailable
+    98: 0,     # cudaErrorInvalidDeviceFunction
+    100: 0,    # cudaErrorNoDevice
+    214: 1,    # cudaErrorECCUncorrectable
+    220: 1,    # cudaErrorNvlinkUncorrectable
+    226: 3,    # cudaErrorContained
+    400: 0,    # cudaErrorInvalidResourceHandle
+    600: 0,    # cudaErrorNotReady
+    700: 3,    # cudaErrorIllegalAddress
+    701: 0,    # cudaErrorLaunchOutOfResources
+    702: 3,    # cudaErrorLaunchTimeout
+    710: 3,    # cudaErrorAssert
+    714: 3,    # cudaErrorHardwareStackError
+    715: 3,    # cudaErrorIllegalInstruction
+    716: 3,    # cudaErrorMisalignedAddress
+    717: 3,    # cudaErrorInvalidAddressSpace
+    718: 3,    # cudaErrorInvalidPc
+    719: 3,    # cudaErrorLaunchFailure
+    802: 1,    # cudaErrorSystemNotReady
+    805: 1, 806: 1, 807: 1, 808: 1, 809: 1, 810: 1,   # MPS failures
+    900: 0,    # cudaErrorStreamCaptureUnsupported
+    909: 1,    # cudaErrorTimeout
+    911: 1,    # cudaErrorExternalDevice
+    999: 1,    # cudaErrorUnknown
+}
+
+
+def test_cuda_status_classes():
+    got = {code: S.cuda_error_class(code) for code in CUDA_STATUS_CLASSES}
+    assert got == CUDA_STATUS_CLASSES
+    assert S.FAULT_DEVICE == 1 and S.FAULT_STICKY == 2
+
+
+def test_key_plan_falls_back_to_a_compact_key(monkeypatch):
+    # large enough that the compact key and its workspace are the smaller plan
+    sc = S.SynthCircuit(seed=901, n_constraints=3000, n_inputs=24, n_public=5)
+    pk = S.ProvingKey.from_bytes(sc.zkey(902))
+    full = pk.plan(1 << 40)
+    assert full["window_tables"] == 1
+    need_full = full["key_bytes"] + full["workspace_bytes"]
+    compact = pk.plan(need_full - 1)
+    assert compact["window_tables"] == 0
+    assert compact["key_bytes"] < full["key_bytes"]
+    assert 8 <= compact["msm_window_bits_witness"] <= 20 and 8 <= compact["msm_window_bits_h"] <= 20
+    assert pk.plan(compact["key_bytes"] + compact["workspace_bytes"])["window_tables"] == 0
+    with pytest.raises(S.DeviceMemoryError, match="compact key"):
+        pk.plan(compact["key_bytes"] + compact["workspace_bytes"] - 1)
+    monkeypatch.setenv("G16_CUDA_WINDOW_TABLES", "0")
+    assert pk.plan(1 << 40)["window_tables"] == 0
+
+
+def test_compact_key_is_much_smaller():
+    sc = S.SynthCircuit(seed=5, n_constraints=1 << 14, n_inputs=64, n_public=4)
+    pk = S.ProvingKey.from_bytes(sc.zkey(6))
+    full = pk.plan(1 << 50)
+    compact = pk.plan(full["key_bytes"] + full["workspace_bytes"] - 1)
+    assert compact["key_bytes"] * 8 < full["key_bytes"]
