@@ -889,32 +889,44 @@ def run_serve(args, backend=None, emit=True, fracs=(0.5, 0.9, 1.5), n_req=None):
         wits.append([sc.witness(7000 + 10 * len(wits) + j) for j in range(2)])
     budget = 120 << 30
 
-    def run(lanes, rate, n_req, seed, max_batch=64):
+    def arrivals(rate, n_req, seed):
         rng = random.Random(seed)
-        srv = S.ProofServer(backend, budget, lanes, max_batch)
-        for i, k in enumerate(keys):
-            srv.register_key(i, k)
-        # warm every key outside the measurement: prepare, one workspace per
-        # lane and its CUDA graph (captured on a workspace's second proof)
-        for i in range(len(keys)):
-            for _ in range(2):
-                r, s_ = blinders(i)
-                for t in [srv.submit(i, wits[i][0], r, s_) for _ in range(lanes)]:
-                    srv.wait(t)
-        reqs = []
-        t = 0.0
+        reqs, t = [], 0.0
         for j in range(n_req):
             t += rng.expovariate(rate)
             i = rng.choices(range(len(keys)), weights=SERVE_WEIGHTS)[0]
             reqs.append((t, i, j))
+        return reqs
+
+    def play(srv, reqs, blind_base):
         tickets = []
         t0 = time.perf_counter()
         for (ta, i, j) in reqs:
             delay = t0 + ta - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
-            r, s_ = blinders(10_000 + j)
+            r, s_ = blinders(blind_base + j)
             tickets.append((srv.submit(i, wits[i][j % 2], r, s_), i, j))
+        return t0, tickets
+
+    def run(lanes, rate, n_req, seed, max_batch=64):
+        srv = S.ProofServer(backend, budget, lanes, max_batch)
+        for i, k in enumerate(keys):
+            srv.register_key(i, k)
+        # warm the server outside the measurement with the same arrival process
+        # (other draws): keys prepared, as many workspaces and engines as the load
+        # keeps busy, their buffers at size and CUDA graphs captured, as in a
+        # server that has been running
+        for i in range(len(keys)):
+            r, s_ = blinders(i)
+            srv.wait(srv.submit(i, wits[i][0], r, s_))
+        _, warm = play(srv, arrivals(rate, n_req, seed + 1000), 20_000)
+        for tk, _, _ in warm:
+            srv.wait(tk)
+        reqs = arrivals(rate, n_req, seed)
+        tickets = []
+        bs0, allocs0 = backend.batch_stats(), S.device_alloc_count()
+        t0, tickets = play(srv, reqs, 10_000)
         lat, proofs = [], {}
         for tk, i, j in tickets:
             p, q, l = srv.wait(tk)
@@ -922,6 +934,9 @@ def run_serve(args, backend=None, emit=True, fracs=(0.5, 0.9, 1.5), n_req=None):
             proofs[j] = p
         t_end = time.perf_counter()
         stats = srv.stats()
+        bs1 = backend.batch_stats()
+        stats["engine"] = {k: bs1[k] - bs0[k] for k in bs1}
+        stats["device_allocs_in_timed_region"] = S.device_alloc_count() - allocs0
         srv.close()
         lat.sort()
         return {"lanes": lanes, "offered_rate": rate, "requests": n_req,
@@ -932,7 +947,7 @@ def run_serve(args, backend=None, emit=True, fracs=(0.5, 0.9, 1.5), n_req=None):
     # plain capacity: mean service time over the mix, one request at a time
     calib, _ = run(1, 1e6, 60, 1, max_batch=1)     # back-to-back arrivals = saturated FIFO
     cap = calib["throughput"]
-    n_req = n_req or max(100, args.steps * 40)
+    n_req = n_req or max(300, args.steps * 100)
     results = []
     mix_ok = True
     for frac in fracs:

@@ -288,11 +288,16 @@ int g16_prove_batch_timed(g16_backend *b, size_t count, g16_circuit *const *circ
 
 /* Served proving (no reference counterpart; the reference proves one request
  * per call).  A request loop with continuous batching: each of `lanes`
- * workers, as soon as it is free, takes every request queued at that moment
- * (in arrival order, up to the batch limits) and proves them together as one
- * g16_prove_batch submission, so requests that arrive while others are on the
- * GPU are admitted with the next free worker's batch, and the workers'
- * batches overlap on the device.  Registered keys are prepared on first use
+ * workers, as soon as it is free, takes every small request queued at that
+ * moment (in arrival order, up to the batch limits) and proves them together
+ * as one g16_prove_batch submission, so requests that arrive while others are
+ * on the GPU are admitted with the next free worker's batch, and the workers'
+ * batches overlap on the device.  A request of at least 2^19 witness wires
+ * (G16_SERVE_SOLO_WIRES; 0 batches every size) is proved alone by the next
+ * free worker when it reaches the head of the queue: it fills the device by
+ * itself, and the small requests of a batch would otherwise wait for it (a
+ * batch's proofs complete together).  A batch of one request is a plain
+ * g16_prove_with_blinders call.  Registered keys are prepared on first use
  * and stay resident in HBM while their device bytes fit key_budget_bytes
  * (0 = unlimited); a key that does not fit evicts least recently used idle
  * keys.  A batch starts when its working set fits the backend's device-memory
@@ -302,6 +307,9 @@ int g16_prove_batch_timed(g16_backend *b, size_t count, g16_circuit *const *circ
 typedef struct g16_server g16_server;
 typedef struct {
     uint64_t submitted, completed, prepared, evicted, resident_keys, resident_bytes, queued;
+    uint64_t batches;        /* batched submissions of two or more requests */
+    uint64_t batched;        /* requests proved in those */
+    uint64_t alone;          /* requests proved alone */
 } g16_server_stats;
 int g16_server_new(g16_backend *b, uint64_t key_budget_bytes, int lanes, g16_server **out);
 /* Requests per batch (at least 1); 1 proves each request alone on a
@@ -318,6 +326,16 @@ int g16_server_wait(g16_server *s, uint64_t ticket, g16_proof *out, double *queu
 int g16_server_stats_get(g16_server *s, g16_server_stats *out);
 /* Finishes the queued requests, then frees every resident key. */
 void g16_server_free(g16_server *s);
+
+/* Counters of a backend's batched-proving engines since it was opened. */
+typedef struct {
+    uint64_t submissions;    /* g16_prove_batch calls run by an engine */
+    uint64_t layouts;        /* of those, ones that laid out a new mix of circuits */
+    uint64_t replays;        /* ones that replayed a captured CUDA graph */
+    uint64_t grown_bytes;    /* device bytes the engines allocated (buffers only grow) */
+    uint64_t engines;        /* engines built */
+} g16_batch_stats;
+int g16_batch_stats_get(const g16_backend *b, g16_batch_stats *out);
 
 /* ---------------- primitives (MsmBackend, crates/msm/src/lib.rs:52-82) ---------------- */
 /* sum_i scalars[i] * bases[i]; host buffers; result affine packed. */

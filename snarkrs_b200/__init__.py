@@ -507,6 +507,13 @@ class CudaBackend:
     def name(self):
         return lib().g16_backend_name(self._h).decode()
 
+    def batch_stats(self):
+        """Counters of the batched-proving engines: submissions, new layouts,
+        graph replays, device bytes grown, engines built."""
+        st = _BatchStats()
+        check(lib().g16_batch_stats_get(self._h, ctypes.byref(st)))
+        return {n: getattr(st, n) for n, _ in st._fields_}
+
     def fault(self):
         """The sticky cudaError_t value that put this backend out of use, or 0."""
         return lib().g16_backend_fault(self._h)
@@ -572,7 +579,12 @@ class CudaBackend:
 
 class _ServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in
-                ("submitted", "completed", "prepared", "evicted", "resident_keys", "resident_bytes", "queued")]
+                ("submitted", "completed", "prepared", "evicted", "resident_keys", "resident_bytes", "queued",
+                 "batches", "batched", "alone")]
+
+
+class _BatchStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("submissions", "layouts", "replays", "grown_bytes", "engines")]
 
 
 class ProofServer:

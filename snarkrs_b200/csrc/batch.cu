@@ -386,6 +386,20 @@ void batch_forget(g16_backend* b, const g16_circuit* c) {
             }
 }
 
+}  // namespace g16
+
+int g16_batch_stats_get(const g16_backend* b, g16_batch_stats* out) {
+    if (!b || !out) return g16::fail(G16_ERR_INVALID_ARGUMENT, "g16_batch_stats_get: null argument");
+    out->submissions = b->batch_submissions.load();
+    out->layouts = b->batch_layouts.load();
+    out->replays = b->batch_replays.load();
+    out->grown_bytes = b->batch_grown.load();
+    out->engines = b->batch_engines.load();
+    return G16_OK;
+}
+
+namespace g16 {
+
 void batch_free(g16_backend* b) {
     std::lock_guard<std::mutex> g(b->batch_mu);
     if (!b->batch) return;
@@ -424,6 +438,7 @@ int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, con
         if (!eng) {
             P.all.push_back(std::make_unique<BatchEngine>());
             eng = P.all.back().get();
+            b->batch_engines++;
         }
     }
     struct GiveBack {
@@ -468,11 +483,14 @@ int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, con
             b->vram_used += need - E.accounted;
             E.accounted = need;
         }
+        const uint64_t allocs0 = timer().device_alloc_bytes.load();
         int rc = build(E, cs, count);
         if (rc != G16_OK) {
             E.drop_layout();
             return rc;
         }
+        b->batch_layouts++;
+        b->batch_grown += timer().device_alloc_bytes.load() - allocs0;
     }
     // witnesses in: gathered into pinned memory by host threads, then one copy
     const size_t threads = host_threads();
@@ -512,7 +530,9 @@ int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, con
         }
     }
     if (rc == G16_OK) {
+        b->batch_submissions++;
         if (use_graph) {
+            b->batch_replays++;
             cudaError_t e = cudaGraphLaunch(E.graph, E.st[0]);
             if (e != cudaSuccess) rc = cuda_fail(e, "batch graph launch");
             else timer().launches.fetch_add(E.graph_kernels);

@@ -40,6 +40,7 @@ struct KernelTimer {
     std::map<std::string, double> bytes;                     // algorithmic HBM bytes, per kernel class
     std::atomic<uint64_t> launches{0};                        // every kernel this library launched
     std::atomic<uint64_t> device_allocs{0};                   // every cudaMalloc this library made
+    std::atomic<uint64_t> device_alloc_bytes{0};              // and their bytes
     std::mutex mu;
 
     void add_units(const char* name, double u) {
@@ -117,6 +118,7 @@ struct TimedLaunch {
 template <class T>
 inline cudaError_t dev_malloc(T** p, size_t bytes) {
     timer().device_allocs.fetch_add(1, std::memory_order_relaxed);
+    timer().device_alloc_bytes.fetch_add(bytes, std::memory_order_relaxed);
     return cudaMalloc((void**)p, bytes);
 }
 

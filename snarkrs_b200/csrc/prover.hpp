@@ -36,6 +36,7 @@ struct g16_backend {
     unsigned long long* h_work = nullptr;
     std::mutex batch_mu;                           // guards batch
     g16::BatchPool* batch = nullptr;               // the batched-proving engines, built on first use
+    std::atomic<uint64_t> batch_submissions{0}, batch_layouts{0}, batch_replays{0}, batch_grown{0}, batch_engines{0};
     std::atomic<int> fault{0};                     // sticky status that put this backend out of use (injected)
     std::atomic<int> inject{0};                    // fault for the next device entry point (g16_backend_inject_fault)
 };

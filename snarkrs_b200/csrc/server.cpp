@@ -69,10 +69,12 @@ struct g16_server {
     std::unordered_map<uint32_t, KeyEntry> keys;
     uint64_t next_ticket = 1, clock = 0, resident_bytes = 0;
     uint64_t submitted = 0, completed = 0, prepared = 0, evicted = 0;
+    uint64_t batches = 0, batched = 0, alone = 0;
     std::vector<std::thread> workers;
     bool stop = false;
     size_t max_batch = 64;          // requests per batch
     uint64_t batch_wires = 1u << 21;   // work cap of a batch: witness wires summed
+    uint64_t solo_wires = 1u << 19;    // requests of at least this many wires are proved alone (0: none)
 };
 
 namespace {
@@ -177,21 +179,36 @@ void complete(g16_server* sv, Request* q, int rc, const std::string& err) {
 // Work of a request for the batch cap: its witness length (wires).
 uint64_t work_of(const Request* q) { return q->witness.size() / 32; }
 
+// A large request is proved alone: its stages fill the device by themselves,
+// and in a batch the small requests beside it would wait for its MSMs (a
+// batch's proofs complete together).
+bool solo(const g16_server* sv, const Request* q) { return sv->solo_wires && work_of(q) >= sv->solo_wires; }
+
 void worker(g16_server* sv) {
     std::unique_lock<std::mutex> lk(sv->mu);
     for (;;) {
         sv->cv_work.wait(lk, [&] { return sv->stop || !sv->queue.empty(); });
         if (sv->stop && sv->queue.empty()) return;
-        // every queued request, in arrival order, while the batch's work stays
-        // under the cap (the first one always goes)
+        // a large request at the head goes alone; otherwise the queued small
+        // requests, in arrival order, while the batch's work stays under the
+        // cap (the first one always goes), leaving large ones for other workers
         std::vector<Request*> batch;
         uint64_t work = 0;
-        while (!sv->queue.empty() && batch.size() < sv->max_batch) {
-            Request* q = sv->queue.front();
-            if (!batch.empty() && work + work_of(q) > sv->batch_wires) break;
+        if (solo(sv, sv->queue.front())) {
+            batch.push_back(sv->queue.front());
             sv->queue.pop_front();
-            work += work_of(q);
-            batch.push_back(q);
+        } else {
+            for (auto it = sv->queue.begin(); it != sv->queue.end() && batch.size() < sv->max_batch;) {
+                Request* q = *it;
+                if (solo(sv, q)) {
+                    ++it;
+                    continue;
+                }
+                if (!batch.empty() && work + work_of(q) > sv->batch_wires) break;
+                work += work_of(q);
+                batch.push_back(q);
+                it = sv->queue.erase(it);
+            }
         }
         if (!sv->queue.empty()) sv->cv_work.notify_one();   // the rest is another worker's
         // keys resident and pinned for the batch; requests refused up front end here
@@ -240,13 +257,12 @@ void worker(g16_server* sv) {
             }
             const Clock::time_point t0 = Clock::now();
             for (Request* q : run) q->started = t0;
-            // max_batch 1 is plain one-proof-at-a-time proving (a workspace per proof)
-            int rc = sv->max_batch == 1
-                         ? g16_prove_with_blinders(circs[0], wits[0], lens[0], run[0]->r, run[0]->s, &proofs[0])
-                         : g16_prove_batch_timed(sv->b, n, circs.data(), wits.data(), lens.data(), rs.data(),
-                                                 ss.data(), proofs.data(), done.data());
-            if (sv->max_batch == 1 && rc == G16_OK)
-                done[0] = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+            // one request is plain proving on a workspace of its circuit (max_batch
+            // 1 is one-proof-at-a-time serving); more go as one batched submission
+            int rc = n == 1 ? g16_prove_with_blinders(circs[0], wits[0], lens[0], run[0]->r, run[0]->s, &proofs[0])
+                            : g16_prove_batch_timed(sv->b, n, circs.data(), wits.data(), lens.data(), rs.data(),
+                                                    ss.data(), proofs.data(), done.data());
+            if (n == 1 && rc == G16_OK) done[0] = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
             std::vector<int> rcs(n, rc);
             std::vector<std::string> errs(n, rc == G16_OK ? std::string() : last_error_text());
             if (rc != G16_OK) {
@@ -258,6 +274,12 @@ void worker(g16_server* sv) {
                 }
             }
             lk.lock();
+            if (n == 1) {
+                sv->alone++;
+            } else {
+                sv->batches++;
+                sv->batched += n;
+            }
             for (size_t i = 0; i < n; i++) {
                 Request* q = run[i];
                 q->finished = t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double, std::milli>(done[i]));
@@ -285,6 +307,7 @@ int g16_server_new(g16_backend* b, uint64_t key_budget_bytes, int lanes, g16_ser
     sv->budget = key_budget_bytes ? key_budget_bytes : ~0ull;
     if (const char* e = std::getenv("G16_SERVE_BATCH")) sv->max_batch = (size_t)std::max(1, std::atoi(e));
     if (const char* e = std::getenv("G16_SERVE_BATCH_WIRES")) sv->batch_wires = std::max<uint64_t>(1, std::strtoull(e, nullptr, 10));
+    if (const char* e = std::getenv("G16_SERVE_SOLO_WIRES")) sv->solo_wires = std::strtoull(e, nullptr, 10);
     for (int i = 0; i < lanes; i++) sv->workers.emplace_back(worker, sv.get());
     *out = sv.release();
     return G16_OK;
@@ -379,6 +402,9 @@ int g16_server_stats_get(g16_server* sv, g16_server_stats* out) {
     for (auto& kv : sv->keys) out->resident_keys += kv.second.circ ? 1 : 0;
     out->resident_bytes = live_bytes(sv);
     out->queued = sv->queue.size();
+    out->batches = sv->batches;
+    out->batched = sv->batched;
+    out->alone = sv->alone;
     return G16_OK;
 }
 
