@@ -22,6 +22,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 SOURCES = ["host_bn254.cpp", "formats.cpp", "synth.cpp", "msm.cu", "msm_noalloc.cu", "ntt.cu", "prover.cu", "batch.cu", "server.cpp", "pairing.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
+# extra nvcc flags for experiments (e.g. -DACC_G2_MIN_BLOCKS=3); pass --force when they change
+EXTRA = os.environ.get("G16_NVCC_EXTRA", "").split()
 
 
 def _headers():
@@ -46,7 +48,7 @@ def _compile(src, verbose):
     if not _stale(obj, [path] + _headers()):
         return obj
     lang = ["-x", "cu"] if src.endswith(".cu") else ["-x", "c++"]
-    cmd = [NVCC] + ARCH + COMMON + lang + ["-c", path, "-o", obj]
+    cmd = [NVCC] + ARCH + COMMON + EXTRA + lang + ["-c", path, "-o", obj]
     if verbose:
         cmd += ["-Xptxas", "-v"]
         print(" ".join(cmd), file=sys.stderr)

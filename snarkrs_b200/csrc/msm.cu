@@ -432,6 +432,11 @@ __device__ __forceinline__ void accumulate_chunks(const uint32_t* __restrict__ e
 
 constexpr int ACC_BLOCK_G1 = 512;   // lockstep block: 16 warps, one block per SM (<= 128 registers)
 constexpr int ACC_BLOCK_G2 = 128;
+// G2 accumulate blocks resident per SM that the register budget must allow
+// (1: the compiler may take 255 registers, which leaves room for 2)
+#ifndef ACC_G2_MIN_BLOCKS
+#define ACC_G2_MIN_BLOCKS 1
+#endif
 
 // Multiprocessors of the current device (148 on a B200), cached per device.
 static uint32_t device_sms() {
@@ -477,7 +482,7 @@ __global__ void __launch_bounds__(ACC_BLOCK_G1, 1) k_accumulate_g1(const uint32_
     accumulate_chunks<Fq, true>(entries, offsets, seg_base, K, M, L, bases, base_offset, n_bases, partials, work);
 }
 
-__global__ void __launch_bounds__(ACC_BLOCK_G2) k_accumulate_g2(const uint32_t* __restrict__ entries,
+__global__ void __launch_bounds__(ACC_BLOCK_G2, ACC_G2_MIN_BLOCKS) k_accumulate_g2(const uint32_t* __restrict__ entries,
                                                                const uint32_t* __restrict__ offsets,
                                                                const uint32_t* __restrict__ seg_base, uint32_t K,
                                                                const uint32_t* __restrict__ d_M,
@@ -808,7 +813,7 @@ __global__ void __launch_bounds__(ACC_BLOCK_G1, 1) k_accumulate_multi_g1(const u
                                       nsegs);
 }
 
-__global__ void __launch_bounds__(ACC_BLOCK_G2) k_accumulate_multi_g2(const uint32_t* __restrict__ entries,
+__global__ void __launch_bounds__(ACC_BLOCK_G2, ACC_G2_MIN_BLOCKS) k_accumulate_multi_g2(const uint32_t* __restrict__ entries,
                                                                      const uint32_t* __restrict__ offsets,
                                                                      const uint32_t* __restrict__ seg_base,
                                                                      uint32_t K, const uint32_t* __restrict__ d_M,

@@ -118,3 +118,26 @@ def test_compact_key_by_environment_matches_oracle():
     c.close()
     b.close()
     ok.close()
+
+
+def test_batch_mixing_compact_and_table_keys(small, backend):
+    """A submission with a compact key runs on host lanes; every proof equals its single proof."""
+    sc, zk, ok = small
+    os.environ["G16_CUDA_WINDOW_TABLES"] = "0"
+    try:
+        compact = backend.prepare(S.ProvingKey.from_bytes(zk))
+    finally:
+        del os.environ["G16_CUDA_WINDOW_TABLES"]
+    tables = backend.prepare(S.ProvingKey.from_bytes(zk))
+    assert not compact.window_tables() and tables.window_tables()
+    jobs = []
+    for k, c in enumerate([tables, compact, tables, compact]):
+        w = sc.witness(70 + k)
+        r, s = blinders(70 + k)
+        jobs.append((c, w, r, s))
+    singles = [c.prove_with_blinders(w, r, s) for c, w, r, s in jobs]
+    assert backend.prove_batch(jobs) == singles
+    # the same key held both ways gives the same proof
+    assert compact.prove_with_blinders(*jobs[0][1:]) == singles[0]
+    compact.close()
+    tables.close()
