@@ -565,10 +565,22 @@ __global__ void __launch_bounds__(64) k_fat_merge_final(uint4* __restrict__ part
     }
 }
 
+// Whether the bucket-sum and reduction kernels inline the G1 addition's
+// products (G16_REDUCE_INLINE_G1=1) or call them out of line (the default).
+#ifndef G16_REDUCE_INLINE_G1
+#define G16_REDUCE_INLINE_G1 0
+#endif
+template <class F>
+constexpr bool REDUCE_INL = std::is_same<F, g16d::Fq>::value && G16_REDUCE_INLINE_G1;
+// Blocks per SM the bucket-sum and pieces kernels' register budget must allow.
+#ifndef REDUCE_MIN_BLOCKS
+#define REDUCE_MIN_BLOCKS 1
+#endif
+
 // Bucket sums S_g: one thread per bucket folds its few partials (a fat
 // bucket's total already sits in its first slot).
 template <class F>
-__global__ void __launch_bounds__(128) k_bucket_sums(const uint4* __restrict__ partials,
+__global__ void __launch_bounds__(128, REDUCE_MIN_BLOCKS) k_bucket_sums(const uint4* __restrict__ partials,
                                                      const uint32_t* __restrict__ offsets,
                                                      const uint32_t* __restrict__ seg_base, uint32_t K,
                                                      const uint32_t* __restrict__ d_L, uint4* __restrict__ buckets) {
@@ -580,7 +592,7 @@ __global__ void __launch_bounds__(128) k_bucket_sums(const uint4* __restrict__ p
     if (ns > FAT_PARTIALS) {
         acc = ld_xyzz<F>(partials, base);
     } else {
-        for (uint32_t s = 0; s < ns; s++) acc = xyzz_add<F, false>(acc, ld_xyzz<F>(partials, base + s));
+        for (uint32_t s = 0; s < ns; s++) acc = xyzz_add<F, REDUCE_INL<F>>(acc, ld_xyzz<F>(partials, base + s));
     }
     st_xyzz<F>(buckets, g, acc);
 }
@@ -603,7 +615,7 @@ __global__ void __launch_bounds__(128) k_bucket_sums(const uint4* __restrict__ p
 // microseconds on an otherwise idle SM, so the depth is what counts here.
 // The block writes T, G_0 .. G_(LB-1) and its run total R (LB + 2 points).
 template <class F, int LB>
-__global__ void __launch_bounds__(1 << LB) k_reduce_pieces(const uint4* __restrict__ buckets, uint32_t B,
+__global__ void __launch_bounds__(1 << LB, REDUCE_MIN_BLOCKS) k_reduce_pieces(const uint4* __restrict__ buckets, uint32_t B,
                                                            uint32_t seg, uint4* __restrict__ out) {
     constexpr uint32_t N = 1u << LB;
     extern __shared__ uint4 smem[];
@@ -621,10 +633,10 @@ __global__ void __launch_bounds__(1 << LB) k_reduce_pieces(const uint4* __restri
         const size_t g0 = (size_t)set * B + (size_t)p * seg;
 #pragma unroll 1
         for (int i = (int)seg - 1; i >= 0; i--) {
-            run = xyzz_add<F, false>(run, ld_xyzz<F>(buckets, g0 + i));
+            run = xyzz_add<F, REDUCE_INL<F>>(run, ld_xyzz<F>(buckets, g0 + i));
             if (weighted) {
-                if constexpr (TOT_SHARED) st_xyzz<F>(s_tot, t, xyzz_add<F, false>(ld_xyzz<F>(s_tot, t), run));
-                else tot = xyzz_add<F, false>(tot, run);
+                if constexpr (TOT_SHARED) st_xyzz<F>(s_tot, t, xyzz_add<F, REDUCE_INL<F>>(ld_xyzz<F>(s_tot, t), run));
+                else tot = xyzz_add<F, REDUCE_INL<F>>(tot, run);
             }
         }
     }
@@ -641,18 +653,18 @@ __global__ void __launch_bounds__(1 << LB) k_reduce_pieces(const uint4* __restri
         // thread t in [h, 2h) reads t - h and t and writes t - h; the trees
         // stay at 2h and above
         if (t < h) {
-            run = xyzz_add<F, false>(run, ld_xyzz<F>(s_run, t + h));
+            run = xyzz_add<F, REDUCE_INL<F>>(run, ld_xyzz<F>(s_run, t + h));
             st_xyzz<F>(s_run, t, run);
         } else if (t < 2 * h) {
             if (weighted) {
-                tot = xyzz_add<F, false>(ld_xyzz<F>(s_tot, t - h), ld_xyzz<F>(s_tot, t));
+                tot = xyzz_add<F, REDUCE_INL<F>>(ld_xyzz<F>(s_tot, t - h), ld_xyzz<F>(s_tot, t));
                 st_xyzz<F>(s_tot, t - h, tot);   // at the last step (t = 1) this is T
             }
         } else {
             // the half [2^lg, 2^(lg+1)) froze at step LB - lg; tree level k - (LB - lg) - 1 now
             const uint32_t hs = 1u << lg, s = 1u << (k - (LB - lg) - 1), o = t - hs;
             if ((o & (2 * s - 1)) == 0 && o + s < hs) {
-                run = xyzz_add<F, false>(run, ld_xyzz<F>(s_run, t + s));
+                run = xyzz_add<F, REDUCE_INL<F>>(run, ld_xyzz<F>(s_run, t + s));
                 st_xyzz<F>(s_run, t, run);
             }
         }
@@ -836,7 +848,7 @@ struct MsmReduceDev {
 // k_reduce_pieces for many segments: block b works on block b - block_start
 // of the segment that owns it, with that segment's B and seg.
 template <class F, int LB>
-__global__ void __launch_bounds__(1 << LB) k_reduce_pieces_multi(const uint4* __restrict__ buckets,
+__global__ void __launch_bounds__(1 << LB, REDUCE_MIN_BLOCKS) k_reduce_pieces_multi(const uint4* __restrict__ buckets,
                                                                  const MsmReduceDev* __restrict__ segs,
                                                                  uint32_t nsegs, uint4* __restrict__ out) {
     constexpr uint32_t N = 1u << LB;
@@ -859,10 +871,10 @@ __global__ void __launch_bounds__(1 << LB) k_reduce_pieces_multi(const uint4* __
         const size_t g0 = (size_t)sd.key_start + (size_t)p * seg;
 #pragma unroll 1
         for (int i = (int)seg - 1; i >= 0; i--) {
-            run = xyzz_add<F, false>(run, ld_xyzz<F>(buckets, g0 + i));
+            run = xyzz_add<F, REDUCE_INL<F>>(run, ld_xyzz<F>(buckets, g0 + i));
             if (weighted) {
-                if constexpr (TOT_SHARED) st_xyzz<F>(s_tot, t, xyzz_add<F, false>(ld_xyzz<F>(s_tot, t), run));
-                else tot = xyzz_add<F, false>(tot, run);
+                if constexpr (TOT_SHARED) st_xyzz<F>(s_tot, t, xyzz_add<F, REDUCE_INL<F>>(ld_xyzz<F>(s_tot, t), run));
+                else tot = xyzz_add<F, REDUCE_INL<F>>(tot, run);
             }
         }
     }
@@ -874,17 +886,17 @@ __global__ void __launch_bounds__(1 << LB) k_reduce_pieces_multi(const uint4* __
         __syncthreads();
         const uint32_t h = N >> k;
         if (t < h) {
-            run = xyzz_add<F, false>(run, ld_xyzz<F>(s_run, t + h));
+            run = xyzz_add<F, REDUCE_INL<F>>(run, ld_xyzz<F>(s_run, t + h));
             st_xyzz<F>(s_run, t, run);
         } else if (t < 2 * h) {
             if (weighted) {
-                tot = xyzz_add<F, false>(ld_xyzz<F>(s_tot, t - h), ld_xyzz<F>(s_tot, t));
+                tot = xyzz_add<F, REDUCE_INL<F>>(ld_xyzz<F>(s_tot, t - h), ld_xyzz<F>(s_tot, t));
                 st_xyzz<F>(s_tot, t - h, tot);
             }
         } else {
             const uint32_t hs = 1u << lg, s2 = 1u << (k - (LB - lg) - 1), o = t - hs;
             if ((o & (2 * s2 - 1)) == 0 && o + s2 < hs) {
-                run = xyzz_add<F, false>(run, ld_xyzz<F>(s_run, t + s2));
+                run = xyzz_add<F, REDUCE_INL<F>>(run, ld_xyzz<F>(s_run, t + s2));
                 st_xyzz<F>(s_run, t, run);
             }
         }
