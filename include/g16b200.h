@@ -100,8 +100,17 @@ typedef struct {
     const uint8_t *b_g1_query;    /* n_vars G1 (section 6) */
     const uint8_t *b_g2_query;    /* n_vars G2 (section 7) */
     const uint8_t *l_query;       /* n_vars - n_public - 1 G1 (section 8) */
-    const uint8_t *h_query;       /* domain_size G1 (section 9) */
+    const uint8_t *h_query;       /* domain_size G1 (section 9), or domain_size - 1 for the gnark basis */
+    uint32_t h_basis;             /* G16_H_SNARKJS or G16_H_GNARK (HBasis, crates/formats/src/lib.rs:60-90) */
 } g16_zkey_view;
+
+/* H bases of a key (HBasis): snarkjs' zkey section 9, the Lagrange bases of the
+ * odd coset (domain_size of them; H is taken on the coset as it is), or gnark's
+ * pk.G1.Z, [tau^bitrev(j) t(tau) / delta] for j < domain_size - 1 (H's
+ * coefficients in bit-reversed order, the MSM result times -1/2).  A gnark key
+ * has no constraint matrices (row_ptr, signal, value_id and values are NULL,
+ * nnz 0) and proves only from A.w and B.w rows. */
+enum { G16_H_SNARKJS = 0, G16_H_GNARK = 1 };
 
 /* ---------------- errors ---------------- */
 /* Copies the calling thread's last error text into buf (NUL-terminated);
@@ -154,6 +163,17 @@ int g16_backend_set_constant_work(g16_backend *b, int on);
 /* ProvingKey::load (formats/src/lib.rs:430-505).  check_points != 0 also runs
  * the on-curve check of every query point (load vs load_unchecked). */
 int g16_zkey_parse(const uint8_t *bytes, size_t len, int check_points, g16_zkey **out);
+/* A gnark v0.14 Groth16 BN254 key (crates/gnark/src/pk.rs, vk.rs): the proving
+ * key's WriteDump bytes and the verifying key's WriteTo / WriteRawTo bytes,
+ * checked against each other (alpha, beta, delta; one K point per public
+ * wire), every point on its curve, no BSB22 commitments.  The key gets the
+ * gnark H basis; its view serves g16_prepare like a .zkey's. */
+int g16_gnark_key_parse(const uint8_t *pk_dump, size_t pk_len, const uint8_t *vk, size_t vk_len, g16_zkey **out);
+/* A gnark witness dump (marker, then W, A.w and B.w as dumped Montgomery Fr
+ * slices; crates/gnark/src/witness.rs).  Pass NULL outputs to learn the
+ * counts: *n_w wires, *n_rows rows of A.w and of B.w. */
+int g16_gnark_witness_parse(const uint8_t *bytes, size_t len, uint8_t *w_mont, size_t w_cap, uint8_t *aw_mont,
+                            uint8_t *bw_mont, size_t rows_cap, size_t *n_w, size_t *n_rows);
 int g16_zkey_view_get(const g16_zkey *k, g16_zkey_view *out);
 void g16_zkey_free(g16_zkey *k);
 /* Witness::load (formats/src/wtns.rs:17-40): values out in Montgomery form.

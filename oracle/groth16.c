@@ -101,7 +101,7 @@ int groth16_compute_h(const zkey_t *k, const fp_t *w, fp_t *h) {
 }
 
 int groth16_msms(const zkey_t *k, const fp_t *w, const fp_t *h, msm_outputs_t *out) {
-    size_t nv = k->n_vars, n = k->domain_size;
+    size_t nv = k->n_vars, n = k->n_h ? k->n_h : k->domain_size;
     fp_t *ws = malloc(nv * sizeof(fp_t)), *hs = malloc(n * sizeof(fp_t));
     for (size_t i = 0; i < nv; i++) fp_from_mont(R, &ws[i], &w[i]);
     for (size_t i = 0; i < n; i++) fp_from_mont(R, &hs[i], &h[i]);
@@ -168,6 +168,33 @@ int groth16_prove(const zkey_t *k, const fp_t *w, const fp_t *r, const fp_t *s, 
     msm_outputs_t m;
     groth16_msms(k, w, h, &m);
     free(h);
+    groth16_assemble(k, &m, r, s, p);
+    return 0;
+}
+
+/* stages 1-11 from the caller's rows (h_and_msms_from_rows, cpu.rs:384-471): for a
+ * gnark key H goes to its bit-reversed coefficients, the MSM runs over the n - 1
+ * Z bases, and its result is multiplied by -1/2, which is 1/t on the odd coset */
+int groth16_prove_rows(const zkey_t *k, const fp_t *w, const fp_t *a_rows, const fp_t *b_rows, size_t n_rows,
+                       const fp_t *r, const fp_t *s, proof_t *p) {
+    fp_t *h = malloc((size_t)k->domain_size * sizeof(fp_t));
+    if (groth16_compute_h_from_rows(k, a_rows, b_rows, n_rows, h) != 0 ||
+        (k->h_basis == 1 && groth16_gnark_coefficients(k, h) != 0)) {
+        free(h);
+        return -1;
+    }
+    msm_outputs_t m;
+    groth16_msms(k, w, h, &m);
+    free(h);
+    if (k->h_basis == 1) {
+        fp_t two, half, neg, neg_std;
+        fp_from_u64(R, &two, 2);
+        fp_inv(R, &half, &two);
+        fp_neg(R, &neg, &half);
+        fp_from_mont(R, &neg_std, &neg);
+        g1j_t t = m.h_g1;
+        g1j_mul(&m.h_g1, &t, &neg_std);
+    }
     groth16_assemble(k, &m, r, s, p);
     return 0;
 }

@@ -45,6 +45,8 @@ typedef struct {
     size_t nnz[2];
     g1a_t *a_query, *b_g1_query, *l_query, *h_query;
     g2a_t *b_g2_query;
+    int h_basis;            /* 0 snarkjs odd coset (n_h = domain_size), 1 gnark bit-reversed (n_h = domain_size - 1) */
+    size_t n_h;             /* H bases */
 } zkey_t;
 
 int  zkey_parse(zkey_t *k, const uint8_t *bytes, size_t len, char *err, size_t errlen);
@@ -60,6 +62,15 @@ int  groth16_compute_h_from_rows(const zkey_t *k, const fp_t *a_rows, const fp_t
 int  groth16_msms(const zkey_t *k, const fp_t *w, const fp_t *h, msm_outputs_t *out);
 void groth16_assemble(const zkey_t *k, const msm_outputs_t *m, const fp_t *r, const fp_t *s, proof_t *p);
 int  groth16_prove(const zkey_t *k, const fp_t *w, const fp_t *r, const fp_t *s, proof_t *p);
+/* stages 1-11 from A.w and B.w rows (h_and_msms_from_rows, cpu.rs:384-471), either H basis */
+int  groth16_prove_rows(const zkey_t *k, const fp_t *w, const fp_t *a_rows, const fp_t *b_rows, size_t n_rows,
+                        const fp_t *r, const fp_t *s, proof_t *p);
+
+/* gnark v0.14 proving-key dump + verifying key -> key with the gnark H basis (gnark.c) */
+int  gnark_parse(zkey_t *k, const uint8_t *pk, size_t pk_len, const uint8_t *vk, size_t vk_len, char *err,
+                 size_t errlen);
+/* coset values of H -> gnark's bit-reversed coefficients; -1 if coefficient n-1 is not zero */
+int  groth16_gnark_coefficients(const zkey_t *k, fp_t *h);
 int  groth16_verify(const g1a_t *alpha, const g2a_t *beta, const g2a_t *gamma, const g2a_t *delta,
                     const g1a_t *ic, size_t n_ic, const fp_t *pub_mont, const proof_t *p);
 

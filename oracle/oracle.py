@@ -33,8 +33,7 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            build()
+        build()   # make rebuilds only when a source is newer than the library
         _lib = ctypes.CDLL(LIB_PATH)
         _lib.oracle_init()
         _lib.oracle_zkey_load.restype = ctypes.c_void_p
@@ -205,14 +204,58 @@ def msm_g2(bases, scalars_std):
 class Zkey:
     """A zkey parsed by the oracle's own reader (independent of the product's)."""
 
-    def __init__(self, data):
-        err = ctypes.create_string_buffer(256)
-        self._h = lib().oracle_zkey_load(bytes(data), len(data), err, 256)
-        if not self._h:
-            raise ValueError(err.value.decode())
+    def __init__(self, data, _handle=None):
+        if _handle is None:
+            err = ctypes.create_string_buffer(256)
+            _handle = lib().oracle_zkey_load(bytes(data), len(data), err, 256)
+            if not _handle:
+                raise ValueError(err.value.decode())
+        self._h = _handle
         info = (ctypes.c_uint32 * 3)()
         lib().oracle_zkey_info(ctypes.c_void_p(self._h), info)
         self.n_vars, self.n_public, self.domain_size = info[0], info[1], info[2]
+        self.gnark = bool(lib().oracle_zkey_h_basis(ctypes.c_void_p(self._h)))
+
+    @classmethod
+    def from_gnark(cls, pk_dump, vk):
+        """A gnark v0.14 proving-key dump and verifying key (the bit-reversed H basis)."""
+        err = ctypes.create_string_buffer(256)
+        L = lib()
+        L.oracle_gnark_load.restype = ctypes.c_void_p
+        h = L.oracle_gnark_load(bytes(pk_dump), ctypes.c_size_t(len(pk_dump)), bytes(vk), ctypes.c_size_t(len(vk)),
+                                err, 256)
+        if not h:
+            raise ValueError(err.value.decode())
+        return cls(None, _handle=h)
+
+    def query(self, which):
+        """A query packed: 'a', 'b1', 'b2', 'l' or 'h'."""
+        i = ["a", "b1", "b2", "l", "h"].index(which)
+        L = lib()
+        L.oracle_zkey_query.restype = ctypes.c_size_t
+        n = L.oracle_zkey_query(ctypes.c_void_p(self._h), i, None)
+        out = ctypes.create_string_buffer(n * (128 if which == "b2" else 64))
+        L.oracle_zkey_query(ctypes.c_void_p(self._h), i, out)
+        return out.raw
+
+    def vk_bytes(self):
+        """alpha_g1 | beta_g2 | gamma_g2 | delta_g2 | ic, packed."""
+        L = lib()
+        L.oracle_zkey_vk.restype = ctypes.c_size_t
+        n = L.oracle_zkey_vk(ctypes.c_void_p(self._h), None)
+        out = ctypes.create_string_buffer(n)
+        L.oracle_zkey_vk(ctypes.c_void_p(self._h), out)
+        return out.raw
+
+    def prove_rows(self, witness_mont, a_rows, b_rows, r_mont, s_mont):
+        """Stages 1-11 from A.w and B.w rows (either H basis)."""
+        out = ctypes.create_string_buffer(256)
+        rc = lib().oracle_prove_rows(ctypes.c_void_p(self._h), bytes(witness_mont),
+                                     ctypes.c_size_t(len(witness_mont) // 32), bytes(a_rows), bytes(b_rows),
+                                     ctypes.c_size_t(len(a_rows) // 32), to_bytes(r_mont), to_bytes(s_mont), out)
+        if rc != 0:
+            raise ValueError("prove_rows failed")
+        return out.raw
 
     def close(self):
         if self._h:
@@ -274,6 +317,24 @@ class Zkey:
         if rc < 0:
             raise ValueError("wrong public input count")
         return bool(rc)
+
+
+def gnark_witness(data):
+    """A gnark witness dump (marker, then W, A.w and B.w as u64 LE count + Montgomery Fr):
+    (w, a_rows, b_rows) as Montgomery bytes."""
+    if len(data) < 8 or data[:8] != (0xdeadbeef).to_bytes(8, "little"):
+        raise ValueError("not a gnark dump")
+    off, out = 8, []
+    for _ in range(3):
+        n = int.from_bytes(data[off:off + 8], "little")
+        off += 8
+        if off + 32 * n > len(data):
+            raise ValueError("truncated witness dump")
+        out.append(bytes(data[off:off + 32 * n]))
+        off += 32 * n
+    if off != len(data):
+        raise ValueError("trailing bytes")
+    return tuple(out)
 
 
 def verify_vk(alpha, beta, gamma, delta, ic, public_mont, proof):

@@ -230,6 +230,58 @@ static void pack_proof(uint8_t *out, const proof_t *p) {
     pack_g1(out + 192, &p->c);
 }
 
+void *oracle_gnark_load(const uint8_t *pk, size_t pk_len, const uint8_t *vk, size_t vk_len, char *err,
+                        size_t errlen) {
+    zkey_t *k = calloc(1, sizeof *k);
+    if (gnark_parse(k, pk, pk_len, vk, vk_len, err, errlen) != 0) {
+        free(k);
+        return NULL;
+    }
+    return k;
+}
+
+int oracle_zkey_h_basis(const void *kv) { return ((const zkey_t *)kv)->h_basis; }
+
+/* one query packed (0 A, 1 B1, 2 B2, 3 L, 4 H), returns its point count; out NULL sizes */
+size_t oracle_zkey_query(const void *kv, int which, uint8_t *out) {
+    const zkey_t *k = kv;
+    const size_t nv = k->n_vars, nl = nv - k->n_public - 1, nh = k->n_h ? k->n_h : k->domain_size;
+    const size_t n = which == 3 ? nl : which == 4 ? nh : nv;
+    if (out)
+        for (size_t i = 0; i < n; i++) {
+            if (which == 2) pack_g2(out + 128 * i, &k->b_g2_query[i]);
+            else pack_g1(out + 64 * i, which == 0 ? &k->a_query[i] : which == 1 ? &k->b_g1_query[i]
+                                       : which == 3 ? &k->l_query[i] : &k->h_query[i]);
+        }
+    return n;
+}
+
+/* alpha_g1 | beta_g2 | gamma_g2 | delta_g2 | ic..., packed */
+size_t oracle_zkey_vk(const void *kv, uint8_t *out) {
+    const zkey_t *k = kv;
+    if (out) {
+        pack_g1(out, &k->alpha_g1);
+        pack_g2(out + 64, &k->beta_g2);
+        pack_g2(out + 192, &k->gamma_g2);
+        pack_g2(out + 320, &k->delta_g2);
+        for (size_t i = 0; i < k->n_ic; i++) pack_g1(out + 448 + 64 * i, &k->ic[i]);
+    }
+    return 448 + 64 * k->n_ic;
+}
+
+int oracle_prove_rows(const void *kv, const uint8_t *w_mont, size_t n, const uint8_t *a_rows, const uint8_t *b_rows,
+                      size_t rows, const uint8_t *r_mont, const uint8_t *s_mont, uint8_t *proof_out) {
+    const zkey_t *k = kv;
+    if (n != k->n_vars) return -1;
+    fp_t r, s;
+    ld(&r, r_mont); ld(&s, s_mont);
+    proof_t p;
+    if (groth16_prove_rows(k, (const fp_t *)w_mont, (const fp_t *)a_rows, (const fp_t *)b_rows, rows, &r, &s, &p) != 0)
+        return -1;
+    pack_proof(proof_out, &p);
+    return 0;
+}
+
 int oracle_prove(const void *kv, const uint8_t *w_mont, size_t n, const uint8_t *r_mont,
                  const uint8_t *s_mont, uint8_t *proof_out) {
     const zkey_t *k = kv;

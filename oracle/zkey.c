@@ -120,6 +120,8 @@ int zkey_parse(zkey_t *k, const uint8_t *d, size_t len, char *err, size_t errlen
     k->b_g2_query = malloc(nv * sizeof(g2a_t));
     k->l_query = malloc((nl ? nl : 1) * sizeof(g1a_t));
     k->h_query = malloc((size_t)n * sizeof(g1a_t));
+    k->h_basis = 0;
+    k->n_h = n;
     for (size_t i = 0; i < nic; i++) if (!unpack_g1(&k->ic[i], d + s3->off + 64 * i)) FAIL("bad IC point");
     for (size_t i = 0; i < nv; i++) {
         if (!unpack_g1(&k->a_query[i], d + s5->off + 64 * i)) FAIL("bad A point");

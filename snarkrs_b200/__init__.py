@@ -228,7 +228,8 @@ class _ZkeyView(ctypes.Structure):
                 ("alpha_g1", P), ("beta_g1", P), ("beta_g2", P), ("gamma_g2", P), ("delta_g1", P), ("delta_g2", P),
                 ("ic", P), ("row_ptr", U * 2), ("signal", U * 2), ("value_id", U * 2), ("nnz", ctypes.c_uint32 * 2),
                 ("values", P), ("n_values", ctypes.c_uint32),
-                ("a_query", P), ("b_g1_query", P), ("b_g2_query", P), ("l_query", P), ("h_query", P)]
+                ("a_query", P), ("b_g1_query", P), ("b_g2_query", P), ("l_query", P), ("h_query", P),
+                ("h_basis", ctypes.c_uint32)]
 
 
 class _KeyPlan(ctypes.Structure):
@@ -255,6 +256,29 @@ class ProvingKey:
         check(lib().g16_zkey_parse(_buf(data), ctypes.c_size_t(_nbytes(data)), int(bool(check_points)),
                                    ctypes.byref(h)))
         return cls(h)
+
+    @classmethod
+    def from_gnark(cls, pk_dump, vk):
+        """A gnark v0.14 key: the proving key's WriteDump bytes and the verifying key's
+        WriteTo bytes (crates/gnark).  Proves only from A.w and B.w rows."""
+        h = ctypes.c_void_p()
+        check(lib().g16_gnark_key_parse(_buf(pk_dump), ctypes.c_size_t(_nbytes(pk_dump)), _buf(vk),
+                                        ctypes.c_size_t(_nbytes(vk)), ctypes.byref(h)))
+        return cls(h)
+
+    @property
+    def gnark(self):
+        """True for gnark's bit-reversed H basis (HBasis::GnarkBitReversed)."""
+        return self._view.h_basis == 1
+
+    def query_bytes(self, name):
+        """One of the five query sections as packed bytes (a_query, b_g1_query, b_g2_query,
+        l_query, h_query)."""
+        v = self._view
+        n = {"a_query": v.n_vars * 64, "b_g1_query": v.n_vars * 64, "b_g2_query": v.n_vars * 128,
+             "l_query": (v.n_vars - v.n_public - 1) * 64,
+             "h_query": (v.domain_size - (1 if v.h_basis == 1 else 0)) * 64}[name]
+        return ctypes.string_at(getattr(v, name), n)
 
     @classmethod
     def load(cls, path, check_points=True):
@@ -806,6 +830,20 @@ def launch_count():
     """Kernels this library has launched since it was loaded."""
     lib().g16_launch_count.restype = ctypes.c_uint64
     return lib().g16_launch_count()
+
+
+def gnark_witness(data):
+    """A gnark witness dump (W, A.w, B.w; crates/gnark/src/witness.rs) as three byte
+    strings of Montgomery Fr."""
+    n_w, n_rows = ctypes.c_size_t(), ctypes.c_size_t()
+    check(lib().g16_gnark_witness_parse(_buf(data), ctypes.c_size_t(_nbytes(data)), None, ctypes.c_size_t(0), None,
+                                        None, ctypes.c_size_t(0), ctypes.byref(n_w), ctypes.byref(n_rows)))
+    w = ctypes.create_string_buffer(32 * n_w.value)
+    aw = ctypes.create_string_buffer(32 * n_rows.value)
+    bw = ctypes.create_string_buffer(32 * n_rows.value)
+    check(lib().g16_gnark_witness_parse(_buf(data), ctypes.c_size_t(_nbytes(data)), w, n_w, aw, bw, n_rows, None,
+                                        None))
+    return w.raw, aw.raw, bw.raw
 
 
 FAULT_DEVICE, FAULT_STICKY = 1, 2

@@ -19,7 +19,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libg16b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["host_bn254.cpp", "formats.cpp", "synth.cpp", "msm.cu", "msm_noalloc.cu", "ntt.cu", "prover.cu", "batch.cu", "server.cpp", "pairing.cpp"]
+SOURCES = ["host_bn254.cpp", "formats.cpp", "gnark.cpp", "synth.cpp", "msm.cu", "msm_noalloc.cu", "ntt.cu", "prover.cu", "batch.cu", "server.cpp", "pairing.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
 # extra nvcc flags for experiments (e.g. -DACC_G2_MIN_BLOCKS=3); pass --force when they change

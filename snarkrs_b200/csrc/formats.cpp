@@ -271,6 +271,7 @@ void zkey_view(const ZkeyHost& k, g16_zkey_view& v) {
     v.b_g2_query = k.b_g2_query.data();
     v.l_query = k.l_query.data();
     v.h_query = k.h_query.data();
+    v.h_basis = k.h_basis;
 }
 
 int wtns_parse(const uint8_t* d, size_t len, std::vector<uint8_t>& out_mont) {

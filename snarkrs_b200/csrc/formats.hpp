@@ -16,9 +16,15 @@ struct ZkeyHost {
     std::vector<uint32_t> row_ptr[2], signal[2], value_id[2];
     std::vector<uint8_t> values;   // interned Fr, Montgomery, 32 bytes each
     std::vector<uint8_t> a_query, b_g1_query, b_g2_query, l_query, h_query;
+    uint32_t h_basis = 0;   // 0 snarkjs odd coset (domain_size H bases), 1 gnark bit-reversed (domain_size - 1)
 };
 
 int zkey_parse(const uint8_t* d, size_t len, bool check_points, ZkeyHost& k);
+// gnark v0.14 proving-key dump + verifying key (gnark.cpp): a key with the gnark
+// H basis and no constraint matrices
+int gnark_key_parse(const uint8_t* pk, size_t pk_len, const uint8_t* vk, size_t vk_len, ZkeyHost& k);
+// gnark witness dump: W, A.w, B.w (Montgomery Fr bytes)
+int gnark_witness_parse(const uint8_t* d, size_t len, std::vector<uint8_t> out[3]);
 void zkey_view(const ZkeyHost& k, g16_zkey_view& v);
 int wtns_parse(const uint8_t* d, size_t len, std::vector<uint8_t>& out_mont);
 std::vector<uint8_t> wtns_write(const uint8_t* w_mont, size_t n);

@@ -166,6 +166,28 @@ __device__ __forceinline__ void ntt_mid_tile(uint4* sm, uint4* data, uint32_t bx
     }
 }
 
+// DIF stages [0, k) with inverse twiddles on contiguous tiles of 2^k, then
+// each position p multiplied by table[p] and stored: the last step of an
+// inverse transform to bit-reversed order with a per-position scale (gnark's
+// H coefficients: table = shift^-bitrev(p) / n).
+__global__ void __launch_bounds__(256) k_ntt_dif_scale(uint4* data, uint32_t log_n, uint32_t k,
+                                                       const uint4* __restrict__ tw_inv,
+                                                       const uint4* __restrict__ table) {
+    extern __shared__ uint4 sm[];
+    const uint32_t tile = 1u << k;
+    const size_t base = (size_t)blockIdx.x << k;
+    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) {
+        sm[2 * e] = data[2 * (base + e)];
+        sm[2 * e + 1] = data[2 * (base + e) + 1];
+    }
+    __syncthreads();
+    for (int j = (int)k - 1; j >= 0; j--) {
+        run_stage<true>(sm, (uint32_t)j, 0, 0, 0, log_n, tile / 2, tw_inv);
+        __syncthreads();
+    }
+    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) st_g(data, base + e, mul(ld_s(sm, e), ld_g(table, base + e)));
+}
+
 __global__ void __launch_bounds__(256) k_ntt_mid(Vec3 vecs, uint32_t log_n, uint32_t k, const uint4* __restrict__ tw,
                                                  const uint4* __restrict__ tw_inv, const uint4* __restrict__ coset,
                                                  const uint4* __restrict__ join_a, const uint4* __restrict__ join_b,
@@ -279,7 +301,8 @@ void NttTables::release() {
     cudaFree(d_tw);
     cudaFree(d_tw_inv);
     cudaFree(d_coset);
-    d_tw = d_tw_inv = d_coset = nullptr;
+    cudaFree(d_coset_inv);
+    d_tw = d_tw_inv = d_coset = d_coset_inv = nullptr;
     log_n = -1;
 }
 
@@ -363,6 +386,7 @@ static void set_attrs() {
     cudaFuncSetAttribute(k_ntt_pass_multi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k_ntt_pass_multi<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k_ntt_mid_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_ntt_dif_scale, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attrs_done = true;
 }
 
@@ -462,6 +486,48 @@ static cudaError_t dit_natural(const NttTables& t, void* a, const void* tw, cons
         G16_CUDA(launch_pass(false, v, 1, log_n, outer[i], tw, i + 1 == outer.size() ? scale : nullptr, nullptr,
                              nullptr, nullptr, st));
     return cudaSuccess;
+}
+
+cudaError_t ntt_gnark_table(NttTables& t, cudaStream_t st) {
+    if (t.d_coset_inv) return cudaSuccess;
+    if (t.log_n < 1) {
+        set_error("gnark table before the domain tables");
+        return cudaErrorInvalidValue;
+    }
+    const size_t n = (size_t)1 << t.log_n;
+    G16_CUDA(g16::dev_malloc(&t.d_coset_inv, n * 32));
+    const g16::Fr shift_inv = g16::Fr::raw(t.shift).inv(), ninv = g16::Fr::raw(t.n_inv);
+    {
+        TimedLaunch tl("ntt_tables", st);
+        k_powers<<<blocks_for((n + 15) / 16, 128), 128, 0, st>>>((uint4*)t.d_coset_inv, to_dev(shift_inv), to_dev(ninv),
+                                                                  n, (uint32_t)t.log_n);
+    }
+    G16_CUDA(cudaGetLastError());
+    return cudaStreamSynchronize(st);
+}
+
+cudaError_t ntt_to_gnark_coefficients(const NttTables& t, void* h, cudaStream_t st) {
+    if (!t.d_coset_inv) {
+        set_error("gnark coefficients without the inverse coset table");
+        return cudaErrorInvalidValue;
+    }
+    set_attrs();
+    const uint32_t log_n = (uint32_t)t.log_n;
+    const uint32_t k0 = inner_k(t.tiling, log_n);
+    auto outer = outer_passes(t.tiling, log_n, k0);
+    Vec3 v = {{(uint4*)h, nullptr, nullptr}};
+    for (size_t i = outer.size(); i-- > 0;)   // inverse, DIF, top stages first
+        G16_CUDA(launch_pass(true, v, 1, log_n, outer[i], t.d_tw_inv, nullptr, nullptr, nullptr, nullptr, st));
+    const uint32_t tile = 1u << k0;
+    const size_t n = (size_t)1 << log_n;
+    const unsigned threads = tile / 2 < 256 ? tile / 2 : 256;
+    timer().add_units("ntt_pass_dif", (double)(n / 2) * k0 + (double)n);
+    timer().add_bytes("ntt_pass_dif", 64.0 * n);
+    TimedLaunch tl("ntt_pass_dif", st);
+    k_ntt_dif_scale<<<(unsigned)(n / tile), threads, (size_t)tile * 32, st>>>((uint4*)h, log_n, k0,
+                                                                            (const uint4*)t.d_tw_inv,
+                                                                            (const uint4*)t.d_coset_inv);
+    return cudaGetLastError();
 }
 
 cudaError_t ntt_forward(const NttTables& t, void* a, cudaStream_t st) { return dit_natural(t, a, t.d_tw, nullptr, st); }

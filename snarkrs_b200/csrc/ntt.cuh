@@ -42,6 +42,7 @@ struct NttTables {
     void* d_tw = nullptr;       // omega^i, i < n/2 (Montgomery Fr)
     void* d_tw_inv = nullptr;   // omega^-i, i < n/2
     void* d_coset = nullptr;    // shift^bitrev(p) / n, p < n (the proving coset shift omega_2n)
+    void* d_coset_inv = nullptr;   // shift^-bitrev(p) / n, for gnark keys only (ntt_gnark_table)
     uint64_t n_inv[4];          // 1/n, Montgomery
     uint64_t shift[4];          // omega_2n, Montgomery
     void release();
@@ -54,6 +55,14 @@ cudaError_t ntt_tables(NttTables& t, int log_n, cudaStream_t st);
 // iNTT -> * shift^i/n -> NTT (natural order in and out, in place) and
 // h = A*B - C is written to h (may alias none of A, B, C).
 cudaError_t ntt_h_pipeline(const NttTables& t, void* a, void* b, void* c, void* h, cudaStream_t st);
+
+// For a gnark key: the table shift^-bitrev(p) / n (built once), and H's values
+// on the odd coset -> H's coefficients, times -2, in bit-reversed order: the
+// inverse transform to bit-reversed order, then position p times
+// shift^-bitrev(p) / n (intt_to_bitrev + coset_scale_bitrev,
+// crates/groth16/src/cpu.rs:265-286).  In place on 2^log_n Fr.
+cudaError_t ntt_gnark_table(NttTables& t, cudaStream_t st);
+cudaError_t ntt_to_gnark_coefficients(const NttTables& t, void* h, cudaStream_t st);
 
 // One vector through the same chain (the reference's intt_coset_ntt).
 cudaError_t ntt_intt_coset_ntt(const NttTables& t, void* a, cudaStream_t st);

@@ -336,7 +336,7 @@ int build_h_table(g16_circuit* c, int ch, cudaStream_t st) {
         c->c_h = ch;
         return G16_OK;
     }
-    const uint64_t n = c->n, W = (uint64_t)msm_windows(ch);
+    const uint64_t n = c->h_count, W = (uint64_t)msm_windows(ch);
     if (n * W >= 0x80000000ull) return fail(G16_ERR_BACKEND, "domain too large for 31-bit MSM entry indices");
     void* th = nullptr;
     cudaError_t e = circuit_alloc(c, &th, 64 * n * W);
@@ -566,11 +566,11 @@ int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
 int enqueue_h_msm(g16_circuit* c, Workspace* ws, const void* d_h) {
     const size_t WIN_SLOT = ws->win_slot;
     cudaStream_t st = ws->stream;
-    const uint32_t nh = c->n * (c->tables ? (uint32_t)msm_windows(c->c_h) : 1u);
+    const uint32_t nh = c->h_count * (c->tables ? (uint32_t)msm_windows(c->c_h) : 1u);
     // the H reduction runs last on the main stream, mostly alone: shorter chains pay
     // (2^21 prove +0.5%, 2^18 +1.5%, 2^20 +1.3% against the 8192-piece default)
     ws->sort_h.reduce_pieces = MSM_REDUCE_PIECES_ALONE;
-    CK(msm_sort(ws->sort_h, d_h, c->n, true, c->c_h, st, c->tables, c->be->constant_work), "H sort");
+    CK(msm_sort(ws->sort_h, d_h, c->h_count, true, c->c_h, st, c->tables, c->be->constant_work), "H sort");
     CK(msm_accumulate_g1(ws->sort_h, ws->acc[4], c->tables ? c->t_h : c->d_h, 0, nh, st), "H accumulate");
     const size_t bytes = ws->acc[4].result_bytes(XYZZ_G1_BYTES);
     if (bytes > WIN_SLOT) return fail(G16_ERR_BACKEND, "MSM result of %zu bytes exceeds its slot", bytes);
@@ -712,10 +712,36 @@ int run_rows_proof(g16_circuit* c, Workspace* ws, const void* d_w, const uint8_t
     CK(cudaGetLastError(), "rows launch");
     CK(stage_event(ws->ev[1], st), "event");
     CK(ntt_h_pipeline(c->ntt, abc, abc + vb, abc + 2 * vb, ws->d_hpoly, st), "NTT pipeline");
+    if (c->rows_only) {
+        // gnark's basis: H's coefficients (times -2) in bit-reversed order; the
+        // last one, coefficient n - 1, comes back to be checked for zero
+        CK(ntt_to_gnark_coefficients(c->ntt, ws->d_hpoly, st), "gnark coefficients");
+        CK(cudaMemcpyAsync(ws->h_work + 8, (const uint8_t*)ws->d_hpoly + 32ull * (c->n - 1), 32,
+                           cudaMemcpyDeviceToHost, st),
+           "coefficient readback");
+    }
     CK(stage_event(ws->ev[2], st), "event");
     if ((rc = enqueue_h_msm(c, ws, ws->d_hpoly)) || (rc = enqueue_join(ws))) return rc;
     if ((rc = collect_msms(c, ws, out))) return rc;
+    if (c->rows_only) {
+        // A B - C vanishes on the domain and has degree at most 2n - 2, so its
+        // quotient by t has degree at most n - 2 (to_gnark_coefficients,
+        // crates/groth16/src/cpu.rs:265-286)
+        if (ws->h_work[8] | ws->h_work[9] | ws->h_work[10] | ws->h_work[11])
+            return fail(G16_ERR_BACKEND, "H has a nonzero coefficient %u, so the quotient by the vanishing polynomial "
+                                         "is not exact", c->n - 1);
+        // gnark's Z bases carry t(tau) / delta; on the odd coset t = -2
+        out.h = g1_mul(out.h, -g16::Fr::from_u64(2).inv());
+    }
     ws->proofs++;
+    return G16_OK;
+}
+
+// The gather-path entry points need the constraint matrices a gnark key lacks.
+int gather_ok(const g16_circuit* c) {
+    if (c->rows_only)
+        return fail(G16_ERR_BACKEND, "this key has no constraint matrices (a gnark key): it proves only from A.w and "
+                                     "B.w rows (g16_prove_with_blinders_from_rows)");
     return G16_OK;
 }
 
@@ -1120,6 +1146,36 @@ int g16_zkey_parse(const uint8_t* bytes, size_t len, int check_points, g16_zkey*
     return G16_OK;
 }
 
+int g16_gnark_key_parse(const uint8_t* pk, size_t pk_len, const uint8_t* vk, size_t vk_len, g16_zkey** out) {
+    if (!pk || !vk || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    auto z = std::make_unique<g16_zkey>();
+    int rc = gnark_key_parse(pk, pk_len, vk, vk_len, z->k);
+    if (rc != G16_OK) return rc;
+    *out = z.release();
+    return G16_OK;
+}
+
+int g16_gnark_witness_parse(const uint8_t* bytes, size_t len, uint8_t* w, size_t w_cap, uint8_t* aw, uint8_t* bw,
+                            size_t rows_cap, size_t* n_w, size_t* n_rows) {
+    if (!bytes) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    std::vector<uint8_t> parts[3];
+    int rc = gnark_witness_parse(bytes, len, parts);
+    if (rc != G16_OK) return rc;
+    const size_t nw = parts[0].size() / 32, nr = parts[1].size() / 32;
+    if (n_w) *n_w = nw;
+    if (n_rows) *n_rows = nr;
+    if (w) {
+        if (w_cap < nw) return fail(G16_ERR_INVALID_ARGUMENT, "witness buffer holds %zu of %zu values", w_cap, nw);
+        std::memcpy(w, parts[0].data(), parts[0].size());
+    }
+    if (aw || bw) {
+        if (!aw || !bw || rows_cap < nr) return fail(G16_ERR_INVALID_ARGUMENT, "row buffers hold %zu of %zu rows", rows_cap, nr);
+        std::memcpy(aw, parts[1].data(), parts[1].size());
+        std::memcpy(bw, parts[2].data(), parts[2].size());
+    }
+    return G16_OK;
+}
+
 int g16_zkey_view_get(const g16_zkey* k, g16_zkey_view* out) {
     if (!k || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     zkey_view(k->k, *out);
@@ -1160,8 +1216,11 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
     if (n < 2 || (n & (n - 1)) || n > (1u << 27)) return fail(G16_ERR_BACKEND, "domain size %u is not a power of two in [2, 2^27]", n);
     if ((uint64_t)k->n_public + 1 > k->n_vars) return fail(G16_ERR_BACKEND, "n_public %u exceeds n_vars %u", k->n_public, k->n_vars);
     if (k->n_vars >= 0x80000000u || n >= 0x80000000u) return fail(G16_ERR_BACKEND, "more than 2^31 wires");
+    if (k->h_basis > G16_H_GNARK) return fail(G16_ERR_BACKEND, "unknown H basis %u", k->h_basis);
+    // a gnark key has no constraint matrices: it proves only from A.w and B.w rows
+    const bool gnark = k->h_basis == G16_H_GNARK;
     // CSR structure (Coefficients::check_structure, formats/src/lib.rs:185-270)
-    for (int m = 0; m < 2; m++) {
+    for (int m = 0; m < 2 && !gnark; m++) {
         const uint32_t* rp = k->row_ptr[m];
         if (!rp || rp[0] != 0 || rp[n] != k->nnz[m]) return fail(G16_ERR_BACKEND, "matrix %d row_ptr is malformed", m);
         for (uint32_t i = 0; i < n; i++)
@@ -1193,6 +1252,8 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
     c->n = n;
     c->tables = plan.window_tables != 0;
     c->ws_estimate = plan.workspace_bytes;
+    c->rows_only = gnark;
+    c->h_count = gnark ? n - 1 : n;
     for (int j = 0; j < 3; j++) c->rows[j] = live.rows[j];
     if (const char* g = std::getenv("G16_CUDA_GRAPHS")) c->graphs = std::strcmp(g, "0") != 0;
     while ((1u << c->log_n) < n) c->log_n++;
@@ -1213,13 +1274,13 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
         const void* src;
         size_t bytes;
     } ups[] = {
-        {(void**)&c->d_rp[0], k->row_ptr[0], 4ull * (n + 1)},
-        {(void**)&c->d_rp[1], k->row_ptr[1], 4ull * (n + 1)},
-        {(void**)&c->d_sig[0], k->signal[0], 4ull * k->nnz[0]},
-        {(void**)&c->d_sig[1], k->signal[1], 4ull * k->nnz[1]},
-        {(void**)&c->d_vid[0], k->value_id[0], 4ull * k->nnz[0]},
-        {(void**)&c->d_vid[1], k->value_id[1], 4ull * k->nnz[1]},
-        {&c->d_values, k->values, 32ull * k->n_values},
+        {(void**)&c->d_rp[0], k->row_ptr[0], gnark ? 0 : 4ull * (n + 1)},
+        {(void**)&c->d_rp[1], k->row_ptr[1], gnark ? 0 : 4ull * (n + 1)},
+        {(void**)&c->d_sig[0], k->signal[0], gnark ? 0 : 4ull * k->nnz[0]},
+        {(void**)&c->d_sig[1], k->signal[1], gnark ? 0 : 4ull * k->nnz[1]},
+        {(void**)&c->d_vid[0], k->value_id[0], gnark ? 0 : 4ull * k->nnz[0]},
+        {(void**)&c->d_vid[1], k->value_id[1], gnark ? 0 : 4ull * k->nnz[1]},
+        {&c->d_values, k->values, gnark ? 0 : 32ull * k->n_values},
         {&c->d_a, live.a.data(), live.a.size()},
         {&c->d_b1, live.b1.data(), live.b1.size()},
         {&c->d_b2, live.b2.data(), live.b2.size()},
@@ -1227,7 +1288,7 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
         {(void**)&c->d_rank[0], live.rank[0].data(), 4ull * nv},
         {(void**)&c->d_rank[1], live.rank[1].data(), 4ull * nv},
         {(void**)&c->d_rank[2], live.rank[2].data(), 4ull * nv},
-        {&c->d_h, k->h_query, 64ull * n},
+        {&c->d_h, k->h_query, 64ull * (gnark ? n - 1 : n)},
     };
     g16_circuit* cp = c.get();
     cudaStream_t st = b->stream;
@@ -1243,6 +1304,7 @@ int g16_prepare(g16_backend* b, const g16_zkey_view* k, g16_circuit** out) {
         }
     }
     cudaError_t e = ntt_tables(cp->ntt, cp->log_n, st);
+    if (e == cudaSuccess && gnark) e = ntt_gnark_table(cp->ntt, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         int rc = cuda_fail(e, "prepare");
@@ -1293,6 +1355,7 @@ int g16_compute_h(g16_circuit* c, const uint8_t* w, size_t n, g16_hpoly** out) {
     if (!c || !w || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
+    if (int rc_g = gather_ok(c)) return rc_g;
     if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     WsGuard g(c);
@@ -1331,6 +1394,7 @@ int g16_msms(g16_circuit* c, const uint8_t* w, size_t n, const g16_hpoly* h, g16
     if (h->owner != c) return fail(G16_ERR_BACKEND, "H handle was computed by another circuit");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
+    if (int rc_g = gather_ok(c)) return rc_g;
     if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     WsGuard g(c);
@@ -1350,6 +1414,7 @@ int g16_h_and_msms(g16_circuit* c, const uint8_t* w, size_t n, g16_msm_outputs* 
     if (!c || !w || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
+    if (int rc_g = gather_ok(c)) return rc_g;
     if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     WsGuard g(c);
@@ -1412,6 +1477,7 @@ int g16_prove_with_blinders(g16_circuit* c, const uint8_t* w, size_t n, const ui
     if (!c || !w || !r || !s || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
+    if (int rc_g = gather_ok(c)) return rc_g;
     if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     WsGuard g(c);
@@ -1425,6 +1491,7 @@ int g16_prove_with_blinders_device(g16_circuit* c, const void* d_w, size_t n, co
     if (!c || !d_w || !r || !s || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
     int rc = check_witness(c, n, nullptr);
     if (rc) return rc;
+    if (int rc_g = gather_ok(c)) return rc_g;
     if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     WsGuard g(c);
@@ -1558,6 +1625,7 @@ int g16_prove_batch_timed(g16_backend* b, size_t count, g16_circuit* const* circ
     for (size_t i = 0; i < count; i++) {
         if (!circuits[i] || !witnesses[i]) return fail(G16_ERR_INVALID_ARGUMENT, "null job %zu", i);
         if (circuits[i]->be != b) return fail(G16_ERR_INVALID_ARGUMENT, "job %zu belongs to another backend", i);
+        if (int rc_g = gather_ok(circuits[i])) return rc_g;
         int rc = check_witness(circuits[i], lens[i], witnesses[i]);
         if (rc) return rc;
     }
@@ -1800,6 +1868,7 @@ int g16_autotune(g16_circuit* c, const uint8_t* w, size_t n, int concurrency, g1
     if (concurrency < 1 || concurrency > 8) return fail(G16_ERR_INVALID_ARGUMENT, "concurrency must be 1..8");
     int rc = check_witness(c, n, w);
     if (rc) return rc;
+    if (int rc_g = gather_ok(c)) return rc_g;
     if (int rc_dev = device_usable(c->be)) return rc_dev;
     CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
     TuningLock lock(c);

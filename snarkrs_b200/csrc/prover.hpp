@@ -72,7 +72,7 @@ struct Workspace {
         if (e == cudaSuccess) e = g16::dev_malloc(&d_abc, 32ull * n * 3);
         if (e == cudaSuccess) e = g16::dev_malloc(&d_hpoly, 32ull * n);
         if (e == cudaSuccess) e = cudaMallocHost((void**)&h_win, 5 * slot);
-        if (e == cudaSuccess) e = cudaMallocHost((void**)&h_work, 8 * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMallocHost((void**)&h_work, 16 * sizeof(unsigned long long));
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
         for (auto& x : side)
             if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
@@ -127,6 +127,10 @@ struct g16_circuit {
     // set; false (compact key, about a tenth of the memory): they read the plain
     // bases with one bucket set per window and a Horner step on the host
     bool tables = true;
+    // a gnark key: no constraint matrices (proves only from A.w and B.w rows),
+    // H taken as gnark's bit-reversed coefficients over h_count = n - 1 bases
+    bool rows_only = false;
+    uint32_t h_count = 0;   // H MSM length: n, or n - 1 for a gnark key
     g16::NttTables ntt;
     g16::G1A alpha1, beta1, delta1;
     g16::G2A beta2, delta2, gamma2;

@@ -13,6 +13,10 @@ argument or in ``G16_REFERENCE`` (there is no default), and writes:
 * ``gnark_toy.json`` -- the committed gnark v0.14 toy fixture
   (test-support/gnark/toy/{vk.bin,proof.bin,public.bin}) as hex: a real
   gnark-produced Groth16 proof that an independent pairing must accept.
+* ``gnark_toy_pk.dump.gz`` and ``gnark_toy_witness.bin.gz`` -- the same
+  fixture's proving-key dump (``ProvingKey.WriteDump``) and witness dump (W,
+  A.w and B.w), gzip-compressed byte for byte: the gnark key the rows path
+  proves with, under gnark's bit-reversed H basis.
 
 Run: ``python tests/golden/make_golden.py <reference checkout>``.
 """
@@ -78,7 +82,13 @@ def main():
     with open(os.path.join(HERE, "gnark_toy.json"), "w") as f:
         json.dump(toy, f, indent=1)
         f.write("\n")
-    print("wrote reference_constants.json and gnark_toy.json", file=sys.stderr)
+    import gzip
+    for name, out in (("pk.dump", "gnark_toy_pk.dump.gz"), ("witness.bin", "gnark_toy_witness.bin.gz")):
+        with open(os.path.join(REF, "test-support/gnark/toy", name), "rb") as f:
+            data = f.read()
+        with gzip.GzipFile(os.path.join(HERE, out), "wb", mtime=0) as g:
+            g.write(data)
+    print("wrote reference_constants.json, gnark_toy.json and the gnark toy dumps", file=sys.stderr)
 
 
 if __name__ == "__main__":
