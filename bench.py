@@ -925,7 +925,7 @@ def run_serve(args, backend=None, emit=True, fracs=(0.5, 0.9, 1.5), n_req=None):
             srv.wait(tk)
         reqs = arrivals(rate, n_req, seed)
         tickets = []
-        bs0, allocs0 = backend.batch_stats(), S.device_alloc_count()
+        bs0, allocs0, ss0 = backend.batch_stats(), S.device_alloc_count(), srv.stats()
         t0, tickets = play(srv, reqs, 10_000)
         lat, proofs = [], {}
         for tk, i, j in tickets:
@@ -934,6 +934,8 @@ def run_serve(args, backend=None, emit=True, fracs=(0.5, 0.9, 1.5), n_req=None):
             proofs[j] = p
         t_end = time.perf_counter()
         stats = srv.stats()
+        for key in ("batches", "batched", "alone", "submitted", "completed"):   # the timed pass alone
+            stats[key] -= ss0[key]
         bs1 = backend.batch_stats()
         stats["engine"] = {k: bs1[k] - bs0[k] for k in bs1}
         stats["device_allocs_in_timed_region"] = S.device_alloc_count() - allocs0
