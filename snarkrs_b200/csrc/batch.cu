@@ -415,6 +415,17 @@ int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, con
                        const size_t* lens, const uint8_t* r, const uint8_t* s, g16_proof* out, double* done_ms) {
     const auto t_start = std::chrono::steady_clock::now();
     if (!count) return G16_OK;
+    // the blinders first: nothing below may return before the device work it
+    // enqueued has finished
+    std::vector<Fr> rr(count), ss(count);
+    for (size_t j = 0; j < count; j++) {
+        uint64_t a[4], c[4];
+        std::memcpy(a, r + 32 * j, 32);
+        std::memcpy(c, s + 32 * j, 32);
+        if (!Fr::canonical(a) || !Fr::canonical(c)) return fail(G16_ERR_INVALID_ARGUMENT, "job %zu: r or s not below r", j);
+        rr[j] = Fr::raw(a);
+        ss[j] = Fr::raw(c);
+    }
     // an idle engine, preferably one whose layout (and graph) is this mix's
     std::vector<BatchKey> want;
     for (size_t j = 0; j < count; j++) want.push_back(key_of(cs[j]));
@@ -498,15 +509,6 @@ int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, con
     CK_BATCH(cudaMemcpyAsync(E.d_arena, E.h_stage, E.w_bytes, cudaMemcpyHostToDevice, E.st[0]));
     // the key-only blinder products on the host while the device runs
     std::vector<BlinderTerms> terms(count);
-    std::vector<Fr> rr(count), ss(count);
-    for (size_t j = 0; j < count; j++) {
-        uint64_t a[4], c[4];
-        std::memcpy(a, r + 32 * j, 32);
-        std::memcpy(c, s + 32 * j, 32);
-        if (!Fr::canonical(a) || !Fr::canonical(c)) return fail(G16_ERR_INVALID_ARGUMENT, "job %zu: r or s not below r", j);
-        rr[j] = Fr::raw(a);
-        ss[j] = Fr::raw(c);
-    }
     std::thread blinders([&] { parallel_for(count, threads, [&](size_t j) { terms[j] = blinder_terms(cs[j], rr[j], ss[j]); }); });
     int rc = G16_OK;
     const bool use_graph = !timer().enabled && E.runs > 0;
@@ -545,7 +547,15 @@ int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, con
         if (e != cudaSuccess) rc = cuda_fail(e, "batched proving");
     }
     blinders.join();
-    if (rc != G16_OK) return rc;
+    if (rc != G16_OK) {
+        // a partly enqueued submission may still run on any of the three
+        // streams: let it finish before the engine is handed out again, and
+        // forget the layout (its graph may be half-built)
+        for (cudaStream_t st : E.st)
+            if (st) cudaStreamSynchronize(st);
+        E.drop_layout();
+        return rc;
+    }
     timer().collect();
     E.runs++;
     // stage 11 for every job
