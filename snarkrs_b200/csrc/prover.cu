@@ -401,12 +401,19 @@ void release(g16_circuit* c, Workspace* ws) {
     c->cv.notify_one();
 }
 
+// Returns the workspace to its circuit's pool once every stream of it is idle:
+// a call that failed after enqueueing may have left work running on a side
+// stream, and the next proof on the workspace may reallocate its scratch (on a
+// success the streams are idle already and the waits return at once).
 struct WsGuard {
     g16_circuit* c;
     Workspace* ws = nullptr;
     explicit WsGuard(g16_circuit* cc) : c(cc) {}
     ~WsGuard() {
-        if (ws) release(c, ws);
+        if (!ws) return;
+        for (cudaStream_t s : {ws->stream, ws->side[0], ws->side[1], ws->side[2], ws->side[3]})
+            if (s) cudaStreamSynchronize(s);
+        release(c, ws);
     }
 };
 
