@@ -566,12 +566,14 @@ def run_ours(args):
         except Exception as e:   # the plain-prove line above stands on its own
             line["batched"] = {"error": repr(e)[:300]}
         try:
-            v = run_serve(args, backend, emit=False, fracs=(1.5,), n_req=160)
+            v = run_serve(args, backend, emit=False, fracs=(1.5,), n_req=300)
             top = v["sweep"][-1]
             line["served"] = {"workload": v["config"]["workload"], "offered_fraction_of_plain_capacity": 1.5,
+                              "requests": top["served"]["requests"],
                               "value": top["served"]["throughput"], "unit": "proofs/s",
                               "p50_ms": top["served"]["p50_ms"], "p99_ms": top["served"]["p99_ms"],
                               "plain_fifo": {k: top["plain_fifo"][k] for k in ("throughput", "p50_ms", "p99_ms")},
+                              "stats": top["served"]["stats"],
                               "results_identical_alone_and_in_mix": v["results_identical_alone_and_in_mix"]}
         except Exception as e:
             line["served"] = {"error": repr(e)[:300]}
