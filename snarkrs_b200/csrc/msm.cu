@@ -1384,6 +1384,23 @@ cudaError_t msm_sort_sets(MsmSort* sorts, const MsmLiveSets& sets, const void* d
     return cudaSuccess;
 }
 
+// The pieces kernels keep two points per thread in shared memory: above 48 KB a
+// block needs the opt-in limit (blocks of 2^8 threads).
+static void reduce_attrs() {
+    static const bool done = [] {
+        const int g1 = 2 * (1 << MSM_REDUCE_LB_G1) * (int)XYZZ_G1_BYTES;
+        const int g2 = 2 * (1 << MSM_REDUCE_LB_G2) * (int)XYZZ_G2_BYTES;
+        cudaFuncSetAttribute(k_reduce_pieces<g16d::Fq, MSM_REDUCE_LB_G1>, cudaFuncAttributeMaxDynamicSharedMemorySize, g1);
+        cudaFuncSetAttribute(k_reduce_pieces_multi<g16d::Fq, MSM_REDUCE_LB_G1>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, g1);
+        cudaFuncSetAttribute(k_reduce_pieces<g16d::Fq2, MSM_REDUCE_LB_G2>, cudaFuncAttributeMaxDynamicSharedMemorySize, g2);
+        cudaFuncSetAttribute(k_reduce_pieces_multi<g16d::Fq2, MSM_REDUCE_LB_G2>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, g2);
+        return true;
+    }();
+    (void)done;
+}
+
 template <class F>
 static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bases, uint32_t base_offset,
                               uint32_t n_bases, cudaStream_t st, size_t xyzz_bytes, const char* tag) {
@@ -1392,9 +1409,11 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     size_t max_partials = (size_t)s.Ks + chunks + 1;
     G16_CUDA(grow_bytes(acc.d_partials, acc.cap_partials, max_partials * xyzz_bytes, acc.fixed));
     const uint32_t Wr = s.shared ? 1u : (uint32_t)s.W;   // bucket sets to reduce
-    constexpr int LB = std::is_same<F, g16d::Fq>::value ? 7 : 6;   // pieces per reduction block: 2^LB
+    constexpr bool G2 = !std::is_same<F, g16d::Fq>::value;
+    constexpr int LB = G2 ? MSM_REDUCE_LB_G2 : MSM_REDUCE_LB_G1;   // pieces per reduction block: 2^LB
+    reduce_attrs();
     const MsmReducePlan plan =
-        msm_reduce_plan(Wr, s.B, LB == 6, s.reduce_pieces ? s.reduce_pieces : msm_reduce_pieces(s.shared));
+        msm_reduce_plan(Wr, s.B, G2, s.reduce_pieces ? s.reduce_pieces : msm_reduce_pieces(s.shared));
     acc.plan = plan;
     G16_CUDA(grow_bytes(acc.d_buckets, acc.cap_buckets, (size_t)s.K * xyzz_bytes, acc.fixed));
     if (!plan.direct)
@@ -1511,15 +1530,16 @@ cudaError_t msm_batch_setup(MsmSources& so, MsmSpace* const* spaces, int nspaces
     }
     for (int i = 0; i < nspaces; i++) {
         MsmSpace& sp = *spaces[i];
-        const uint32_t LB = sp.g2 ? 6 : 7;
+        const uint32_t LB = sp.g2 ? MSM_REDUCE_LB_G2 : MSM_REDUCE_LB_G1;   // as space_accumulate's kernels
         const size_t pb = sp.g2 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES;
         uint64_t K = 0, blocks = 0, out_block = 0, out_set = 0;
         sp.max_hb = 0;
         for (auto& g : sp.segs) K += g.B;
         // one piece length for the space: its pieces about fill the device
-        // (two reduction blocks of 2^LB threads per SM), runs of at most 32
+        // (two reduction blocks of 2^LB threads per SM, and at most the 256 threads
+        // of ~250 registers an SM holds), runs of at most 32
         uint32_t piece_len = 1;
-        const uint64_t fill = (uint64_t)device_sms() * 2 * (1u << LB);
+        const uint64_t fill = (uint64_t)device_sms() * std::min<uint64_t>(2ull << LB, 256);
         while (piece_len < MSM_REDUCE_MAX_SEG && K / piece_len > fill) piece_len *= 2;
         if (const char* e = std::getenv("G16_BATCH_PIECE_LEN")) {   // tuning knob: 1, 2, 4, ..., 32
             const int v = std::atoi(e);
@@ -1540,7 +1560,7 @@ cudaError_t msm_batch_setup(MsmSources& so, MsmSpace* const* spaces, int nspaces
             red.push_back({g.key_start, g.B, g.plan.seg, g.plan.nb, g.plan.hb, g.block_start, g.out_block, g.out_set});
             K += g.B;
             blocks += g.plan.nb;
-            out_block += (uint64_t)g.plan.nb * (LB + 2);
+            out_block += (uint64_t)g.plan.nb * g.plan.block_terms();
             out_set += g.plan.set_terms();
             sp.max_hb = std::max(sp.max_hb, g.plan.hb);
         }
@@ -1668,6 +1688,12 @@ static cudaError_t space_accumulate(MsmSpace& sp, cudaStream_t st, size_t xyzz_b
     G16_CUDA(cudaMemsetAsync(a.d_work, 0, sizeof(unsigned long long), st));
     uint4* partials = (uint4*)a.d_partials;
     const uint32_t nsegs = (uint32_t)sp.segs.size();
+    // the blocks' output was laid out from the plans: they must use this LB
+    for (const auto& g : sp.segs)
+        if (g.plan.lb != (uint32_t)LB) {
+            set_error("batched MSM reduction planned with 2^%u pieces per block, launched with 2^%d", g.plan.lb, LB);
+            return cudaErrorInvalidValue;
+        }
     if (chunks) {
         TimedLaunch tl(tag, st);
         if (std::is_same<F, g16d::Fq>::value)
@@ -1712,8 +1738,9 @@ static cudaError_t space_accumulate(MsmSpace& sp, cudaStream_t st, size_t xyzz_b
 }
 
 cudaError_t msm_space_accumulate(MsmSpace& sp, cudaStream_t st) {
-    if (sp.g2) return space_accumulate<g16d::Fq2, 6>(sp, st, XYZZ_G2_BYTES, "msm_accumulate_g2");
-    return space_accumulate<g16d::Fq, 7>(sp, st, XYZZ_G1_BYTES, "msm_accumulate_g1");
+    reduce_attrs();
+    if (sp.g2) return space_accumulate<g16d::Fq2, MSM_REDUCE_LB_G2>(sp, st, XYZZ_G2_BYTES, "msm_accumulate_g2");
+    return space_accumulate<g16d::Fq, MSM_REDUCE_LB_G1>(sp, st, XYZZ_G1_BYTES, "msm_accumulate_g1");
 }
 
 // ---- host: window sums -> Horner ----

@@ -40,9 +40,9 @@ namespace g16 {
 
 // Bucket reduction plan for `sets` bucket sets of B buckets each (B a power of
 // two).  A set's sum is sum_b (b + 1) S_b.  Its buckets are cut into pieces of
-// seg buckets (one thread's running sums), 2^lb pieces per block (lb = 7 for
-// G1, 6 for G2, so that a block's two shared-memory point arrays fit in 32 KiB),
-// nb = 2^hb blocks per set.  Each block leaves lb + 2 points, T, G_0 .. G_(lb-1)
+// seg buckets (one thread's running sums), 2^lb pieces per block (lb =
+// MSM_REDUCE_LB_G1 or _G2 below; a block keeps two arrays of 2^lb points in
+// shared memory), nb = 2^hb blocks per set.  Each block leaves lb + 2 points, T, G_0 .. G_(lb-1)
 // and its run total R; with more than two blocks in all, a second kernel sums
 // them per set into lb + 1 + hb points, T, G_0 .. G_(lb-1), Gb_0 .. Gb_(hb-1),
 // and the host forms
@@ -63,8 +63,27 @@ constexpr uint64_t msm_reduce_pieces(bool shared_windows) {
     return shared_windows ? MSM_REDUCE_PIECES : MSM_REDUCE_PIECES_ALONE;
 }
 
+// Pieces per reduction block, 2^LB: one block of 2^LB threads halves its pieces'
+// run sums LB times.  The pieces kernels hold ~250 registers a thread, so 2^8
+// threads is the largest block an SM takes, and a block of 2^8 fills one SM's
+// register file.  The reduction's chains are latency-bound and run beside the
+// other MSMs' accumulations, whose 512-thread blocks each need a whole SM:
+// 8192 pieces as 32 blocks of 2^8 hold 32 SMs, as 64 blocks of 2^7 (or 128 of
+// 2^6, G2) up to 64 (128).  Measured on the 2^21-constraint prove: 2^8 for both
+// groups 53.55-53.61 proofs/s against 53.04-53.20 with 2^7 (G1) and 2^6 (G2),
+// the batched workload 1179-1221 against 1135-1156, although the reduction's
+// own serialized time grows from 2.95 to 3.54 ms per proof.
+#ifndef G16_REDUCE_LB_G1
+#define G16_REDUCE_LB_G1 8
+#endif
+#ifndef G16_REDUCE_LB_G2
+#define G16_REDUCE_LB_G2 8
+#endif
+constexpr uint32_t MSM_REDUCE_LB_G1 = G16_REDUCE_LB_G1;
+constexpr uint32_t MSM_REDUCE_LB_G2 = G16_REDUCE_LB_G2;
+
 struct MsmReducePlan {
-    uint32_t sets = 0, B = 0, seg = 1, lb = 7, nb = 1, hb = 0;
+    uint32_t sets = 0, B = 0, seg = 1, lb = MSM_REDUCE_LB_G1, nb = 1, hb = 0;
     bool direct = true;   // the host reads the blocks' own points
     constexpr uint32_t block_terms() const { return lb + 2; }
     constexpr uint32_t set_terms() const { return direct ? nb * (lb + 2) : lb + 1 + hb; }
@@ -76,7 +95,7 @@ constexpr MsmReducePlan msm_reduce_plan(uint32_t sets, uint32_t B, bool g2, uint
     MsmReducePlan r;
     r.sets = sets;
     r.B = B;
-    r.lb = g2 ? 6 : 7;
+    r.lb = g2 ? MSM_REDUCE_LB_G2 : MSM_REDUCE_LB_G1;
     r.seg = 1;
     while (r.seg < MSM_REDUCE_MAX_SEG && r.seg < B && (uint64_t)sets * B / r.seg > pieces_target) r.seg *= 2;
     const uint32_t pieces = B / r.seg;

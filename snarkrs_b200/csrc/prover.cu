@@ -357,6 +357,16 @@ int build_h_table(g16_circuit* c, int ch, cudaStream_t st) {
 // tables; with a compact key one set per window, W (lb + 1 + hb) points, at
 // most 32 x 15 G2 points for window bits in [8, 20].
 constexpr size_t WIN_SLOT_COMPACT = 128 * 1024;
+// Bucket-reduction piece target of the witness MSMs (0: the library default for
+// MSMs whose reductions run beside other work); G16_WITNESS_REDUCE_PIECES overrides it.
+uint64_t witness_reduce_pieces() {
+    static const uint64_t v = [] {
+        const char* e = std::getenv("G16_WITNESS_REDUCE_PIECES");
+        return e ? std::strtoull(e, nullptr, 10) : 0ull;
+    }();
+    return v;
+}
+
 size_t win_slot(const g16_circuit* c) { return c->tables ? MSM_RESULT_SLOT_BYTES : WIN_SLOT_COMPACT; }
 
 // Take an idle workspace, or build one while the pool is below its cap and the
@@ -539,6 +549,7 @@ int enqueue_witness_msms(g16_circuit* c, Workspace* ws, const void* d_w) {
     CK(cudaEventRecord(ws->ev_fork, ws->stream), "event");
     CK(cudaStreamWaitEvent(st[0], ws->ev_fork, 0), "stream wait");
     // one pass over the witness digits sorts the A, B and L live sets
+    for (auto& x : ws->sort_w) x.reduce_pieces = witness_reduce_pieces();
     MsmLiveSets sets;
     sets.count = 3;
     for (int j = 0; j < 3; j++) {

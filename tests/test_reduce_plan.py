@@ -19,7 +19,7 @@ PROBE = r"""
 #include <cstdio>
 #include "msm.cuh"
 int main() {
-    printf("%zu\n", g16::MSM_RESULT_SLOT_BYTES);
+    printf("%zu %u %u\n", g16::MSM_RESULT_SLOT_BYTES, g16::MSM_REDUCE_LB_G1, g16::MSM_REDUCE_LB_G2);
     unsigned sets, B, g2;
     unsigned long long target;
     while (scanf("%u %u %u %llu", &sets, &B, &g2, &target) == 4) {
@@ -46,7 +46,7 @@ def plan():
     def run(cases):
         text = "\n".join("%d %d %d %d" % c for c in cases) + "\n"
         out = subprocess.run([exe], input=text, capture_output=True, text=True, check=True).stdout.split("\n")
-        run.slot_bytes = int(out[0])
+        run.slot_bytes, run.lb_g1, run.lb_g2 = map(int, out[0].split())
         keys = ("seg", "lb", "nb", "hb", "direct", "set_terms", "block_points", "result_points")
         return [dict(zip(keys, map(int, l.split()))) for l in out[1:] if l.strip()]
     yield run
@@ -63,7 +63,7 @@ def test_plans_cover_every_bucket(plan):
                     cases.append((sets, B, g2, target))
     for (sets, B, g2, target), p in zip(cases, plan(cases)):
         seg, lb, nb = p["seg"], p["lb"], p["nb"]
-        assert lb == (6 if g2 else 7)
+        assert lb == (plan.lb_g2 if g2 else plan.lb_g1)
         assert seg & (seg - 1) == 0 and 1 <= seg <= 32 and seg <= B
         pieces = B // seg
         assert pieces * seg == B
@@ -86,5 +86,7 @@ def test_prover_results_fit_the_readback_slot(plan):
     cases = [(1, 1 << (c - 1), g2, t) for c in range(1, 23) for g2 in (0, 1) for t in (8192, 32768)]
     results = plan(cases)
     assert plan.slot_bytes == 32 * 256
+    # a block of 2^lb threads at ~250 registers: at most 256 threads fit an SM's register file
+    assert 1 <= plan.lb_g1 <= 8 and 1 <= plan.lb_g2 <= 8
     for (_, _, g2, _), p in zip(cases, results):
         assert p["result_points"] * (256 if g2 else 128) <= plan.slot_bytes
