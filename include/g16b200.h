@@ -356,6 +356,17 @@ typedef struct {
     uint64_t engines;        /* engines built */
 } g16_batch_stats;
 int g16_batch_stats_get(const g16_backend *b, g16_batch_stats *out);
+/* Sizes the backend's batched-proving engines for a batch of these circuits
+ * (repeats allowed) without proving it: every engine lays the batch out once,
+ * so that its buffers, which only grow, are at that batch's sizes; a later
+ * g16_prove_batch of that mix allocates nothing on any engine, and smaller mixes
+ * of the same circuits need at most small additions.  Takes each
+ * engine in turn when it is idle.  The engines' device bytes count against the backend's
+ * budget (G16_ERR_DEVICE_MEMORY when they do not fit).  Nothing to do, and
+ * G16_OK, for a batch that g16_prove_batch would prove on host lanes (compact
+ * keys, constant-work MSMs, G16_BATCH_ENGINE=0).  Gather-path keys only, as
+ * g16_prove_batch. */
+int g16_batch_reserve(g16_backend *b, size_t count, g16_circuit *const *circuits);
 
 /* ---------------- primitives (MsmBackend, crates/msm/src/lib.rs:52-82) ---------------- */
 /* sum_i scalars[i] * bases[i]; host buffers; result affine packed. */

@@ -538,6 +538,14 @@ class CudaBackend:
         check(lib().g16_batch_stats_get(self._h, ctypes.byref(st)))
         return {n: getattr(st, n) for n, _ in st._fields_}
 
+    def batch_reserve(self, circuits):
+        """Size every batched-proving engine for a batch of these circuits (repeats
+        allowed) without proving it: a later prove_batch of that mix allocates no
+        device memory (g16_batch_reserve)."""
+        n = len(circuits)
+        arr = (ctypes.c_void_p * max(n, 1))(*[c._h for c in circuits])
+        check(lib().g16_batch_reserve(self._h, ctypes.c_size_t(n), arr))
+
     def fault(self):
         """The sticky cudaError_t value that put this backend out of use, or 0."""
         return lib().g16_backend_fault(self._h)

@@ -173,25 +173,25 @@ uint64_t plan_estimate(g16_circuit* const* cs, size_t count) {
     return b + (8ull << 20);
 }
 
-// device buffer that only grows
-cudaError_t grow_dev(void*& p, size_t& cap, size_t need) {
+// device buffer that only grows, reallocated in stream order on st (the engine
+// is idle when it grows; dev_realloc_async)
+cudaError_t grow_dev(cudaStream_t st, void*& p, size_t& cap, size_t need) {
     if (p && need <= cap) return cudaSuccess;
-    cudaFree(p);
-    p = nullptr;
     cap = 0;
     const size_t n = need + need / 4 + 256;
-    cudaError_t e = g16::dev_malloc_values(&p, n);
+    cudaError_t e = g16::dev_realloc_async(&p, n, st, true);
     if (e == cudaSuccess) cap = n;
     return e;
 }
 
-// pinned host buffer that only grows
+// pinned host buffer that only grows; a page-locked allocation serialises the
+// device's streams, so it grows to twice what it needs
 cudaError_t grow_pinned(uint8_t*& p, size_t& cap, size_t need) {
     if (p && need <= cap) return cudaSuccess;
     if (p) cudaFreeHost(p);
     p = nullptr;
     cap = 0;
-    const size_t n = need + need / 4 + 256;
+    const size_t n = 2 * need + 256;
     cudaError_t e = cudaMallocHost((void**)&p, n);
     if (e == cudaSuccess) cap = n;
     if (e == cudaSuccess && value_fill_byte() >= 0) std::memset(p, value_fill_byte(), n);
@@ -222,7 +222,7 @@ int build(BatchEngine& E, g16_circuit* const* cs, size_t count) {
         E.off_h.push_back(off);
         off = align256(off + 32ull * cs[j]->n);
     }
-    CK_BATCH(grow_dev(E.d_arena, E.cap_arena, off));
+    CK_BATCH(grow_dev(E.st[0], E.d_arena, E.cap_arena, off));
     CK_BATCH(grow_pinned(E.h_stage, E.cap_stage, E.w_bytes));
     uint8_t* arena = (uint8_t*)E.d_arena;
     // MSM spaces: G1 (A, B1, L of every job), G2 (B2), H
@@ -299,7 +299,7 @@ int build(BatchEngine& E, g16_circuit* const* cs, size_t count) {
         gj.push_back(g);
     }
     CK_BATCH(ntt_batch_setup(E.ntt, items, E.st[0]));
-    CK_BATCH(grow_dev(E.d_gather, E.cap_gather, gj.size() * sizeof(g16d::GatherJob)));
+    CK_BATCH(grow_dev(E.st[0], E.d_gather, E.cap_gather, gj.size() * sizeof(g16d::GatherJob)));
     // on st[0] and waited for: a plain cudaMemcpy from pageable memory may return
     // before its DMA lands, on the legacy stream, which orders nothing against
     // the engine's non-blocking streams (the gather would read the previous
@@ -411,6 +411,107 @@ void batch_free(g16_backend* b) {
     b->batch = nullptr;
 }
 
+// Engines a backend keeps (G16_BATCH_ENGINES, 1-8; default 4).
+size_t batch_max_engines() {
+    size_t n = 4;
+    if (const char* e = std::getenv("G16_BATCH_ENGINES")) n = (size_t)std::max(1, std::min(8, std::atoi(e)));
+    return n;
+}
+
+// While it lives, no circuit of the batch is retuned (g16_autotune waits for
+// batch_users to drop to zero): the batch reads their tables.
+struct BatchUsers {
+    std::vector<g16_circuit*> cs;
+    BatchUsers(g16_circuit* const* c, size_t n) : cs(c, c + n) {
+        std::sort(cs.begin(), cs.end());
+        cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
+        for (g16_circuit* x : cs) {
+            std::unique_lock<std::mutex> lk(x->mu);
+            x->cv.wait(lk, [&] { return !x->tuning; });
+            x->batch_users++;
+        }
+    }
+    ~BatchUsers() {
+        for (g16_circuit* x : cs) {
+            {
+                std::lock_guard<std::mutex> g(x->mu);
+                x->batch_users--;
+            }
+            x->cv.notify_all();
+        }
+    }
+};
+
+// Layout E for the batch, its grow-only buffers counted against the backend's
+// device budget; on failure E keeps no layout.
+int layout_engine(g16_backend* b, BatchEngine& E, g16_circuit* const* cs, size_t count) {
+    const uint64_t need = plan_estimate(cs, count);
+    if (need > E.accounted) {   // the engine's buffers grow: check and count the difference
+        if (b->vram_used + (need - E.accounted) > b->vram_limit)
+            return fail(G16_ERR_DEVICE_MEMORY, "batch of %zu proofs needs about %llu MiB of device memory", count,
+                        (unsigned long long)(need >> 20));
+        b->vram_used += need - E.accounted;
+        E.accounted = need;
+    }
+    const uint64_t allocs0 = timer().device_alloc_bytes.load();
+    int rc = build(E, cs, count);
+    if (rc != G16_OK) {
+        E.drop_layout();
+        return rc;
+    }
+    b->batch_layouts++;
+    b->batch_grown += timer().device_alloc_bytes.load() - allocs0;
+    return G16_OK;
+}
+
+int reserve_batch_engines(g16_backend* b, g16_circuit* const* cs, size_t count) {
+    if (!count) return G16_OK;
+    const size_t max_engines = batch_max_engines();
+    BatchUsers users(cs, count);
+    // one engine at a time, each as soon as it is idle, so that batches running
+    // meanwhile keep the others
+    std::vector<BatchEngine*> sized;
+    for (;;) {
+        BatchEngine* eng = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(b->batch_mu);
+            if (!b->batch) b->batch = new BatchPool();
+            BatchPool& P = *b->batch;
+            while (P.all.size() < max_engines) {
+                P.all.push_back(std::make_unique<BatchEngine>());
+                P.idle.push_back(P.all.back().get());
+                b->batch_engines++;
+            }
+            if (sized.size() >= P.all.size()) break;
+            auto fresh = [&] {
+                for (size_t i = 0; i < P.idle.size(); i++)
+                    if (std::find(sized.begin(), sized.end(), P.idle[i]) == sized.end()) return (long)i;
+                return -1L;
+            };
+            P.cv.wait(lk, [&] { return fresh() >= 0; });
+            const long i = fresh();
+            eng = P.idle[(size_t)i];
+            P.idle.erase(P.idle.begin() + i);
+        }
+        struct GiveBack {
+            g16_backend* b;
+            BatchEngine* e;
+            ~GiveBack() {
+                {
+                    std::lock_guard<std::mutex> g(b->batch_mu);
+                    b->batch->idle.push_back(e);
+                }
+                b->batch->cv.notify_all();
+            }
+        } give_back{b, eng};
+        int rc = layout_engine(b, *eng, cs, count);
+        if (rc != G16_OK) return rc;
+        eng->drop_layout();   // sized; the next batch lays itself out
+        sized.push_back(eng);
+    }
+    return G16_OK;
+}
+
 int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, const uint8_t* const* witnesses,
                        const size_t* lens, const uint8_t* r, const uint8_t* s, g16_proof* out, double* done_ms) {
     const auto t_start = std::chrono::steady_clock::now();
@@ -430,8 +531,7 @@ int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, con
     std::vector<BatchKey> want;
     for (size_t j = 0; j < count; j++) want.push_back(key_of(cs[j]));
     BatchEngine* eng = nullptr;
-    size_t max_engines = 4;
-    if (const char* e = std::getenv("G16_BATCH_ENGINES")) max_engines = (size_t)std::max(1, std::min(8, std::atoi(e)));
+    const size_t max_engines = batch_max_engines();
     {
         std::unique_lock<std::mutex> lk(b->batch_mu);
         if (!b->batch) b->batch = new BatchPool();
@@ -463,45 +563,11 @@ int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* cs, con
             b->batch->cv.notify_all();
         }
     } give_back{b, eng};
-    // no circuit may be retuned while the batch reads its tables
-    std::vector<g16_circuit*> distinct(cs, cs + count);
-    std::sort(distinct.begin(), distinct.end());
-    distinct.erase(std::unique(distinct.begin(), distinct.end()), distinct.end());
-    for (g16_circuit* c : distinct) {
-        std::unique_lock<std::mutex> lk(c->mu);
-        c->cv.wait(lk, [&] { return !c->tuning; });
-        c->batch_users++;
-    }
-    struct Release {
-        std::vector<g16_circuit*>& cs;
-        ~Release() {
-            for (g16_circuit* c : cs) {
-                {
-                    std::lock_guard<std::mutex> g(c->mu);
-                    c->batch_users--;
-                }
-                c->cv.notify_all();
-            }
-        }
-    } release_guard{distinct};
+    BatchUsers users(cs, count);
     BatchEngine& E = *eng;
     if (!(E.key == want)) {
-        const uint64_t need = plan_estimate(cs, count);
-        if (need > E.accounted) {   // the engine's buffers grow: check and count the difference
-            if (b->vram_used + (need - E.accounted) > b->vram_limit)
-                return fail(G16_ERR_DEVICE_MEMORY, "batch of %zu proofs needs about %llu MiB of device memory", count,
-                            (unsigned long long)(need >> 20));
-            b->vram_used += need - E.accounted;
-            E.accounted = need;
-        }
-        const uint64_t allocs0 = timer().device_alloc_bytes.load();
-        int rc = build(E, cs, count);
-        if (rc != G16_OK) {
-            E.drop_layout();
-            return rc;
-        }
-        b->batch_layouts++;
-        b->batch_grown += timer().device_alloc_bytes.load() - allocs0;
+        int rc = layout_engine(b, E, cs, count);
+        if (rc != G16_OK) return rc;
     }
     // witnesses in: gathered into pinned memory by host threads, then one copy
     const size_t threads = host_threads();

@@ -150,6 +150,31 @@ inline cudaError_t dev_malloc_values(T** p, size_t bytes) {
     return e;
 }
 
+// Growable scratch (sort, bucket and engine buffers) is allocated and freed in
+// stream order, from the device's default memory pool.  cudaMalloc and cudaFree
+// are not: an allocation serialises every stream of the device and a free waits
+// for all of its work, so a buffer that grows while other proofs run would stall
+// them all.  The old buffer goes back on the same stream, which must be the only
+// one with work on it in flight (a workspace or engine is idle when it grows).
+// Such memory may still be released with cudaFree.  No buffer grows inside a
+// stream capture: there the allocation would belong to the graph.
+template <class T>
+inline cudaError_t dev_realloc_async(T** p, size_t bytes, cudaStream_t st, bool values) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess) return e;
+    if (cs != cudaStreamCaptureStatusNone) return cudaErrorStreamCaptureUnsupported;
+    if (*p) e = cudaFreeAsync((void*)*p, st);
+    *p = nullptr;
+    if (e != cudaSuccess) return e;
+    timer().device_allocs.fetch_add(1, std::memory_order_relaxed);
+    timer().device_alloc_bytes.fetch_add(bytes, std::memory_order_relaxed);
+    e = cudaMallocAsync((void**)p, bytes, st);
+    const int fill = values ? value_fill_byte() : -1;
+    if (e == cudaSuccess && fill >= 0 && bytes) e = cudaMemsetAsync((void*)*p, fill, bytes, st);
+    return e;
+}
+
 inline unsigned blocks_for(size_t n, unsigned threads) { return (unsigned)((n + threads - 1) / threads); }
 
 }  // namespace g16

@@ -1159,14 +1159,14 @@ static cudaError_t fixed_too_small(size_t need_bytes, size_t cap_bytes) {
     return cudaErrorInvalidValue;
 }
 
+// Grow-only scratch, reallocated in stream order on st (dev_realloc_async).
 template <class T>
-static cudaError_t grow(T*& p, size_t& cap, size_t need_elems, bool fixed = false) {
+static cudaError_t grow(cudaStream_t st, T*& p, size_t& cap, size_t need_elems, bool fixed = false) {
     if (need_elems <= cap && p) return cudaSuccess;
     if (fixed) return fixed_too_small(need_elems * sizeof(T), cap * sizeof(T));
-    cudaFree(p);
-    p = nullptr;
+    cap = 0;
     size_t n = need_elems + need_elems / 8 + 64;
-    cudaError_t e = g16::dev_malloc((void**)&p, n * sizeof(T));
+    cudaError_t e = g16::dev_realloc_async(&p, n * sizeof(T), st, false);
     if (e != cudaSuccess) {
         cap = 0;
         set_error("cudaMalloc of %zu bytes for MSM scratch failed: %s", n * sizeof(T), cudaGetErrorString(e));
@@ -1176,13 +1176,12 @@ static cudaError_t grow(T*& p, size_t& cap, size_t need_elems, bool fixed = fals
     return cudaSuccess;
 }
 
-static cudaError_t grow_bytes(void*& p, size_t& cap, size_t need, bool fixed = false) {
+static cudaError_t grow_bytes(cudaStream_t st, void*& p, size_t& cap, size_t need, bool fixed = false) {
     if (need <= cap && p) return cudaSuccess;
     if (fixed) return fixed_too_small(need, cap);
-    cudaFree(p);
-    p = nullptr;
+    cap = 0;
     size_t n = need + need / 8 + 256;
-    cudaError_t e = g16::dev_malloc_values(&p, n);
+    cudaError_t e = g16::dev_realloc_async(&p, n, st, true);
     if (e != cudaSuccess) {
         cap = 0;
         set_error("cudaMalloc of %zu bytes for MSM scratch failed: %s", n, cudaGetErrorString(e));
@@ -1237,28 +1236,28 @@ cudaError_t msm_sort(MsmSort& s, const void* d_scalars, size_t n, bool montgomer
     const uint32_t kw = shared_windows ? 0u : s.B, ew = shared_windows ? (uint32_t)n : 0u;
     const uint32_t sink = constant_work ? s.K : NO_KEY;
     size_t nn = n ? n : 1;
-    G16_CUDA(grow(s.d_scalars_std, s.cap_scalars, nn * 8, s.fixed));
+    G16_CUDA(grow(st, s.d_scalars_std, s.cap_scalars, nn * 8, s.fixed));
     size_t kk = (size_t)s.Ks + 1;
     if (s.fixed && (kk > s.cap_k || !s.d_counts || !s.d_offsets || !s.d_cursor || !s.d_seg_base || !s.d_fat_list))
         G16_CUDA(fixed_too_small(kk * sizeof(uint32_t), s.cap_k * sizeof(uint32_t)));
     if (kk > s.cap_k || !s.d_counts) {
         size_t cap = 0;
-        G16_CUDA(grow(s.d_counts, cap, kk));
+        G16_CUDA(grow(st, s.d_counts, cap, kk));
         cap = 0;
-        G16_CUDA(grow(s.d_offsets, cap, kk));
+        G16_CUDA(grow(st, s.d_offsets, cap, kk));
         cap = 0;
-        G16_CUDA(grow(s.d_cursor, cap, kk));
+        G16_CUDA(grow(st, s.d_cursor, cap, kk));
         cap = 0;
-        G16_CUDA(grow(s.d_seg_base, cap, kk));
+        G16_CUDA(grow(st, s.d_seg_base, cap, kk));
         cap = 0;
-        G16_CUDA(grow(s.d_fat_list, cap, kk));
+        G16_CUDA(grow(st, s.d_fat_list, cap, kk));
         s.cap_k = cap;
     }
-    G16_CUDA(grow(s.d_scan_tmp, s.cap_tmp, kk / 1024 + 2, s.fixed));
-    G16_CUDA(grow(s.d_entries, s.cap_entries, nn * s.W, s.fixed));
+    G16_CUDA(grow(st, s.d_scan_tmp, s.cap_tmp, kk / 1024 + 2, s.fixed));
+    G16_CUDA(grow(st, s.d_entries, s.cap_entries, nn * s.W, s.fixed));
     if (!s.d_total) {
         if (s.fixed) G16_CUDA(fixed_too_small(4 * sizeof(uint32_t), 0));
-        G16_CUDA(g16::dev_malloc((void**)&s.d_total, 4 * sizeof(uint32_t)));
+        G16_CUDA(g16::dev_realloc_async(&s.d_total, 4 * sizeof(uint32_t), st, false));
     }
 
     G16_CUDA(cudaMemsetAsync(s.d_counts, 0, kk * sizeof(uint32_t), st));
@@ -1325,20 +1324,20 @@ cudaError_t msm_sort_sets(MsmSort* sorts, const MsmLiveSets& sets, const void* d
         const size_t kk = (size_t)s.Ks + 1;
         if (kk > s.cap_k || !s.d_counts) {
             size_t cap = 0;
-            G16_CUDA(grow(s.d_counts, cap, kk));
+            G16_CUDA(grow(st, s.d_counts, cap, kk));
             cap = 0;
-            G16_CUDA(grow(s.d_offsets, cap, kk));
+            G16_CUDA(grow(st, s.d_offsets, cap, kk));
             cap = 0;
-            G16_CUDA(grow(s.d_cursor, cap, kk));
+            G16_CUDA(grow(st, s.d_cursor, cap, kk));
             cap = 0;
-            G16_CUDA(grow(s.d_seg_base, cap, kk));
+            G16_CUDA(grow(st, s.d_seg_base, cap, kk));
             cap = 0;
-            G16_CUDA(grow(s.d_fat_list, cap, kk));
+            G16_CUDA(grow(st, s.d_fat_list, cap, kk));
             s.cap_k = cap;
         }
-        G16_CUDA(grow(s.d_scan_tmp, s.cap_tmp, kk / 1024 + 2));
-        G16_CUDA(grow(s.d_entries, s.cap_entries, (size_t)(sets.rows[j] ? sets.rows[j] : 1) * W));
-        if (!s.d_total) G16_CUDA(g16::dev_malloc((void**)&s.d_total, 4 * sizeof(uint32_t)));
+        G16_CUDA(grow(st, s.d_scan_tmp, s.cap_tmp, kk / 1024 + 2));
+        G16_CUDA(grow(st, s.d_entries, s.cap_entries, (size_t)(sets.rows[j] ? sets.rows[j] : 1) * W));
+        if (!s.d_total) G16_CUDA(g16::dev_realloc_async(&s.d_total, 4 * sizeof(uint32_t), st, false));
         G16_CUDA(cudaMemsetAsync(s.d_counts, 0, kk * sizeof(uint32_t), st));
         G16_CUDA(cudaMemsetAsync(s.d_total, 0, 4 * sizeof(uint32_t), st));
         a.rank[j] = sets.d_rank[j];
@@ -1350,7 +1349,7 @@ cudaError_t msm_sort_sets(MsmSort* sorts, const MsmLiveSets& sets, const void* d
     a.key_stride = shared ? 0u : (1u << (c - 1));
     // the standard-form copy of the scalars, shared by the sets, lives in the first
     MsmSort& s0 = sorts[0];
-    G16_CUDA(grow(s0.d_scalars_std, s0.cap_scalars, (n ? n : 1) * 8));
+    G16_CUDA(grow(st, s0.d_scalars_std, s0.cap_scalars, (n ? n : 1) * 8));
     const uint32_t sink = constant_work ? sorts[0].K : NO_KEY;
     if (n) {
         timer().add_bytes("msm_digits", 64.0 * n);   // scalars in, standard-form copy out
@@ -1407,7 +1406,7 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     size_t max_entries = (s.n ? s.n : 1) * (size_t)s.W;
     size_t chunks = (max_entries + s.chunk - 1) / s.chunk;
     size_t max_partials = (size_t)s.Ks + chunks + 1;
-    G16_CUDA(grow_bytes(acc.d_partials, acc.cap_partials, max_partials * xyzz_bytes, acc.fixed));
+    G16_CUDA(grow_bytes(st, acc.d_partials, acc.cap_partials, max_partials * xyzz_bytes, acc.fixed));
     const uint32_t Wr = s.shared ? 1u : (uint32_t)s.W;   // bucket sets to reduce
     constexpr bool G2 = !std::is_same<F, g16d::Fq>::value;
     constexpr int LB = G2 ? MSM_REDUCE_LB_G2 : MSM_REDUCE_LB_G1;   // pieces per reduction block: 2^LB
@@ -1415,13 +1414,13 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     const MsmReducePlan plan =
         msm_reduce_plan(Wr, s.B, G2, s.reduce_pieces ? s.reduce_pieces : msm_reduce_pieces(s.shared));
     acc.plan = plan;
-    G16_CUDA(grow_bytes(acc.d_buckets, acc.cap_buckets, (size_t)s.K * xyzz_bytes, acc.fixed));
+    G16_CUDA(grow_bytes(st, acc.d_buckets, acc.cap_buckets, (size_t)s.K * xyzz_bytes, acc.fixed));
     if (!plan.direct)
-        G16_CUDA(grow_bytes(acc.d_segments, acc.cap_segments, plan.block_points() * xyzz_bytes, acc.fixed));
-    G16_CUDA(grow_bytes(acc.d_windows, acc.cap_windows, plan.result_points() * xyzz_bytes, acc.fixed));
+        G16_CUDA(grow_bytes(st, acc.d_segments, acc.cap_segments, plan.block_points() * xyzz_bytes, acc.fixed));
+    G16_CUDA(grow_bytes(st, acc.d_windows, acc.cap_windows, plan.result_points() * xyzz_bytes, acc.fixed));
     if (!acc.d_work) {
         if (acc.fixed) G16_CUDA(fixed_too_small(sizeof(unsigned long long), 0));
-        G16_CUDA(g16::dev_malloc((void**)&acc.d_work, sizeof(unsigned long long)));
+        G16_CUDA(g16::dev_realloc_async(&acc.d_work, sizeof(unsigned long long), st, false));
     }
     G16_CUDA(cudaMemsetAsync(acc.d_work, 0, sizeof(unsigned long long), st));
     uint4* partials = (uint4*)acc.d_partials;
@@ -1504,7 +1503,7 @@ void MsmSources::release() {
 // Upload a descriptor table into a device buffer that only grows (cap in bytes).
 template <class T>
 static cudaError_t upload_vec(void*& d, size_t& cap, const std::vector<T>& v, cudaStream_t st) {
-    G16_CUDA(grow_bytes(d, cap, (v.empty() ? 1 : v.size()) * sizeof(T)));
+    G16_CUDA(grow_bytes(st, d, cap, (v.empty() ? 1 : v.size()) * sizeof(T)));
     if (!v.empty()) G16_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
     return cudaSuccess;
 }
@@ -1582,27 +1581,27 @@ cudaError_t msm_batch_setup(MsmSources& so, MsmSpace* const* spaces, int nspaces
         const size_t kk = (size_t)sp.K + 1;
         if (kk > s.cap_k || !s.d_counts) {
             size_t cap = 0;
-            G16_CUDA(grow(s.d_counts, cap, kk));
+            G16_CUDA(grow(st, s.d_counts, cap, kk));
             cap = 0;
-            G16_CUDA(grow(s.d_offsets, cap, kk));
+            G16_CUDA(grow(st, s.d_offsets, cap, kk));
             cap = 0;
-            G16_CUDA(grow(s.d_cursor, cap, kk));
+            G16_CUDA(grow(st, s.d_cursor, cap, kk));
             cap = 0;
-            G16_CUDA(grow(s.d_seg_base, cap, kk));
+            G16_CUDA(grow(st, s.d_seg_base, cap, kk));
             cap = 0;
-            G16_CUDA(grow(s.d_fat_list, cap, kk));
+            G16_CUDA(grow(st, s.d_fat_list, cap, kk));
             s.cap_k = cap;
         }
-        G16_CUDA(grow(s.d_scan_tmp, s.cap_tmp, kk / 1024 + 2));
-        G16_CUDA(grow(s.d_entries, s.cap_entries, sp.max_entries ? sp.max_entries : 1));
-        if (!s.d_total) G16_CUDA(g16::dev_malloc((void**)&s.d_total, 4 * sizeof(uint32_t)));
+        G16_CUDA(grow(st, s.d_scan_tmp, s.cap_tmp, kk / 1024 + 2));
+        G16_CUDA(grow(st, s.d_entries, s.cap_entries, sp.max_entries ? sp.max_entries : 1));
+        if (!s.d_total) G16_CUDA(g16::dev_realloc_async(&s.d_total, 4 * sizeof(uint32_t), st, false));
         MsmAccum& a = sp.acc;
         const size_t chunks = (sp.max_entries + s.chunk - 1) / s.chunk;
-        G16_CUDA(grow_bytes(a.d_partials, a.cap_partials, ((size_t)sp.K + chunks + 1) * pb));
-        G16_CUDA(grow_bytes(a.d_buckets, a.cap_buckets, ((size_t)sp.K + 1) * pb));
-        G16_CUDA(grow_bytes(a.d_segments, a.cap_segments, (out_block + 1) * pb));
-        G16_CUDA(grow_bytes(a.d_windows, a.cap_windows, (out_set + 1) * pb));
-        if (!a.d_work) G16_CUDA(g16::dev_malloc((void**)&a.d_work, sizeof(unsigned long long)));
+        G16_CUDA(grow_bytes(st, a.d_partials, a.cap_partials, ((size_t)sp.K + chunks + 1) * pb));
+        G16_CUDA(grow_bytes(st, a.d_buckets, a.cap_buckets, ((size_t)sp.K + 1) * pb));
+        G16_CUDA(grow_bytes(st, a.d_segments, a.cap_segments, (out_block + 1) * pb));
+        G16_CUDA(grow_bytes(st, a.d_windows, a.cap_windows, (out_set + 1) * pb));
+        if (!a.d_work) G16_CUDA(g16::dev_realloc_async(&a.d_work, sizeof(unsigned long long), st, false));
         G16_CUDA(upload_vec(sp.d_segdev, sp.cap_segdev, segdev, st));
         G16_CUDA(upload_vec(sp.d_reduce, sp.cap_reduce, red, st));
     }
@@ -1611,7 +1610,7 @@ cudaError_t msm_batch_setup(MsmSources& so, MsmSpace* const* spaces, int nspaces
     std::vector<uint32_t> blk;
     size_t std_elems = 0;
     for (auto& src : so.srcs) std_elems += src.n;
-    G16_CUDA(grow_bytes(so.d_std, so.cap_std, (std_elems ? std_elems : 1) * 32));
+    G16_CUDA(grow_bytes(st, so.d_std, so.cap_std, (std_elems ? std_elems : 1) * 32));
     uint64_t blocks = 0, off = 0;
     for (auto& src : so.srcs) {
         MsmSourceDev d = {};

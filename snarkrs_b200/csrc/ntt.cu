@@ -673,11 +673,9 @@ cudaError_t ntt_batch_setup(NttBatch& nb, const std::vector<NttBatchItem>& items
         add_phase(1, passes);
     }
     const size_t need = (all.empty() ? 1 : all.size()) * sizeof(NttJob);
-    if (need > nb.cap_jobs) {   // the job table only grows
-        cudaFree(nb.d_jobs);
-        nb.d_jobs = nullptr;
+    if (need > nb.cap_jobs) {   // the job table only grows, in stream order (dev_realloc_async)
         nb.cap_jobs = 0;
-        G16_CUDA(g16::dev_malloc(&nb.d_jobs, need + need / 2));
+        G16_CUDA(g16::dev_realloc_async(&nb.d_jobs, need + need / 2, st, false));
         nb.cap_jobs = need + need / 2;
     }
     if (!all.empty()) G16_CUDA(cudaMemcpyAsync(nb.d_jobs, all.data(), all.size() * sizeof(NttJob), cudaMemcpyHostToDevice, st));

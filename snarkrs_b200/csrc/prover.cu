@@ -1629,6 +1629,23 @@ int g16_prove_batch_timed(g16_backend* b, size_t count, g16_circuit* const* circ
                           const uint8_t* const* witnesses, const size_t* lens, const uint8_t* r, const uint8_t* s,
                           g16_proof* out, double* done_ms);
 
+int g16_batch_reserve(g16_backend* b, size_t count, g16_circuit* const* circuits) {
+    if (!b || (count && !circuits)) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");
+    bool all_tables = true;
+    for (size_t i = 0; i < count; i++) {
+        if (!circuits[i]) return fail(G16_ERR_INVALID_ARGUMENT, "null circuit %zu", i);
+        if (circuits[i]->be != b) return fail(G16_ERR_INVALID_ARGUMENT, "circuit %zu belongs to another backend", i);
+        if (int rc_g = gather_ok(circuits[i])) return rc_g;
+        all_tables &= circuits[i]->tables;
+    }
+    if (int rc_dev = device_usable(b)) return rc_dev;
+    // the same choice as g16_prove_batch_timed: only the engine path has buffers to size
+    const char* eng = std::getenv("G16_BATCH_ENGINE");
+    if (!count || b->constant_work || !all_tables || (eng && std::strcmp(eng, "0") == 0)) return G16_OK;
+    CK(cudaSetDevice(b->ordinal), "cudaSetDevice");
+    return reserve_batch_engines(b, circuits, count);
+}
+
 int g16_prove_batch(g16_backend* b, size_t count, g16_circuit* const* circuits, const uint8_t* const* witnesses,
                     const size_t* lens, const uint8_t* r, const uint8_t* s, g16_proof* out) {
     return g16_prove_batch_timed(b, count, circuits, witnesses, lens, r, s, out, nullptr);

@@ -189,6 +189,9 @@ int check_witness(const g16_circuit* c, size_t n, const uint8_t* w_host);
 // does not fit and the caller may prove it another way.
 int prove_batch_engine(g16_backend* b, size_t count, g16_circuit* const* circuits, const uint8_t* const* witnesses,
                        const size_t* lens, const uint8_t* r, const uint8_t* s, g16_proof* out, double* done_ms);
+// Sizes every engine of the backend (creating them up to their limit) for a
+// batch of these circuits without proving it, taking each engine in turn when idle.
+int reserve_batch_engines(g16_backend* b, g16_circuit* const* circuits, size_t count);
 // Drops the batched-proving engine's state that refers to circuit c (before c is freed).
 void batch_forget(g16_backend* b, const g16_circuit* c);
 // Frees the batched-proving engine of a backend.

@@ -86,6 +86,24 @@ uint64_t live_bytes(g16_server* sv) {
     return t;
 }
 
+// The batch engines, sized for a quarter more than the largest batch of this
+// key alone that the caps allow (at most max_batch requests and batch_wires
+// wires).  Under load the queue grows and so do the batches: an engine that
+// first met them then would reallocate its buffers while other requests run,
+// which slows the server when it is already behind.  A mix of keys can need
+// more than each key's own largest batch (its bucket arrays sum over the jobs,
+// about a fifth more for the served mix of 2^14-2^18 constraints), hence the
+// quarter.  Best effort: a mix that needs more still grows.
+void reserve_engines_for(g16_server* sv, g16_circuit* c, size_t max_batch, uint64_t batch_wires, uint64_t solo_wires) {
+    const uint64_t wires = g16_circuit_n_vars(c);
+    if (!wires || (solo_wires && wires >= solo_wires)) return;   // proved alone
+    const size_t largest = (size_t)std::min<uint64_t>(max_batch, std::max<uint64_t>(1, batch_wires / wires));
+    if (largest < 2) return;   // a batch of one is proved alone
+    const size_t copies = largest + (largest + 3) / 4;
+    std::vector<g16_circuit*> cs(copies, c);
+    g16_batch_reserve(sv->b, copies, cs.data());
+}
+
 // ensure_resident could only go on by waiting, which a worker already holding
 // keys must not do: the request goes back to the queue for a later batch
 constexpr int DEFER = -1;
@@ -135,6 +153,8 @@ int ensure_resident(g16_server* sv, uint32_t id, std::unique_lock<std::mutex>& l
         lk.lock();
     }
     std::vector<uint8_t> bytes = k.zkey;   // stable copy while unlocked
+    const size_t max_batch = sv->max_batch;
+    const uint64_t batch_wires = sv->batch_wires, solo_wires = sv->solo_wires;
     lk.unlock();
     g16_zkey* z = nullptr;
     g16_circuit* c = nullptr;
@@ -145,6 +165,7 @@ int ensure_resident(g16_server* sv, uint32_t id, std::unique_lock<std::mutex>& l
         rc = g16_prepare(sv->b, &v, &c);
         g16_zkey_free(z);
     }
+    if (rc == G16_OK) reserve_engines_for(sv, c, max_batch, batch_wires, solo_wires);
     if (rc != G16_OK) {
         char buf[512];
         g16_last_error(buf, sizeof buf);

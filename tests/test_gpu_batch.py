@@ -66,6 +66,30 @@ def test_batch_engine_equals_singles_and_oracle(backend, mix):
     assert S.launch_count() > launches
 
 
+def test_reserved_engines_allocate_nothing(backend, mix):
+    # a mix larger than the module's other batches: reserving it sizes every engine,
+    # so proving it on whichever engine it lands allocates no device memory
+    order = [3, 3, 3, 2, 2, 1, 0, 3, 2, 3, 3, 1]
+    before = backend.batch_stats()
+    backend.batch_reserve([mix[i][3] for i in order])
+    assert backend.batch_stats()["engines"] >= 1
+    for rep in range(3):
+        jobs, meta = jobs_of(mix, order, 500 + 50 * rep)
+        allocs = S.device_alloc_count()
+        out = backend.prove_batch(jobs)
+        assert S.device_alloc_count() == allocs, "a reserved mix allocated device memory"
+        check(out, jobs, meta)
+    assert backend.batch_stats()["submissions"] - before["submissions"] == 3
+
+
+def test_batch_reserve_arguments(backend, mix):
+    backend.batch_reserve([])   # nothing to size
+    with pytest.raises(S.InvalidArgumentError):
+        S.check(S.lib().g16_batch_reserve(None, 0, None))
+    with pytest.raises(S.InvalidArgumentError):   # a null circuit
+        S.check(S.lib().g16_batch_reserve(backend._h, 1, (S.ctypes.c_void_p * 1)(None)))
+
+
 def test_batch_engine_after_retuning(backend, mix):
     sc, zk, ok, circ = mix[2]
     t = circ.tuning()
