@@ -245,6 +245,14 @@ int g16_prove_with_blinders_from_rows(g16_circuit *c, const uint8_t *witness_mon
 int g16_prove_with_blinders_device(g16_circuit *c, const void *d_witness_mont, size_t n, const uint8_t *r_mont,
                                    const uint8_t *s_mont, g16_proof *out);
 int g16_stage_timings_get(const g16_circuit *c, g16_stage_timings *out);
+/* Readies up to `count` workspaces of c (one per proof in flight; as many as
+ * its pool, 8, and the device budget allow) by proving a throwaway witness
+ * (the constant wire 1, every other wire 0, r = s = 1) twice on each: the
+ * first proof sizes the workspace's scratch, the second captures its CUDA
+ * graph.  Up to that many concurrent proofs of c then allocate nothing and
+ * replay graphs.  The throwaway proofs count in c's stage timings.  Gather-path
+ * keys only. */
+int g16_circuit_warm(g16_circuit *c, uint32_t count);
 /* prove::prove (crates/groth16/src/prove.rs:34-92): r and s drawn from the
  * operating system's CSPRNG, stages 0-11, then the proof is verified against
  * the circuit's verifying key (timed as verify_us); G16_ERR_SELF_VERIFY when

@@ -425,6 +425,11 @@ class CudaCircuit:
                                             bytes(r_mont), bytes(s_mont), ctypes.byref(p)))
         return Proof(p.a, p.b, p.c)
 
+    def warm(self, count):
+        """Ready up to `count` workspaces (g16_circuit_warm): that many concurrent
+        proofs then allocate nothing and replay CUDA graphs."""
+        check(lib().g16_circuit_warm(self._h, ctypes.c_uint32(count)))
+
     def prove_with_blinders_device(self, d_witness, n, r_mont, s_mont):
         p = _Proof()
         check(lib().g16_prove_with_blinders_device(self._h, ctypes.c_void_p(d_witness), ctypes.c_size_t(n),

@@ -1504,6 +1504,56 @@ int g16_prove_with_blinders(g16_circuit* c, const uint8_t* w, size_t n, const ui
     return prove_on_device(c, g.ws, g.ws->d_w, r, s, out);
 }
 
+int g16_circuit_warm(g16_circuit* c, uint32_t count) {
+    if (!c) return fail(G16_ERR_INVALID_ARGUMENT, "null circuit");
+    if (int rc_g = gather_ok(c)) return rc_g;
+    if (int rc_dev = device_usable(c->be)) return rc_dev;
+    CK(cudaSetDevice(c->be->ordinal), "cudaSetDevice");
+    // hold up to `count` workspaces at once: idle ones, or new ones while the pool
+    // and the device budget allow (never waiting, since they may all be held here)
+    std::vector<std::unique_ptr<WsGuard>> held;
+    {
+        std::unique_lock<std::mutex> lk(c->mu);
+        c->cv.wait(lk, [&] { return !c->tuning; });
+        while (held.size() < count) {
+            Workspace* ws = nullptr;
+            if (!c->idle.empty()) {
+                ws = c->idle.back();
+                c->idle.pop_back();
+            } else if (c->pool.size() < c->max_workspaces && c->be->vram_used + c->ws_estimate <= c->be->vram_limit) {
+                auto w = std::make_unique<Workspace>();
+                cudaError_t e = w->init(c->n_vars, c->n, win_slot(c));
+                if (e != cudaSuccess) {
+                    w->release();
+                    cudaGetLastError();
+                    break;
+                }
+                c->device_bytes += c->ws_estimate;
+                c->be->vram_used += c->ws_estimate;
+                ws = w.get();
+                c->pool.push_back(std::move(w));
+            } else {
+                break;
+            }
+            held.push_back(std::make_unique<WsGuard>(c));
+            held.back()->ws = ws;
+        }
+    }
+    // a throwaway witness: the constant wire 1, every other wire 0; r = s = 1
+    host_init();
+    std::vector<uint8_t> w(32ull * c->n_vars, 0);
+    std::memcpy(w.data(), FR_P.one.v, 32);
+    const uint8_t* one = (const uint8_t*)FR_P.one.v;
+    g16_proof p;
+    for (int pass = 0; pass < 2; pass++)   // the first sizes the scratch, the second captures the graph
+        for (auto& g : held) {
+            int rc = upload_witness(g->ws, w.data(), c->n_vars);
+            if (rc == G16_OK) rc = prove_on_device(c, g->ws, g->ws->d_w, one, one, &p);
+            if (rc != G16_OK) return rc;
+        }
+    return G16_OK;
+}
+
 int g16_prove_with_blinders_device(g16_circuit* c, const void* d_w, size_t n, const uint8_t* r, const uint8_t* s,
                                    g16_proof* out) {
     if (!c || !d_w || !r || !s || !out) return fail(G16_ERR_INVALID_ARGUMENT, "null argument");

@@ -155,6 +155,7 @@ int ensure_resident(g16_server* sv, uint32_t id, std::unique_lock<std::mutex>& l
     std::vector<uint8_t> bytes = k.zkey;   // stable copy while unlocked
     const size_t max_batch = sv->max_batch;
     const uint64_t batch_wires = sv->batch_wires, solo_wires = sv->solo_wires;
+    const uint32_t lanes = (uint32_t)sv->workers.size();
     lk.unlock();
     g16_zkey* z = nullptr;
     g16_circuit* c = nullptr;
@@ -165,7 +166,13 @@ int ensure_resident(g16_server* sv, uint32_t id, std::unique_lock<std::mutex>& l
         rc = g16_prepare(sv->b, &v, &c);
         g16_zkey_free(z);
     }
-    if (rc == G16_OK) reserve_engines_for(sv, c, max_batch, batch_wires, solo_wires);
+    if (rc == G16_OK) {
+        // as many ready workspaces as workers that may prove this key alone at once,
+        // and engines sized for its batches: first requests then allocate nothing
+        // and replay graphs (best effort)
+        g16_circuit_warm(c, lanes);
+        reserve_engines_for(sv, c, max_batch, batch_wires, solo_wires);
+    }
     if (rc != G16_OK) {
         char buf[512];
         g16_last_error(buf, sizeof buf);

@@ -91,3 +91,24 @@ def test_tuning_refusals(backend, circuit):
         with pytest.raises(S.InvalidArgumentError):
             circ.autotune(sc.witness(1), concurrency=bad)
     circ.close()
+
+
+def test_warmed_workspaces_allocate_nothing(backend, circuit):
+    # g16_circuit_warm readies workspaces with throwaway proofs; real proofs after it
+    # allocate no device memory and still equal the oracle's
+    sc, zk, ok = circuit
+    circ = backend.prepare(S.ProvingKey.from_bytes(zk))
+    try:
+        circ.warm(3)
+        circ.warm(100)   # more than the pool holds: as many as it can, no error
+        held = circ.device_bytes()
+        allocs = S.device_alloc_count()
+        for i in range(3):
+            w = sc.witness(900 + i)
+            r, s = blinders(900 + i)
+            p = circ.prove_with_blinders(w, r, s)
+            assert p.to_bytes() == ok.prove(w, O.from_bytes(r), O.from_bytes(s))
+        assert S.device_alloc_count() == allocs, "a proof on a warmed circuit allocated device memory"
+        assert circ.device_bytes() == held
+    finally:
+        circ.close()
