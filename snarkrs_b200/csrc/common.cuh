@@ -156,8 +156,10 @@ inline cudaError_t dev_malloc_values(T** p, size_t bytes) {
 // for all of its work, so a buffer that grows while other proofs run would stall
 // them all.  The old buffer goes back on the same stream, which must be the only
 // one with work on it in flight (a workspace or engine is idle when it grows).
-// Such memory may still be released with cudaFree.  No buffer grows inside a
-// stream capture: there the allocation would belong to the graph.
+// Such memory may still be released with cudaFree, which for it does not wait
+// for the device: every owner's release synchronises the owner's streams first
+// (Workspace, BatchEngine, the backend's own MSM scratch).  No buffer grows
+// inside a stream capture: there the allocation would belong to the graph.
 template <class T>
 inline cudaError_t dev_realloc_async(T** p, size_t bytes, cudaStream_t st, bool values) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
