@@ -577,10 +577,16 @@ constexpr bool REDUCE_INL = std::is_same<F, g16d::Fq>::value && G16_REDUCE_INLIN
 #define REDUCE_MIN_BLOCKS 1
 #endif
 
+// Threads per k_bucket_sums block.
+#ifndef G16_BUCKET_SUMS_BLOCK
+#define G16_BUCKET_SUMS_BLOCK 128
+#endif
+constexpr unsigned BUCKET_SUMS_BLOCK = G16_BUCKET_SUMS_BLOCK;
+
 // Bucket sums S_g: one thread per bucket folds its few partials (a fat
 // bucket's total already sits in its first slot).
 template <class F>
-__global__ void __launch_bounds__(128, REDUCE_MIN_BLOCKS) k_bucket_sums(const uint4* __restrict__ partials,
+__global__ void __launch_bounds__(BUCKET_SUMS_BLOCK, REDUCE_MIN_BLOCKS) k_bucket_sums(const uint4* __restrict__ partials,
                                                      const uint32_t* __restrict__ offsets,
                                                      const uint32_t* __restrict__ seg_base, uint32_t K,
                                                      const uint32_t* __restrict__ d_L, uint4* __restrict__ buckets) {
@@ -1451,7 +1457,7 @@ static cudaError_t accumulate(const MsmSort& s, MsmAccum& acc, const void* d_bas
     G16_CUDA(cudaGetLastError());
     {
         TimedLaunch tl("msm_bucket_sums", st);
-        k_bucket_sums<F><<<blocks_for(s.K, 128), 128, 0, st>>>(partials, s.d_offsets, s.d_seg_base, s.K, s.d_total + 3,
+        k_bucket_sums<F><<<blocks_for(s.K, BUCKET_SUMS_BLOCK), BUCKET_SUMS_BLOCK, 0, st>>>(partials, s.d_offsets, s.d_seg_base, s.K, s.d_total + 3,
                                                                 (uint4*)acc.d_buckets);
     }
     {
@@ -1719,7 +1725,7 @@ static cudaError_t space_accumulate(MsmSpace& sp, cudaStream_t st, size_t xyzz_b
     G16_CUDA(cudaGetLastError());
     if (s.K) {
         TimedLaunch tl("msm_bucket_sums", st);
-        k_bucket_sums<F><<<blocks_for(s.K, 128), 128, 0, st>>>(partials, s.d_offsets, s.d_seg_base, s.K, s.d_total + 3,
+        k_bucket_sums<F><<<blocks_for(s.K, BUCKET_SUMS_BLOCK), BUCKET_SUMS_BLOCK, 0, st>>>(partials, s.d_offsets, s.d_seg_base, s.K, s.d_total + 3,
                                                                 (uint4*)a.d_buckets);
     }
     if (sp.blocks) {
