@@ -467,9 +467,10 @@ int layout_engine(g16_backend* b, BatchEngine& E, g16_circuit* const* cs, size_t
 int reserve_batch_engines(g16_backend* b, g16_circuit* const* cs, size_t count) {
     if (!count) return G16_OK;
     const size_t max_engines = batch_max_engines();
-    BatchUsers users(cs, count);
     // one engine at a time, each as soon as it is idle, so that batches running
-    // meanwhile keep the others
+    // meanwhile keep the others; as in prove_batch_engine, the engine is taken
+    // before the circuits' retuning guard (g16_autotune waits for batch users, a
+    // batch holding an engine waits for tuning to end)
     std::vector<BatchEngine*> sized;
     for (;;) {
         BatchEngine* eng = nullptr;
@@ -504,6 +505,7 @@ int reserve_batch_engines(g16_backend* b, g16_circuit* const* cs, size_t count) 
                 b->batch->cv.notify_all();
             }
         } give_back{b, eng};
+        BatchUsers users(cs, count);
         int rc = layout_engine(b, *eng, cs, count);
         if (rc != G16_OK) return rc;
         eng->drop_layout();   // sized; the next batch lays itself out
