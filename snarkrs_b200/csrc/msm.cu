@@ -1535,40 +1535,26 @@ cudaError_t msm_batch_setup(MsmSources& so, MsmSpace* const* spaces, int nspaces
     }
     for (int i = 0; i < nspaces; i++) {
         MsmSpace& sp = *spaces[i];
-        const uint32_t LB = sp.g2 ? MSM_REDUCE_LB_G2 : MSM_REDUCE_LB_G1;   // as space_accumulate's kernels
         const size_t pb = sp.g2 ? XYZZ_G2_BYTES : XYZZ_G1_BYTES;
-        uint64_t K = 0, blocks = 0, out_block = 0, out_set = 0;
-        sp.max_hb = 0;
-        for (auto& g : sp.segs) K += g.B;
-        // one piece length for the space: its pieces about fill the device
-        // (two reduction blocks of 2^LB threads per SM, and at most the 256 threads
-        // of ~250 registers an SM holds), runs of at most 32
-        uint32_t piece_len = 1;
-        const uint64_t fill = (uint64_t)device_sms() * std::min<uint64_t>(2ull << LB, 256);
-        while (piece_len < MSM_REDUCE_MAX_SEG && K / piece_len > fill) piece_len *= 2;
-        if (const char* e = std::getenv("G16_BATCH_PIECE_LEN")) {   // tuning knob: 1, 2, 4, ..., 32
-            const int v = std::atoi(e);
-            if (v >= 1 && v <= (int)MSM_REDUCE_MAX_SEG && !(v & (v - 1))) piece_len = (uint32_t)v;
-        }
-        K = 0;
+        uint32_t piece_len = 0;
+        if (const char* e = std::getenv("G16_BATCH_PIECE_LEN")) piece_len = (uint32_t)std::max(0, std::atoi(e));   // tuning knob: 1, 2, 4, ..., 32
+        std::vector<uint32_t> seg_B;
+        for (auto& g : sp.segs) seg_B.push_back(g.B);
+        const MsmSpaceReduceLayout L = msm_space_reduce_layout(seg_B, sp.g2, sp.pieces_target, device_sms(), piece_len);
         std::vector<MsmSegDev> segdev;
         std::vector<MsmReduceDev> red;
-        for (auto& g : sp.segs) {
-            g.key_start = (uint32_t)K;
-            const uint64_t target = sp.pieces_target ? sp.pieces_target : std::max<uint64_t>(1, g.B / piece_len);
-            g.plan = msm_reduce_plan(1, g.B, sp.g2, target);
-            g.plan.direct = false;   // every segment's block terms are summed on the device
-            g.block_start = (uint32_t)blocks;
-            g.out_block = (uint32_t)out_block;
-            g.out_set = (uint32_t)out_set;
+        for (size_t j = 0; j < sp.segs.size(); j++) {
+            MsmSpaceSeg& g = sp.segs[j];
+            g.key_start = L.key_start[j];
+            g.plan = L.plans[j];
+            g.block_start = L.block_start[j];
+            g.out_block = L.out_block[j];
+            g.out_set = L.out_set[j];
             segdev.push_back({(const uint4*)g.table, g.key_start, g.n_bases});
             red.push_back({g.key_start, g.B, g.plan.seg, g.plan.nb, g.plan.hb, g.block_start, g.out_block, g.out_set});
-            K += g.B;
-            blocks += g.plan.nb;
-            out_block += (uint64_t)g.plan.nb * g.plan.block_terms();
-            out_set += g.plan.set_terms();
-            sp.max_hb = std::max(sp.max_hb, g.plan.hb);
         }
+        sp.max_hb = L.max_hb;
+        const uint64_t K = L.K, blocks = L.blocks, out_block = L.block_points, out_set = L.result_points;
         if (K >= 0x80000000ull || sp.max_entries >= 0x80000000ull) {
             set_error("batched MSM space of %llu buckets and %zu entries exceeds 32-bit indices",
                       (unsigned long long)K, sp.max_entries);

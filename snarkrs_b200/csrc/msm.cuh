@@ -106,6 +106,52 @@ constexpr MsmReducePlan msm_reduce_plan(uint32_t sets, uint32_t B, bool g2, uint
     return r;
 }
 
+// The bucket-reduction layout of a batched MSM space (msm_batch_setup): its
+// segments' buckets back to back (key_start), and per segment a plan with one
+// bucket set, its first k_reduce_pieces_multi block, its first block-output
+// point (each block writes plan.block_terms() points) and its first result
+// point (plan.set_terms(), summed on the device).  One piece length for the
+// space: its pieces about fill the SMs' resident reduction threads (two
+// blocks of 2^lb, at most 256 threads, per SM), runs of at most 32 buckets;
+// piece_len_override (a power of two up to 32) replaces it, and
+// pieces_target (non-zero) replaces the per-segment target.  Host arithmetic
+// only, so that the kernels' indexing can be checked against it on the CPU.
+struct MsmSpaceReduceLayout {
+    std::vector<MsmReducePlan> plans;
+    std::vector<uint32_t> key_start, block_start, out_block, out_set;
+    uint64_t K = 0, blocks = 0, block_points = 0, result_points = 0;
+    uint32_t max_hb = 0, piece_len = 1;
+};
+
+inline MsmSpaceReduceLayout msm_space_reduce_layout(const std::vector<uint32_t>& seg_B, bool g2, uint64_t pieces_target,
+                                                    uint32_t sms, uint32_t piece_len_override) {
+    MsmSpaceReduceLayout L;
+    const uint32_t lb = g2 ? MSM_REDUCE_LB_G2 : MSM_REDUCE_LB_G1;
+    uint64_t K = 0;
+    for (uint32_t B : seg_B) K += B;
+    const uint64_t resident = (2ull << lb) < 256 ? (2ull << lb) : 256;
+    const uint64_t fill = (uint64_t)sms * resident;
+    while (L.piece_len < MSM_REDUCE_MAX_SEG && K / L.piece_len > fill) L.piece_len *= 2;
+    if (piece_len_override >= 1 && piece_len_override <= MSM_REDUCE_MAX_SEG && !(piece_len_override & (piece_len_override - 1)))
+        L.piece_len = piece_len_override;
+    for (uint32_t B : seg_B) {
+        const uint64_t target = pieces_target ? pieces_target : (B / L.piece_len ? B / L.piece_len : 1);
+        MsmReducePlan pl = msm_reduce_plan(1, B, g2, target);
+        pl.direct = false;   // every segment's block terms are summed on the device
+        L.key_start.push_back((uint32_t)L.K);
+        L.block_start.push_back((uint32_t)L.blocks);
+        L.out_block.push_back((uint32_t)L.block_points);
+        L.out_set.push_back((uint32_t)L.result_points);
+        L.K += B;
+        L.blocks += pl.nb;
+        L.block_points += (uint64_t)pl.nb * pl.block_terms();
+        L.result_points += pl.set_terms();
+        if (pl.hb > L.max_hb) L.max_hb = pl.hb;
+        L.plans.push_back(pl);
+    }
+    return L;
+}
+
 struct MsmSort {
     // parameters
     int c = 0, W = 0;

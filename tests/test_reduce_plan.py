@@ -90,3 +90,106 @@ def test_prover_results_fit_the_readback_slot(plan):
     assert 1 <= plan.lb_g1 <= 8 and 1 <= plan.lb_g2 <= 8
     for (_, _, g2, _), p in zip(cases, results):
         assert p["result_points"] * (256 if g2 else 128) <= plan.slot_bytes
+
+
+LAYOUT_PROBE = r"""
+#include <cstdio>
+#include <vector>
+#include "msm.cuh"
+int main() {
+    printf("%u %u %u\n", g16::MSM_REDUCE_LB_G1, g16::MSM_REDUCE_LB_G2, g16::MSM_REDUCE_MAX_SEG);
+    unsigned nseg, g2, sms, override_len;
+    unsigned long long target;
+    while (scanf("%u %u %llu %u %u", &nseg, &g2, &target, &sms, &override_len) == 5) {
+        std::vector<uint32_t> B(nseg);
+        for (auto& b : B) scanf("%u", &b);
+        g16::MsmSpaceReduceLayout L = g16::msm_space_reduce_layout(B, g2 != 0, target, sms, override_len);
+        printf("%llu %llu %llu %llu %u %u\n", (unsigned long long)L.K, (unsigned long long)L.blocks,
+               (unsigned long long)L.block_points, (unsigned long long)L.result_points, L.max_hb, L.piece_len);
+        for (size_t j = 0; j < B.size(); j++) {
+            const g16::MsmReducePlan& p = L.plans[j];
+            printf("%u %u %u %u %u %d %u %u %u %u %u\n", p.seg, p.lb, p.nb, p.hb, p.sets, p.direct ? 1 : 0,
+                   L.key_start[j], L.block_start[j], L.out_block[j], L.out_set[j], p.set_terms());
+        }
+    }
+    return 0;
+}
+"""
+
+
+@pytest.fixture(scope="module")
+def layout():
+    if shutil.which("nvcc") is None:
+        pytest.skip("nvcc not on PATH")
+    import tempfile
+    d = tempfile.mkdtemp(prefix="layout_probe")
+    src, exe = os.path.join(d, "probe.cu"), os.path.join(d, "probe")
+    open(src, "w").write(LAYOUT_PROBE)
+    subprocess.run(["nvcc", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "snarkrs_b200", "csrc"), "-I",
+                    os.path.join(ROOT, "include"), "-o", exe, src], check=True, capture_output=True)
+
+    def run(cases):
+        text = "".join("%d %d %d %d %d %s\n" % (len(Bs), g2, target, sms, ovr, " ".join(map(str, Bs)))
+                       for Bs, g2, target, sms, ovr in cases)
+        out = subprocess.run([exe], input=text, capture_output=True, text=True, check=True).stdout.split("\n")
+        run.lb_g1, run.lb_g2, run.max_seg = map(int, out[0].split())
+        res, i = [], 1
+        for Bs, *_ in cases:
+            tot = dict(zip(("K", "blocks", "block_points", "result_points", "max_hb", "piece_len"),
+                           map(int, out[i].split())))
+            segs = [dict(zip(("seg", "lb", "nb", "hb", "sets", "direct", "key_start", "block_start", "out_block",
+                              "out_set", "set_terms"), map(int, out[i + 1 + j].split()))) for j in range(len(Bs))]
+            res.append((tot, segs))
+            i += 1 + len(Bs)
+        return res
+    yield run
+    shutil.rmtree(d, ignore_errors=True)
+
+
+def test_batched_reduction_layout_matches_the_kernels(layout):
+    # Random mixes of segments (the batched engine's spaces) laid out by
+    # msm_space_reduce_layout, then the indexing of k_reduce_pieces_multi and
+    # k_reduce_sets_multi replayed on that layout: every block finds its own
+    # segment, reads only its segment's buckets, and writes only its own points;
+    # every sets-kernel read and write stays inside its segment and the buffers.
+    import random
+    rng = random.Random(11)
+    cases = []
+    for _ in range(300):
+        nseg = rng.randrange(1, 40)
+        Bs = [1 << (rng.randrange(4, 22) - 1) for _ in range(nseg)]
+        g2 = rng.randrange(2)
+        target = rng.choice([0, 0, 0, 8192, 32768, 1 << rng.randrange(4, 18)])
+        sms = rng.choice([148, 132, 1, 7])
+        ovr = rng.choice([0, 0, 0, 0, 1, 2, 8, 32, 3, 64])
+        cases.append((Bs, g2, target, sms, ovr))
+    for (Bs, g2, target, sms, ovr), (tot, segs) in zip(cases, layout(cases)):
+        LB = layout.lb_g2 if g2 else layout.lb_g1   # the kernels' template argument
+        assert tot["K"] == sum(Bs)
+        if ovr in (1, 2, 4, 8, 16, 32):
+            assert tot["piece_len"] == ovr
+        k = b = bp = rp = 0
+        for B, s in zip(Bs, segs):
+            assert s["lb"] == LB and s["sets"] == 1 and s["direct"] == 0
+            assert (s["key_start"], s["block_start"], s["out_block"], s["out_set"]) == (k, b, bp, rp)
+            pieces = B // s["seg"]
+            assert pieces * s["seg"] == B and 1 <= s["seg"] <= layout.max_seg
+            nb, hb = s["nb"], s["hb"]
+            assert nb >= 1 and (nb << LB) >= pieces and ((nb - 1) << LB) < pieces and (1 << hb) == nb
+            # k_reduce_pieces_multi: block jb < nb of this segment reads buckets
+            # key_start + p*seg + i (p*seg < B) and writes out_block + jb*(LB+2) + [0, LB+1]
+            last_write = s["out_block"] + (nb - 1) * (LB + 2) + LB + 1
+            assert last_write < bp + nb * (LB + 2) <= tot["block_points"]
+            # k_reduce_sets_multi: term o < LB+1+hb reads out_block + j*(LB+2) + min(o, LB+1), j < nb,
+            # and writes out_set + o
+            assert s["set_terms"] == LB + 1 + hb
+            assert s["out_set"] + LB + hb < rp + s["set_terms"] <= tot["result_points"]
+            k += B
+            b += nb
+            bp += nb * (LB + 2)
+            rp += s["set_terms"]
+        assert (k, b, bp, rp) == (tot["K"], tot["blocks"], tot["block_points"], tot["result_points"])
+        assert tot["max_hb"] == max(s["hb"] for s in segs)
+        # a block finds its segment by the last block_start <= block (strictly increasing)
+        starts = [s["block_start"] for s in segs]
+        assert all(x < y for x, y in zip(starts, starts[1:]))
