@@ -178,3 +178,11 @@ def test_compact_key_is_much_smaller():
     full = pk.plan(1 << 50)
     compact = pk.plan(full["key_bytes"] + full["workspace_bytes"] - 1)
     assert compact["key_bytes"] * 8 < full["key_bytes"]
+
+
+def test_readiness_entry_points_refuse_null_handles():
+    # g16_batch_reserve and g16_circuit_warm check their handles before any CUDA call
+    with pytest.raises(S.InvalidArgumentError):
+        S.check(S.lib().g16_batch_reserve(None, 0, None))
+    with pytest.raises(S.InvalidArgumentError):
+        S.check(S.lib().g16_circuit_warm(None, 2))
