@@ -193,3 +193,139 @@ def test_batched_reduction_layout_matches_the_kernels(layout):
         # a block finds its segment by the last block_start <= block (strictly increasing)
         starts = [s["block_start"] for s in segs]
         assert all(x < y for x, y in zip(starts, starts[1:]))
+
+
+def _plan_probe(defines):
+    """The plan probe compiled with extra -D flags (another reduction block size)."""
+    import tempfile
+    d = tempfile.mkdtemp(prefix="plan_probe_d")
+    src, exe = os.path.join(d, "probe.cu"), os.path.join(d, "probe")
+    open(src, "w").write(PROBE)
+    subprocess.run(["nvcc", "-std=c++17", "-O1"] + defines + ["-I", os.path.join(ROOT, "snarkrs_b200", "csrc"), "-I",
+                    os.path.join(ROOT, "include"), "-o", exe, src], check=True, capture_output=True)
+
+    def run(cases):
+        text = "\n".join("%d %d %d %d" % c for c in cases) + "\n"
+        out = subprocess.run([exe], input=text, capture_output=True, text=True, check=True).stdout.split("\n")
+        keys = ("seg", "lb", "nb", "hb", "direct", "set_terms", "block_points", "result_points")
+        return [dict(zip(keys, map(int, l.split()))) for l in out[1:] if l.strip()]
+    return run, d
+
+
+def _emulate_reduction(S, sets, B, p):
+    """k_reduce_pieces, k_reduce_sets and the host's set_sum (msm.cu) on integers standing
+    in for points (addition is +, doubling is *2), step by step as the kernels index them.
+    Returns each set's sum_b (b + 1) S_b as the device and host would form it."""
+    LB, seg, nb, hb = p["lb"], p["seg"], p["nb"], p["hb"]
+    N = 1 << LB
+    weighted = seg > 1
+    terms = LB + 2
+    blocks_out = [0] * (sets * nb * terms)
+    for st in range(sets):
+        for jb in range(nb):
+            run, tot = [0] * N, [0] * N
+            for t in range(N):
+                pc = jb * N + t
+                if pc * seg < B:
+                    g0 = st * B + pc * seg
+                    for i in range(seg - 1, -1, -1):
+                        run[t] += S[g0 + i]
+                        if weighted:
+                            tot[t] += run[t]
+            s_run, s_tot = list(run), list(tot)
+            lg = [0 if t == 0 else t.bit_length() - 1 for t in range(N)]
+            for k in range(1, LB + 1):
+                h = N >> k
+                r_run, r_tot = list(s_run), list(s_tot)   # a step reads the state the barrier left
+                for t in range(N):
+                    if t < h:
+                        run[t] = run[t] + r_run[t + h]
+                        s_run[t] = run[t]
+                    elif t < 2 * h:
+                        if weighted:
+                            tot[t] = r_tot[t - h] + r_tot[t]
+                            s_tot[t - h] = tot[t]
+                    else:
+                        hs, s = 1 << lg[t], 1 << (k - (LB - lg[t]) - 1)
+                        o = t - hs
+                        if (o & (2 * s - 1)) == 0 and o + s < hs:
+                            run[t] = run[t] + r_run[t + s]
+                            s_run[t] = run[t]
+            o0 = (st * nb + jb) * terms
+            for t in range(N):
+                if t == 0:
+                    if not weighted:
+                        blocks_out[o0] = run[0]
+                    blocks_out[o0 + LB + 1] = run[0]
+                elif t & (t - 1) == 0:
+                    blocks_out[o0 + 1 + lg[t]] = run[t]
+                    if t == 1 and weighted:
+                        blocks_out[o0] = tot[1]
+    sums = []
+    for st in range(sets):
+        base = st * nb * terms
+        if p["direct"]:
+            T, G, Gb = 0, [0] * LB, [0] * hb
+            for j in range(nb):
+                o = base + j * terms
+                T += blocks_out[o]
+                for i in range(LB):
+                    G[i] += blocks_out[o + 1 + i]
+                for i in range(hb):
+                    if (j >> i) & 1:
+                        Gb[i] += blocks_out[o + LB + 1]
+        else:   # k_reduce_sets: term o of the set over its nb blocks
+            res = []
+            for o in range(LB + 1 + hb):
+                acc = 0
+                for j in range(nb):
+                    if o <= LB:
+                        acc += blocks_out[base + j * terms + o]
+                    elif (j >> (o - LB - 1)) & 1:
+                        acc += blocks_out[base + j * terms + LB + 1]
+                res.append(acc)
+            T, G, Gb = res[0], res[1:1 + LB], res[LB + 1:]
+        acc = 0
+        for i in range(hb - 1, -1, -1):
+            acc = 2 * acc + Gb[i]
+        for j in range(LB - 1, -1, -1):
+            acc = 2 * acc + G[j]
+        s = seg
+        while s > 1:
+            acc *= 2
+            s >>= 1
+        sums.append(acc + T)
+    return sums
+
+
+@pytest.mark.parametrize("defines", [[], ["-DG16_REDUCE_LB_G1=7", "-DG16_REDUCE_LB_G2=6"]],
+                         ids=["blocks-of-2^8", "blocks-of-2^7-and-2^6"])
+def test_reduction_algebra_by_integer_emulation(defines):
+    # the pieces kernel's running sums, halvings and per-bit trees, the sets kernel and the
+    # host's combination give sum_b (b + 1) S_b for every plan shape: direct and summed on
+    # the device, weighted (seg > 1) and not, one or several sets
+    if shutil.which("nvcc") is None:
+        pytest.skip("nvcc not on PATH")
+    import random
+    run, d = _plan_probe(defines)
+    try:
+        rng = random.Random(5)
+        cases = []
+        for B in (1, 2, 8, 64, 256, 1024, 4096):
+            for sets in (1, 2, 3):
+                for g2 in (0, 1):
+                    for target in (1, 16, 256, 8192, 32768):
+                        cases.append((sets, B, g2, target))
+        shapes = set()
+        for (sets, B, g2, target), p in zip(cases, run(cases)):
+            shape = (sets, B, p["seg"], p["nb"], p["direct"], p["lb"])
+            if shape in shapes:
+                continue
+            shapes.add(shape)
+            S = [rng.randrange(1, 1 << 20) for _ in range(sets * B)]
+            want = [sum((b + 1) * S[st * B + b] for b in range(B)) for st in range(sets)]
+            assert _emulate_reduction(S, sets, B, p) == want, (sets, B, g2, target, p)
+        assert any(s[4] == 1 for s in shapes) and any(s[4] == 0 for s in shapes)
+        assert any(s[2] > 1 for s in shapes) and any(s[2] == 1 for s in shapes)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
