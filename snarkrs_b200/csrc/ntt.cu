@@ -293,10 +293,6 @@ namespace g16 {
 
 using namespace g16d;
 
-bool ntt_tiling_valid(const NttTiling& t) {
-    return t.tile_log >= 2 && t.tile_log <= NTT_MAX_TILE_LOG && t.outer_log_l < t.tile_log && t.outer_log_l <= 4;
-}
-
 void NttTables::release() {
     cudaFree(d_tw);
     cudaFree(d_tw_inv);
@@ -352,28 +348,10 @@ cudaError_t ntt_tables(NttTables& t, int log_n, cudaStream_t st) {
     return cudaSuccess;
 }
 
-struct Pass {
-    uint32_t s_lo, k, log_L;
-};
-
-// the inner pass's stage count
-static uint32_t inner_k(const NttTiling& tl, uint32_t log_n) { return log_n < tl.tile_log ? log_n : tl.tile_log; }
-
-// outer passes covering stages [k0, log_n), in increasing s_lo
+using Pass = NttPass;
+static uint32_t inner_k(const NttTiling& tl, uint32_t log_n) { return ntt_inner_k(tl, log_n); }
 static std::vector<Pass> outer_passes(const NttTiling& tl, uint32_t log_n, uint32_t k0) {
-    std::vector<Pass> v;
-    uint32_t rem = log_n - k0;
-    if (!rem) return v;
-    uint32_t kmax = tl.tile_log - tl.outer_log_l;
-    uint32_t np = (rem + kmax - 1) / kmax;
-    uint32_t s = k0;
-    for (uint32_t i = 0; i < np; i++) {
-        uint32_t k = rem / np + (i < rem % np ? 1 : 0);
-        uint32_t ll = tl.outer_log_l < s ? tl.outer_log_l : s;
-        v.push_back({s, k, ll});
-        s += k;
-    }
-    return v;
+    return ntt_outer_passes(tl, log_n, k0);
 }
 
 static bool attrs_done = false;

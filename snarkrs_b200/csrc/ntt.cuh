@@ -34,7 +34,38 @@ struct NttTiling {
 constexpr uint32_t NTT_MAX_TILE_LOG = 12;   // 128 KiB of shared memory
 
 // Is the tiling one the kernels accept?
-bool ntt_tiling_valid(const NttTiling& t);
+inline bool ntt_tiling_valid(const NttTiling& t) {
+    return t.tile_log >= 2 && t.tile_log <= NTT_MAX_TILE_LOG && t.outer_log_l < t.tile_log && t.outer_log_l <= 4;
+}
+
+// The passes of a transform of 2^log_n under a tiling (host arithmetic only, so
+// that the kernels' indexing can be checked against it on the CPU): the inner
+// pass covers stages [0, k0) on contiguous tiles of 2^k0; each outer pass covers
+// stages [s_lo, s_lo + k) on tiles of 2^k rows of 2^log_L consecutive columns.
+struct NttPass {
+    uint32_t s_lo, k, log_L;
+};
+
+// the inner pass's stage count
+inline uint32_t ntt_inner_k(const NttTiling& tl, uint32_t log_n) { return log_n < tl.tile_log ? log_n : tl.tile_log; }
+
+// outer passes covering stages [k0, log_n) in increasing s_lo, as even as the
+// tile's row count 2^(tile_log - outer_log_l) allows
+inline std::vector<NttPass> ntt_outer_passes(const NttTiling& tl, uint32_t log_n, uint32_t k0) {
+    std::vector<NttPass> v;
+    uint32_t rem = log_n - k0;
+    if (!rem) return v;
+    uint32_t kmax = tl.tile_log - tl.outer_log_l;
+    uint32_t np = (rem + kmax - 1) / kmax;
+    uint32_t s = k0;
+    for (uint32_t i = 0; i < np; i++) {
+        uint32_t k = rem / np + (i < rem % np ? 1 : 0);
+        uint32_t ll = tl.outer_log_l < s ? tl.outer_log_l : s;
+        v.push_back({s, k, ll});
+        s += k;
+    }
+    return v;
+}
 
 struct NttTables {
     int log_n = -1;
