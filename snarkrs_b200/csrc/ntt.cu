@@ -546,23 +546,15 @@ void NttBatch::release() {
 cudaError_t ntt_batch_setup(NttBatch& nb, const std::vector<NttBatchItem>& items, cudaStream_t st) {
     set_attrs();
     nb.phases.clear();
-    struct ItemPlan {
-        uint32_t log_n, k0;
-        std::vector<Pass> outer;
-    };
-    std::vector<ItemPlan> plans;
-    uint32_t dmax = 0;
+    std::vector<uint32_t> logs;
+    std::vector<NttTiling> tilings;
     for (auto& it : items) {
         if (!it.t || it.t->log_n < 1) {
             set_error("batched NTT item without tables");
             return cudaErrorInvalidValue;
         }
-        ItemPlan p;
-        p.log_n = (uint32_t)it.t->log_n;
-        p.k0 = inner_k(it.t->tiling, p.log_n);
-        p.outer = outer_passes(it.t->tiling, p.log_n, p.k0);
-        dmax = std::max(dmax, (uint32_t)p.outer.size());
-        plans.push_back(p);
+        logs.push_back((uint32_t)it.t->log_n);
+        tilings.push_back(it.t->tiling);
     }
     std::vector<NttJob> all;
     auto add_phase = [&](int kind, std::vector<NttJob>& jobs) {
@@ -596,13 +588,13 @@ cudaError_t ntt_batch_setup(NttBatch& nb, const std::vector<NttBatchItem>& items
             j.join_b = (const uint4*)it.b;
             j.join_out = (uint4*)it.h;
         }
-        j.log_n = plans[i].log_n;
+        j.log_n = logs[i];
         j.s_lo = p.s_lo;
         j.k = p.k;
         j.log_L = p.log_L;
         return j;
     };
-    auto mid_job = [&](size_t i, int v, bool join) {
+    auto mid_job = [&](size_t i, int v, uint32_t k0, bool join) {
         const NttBatchItem& it = items[i];
         NttJob j = {};
         j.data = (uint4*)(v == 0 ? it.a : v == 1 ? it.b : it.c);
@@ -614,41 +606,16 @@ cudaError_t ntt_batch_setup(NttBatch& nb, const std::vector<NttBatchItem>& items
             j.join_b = (const uint4*)it.b;
             j.join_out = (uint4*)it.h;
         }
-        j.log_n = plans[i].log_n;
-        j.k = plans[i].k0;
+        j.log_n = logs[i];
+        j.k = k0;
         return j;
     };
-    for (uint32_t m = 0; m < dmax; m++) {   // inverse outer passes, right-aligned
+    for (const NttPhasePlan& ph : ntt_batch_plan(logs, tilings)) {
         std::vector<NttJob> jobs;
-        const uint32_t q = dmax - 1 - m;
-        for (size_t i = 0; i < items.size(); i++)
-            if (plans[i].outer.size() > q)
-                for (int v = 0; v < 3; v++) jobs.push_back(pass_job(i, v, plans[i].outer[q], true, false));
-        add_phase(0, jobs);
-    }
-    {
-        std::vector<NttJob> jobs;
-        for (size_t i = 0; i < items.size(); i++)
-            for (int v = 0; v < (plans[i].outer.empty() ? 2 : 3); v++) jobs.push_back(mid_job(i, v, false));
-        add_phase(2, jobs);
-    }
-    for (uint32_t m = 0; m < dmax; m++) {   // forward outer passes, left-aligned
-        std::vector<NttJob> jobs;
-        for (size_t i = 0; i < items.size(); i++) {
-            const size_t np = plans[i].outer.size();
-            if (m >= np) continue;
-            for (int v = 0; v < (m + 1 == np ? 2 : 3); v++) jobs.push_back(pass_job(i, v, plans[i].outer[m], false, false));
-        }
-        add_phase(1, jobs);
-    }
-    {   // C's last pass with the join: middles (no outer passes), then last forward passes
-        std::vector<NttJob> mids, passes;
-        for (size_t i = 0; i < items.size(); i++) {
-            if (plans[i].outer.empty()) mids.push_back(mid_job(i, 2, true));
-            else passes.push_back(pass_job(i, 2, plans[i].outer.back(), false, true));
-        }
-        add_phase(2, mids);
-        add_phase(1, passes);
+        for (const NttJobPlan& jp : ph.jobs)
+            jobs.push_back(jp.kind == 2 ? mid_job(jp.item, jp.vec, jp.pass.k, jp.join)
+                                        : pass_job(jp.item, jp.vec, jp.pass, jp.kind == 0, jp.join));
+        add_phase(ph.kind, jobs);
     }
     const size_t need = (all.empty() ? 1 : all.size()) * sizeof(NttJob);
     if (need > nb.cap_jobs) {   // the job table only grows, in stream order (dev_realloc_async)

@@ -107,6 +107,77 @@ cudaError_t ntt_distribute_powers(void* a, size_t n, const uint64_t* shift_mont,
 // ---- many prover chains per launch (batched proving) ----
 // ntt_h_pipeline for many proofs of any sizes and tilings: every launch
 // covers one step of every chain (ntt_batch_setup lays the steps out).
+// The launches of a batch of H pipelines (ntt_batch_setup) before they are
+// bound to device vectors.  A job is item `item`'s vector `vec` (0 A, 1 B, 2 C)
+// in an outer pass (kind 0: inverse DIF with inverse twiddles, 1: forward DIT)
+// or in the fused middle (kind 2; pass.k = the inner stage count); `join`:
+// its epilogue writes h = A B - C instead of the vector.  The jobs of a phase
+// run in one launch, side by side.  Phases: the inverse outer passes
+// right-aligned (an item with fewer passes joins later), the middles (of A and
+// B only for an item without outer passes), the forward outer passes
+// left-aligned (an item's last one for A and B only), then C's last step with
+// the join: the middles of items without outer passes, then the last forward
+// passes.  Host arithmetic only, so that the order can be checked on the CPU.
+struct NttJobPlan {
+    uint32_t item;
+    int vec, kind;
+    NttPass pass;
+    bool join;
+};
+struct NttPhasePlan {
+    int kind;
+    std::vector<NttJobPlan> jobs;
+};
+
+inline std::vector<NttPhasePlan> ntt_batch_plan(const std::vector<uint32_t>& log_n, const std::vector<NttTiling>& tiling) {
+    const size_t n = log_n.size();
+    std::vector<uint32_t> k0(n);
+    std::vector<std::vector<NttPass>> outer(n);
+    size_t dmax = 0;
+    for (size_t i = 0; i < n; i++) {
+        k0[i] = ntt_inner_k(tiling[i], log_n[i]);
+        outer[i] = ntt_outer_passes(tiling[i], log_n[i], k0[i]);
+        if (outer[i].size() > dmax) dmax = outer[i].size();
+    }
+    std::vector<NttPhasePlan> phases;
+    auto add = [&](int kind, std::vector<NttJobPlan>& jobs) {
+        if (!jobs.empty()) phases.push_back({kind, jobs});
+    };
+    for (size_t m = 0; m < dmax; m++) {   // inverse outer passes, right-aligned
+        std::vector<NttJobPlan> jobs;
+        const size_t q = dmax - 1 - m;
+        for (uint32_t i = 0; i < n; i++)
+            if (outer[i].size() > q)
+                for (int v = 0; v < 3; v++) jobs.push_back({i, v, 0, outer[i][q], false});
+        add(0, jobs);
+    }
+    {
+        std::vector<NttJobPlan> jobs;
+        for (uint32_t i = 0; i < n; i++)
+            for (int v = 0; v < (outer[i].empty() ? 2 : 3); v++) jobs.push_back({i, v, 2, {0, k0[i], 0}, false});
+        add(2, jobs);
+    }
+    for (size_t m = 0; m < dmax; m++) {   // forward outer passes, left-aligned
+        std::vector<NttJobPlan> jobs;
+        for (uint32_t i = 0; i < n; i++) {
+            const size_t np = outer[i].size();
+            if (m >= np) continue;
+            for (int v = 0; v < (m + 1 == np ? 2 : 3); v++) jobs.push_back({i, v, 1, outer[i][m], false});
+        }
+        add(1, jobs);
+    }
+    {   // C's last step with the join
+        std::vector<NttJobPlan> mids, passes;
+        for (uint32_t i = 0; i < n; i++) {
+            if (outer[i].empty()) mids.push_back({i, 2, 2, {0, k0[i], 0}, true});
+            else passes.push_back({i, 2, 1, outer[i].back(), true});
+        }
+        add(2, mids);
+        add(1, passes);
+    }
+    return phases;
+}
+
 struct NttBatchItem {
     const NttTables* t;     // the proof's domain tables and tiling
     void *a, *b, *c, *h;    // device vectors of 2^t->log_n Fr; h = A B - C out

@@ -232,3 +232,98 @@ def test_h_pipeline_gives_the_oracle_h(plans):
         A, B, C = oracle_icn(log_n, a), oracle_icn(log_n, b), oracle_icn(log_n, c)
         want = [(x * y - z) % R for x, y, z in zip(A, B, C)]
         assert emulate_h_pipeline(plan, log_n, a, b, c, tabs) == want, (t, l, log_n)
+
+
+BATCH_PROBE = r"""
+#include <cstdio>
+#include <vector>
+#include "ntt.cuh"
+int main() {
+    unsigned items;
+    while (scanf("%u", &items) == 1) {
+        std::vector<uint32_t> logs(items);
+        std::vector<g16::NttTiling> tl(items);
+        for (unsigned i = 0; i < items; i++) scanf("%u %u %u", &logs[i], &tl[i].tile_log, &tl[i].outer_log_l);
+        auto phases = g16::ntt_batch_plan(logs, tl);
+        printf("%zu\n", phases.size());
+        for (auto& ph : phases) {
+            printf("%d %zu", ph.kind, ph.jobs.size());
+            for (auto& j : ph.jobs)
+                printf(" %u %d %d %u %u %u %d", j.item, j.vec, j.kind, j.pass.s_lo, j.pass.k, j.pass.log_L, j.join ? 1 : 0);
+            printf("\n");
+        }
+    }
+    return 0;
+}
+"""
+
+
+@pytest.fixture(scope="module")
+def batch_plans():
+    if shutil.which("nvcc") is None:
+        pytest.skip("nvcc not on PATH")
+    import tempfile
+    d = tempfile.mkdtemp(prefix="ntt_batch_probe")
+    src, exe = os.path.join(d, "probe.cu"), os.path.join(d, "probe")
+    open(src, "w").write(BATCH_PROBE)
+    subprocess.run(["nvcc", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "snarkrs_b200", "csrc"), "-I",
+                    os.path.join(ROOT, "include"), "-o", exe, src], check=True, capture_output=True)
+
+    def run(batches):
+        text = "".join("%d %s\n" % (len(b), " ".join("%d %d %d" % x for x in b)) for b in batches)
+        out = subprocess.run([exe], input=text, capture_output=True, text=True, check=True).stdout.split("\n")
+        res, i = [], 0
+        for _ in batches:
+            nph = int(out[i])
+            phases = []
+            for line in out[i + 1:i + 1 + nph]:
+                v = list(map(int, line.split()))
+                jobs = [tuple(v[2 + 7 * j:9 + 7 * j]) for j in range(v[1])]
+                phases.append((v[0], jobs))
+            res.append(phases)
+            i += 1 + nph
+        return res
+    yield run
+    shutil.rmtree(d, ignore_errors=True)
+
+
+def test_batched_h_pipelines_give_the_oracle_h(batch_plans):
+    # several items of different sizes and tilings in one batch (ntt_batch_plan), the
+    # phases run in order; the jobs of a phase run side by side on the GPU, so no job
+    # may read a vector that another job of its phase writes
+    rng = random.Random(9)
+    tilings = [(2, 0), (2, 1), (3, 1), (4, 2), (5, 4), (11, 2), (3, 0)]
+    batches = []
+    for _ in range(25):
+        batches.append([(rng.randrange(1, 9),) + rng.choice(tilings) for _ in range(rng.randrange(1, 5))])
+    for batch, phases in zip(batches, batch_plans(batches)):
+        vecs, want, tabs = [], [], []
+        for log_n, t, l in batch:
+            n = 1 << log_n
+            a, b, c = ([rng.randrange(R) for _ in range(n)] for _ in range(3))
+            A, B, C = oracle_icn(log_n, a), oracle_icn(log_n, b), oracle_icn(log_n, c)
+            want.append([(x * y - z) % R for x, y, z in zip(A, B, C)])
+            vecs.append([a, b, c, [0] * n])
+            tabs.append(tables(log_n))
+        for kind, jobs in phases:
+            for item, vec, jkind, s_lo, k, log_L, join in jobs:
+                assert jkind == kind
+                log_n = batch[item][0]
+                n = 1 << log_n
+                tw, tw_inv, coset = tabs[item]
+                v = vecs[item]
+                jn = (v[0], v[1], v[3]) if join else None
+                if kind == 2:
+                    for bx in grid(n, 1 << k):
+                        mid_tile(v[vec], bx, log_n, k, tw, tw_inv, coset, join=jn)
+                else:
+                    for bx in grid(n, (1 << k) << log_L):
+                        pass_tile(kind == 0, v[vec], bx, log_n, s_lo, k, log_L, tw_inv if kind == 0 else tw, join=jn)
+            # a job may rewrite its own vector; no job touches what another writes
+            per_job = [((it, 3 if jn_ else vc), {(it, vc)} | ({(it, 0), (it, 1)} if jn_ else set()))
+                       for it, vc, _, _, _, _, jn_ in jobs]
+            for i, (w, _) in enumerate(per_job):
+                for j, (_, r) in enumerate(per_job):
+                    assert i == j or w not in r, (batch, kind, jobs[i], jobs[j])
+        for item in range(len(batch)):
+            assert vecs[item][3] == want[item], (batch, item)
