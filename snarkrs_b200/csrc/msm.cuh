@@ -264,8 +264,10 @@ constexpr size_t XYZZ_G1_BYTES = 128;
 constexpr size_t XYZZ_G2_BYTES = 256;
 
 // The prover reads each of its five MSM results (the reduction's points) back
-// into a pinned host slot of this many bytes.
+// into a pinned host slot of this many bytes: one bucket set with window tables;
+// with a compact key one set per window, W (lb + 1 + hb) points.
 constexpr size_t MSM_RESULT_SLOT_BYTES = 32 * 256;
+constexpr size_t MSM_RESULT_SLOT_COMPACT_BYTES = 128 * 1024;
 
 // ---- batched MSMs (many MSMs in one launch per step) ----
 // A space holds the buckets of many MSMs of one group (segments) back to back;

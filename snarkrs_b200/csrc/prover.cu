@@ -353,10 +353,9 @@ int build_h_table(g16_circuit* c, int ch, cudaStream_t st) {
     return G16_OK;
 }
 
-// Host readback slot of one MSM's reduction terms: one bucket set with window
-// tables; with a compact key one set per window, W (lb + 1 + hb) points, at
-// most 32 x 15 G2 points for window bits in [8, 20].
-constexpr size_t WIN_SLOT_COMPACT = 128 * 1024;
+// Host readback slot of one MSM's reduction terms (sizes checked against every
+// window width by tests/test_reduce_plan.py).
+constexpr size_t WIN_SLOT_COMPACT = MSM_RESULT_SLOT_COMPACT_BYTES;
 // Bucket-reduction piece target of the witness MSMs (0: the library default for
 // MSMs whose reductions run beside other work); G16_WITNESS_REDUCE_PIECES overrides it.
 uint64_t witness_reduce_pieces() {

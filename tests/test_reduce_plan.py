@@ -19,7 +19,8 @@ PROBE = r"""
 #include <cstdio>
 #include "msm.cuh"
 int main() {
-    printf("%zu %u %u\n", g16::MSM_RESULT_SLOT_BYTES, g16::MSM_REDUCE_LB_G1, g16::MSM_REDUCE_LB_G2);
+    printf("%zu %u %u %zu\n", g16::MSM_RESULT_SLOT_BYTES, g16::MSM_REDUCE_LB_G1, g16::MSM_REDUCE_LB_G2,
+           g16::MSM_RESULT_SLOT_COMPACT_BYTES);
     unsigned sets, B, g2;
     unsigned long long target;
     while (scanf("%u %u %u %llu", &sets, &B, &g2, &target) == 4) {
@@ -46,7 +47,7 @@ def plan():
     def run(cases):
         text = "\n".join("%d %d %d %d" % c for c in cases) + "\n"
         out = subprocess.run([exe], input=text, capture_output=True, text=True, check=True).stdout.split("\n")
-        run.slot_bytes, run.lb_g1, run.lb_g2 = map(int, out[0].split())
+        run.slot_bytes, run.lb_g1, run.lb_g2, run.compact_slot_bytes = map(int, out[0].split())
         keys = ("seg", "lb", "nb", "hb", "direct", "set_terms", "block_points", "result_points")
         return [dict(zip(keys, map(int, l.split()))) for l in out[1:] if l.strip()]
     yield run
@@ -77,6 +78,16 @@ def test_plans_cover_every_bucket(plan):
         assert p["block_points"] == sets * nb * (lb + 2)
         terms = nb * (lb + 2) if p["direct"] else lb + 1 + p["hb"]
         assert p["set_terms"] == terms and p["result_points"] == sets * terms
+
+
+def test_compact_key_results_fit_the_readback_slot(plan):
+    # a compact key reduces one bucket set per window (the standalone MSM's plan, aiming at
+    # 32768 pieces), for every window width a tuning may set (8 to 20 bits)
+    cases = [((255 + c - 1) // c, 1 << (c - 1), g2, 32768) for c in range(8, 21) for g2 in (0, 1)]
+    results = plan(cases)
+    assert plan.compact_slot_bytes == 128 * 1024
+    for (_, _, g2, _), p in zip(cases, results):
+        assert p["result_points"] * (256 if g2 else 128) <= plan.compact_slot_bytes
 
 
 def test_prover_results_fit_the_readback_slot(plan):
