@@ -113,3 +113,37 @@ def test_element_and_key_refusals(synth):
         S.verify((alpha, beta, gamma, delta, []), b"", proof)
     with pytest.raises(S.InvalidArgumentError):
         S.verify(vk, pub[:-32], proof)
+
+
+def test_b_outside_the_prime_order_subgroup_is_refused(synth):
+    # a point on the twist E'(Fq2) whose order is not r (the twist's cofactor is large):
+    # on the curve, so only the subgroup check (verify.rs:57-66) can refuse it, and the
+    # refusal names B rather than the pairing
+    sc, ok, pk = synth
+    vk = pk.verifying_key()
+    w = sc.witness(1)
+    proof = ok.prove(w, O.to_mont(5), O.to_mont(7))
+    pub = w[32:32 * (1 + ok.n_public)]
+    k = 1
+    while True:
+        x = (k, 1)
+        y = P.f2_sqrt(P.f2_add(P.f2_mul(P.f2_mul(x, x), x), P.B2))
+        if y is not None:
+            break
+        k += 1
+    pt = (x, y)
+
+    def times(p, n):   # n * p without reducing n mod r (P.pt_mul reduces)
+        acc = None
+        while n:
+            if n & 1:
+                acc = P.pt_add(acc, p)
+            p = P.pt_add(p, p)
+            n >>= 1
+        return acc
+    assert P.on_curve(pt) and times(pt, P.R) is not None
+    with pytest.raises(S.VerifyError, match="B is not a valid G2 point"):
+        S.verify(vk, pub, proof[:64] + P.pack_g2(pt) + proof[192:])
+    # an in-subgroup B that is simply wrong fails the pairing instead
+    with pytest.raises(S.VerifyError, match="pairing check failed"):
+        S.verify(vk, pub, proof[:64] + P.pack_g2(P.pt_mul(P.G2, 3)) + proof[192:])
