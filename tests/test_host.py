@@ -186,3 +186,30 @@ def test_readiness_entry_points_refuse_null_handles():
         S.check(S.lib().g16_batch_reserve(None, 0, None))
     with pytest.raises(S.InvalidArgumentError):
         S.check(S.lib().g16_circuit_warm(None, 2))
+
+
+def _zkey_sections(zk):
+    import struct
+    out, off = {}, 12
+    while off + 12 <= len(zk):
+        sid, size = struct.unpack_from("<IQ", zk, off)
+        out[sid] = (off + 12, size)
+        off += 12 + size
+    return out
+
+
+def test_query_point_checks_follow_load_and_load_unchecked(small):
+    # ProvingKey::load checks every query point on its curve; load_unchecked does not
+    # (formats/src/lib.rs:430-505): a corrupted A-query point is refused only by the first
+    _, zk, _ = small
+    start, size = _zkey_sections(zk)[5]            # section 5: the A query, packed G1
+    bad = bytearray(zk)
+    for i in range(0, size, 64):                   # the first finite point
+        if any(bad[start + i:start + i + 64]):
+            bad[start + i + 40] ^= 0x01            # its y, one bit off: off the curve
+            break
+    else:
+        pytest.skip("no finite A-query point")
+    with pytest.raises(S.FormatError):
+        S.ProvingKey.from_bytes(bytes(bad), check_points=True)
+    S.ProvingKey.from_bytes(bytes(bad), check_points=False).close()
