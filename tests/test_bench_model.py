@@ -46,3 +46,27 @@ def test_work_model_counts_zeros_and_ones():
     c = bench.reference_window_size(300)
     w, b = -(-255 // c), 1 << (c - 1)
     assert m["fq_products"] == 10 * 300 * w + 28 * b * w + 10 * 300
+
+
+def test_reference_arm_prints_the_contract_line(tmp_path):
+    # `bench.py --impl reference` runs on host cores only; its one JSON line carries the
+    # keys the driver reads, on the same metric and config as the GPU arm
+    import json
+    import subprocess
+    env = dict(os.environ, G16_BENCH_CACHE=str(tmp_path))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--constraints", "3000",
+                        "--steps", "2", "--warmup", "1"], capture_output=True, text=True, env=env, timeout=600, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == "proofs/s" and d["unit"] == "proofs/s"
+    assert d["value"] > 0 and d["higher_is_better"] is True and d["n_gpus"] == 1
+    assert (d["steps"], d["warmup"]) == (2, 1) and d["ms_per_step"] > 0
+    assert d["scaling"] == "weak" and d["vs_baseline"] is None and d["data"] == "synthetic"
+    assert d["config"]["n_constraints"] == 3000 and "workload" in d["config"]
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["value"] == d["value"] and cb["cores"] >= 1 and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert d["parity"]["pairing_checked"] == d["parity"]["of"] == 3 and d["parity"]["bit_exact_vs_oracle"] is True
